@@ -1,0 +1,17 @@
+// gdfv_launch.h -- interface between the host runtime and the two kernel
+// translation units (FP64 flux and FP32 flux, compiled with different flags).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "gdfv_stage.cuh"
+
+namespace gdfv {
+
+// Launch one stage (0 = residual only, 1 = predictor, 2 = corrector) over A.n_tiles tiles.
+cudaError_t launch_stage_fp64(int stage, int flux, bool mhd, const StageArgs& A, cudaStream_t s);
+cudaError_t launch_stage_fp32(int stage, int flux, bool mhd, const StageArgs& A, cudaStream_t s);
+// Raise the dynamic shared-memory limit of every instantiation (once per device).
+cudaError_t configure_stage_fp64();
+cudaError_t configure_stage_fp32();
+
+}  // namespace gdfv

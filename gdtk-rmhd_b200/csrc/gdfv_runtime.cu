@@ -1,0 +1,956 @@
+// gdfv_runtime.cu -- host runtime behind the C ABI (include/gdfv.h): contexts,
+// configuration by the reference's option names, block and boundary tables,
+// device memory, the device-resident step controller and CUDA-graph replay.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/gdfv.h"
+#include "gdfv_launch.h"
+
+namespace gdfv {
+
+// ---------------------------------------------------------------- device kernels
+struct StepParams {
+    int cfl_count, n_stages, fixed_time_step, mhd_cleaning;
+    int max_attempts, max_invalid_cells, nblocks, pad_;
+    double cfl_value, dt_init, dt_max;
+};
+
+// e4/simcore_gasdynamic_step.d:60-160 (global dt rule) with the block rule of
+// e4/fluidblock.d:998-1095 and c_h of e4/fluidblock.d:975-995 / e4/simcore.d:1625-1648.
+// One thread; inputs are the per-block maxima of the signal frequency that the
+// previous corrector stage (or the initial scan) left behind.
+__global__ void step_begin_kernel(Control* c, const BlockDesc* blocks, unsigned long long* maxsig,
+                                  const double* lastsig, StepParams sp) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (c->halted || c->status != ST_OK) return;
+    if (c->step >= c->step_limit || (c->max_time > 0.0 && c->time >= c->max_time)) {
+        c->halted = 1;
+        return;
+    }
+    if (!c->retrying) {
+        if (!sp.fixed_time_step && (c->step % sp.cfl_count) == 0) {
+            const double cfl_allow = sp.n_stages == 1 ? 0.9 : (sp.n_stages == 2 ? 1.2 : 1.6);
+            const double cfl_adjust = 0.5;
+            const bool check_cfl = c->step > 0;
+            double dt_allow_all = 1.79769313486231570e+308;
+            double cfl_max_all = 0.0;
+            for (int b = 0; b < sp.nblocks; ++b) {
+                double smax = __longlong_as_double((long long)maxsig[b]);
+                // max over cells of (dt*signal) and min of (cfl/signal) follow from the max signal
+                double cfl_max = c->dt_global * smax;
+                double dt_allow = sp.cfl_value / smax;
+                if (check_cfl && (cfl_max < 0.0 || cfl_max > cfl_allow)) {
+                    cfl_max = cfl_adjust * cfl_allow;
+                    dt_allow = cfl_max / lastsig[b];  // signal of the last cell visited
+                }
+                dt_allow_all = fmin(dt_allow_all, dt_allow);
+                cfl_max_all = fmax(cfl_max_all, cfl_max);
+            }
+            c->dt_allow = dt_allow_all;
+            c->cfl_max = cfl_max_all;
+            if (c->step == 0) c->dt_allow = fmin(sp.dt_init, c->dt_allow);
+            if (c->dt_allow <= c->dt_global) {
+                c->dt_global = c->dt_allow;
+            } else {
+                c->dt_global = fmin(c->dt_global * 1.5, c->dt_allow);
+                c->dt_global = fmin(c->dt_global, sp.dt_max);
+            }
+        }
+        if (sp.mhd_cleaning) {
+            bool first = true;
+            for (int b = 0; b < sp.nblocks; ++b) {
+                double smax = __longlong_as_double((long long)maxsig[b]);
+                double cfl_max = smax * c->dt_global;
+                double ch = cfl_max * blocks[b].L_min / c->dt_global;
+                c->c_h = first ? ch : fmin(ch, c->c_h);
+                first = false;
+            }
+        }
+        c->t0 = c->time;
+    }
+    c->n_fail = 0;
+    c->n_invalid1 = 0;
+    c->n_invalid2 = 0;
+    c->first_bad_cell = LLONG_MAX;
+    for (int b = 0; b < sp.nblocks; ++b) maxsig[b] = 0ull;
+}
+
+// Phase 14 and the retry loop of e4/simcore_gasdynamic_step.d:1437-1560.
+__global__ void step_end_kernel(Control* c, StepParams sp) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (c->halted || c->status != ST_OK) return;
+    if (c->n_fail > 0) {
+        c->attempt += 1;
+        c->dt_global = c->dt_global * 0.2;
+        if (c->attempt >= sp.max_attempts) {
+            c->status = ST_DECODE_FAILED;
+            c->halted = 1;
+        } else {
+            c->retrying = 1;
+        }
+        return;
+    }
+    if (c->n_invalid1 > sp.max_invalid_cells || c->n_invalid2 > sp.max_invalid_cells) {
+        c->status = ST_TOO_MANY_BAD_CELLS;
+        c->halted = 1;
+        return;
+    }
+    c->time = c->t0 + c->dt_global;
+    c->step += 1;
+    c->attempt = 0;
+    c->retrying = 0;
+    c->steps_done += 1;
+}
+
+struct BlockRange {
+    long long offset, n;
+    int blk;
+};
+
+// rhoT -> conserved (update_thermo_from_rhoT then encode_conserved)
+__global__ void encode_rhoT_kernel(const double* prim, long long n, double* U, long long total, long long offset,
+                                   NumParams P, int* bad) {
+    long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    double rho = prim[c], vx = prim[n + c], vy = prim[2 * n + c], vz = prim[3 * n + c], T = prim[4 * n + c];
+    double Bx = prim[5 * n + c], By = prim[6 * n + c], Bz = prim[7 * n + c], psi = prim[8 * n + c];
+    if (T <= 0.0 || rho <= 0.0) { atomicAdd(bad, 1); return; }
+    double u = P.gas.Cv * T;
+    const long long g = offset + c;
+    U[MASS * total + g] = rho;
+    U[XMOM * total + g] = rho * vx;
+    U[YMOM * total + g] = rho * vy;
+    U[ZMOM * total + g] = rho * vz;
+    double ke = 0.5 * (vx * vx + vy * vy + vz * vz);
+    double E = rho * (u + ke);
+    if (P.mhd) {
+        U[XB * total + g] = Bx; U[YB * total + g] = By; U[ZB * total + g] = Bz;
+        U[PSI * total + g] = psi; U[DIVB * total + g] = 0.0;
+        double me = 0.5 * (Bx * Bx + By * By + Bz * Bz);
+        E = E + me;
+    }
+    U[TOTENERGY * total + g] = E;
+}
+
+__global__ void decode_kernel(const double* U, long long total, long long offset, long long n, NumParams P,
+                              double* out) {
+    long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    double u[10];
+    for (int q = 0; q < P.nq; ++q) u[q] = U[q * total + offset + c];
+    Prim<double> s;
+    double p = 0, T = 0;
+    int st = decode(P, u, s, p, T);
+    if (st != 0) { s.a = p = T = nan(""); }
+    double v[12] = {s.rho, s.v[0], s.v[1], s.v[2], s.u, p, T, s.a, s.B[0], s.B[1], s.B[2], s.psi};
+    for (int q = 0; q < 12; ++q) out[q * n + c] = v[q];
+}
+
+// Signal frequency of the current state: per-block max and the last cell's value.
+__global__ void signal_scan_kernel(const double* U, long long total, const BlockDesc* blocks, int blk, NumParams P,
+                                   unsigned long long* maxsig, double* lastsig, int* bad) {
+    const BlockDesc& B = blocks[blk];
+    long long n = (long long)B.n[0] * B.n[1] * B.n[2];
+    long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    double sig = 0.0;
+    if (c < n) {
+        double u[10];
+        for (int q = 0; q < P.nq; ++q) u[q] = U[q * total + B.offset + c];
+        Prim<double> s;
+        double p, T;
+        if (decode(P, u, s, p, T) == 0) {
+            sig = signal_frequency(P, B, s);
+            if (c == n - 1) lastsig[blk] = sig;
+        } else {
+            atomicAdd(bad, 1);
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) sig = fmax(sig, __shfl_xor_sync(0xffffffffu, sig, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(&maxsig[blk], (unsigned long long)__double_as_longlong(sig));
+}
+
+// ---------------------------------------------------------------- host side
+struct HostBC {
+    int type = BC_SLIP_WALL;
+    int x_order = 0;
+    int other = -1, other_face = -1;
+    double inflow[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+};
+
+struct HostBlock {
+    int n[3];
+    double len[3];
+    double origin[3];
+    HostBC bc[6];
+    long long offset = 0;
+};
+
+struct Config {
+    int flux = FLUX_AUSMDV;
+    int precision = 0;  // 0 fp64, 1 fp32 flux
+    int dims = 3;
+    int mhd = 0, divergence_cleaning = 0;
+    int apply_limiter = 1, extrema_clipping = 1, apply_entropy_fix = 1, glm_reference_indexing = 1;
+    int stringent_cfl = 0, cfl_count = 10, max_attempts = 3, max_invalid_cells = 0;
+    int fixed_time_step = 0;
+    int tile_kchunk = 0;  // 0: chosen per block
+    double cfl_value = 0.5, dt_init = 1.0e-3, dt_max = 1.0e-3;
+    double eps_van_albada = 1.0e-12, R = 287.1, gamma = 1.4, divB_damping_length = 1.0;
+    double max_velocity = 30000.0, max_temp = 50000.0, min_temp = 0.0;
+};
+
+struct Context {
+    Config cfg;
+    std::vector<HostBlock> blocks;
+    bool prepared = false;
+    std::string err;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    long long total = 0;
+    int nq = 5;
+    int n_tiles = 0;
+    double* U[2] = {nullptr, nullptr};
+    double* dU0 = nullptr;
+    BlockDesc* d_blocks = nullptr;
+    TileDesc* d_tiles = nullptr;
+    InflowState* d_inflow = nullptr;
+    Control* d_ctl = nullptr;
+    Control* h_ctl = nullptr;  // pinned mirror
+    unsigned long long* d_maxsig = nullptr;
+    double* d_lastsig = nullptr;
+    int* d_bad = nullptr;
+    std::vector<BlockDesc> h_blocks;
+    NumParams P{};
+    StepParams sp{};
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = 0;
+    bool signal_valid = false;
+
+    ~Context() {
+        if (graph) cudaGraphExecDestroy(graph);
+        for (void* p : {(void*)U[0], (void*)U[1], (void*)dU0, (void*)d_blocks, (void*)d_tiles, (void*)d_inflow,
+                        (void*)d_ctl, (void*)d_maxsig, (void*)d_lastsig, (void*)d_bad})
+            if (p) cudaFree(p);
+        if (h_ctl) cudaFreeHost(h_ctl);
+        if (own_stream && stream) cudaStreamDestroy(stream);
+    }
+};
+
+std::mutex g_mutex;
+std::map<int, std::unique_ptr<Context>> g_ctx;
+int g_next = 0;
+std::string g_err;
+bool g_configured[64] = {false};
+
+Context* get_ctx(int h) {
+    std::lock_guard<std::mutex> lk(g_mutex);
+    auto it = g_ctx.find(h);
+    return it == g_ctx.end() ? nullptr : it->second.get();
+}
+
+int fail(Context* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    else g_err = msg;
+    return code;
+}
+
+int cuda_fail(Context* c, cudaError_t e, const char* where) {
+    return fail(c, GDFV_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call)                                                      \
+    do {                                                              \
+        cudaError_t e_ = (call);                                      \
+        if (e_ != cudaSuccess) return cuda_fail(c, e_, #call);        \
+    } while (0)
+
+std::string norm(const char* s) {
+    std::string r(s ? s : "");
+    for (auto& ch : r) if (ch == '-') ch = '_';
+    return r;
+}
+
+StageArgs stage_args(Context* c) {
+    StageArgs A{};
+    A.blocks = c->d_blocks;
+    A.tiles = c->d_tiles;
+    A.inflow = c->d_inflow;
+    A.Ubuf[0] = c->U[0];
+    A.Ubuf[1] = c->U[1];
+    A.U_in = nullptr;
+    A.dU0 = c->dU0;
+    A.R_out = nullptr;
+    A.ctl = c->d_ctl;
+    A.max_signal = c->d_maxsig;
+    A.last_signal = c->d_lastsig;
+    A.total = c->total;
+    A.P = c->P;
+    A.n_tiles = c->n_tiles;
+    A.max_invalid_cells = c->cfg.max_invalid_cells;
+    return A;
+}
+
+cudaError_t launch_stage(Context* c, int stage, const StageArgs& A) {
+    if (c->cfg.precision == 0) return launch_stage_fp64(stage, c->cfg.flux, c->cfg.mhd, A, c->stream);
+    return launch_stage_fp32(stage, c->cfg.flux, c->cfg.mhd, A, c->stream);
+}
+
+cudaError_t enqueue_step(Context* c) {
+    StageArgs A = stage_args(c);
+    step_begin_kernel<<<1, 1, 0, c->stream>>>(c->d_ctl, c->d_blocks, c->d_maxsig, c->d_lastsig, c->sp);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    if ((e = launch_stage(c, 1, A)) != cudaSuccess) return e;
+    if ((e = launch_stage(c, 2, A)) != cudaSuccess) return e;
+    step_end_kernel<<<1, 1, 0, c->stream>>>(c->d_ctl, c->sp);
+    return cudaGetLastError();
+}
+
+// Per-block signal maxima of the current state (needed by the first dt check).
+int scan_signal(Context* c) {
+    CK(cudaMemsetAsync(c->d_maxsig, 0, sizeof(unsigned long long) * c->blocks.size(), c->stream));
+    CK(cudaMemsetAsync(c->d_bad, 0, sizeof(int), c->stream));
+    CK(cudaMemcpyAsync(c->h_ctl, c->d_ctl, sizeof(Control), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    const double* Ucur = c->U[c->h_ctl->step & 1];
+    for (size_t b = 0; b < c->blocks.size(); ++b) {
+        long long n = (long long)c->blocks[b].n[0] * c->blocks[b].n[1] * c->blocks[b].n[2];
+        int nb = (int)((n + 255) / 256);
+        signal_scan_kernel<<<nb, 256, 0, c->stream>>>(Ucur, c->total, c->d_blocks, (int)b, c->P, c->d_maxsig,
+                                                       c->d_lastsig, c->d_bad);
+        CK(cudaGetLastError());
+    }
+    int bad = 0;
+    CK(cudaMemcpyAsync(&bad, c->d_bad, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (bad) return fail(c, GDFV_ERR_ARG, "state contains cells that do not decode");
+    c->signal_valid = true;
+    return GDFV_OK;
+}
+
+void fill_weights(double len, double* w) {
+    // e4/onedinterp.d:338-355 l2r2_prepare with all four lengths equal
+    const double lenL1 = len, lenL0 = len, lenR0 = len, lenR1 = len;
+    w[W_LENL0] = lenL0;
+    w[W_LENR0] = lenR0;
+    w[W_AL0] = 0.5 * lenL0 / (lenL1 + 2.0 * lenL0 + lenR0);
+    w[W_AR0] = 0.5 * lenR0 / (lenL0 + 2.0 * lenR0 + lenR1);
+    w[W_TOL] = 2.0 / (lenL0 + lenL1);
+    w[W_TOC] = 2.0 / (lenR0 + lenL0);
+    w[W_TOR] = 2.0 / (lenR1 + lenR0);
+    w[W_TWOL] = (2.0 * lenL0 + lenL1);
+    w[W_TWOR] = (2.0 * lenR0 + lenR1);
+}
+
+int do_prepare(Context* c) {
+    Config& g = c->cfg;
+    if (c->blocks.empty()) return fail(c, GDFV_ERR_STATE, "no blocks");
+    if (g.flux == FLUX_HLLE && !g.mhd) return fail(c, GDFV_ERR_ARG, "hlle is the MHD flux: set MHD=1");
+    if (g.mhd && g.flux != FLUX_HLLE) return fail(c, GDFV_ERR_ARG, "MHD runs use flux_calculator=hlle");
+    if (g.dims != 2 && g.dims != 3) return fail(c, GDFV_ERR_ARG, "dimensions must be 2 or 3");
+    c->nq = g.mhd ? 10 : 5;
+    const int nfaces = g.dims == 3 ? 6 : 4;
+    long long off = 0;
+    std::vector<InflowState> inflows;
+    c->h_blocks.clear();
+    std::vector<TileDesc> tiles;
+    const double Cv = g.R / (g.gamma - 1.0);
+    for (size_t b = 0; b < c->blocks.size(); ++b) {
+        HostBlock& hb = c->blocks[b];
+        if (g.dims == 2 && hb.n[2] != 1) return fail(c, GDFV_ERR_ARG, "2D blocks have nkc = 1");
+        for (int d = 0; d < (g.dims == 3 ? 3 : 2); ++d)
+            if (hb.n[d] < 2) return fail(c, GDFV_ERR_ARG, "blocks need at least 2 cells per active direction");
+        hb.offset = off;
+        BlockDesc B{};
+        for (int d = 0; d < 3; ++d) { B.n[d] = hb.n[d]; B.len[d] = hb.len[d]; fill_weights(hb.len[d], B.w[d]); }
+        B.offset = off;
+        if (g.dims == 2) {
+            B.area[0] = hb.len[1]; B.area[1] = hb.len[0]; B.area[2] = 0.0;
+            B.vol_inv = 1.0 / (hb.len[0] * hb.len[1]);
+            B.L_min = std::min(hb.len[0], hb.len[1]);
+        } else {
+            B.area[0] = hb.len[1] * hb.len[2];
+            B.area[1] = hb.len[2] * hb.len[0];
+            B.area[2] = hb.len[0] * hb.len[1];
+            B.vol_inv = 1.0 / (hb.len[0] * hb.len[1] * hb.len[2]);
+            B.L_min = std::min(std::min(hb.len[0], hb.len[1]), hb.len[2]);
+        }
+        B.x0 = hb.origin[0]; B.y0 = hb.origin[1]; B.z0 = hb.origin[2];
+        for (int f = 0; f < 6; ++f) {
+            const HostBC& bc = hb.bc[f];
+            B.bc_type[f] = bc.type;
+            B.bc_xorder[f] = bc.x_order;
+            B.bc_other[f] = bc.other;
+            B.bc_other_face[f] = bc.other_face;
+            B.bc_inflow[f] = -1;
+            if (f >= nfaces) continue;
+            if (bc.type == BC_EXCHANGE) {
+                if (bc.other < 0 || bc.other >= (int)c->blocks.size())
+                    return fail(c, GDFV_ERR_ARG, "exchange partner block does not exist");
+                if (bc.other_face / 2 != f / 2 || bc.other_face == f)
+                    return fail(c, GDFV_ERR_ARG, "exchange (orientation 0) joins opposite faces of the same index direction");
+                const HostBlock& ob = c->blocks[bc.other];
+                for (int d = 0; d < 3; ++d)
+                    if (d != f / 2 && ob.n[d] != hb.n[d]) return fail(c, GDFV_ERR_ARG, "exchange faces differ in size");
+                if (ob.n[f / 2] < 2) return fail(c, GDFV_ERR_ARG, "exchange partner is too thin");
+            }
+            if (bc.type == BC_EXTRAPOLATE && (bc.x_order < 0 || bc.x_order > 1))
+                return fail(c, GDFV_ERR_ARG, "x_order must be 0 or 1");
+            if (bc.type == BC_INFLOW) {
+                // FlowState:new{p=, T=, ...}: update_thermo_from_pT + update_sound_speed
+                InflowState s{};
+                double p = bc.inflow[0], T = bc.inflow[1];
+                if (!(p > 0.0) || !(T > 0.0)) return fail(c, GDFV_ERR_ARG, "inflow needs p > 0 and T > 0");
+                s.p = p;
+                s.rho = p / (T * g.R);
+                s.u = Cv * T;
+                s.a = std::sqrt(g.gamma * g.R * T);
+                for (int d = 0; d < 3; ++d) { s.vel[d] = bc.inflow[2 + d]; s.B[d] = bc.inflow[5 + d]; }
+                s.psi = bc.inflow[8];
+                B.bc_inflow[f] = (int)inflows.size();
+                inflows.push_back(s);
+            }
+        }
+        c->h_blocks.push_back(B);
+        // tile table: TI x TJ columns, k chunks
+        int kc = g.tile_kchunk > 0 ? g.tile_kchunk : std::min(hb.n[2], 32);
+        if (g.dims == 2) kc = 1;
+        for (int k0 = 0; k0 < hb.n[2]; k0 += kc)
+            for (int j0 = 0; j0 < hb.n[1]; j0 += TJ)
+                for (int i0 = 0; i0 < hb.n[0]; i0 += TI) {
+                    TileDesc t{};
+                    t.block = (int)b; t.i0 = i0; t.j0 = j0; t.k0 = k0; t.k1 = std::min(k0 + kc, hb.n[2]);
+                    tiles.push_back(t);
+                }
+        off += (long long)hb.n[0] * hb.n[1] * hb.n[2];
+    }
+    c->total = off;
+    c->n_tiles = (int)tiles.size();
+    NumParams& P = c->P;
+    P.gas.R = g.R; P.gas.gamma = g.gamma; P.gas.Cv = Cv; P.gas.Cvinv = 1.0 / Cv;
+    P.eps_van_albada = g.eps_van_albada;
+    P.divB_damping_length = g.divB_damping_length;
+    P.max_velocity = g.max_velocity; P.max_temp = g.max_temp; P.min_temp = g.min_temp;
+    P.apply_limiter = g.apply_limiter; P.extrema_clipping = g.extrema_clipping;
+    P.apply_entropy_fix = g.apply_entropy_fix; P.glm_reference_indexing = g.glm_reference_indexing;
+    P.mhd = g.mhd; P.divergence_cleaning = g.divergence_cleaning; P.dims = g.dims;
+    P.stringent_cfl = g.stringent_cfl; P.nq = c->nq;
+    StepParams& sp = c->sp;
+    sp.cfl_count = g.cfl_count; sp.n_stages = 2; sp.fixed_time_step = g.fixed_time_step;
+    sp.mhd_cleaning = g.mhd && g.divergence_cleaning;
+    sp.max_attempts = g.max_attempts; sp.max_invalid_cells = g.max_invalid_cells;
+    sp.nblocks = (int)c->blocks.size();
+    sp.cfl_value = g.cfl_value; sp.dt_init = g.dt_init; sp.dt_max = g.dt_max;
+
+    CK(cudaGetDevice(&c->device));
+    if (c->device < 64 && !g_configured[c->device]) {
+        CK(configure_stage_fp64());
+        CK(configure_stage_fp32());
+        g_configured[c->device] = true;
+    }
+    if (!c->stream) {
+        CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        c->own_stream = true;
+    }
+    const size_t bytes = sizeof(double) * (size_t)c->nq * (size_t)c->total;
+    CK(cudaMalloc(&c->U[0], bytes));
+    CK(cudaMalloc(&c->U[1], bytes));
+    CK(cudaMalloc(&c->dU0, bytes));
+    CK(cudaMemset(c->U[0], 0, bytes));
+    CK(cudaMemset(c->U[1], 0, bytes));
+    CK(cudaMemset(c->dU0, 0, bytes));
+    CK(cudaMalloc(&c->d_blocks, sizeof(BlockDesc) * c->h_blocks.size()));
+    CK(cudaMemcpy(c->d_blocks, c->h_blocks.data(), sizeof(BlockDesc) * c->h_blocks.size(), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&c->d_tiles, sizeof(TileDesc) * tiles.size()));
+    CK(cudaMemcpy(c->d_tiles, tiles.data(), sizeof(TileDesc) * tiles.size(), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&c->d_inflow, sizeof(InflowState) * std::max<size_t>(1, inflows.size())));
+    if (!inflows.empty())
+        CK(cudaMemcpy(c->d_inflow, inflows.data(), sizeof(InflowState) * inflows.size(), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&c->d_ctl, sizeof(Control)));
+    CK(cudaMallocHost(&c->h_ctl, sizeof(Control)));
+    std::memset(c->h_ctl, 0, sizeof(Control));
+    c->h_ctl->dt_global = g.dt_init;  // e4/simcore.d:761
+    c->h_ctl->first_bad_cell = LLONG_MAX;
+    CK(cudaMemcpy(c->d_ctl, c->h_ctl, sizeof(Control), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&c->d_maxsig, sizeof(unsigned long long) * c->blocks.size()));
+    CK(cudaMalloc(&c->d_lastsig, sizeof(double) * c->blocks.size()));
+    CK(cudaMalloc(&c->d_bad, sizeof(int)));
+    CK(cudaMemset(c->d_maxsig, 0, sizeof(unsigned long long) * c->blocks.size()));
+    CK(cudaMemset(c->d_lastsig, 0, sizeof(double) * c->blocks.size()));
+    c->prepared = true;
+    return GDFV_OK;
+}
+
+int read_ctl(Context* c) {
+    CK(cudaMemcpyAsync(c->h_ctl, c->d_ctl, sizeof(Control), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return GDFV_OK;
+}
+
+int write_ctl(Context* c) {
+    CK(cudaMemcpyAsync(c->d_ctl, c->h_ctl, sizeof(Control), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return GDFV_OK;
+}
+
+constexpr int kGraphSteps = 8;
+
+int build_graph(Context* c) {
+    if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = cudaSuccess;
+    for (int s = 0; s < kGraphSteps && e == cudaSuccess; ++s) e = enqueue_step(c);
+    cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
+    if (e != cudaSuccess) { if (g) cudaGraphDestroy(g); return cuda_fail(c, e, "capture step"); }
+    if (e2 != cudaSuccess) return cuda_fail(c, e2, "cudaStreamEndCapture");
+    e = cudaGraphInstantiate(&c->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(c, e, "cudaGraphInstantiate");
+    c->graph_steps = kGraphSteps;
+    return GDFV_OK;
+}
+
+}  // namespace gdfv
+
+// ====================================================================== C ABI
+using namespace gdfv;
+
+extern "C" {
+
+int gdfv_context_new(void) {
+    std::lock_guard<std::mutex> lk(g_mutex);
+    int h = g_next++;
+    g_ctx[h] = std::make_unique<Context>();
+    return h;
+}
+
+int gdfv_context_free(int ctx) {
+    std::unique_ptr<Context> victim;
+    {
+        std::lock_guard<std::mutex> lk(g_mutex);
+        auto it = g_ctx.find(ctx);
+        if (it == g_ctx.end()) return GDFV_ERR_ARG;
+        victim = std::move(it->second);
+        g_ctx.erase(it);
+    }
+    if (victim->stream) cudaStreamSynchronize(victim->stream);
+    return GDFV_OK;
+}
+
+int gdfv_config_set_str(int ctx, const char* key, const char* value) {
+    Context* c = get_ctx(ctx);
+    if (!c) return fail(nullptr, GDFV_ERR_ARG, "bad context");
+    if (c->prepared) return fail(c, GDFV_ERR_STATE, "configuration is frozen after gdfv_prepare");
+    std::string k = norm(key), v = norm(value);
+    if (k == "flux_calculator") {
+        if (v == "ausmdv") c->cfg.flux = FLUX_AUSMDV;
+        else if (v == "hllc") c->cfg.flux = FLUX_HLLC;
+        else if (v == "hlle") c->cfg.flux = FLUX_HLLE;
+        else return fail(c, GDFV_ERR_ARG, "unsupported flux_calculator: " + v);
+    } else if (k == "gasdynamic_update_scheme") {
+        if (v != "predictor_corrector" && v != "pc")
+            return fail(c, GDFV_ERR_ARG, "unsupported gasdynamic_update_scheme: " + v);
+    } else if (k == "thermo_interpolator") {
+        if (v != "rhou") return fail(c, GDFV_ERR_ARG, "unsupported thermo_interpolator: " + v);
+    } else if (k == "flux_precision") {
+        if (v == "fp64" || v == "double") c->cfg.precision = 0;
+        else if (v == "fp32" || v == "float") c->cfg.precision = 1;
+        else return fail(c, GDFV_ERR_ARG, "flux_precision is fp64 or fp32");
+    } else {
+        return fail(c, GDFV_ERR_ARG, "unknown string option: " + k);
+    }
+    return GDFV_OK;
+}
+
+int gdfv_config_set_int(int ctx, const char* key, long long value) {
+    Context* c = get_ctx(ctx);
+    if (!c) return fail(nullptr, GDFV_ERR_ARG, "bad context");
+    if (c->prepared) return fail(c, GDFV_ERR_STATE, "configuration is frozen after gdfv_prepare");
+    std::string k = norm(key);
+    Config& g = c->cfg;
+    int v = (int)value;
+    if (k == "interpolation_order") { if (v != 2) return fail(c, GDFV_ERR_ARG, "interpolation_order must be 2"); }
+    else if (k == "n_ghost_cell_layers") { if (v != 2) return fail(c, GDFV_ERR_ARG, "n_ghost_cell_layers must be 2"); }
+    else if (k == "interpolate_in_local_frame") { if (v != 1) return fail(c, GDFV_ERR_ARG, "interpolate_in_local_frame must be true"); }
+    else if (k == "dimensions") g.dims = v;
+    else if (k == "mhd") g.mhd = v != 0;
+    else if (k == "divergence_cleaning") g.divergence_cleaning = v != 0;
+    else if (k == "apply_limiter") g.apply_limiter = v != 0;
+    else if (k == "extrema_clipping") g.extrema_clipping = v != 0;
+    else if (k == "apply_entropy_fix") g.apply_entropy_fix = v != 0;
+    else if (k == "glm_reference_indexing") g.glm_reference_indexing = v != 0;
+    else if (k == "stringent_cfl") g.stringent_cfl = v != 0;
+    else if (k == "cfl_count") { if (v < 1) return fail(c, GDFV_ERR_ARG, "cfl_count >= 1"); g.cfl_count = v; }
+    else if (k == "max_attempts_for_step") { if (v < 1) return fail(c, GDFV_ERR_ARG, "max_attempts_for_step >= 1"); g.max_attempts = v; }
+    else if (k == "max_invalid_cells") g.max_invalid_cells = v;
+    else if (k == "fixed_time_step") g.fixed_time_step = v != 0;
+    else if (k == "tile_kchunk") { if (v < 0) return fail(c, GDFV_ERR_ARG, "tile_kchunk >= 0"); g.tile_kchunk = v; }
+    else return fail(c, GDFV_ERR_ARG, "unknown integer option: " + k);
+    return GDFV_OK;
+}
+
+int gdfv_config_set_double(int ctx, const char* key, double value) {
+    Context* c = get_ctx(ctx);
+    if (!c) return fail(nullptr, GDFV_ERR_ARG, "bad context");
+    if (c->prepared) return fail(c, GDFV_ERR_STATE, "configuration is frozen after gdfv_prepare");
+    std::string k = norm(key);
+    Config& g = c->cfg;
+    if (k == "cfl_value") g.cfl_value = value;
+    else if (k == "dt_init") g.dt_init = value;
+    else if (k == "dt_max") g.dt_max = value;
+    else if (k == "epsilon_van_albada") g.eps_van_albada = value;
+    else if (k == "r" || k == "R") g.R = value;
+    else if (k == "gamma") g.gamma = value;
+    else if (k == "divb_damping_length" || k == "divB_damping_length") g.divB_damping_length = value;
+    else if (k == "flowstate_limits_max_velocity") g.max_velocity = value;
+    else if (k == "flowstate_limits_max_temp") g.max_temp = value;
+    else if (k == "flowstate_limits_min_temp") g.min_temp = value;
+    else return fail(c, GDFV_ERR_ARG, "unknown real option: " + k);
+    return GDFV_OK;
+}
+
+int gdfv_config_get_double(int ctx, const char* key, double* value) {
+    Context* c = get_ctx(ctx);
+    if (!c || !value) return fail(c, GDFV_ERR_ARG, "bad argument");
+    std::string k = norm(key);
+    Config& g = c->cfg;
+    if (k == "cfl_value") *value = g.cfl_value;
+    else if (k == "dt_init") *value = g.dt_init;
+    else if (k == "dt_max") *value = g.dt_max;
+    else if (k == "epsilon_van_albada") *value = g.eps_van_albada;
+    else if (k == "R" || k == "r") *value = g.R;
+    else if (k == "gamma") *value = g.gamma;
+    else if (k == "divB_damping_length" || k == "divb_damping_length") *value = g.divB_damping_length;
+    else return fail(c, GDFV_ERR_ARG, "unknown real option: " + k);
+    return GDFV_OK;
+}
+
+int gdfv_block_new(int ctx, int nic, int njc, int nkc, double dx, double dy, double dz, double x0, double y0,
+                   double z0) {
+    Context* c = get_ctx(ctx);
+    if (!c) return fail(nullptr, GDFV_ERR_ARG, "bad context");
+    if (c->prepared) return fail(c, GDFV_ERR_STATE, "blocks are frozen after gdfv_prepare");
+    if (nic < 1 || njc < 1 || nkc < 1 || !(dx > 0) || !(dy > 0) || !(dz > 0))
+        return fail(c, GDFV_ERR_ARG, "block sizes and spacings must be positive");
+    if ((long long)nic * njc * nkc > (1ll << 34)) return fail(c, GDFV_ERR_ARG, "block too large");
+    HostBlock b;
+    b.n[0] = nic; b.n[1] = njc; b.n[2] = nkc;
+    b.len[0] = dx; b.len[1] = dy; b.len[2] = dz;
+    b.origin[0] = x0; b.origin[1] = y0; b.origin[2] = z0;
+    c->blocks.push_back(b);
+    return (int)c->blocks.size() - 1;
+}
+
+int gdfv_block_set_bc(int ctx, int blk, int face, const char* bc_type, int x_order, int other_blk, int other_face,
+                      const double* inflow) {
+    Context* c = get_ctx(ctx);
+    if (!c) return fail(nullptr, GDFV_ERR_ARG, "bad context");
+    if (c->prepared) return fail(c, GDFV_ERR_STATE, "boundary conditions are frozen after gdfv_prepare");
+    if (blk < 0 || blk >= (int)c->blocks.size() || face < 0 || face > 5) return fail(c, GDFV_ERR_ARG, "bad block or face");
+    std::string t = norm(bc_type);
+    HostBC bc;
+    if (t == "wall_with_slip" || t == "wallbc_withslip" || t == "slip_wall") bc.type = BC_SLIP_WALL;
+    else if (t == "outflow_simple_extrapolate" || t == "extrapolate") bc.type = BC_EXTRAPOLATE;
+    else if (t == "inflow_supersonic") bc.type = BC_INFLOW;
+    else if (t == "exchange_over_full_face" || t == "exchange" || t == "full_face_copy") bc.type = BC_EXCHANGE;
+    else return fail(c, GDFV_ERR_ARG, "unsupported boundary condition: " + t);
+    bc.x_order = x_order;
+    bc.other = other_blk;
+    bc.other_face = other_face;
+    if (bc.type == BC_INFLOW) {
+        if (!inflow) return fail(c, GDFV_ERR_ARG, "inflow_supersonic needs a flow state");
+        for (int q = 0; q < 9; ++q) bc.inflow[q] = inflow[q];
+    }
+    c->blocks[blk].bc[face] = bc;
+    return GDFV_OK;
+}
+
+int gdfv_prepare(int ctx) {
+    Context* c = get_ctx(ctx);
+    if (!c) return fail(nullptr, GDFV_ERR_ARG, "bad context");
+    if (c->prepared) return GDFV_OK;
+    return do_prepare(c);
+}
+
+long long gdfv_block_ncells(int ctx, int blk) {
+    Context* c = get_ctx(ctx);
+    if (!c || blk < 0 || blk >= (int)c->blocks.size()) return -1;
+    const HostBlock& b = c->blocks[blk];
+    return (long long)b.n[0] * b.n[1] * b.n[2];
+}
+
+long long gdfv_total_cells(int ctx) {
+    Context* c = get_ctx(ctx);
+    if (!c) return -1;
+    long long t = 0;
+    for (auto& b : c->blocks) t += (long long)b.n[0] * b.n[1] * b.n[2];
+    return t;
+}
+
+static int check_ready(Context* c, int blk) {
+    if (!c) return fail(nullptr, GDFV_ERR_ARG, "bad context");
+    if (!c->prepared) return fail(c, GDFV_ERR_STATE, "call gdfv_prepare first");
+    if (blk < -1 || blk >= (int)c->blocks.size()) return fail(c, GDFV_ERR_ARG, "bad block");
+    return GDFV_OK;
+}
+
+int gdfv_block_set_flow_rhoT(int ctx, int blk, const double* prim) {
+    Context* c = get_ctx(ctx);
+    int st = check_ready(c, blk);
+    if (st) return st;
+    if (!prim || blk < 0) return fail(c, GDFV_ERR_ARG, "bad argument");
+    if (read_ctl(c)) return GDFV_ERR_CUDA;
+    const HostBlock& b = c->blocks[blk];
+    long long n = (long long)b.n[0] * b.n[1] * b.n[2];
+    double* d_prim = nullptr;
+    CK(cudaMalloc(&d_prim, sizeof(double) * 9 * n));
+    cudaError_t e = cudaMemcpyAsync(d_prim, prim, sizeof(double) * 9 * n, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->d_bad, 0, sizeof(int), c->stream);
+    if (e == cudaSuccess) {
+        encode_rhoT_kernel<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(
+            d_prim, n, c->U[c->h_ctl->step & 1], c->total, b.offset, c->P, c->d_bad);
+        e = cudaGetLastError();
+    }
+    int bad = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&bad, c->d_bad, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(d_prim);
+    if (e != cudaSuccess) return cuda_fail(c, e, "set_flow_rhoT");
+    if (bad) return fail(c, GDFV_ERR_ARG, "initial state has T <= 0 or rho <= 0");
+    c->signal_valid = false;
+    return GDFV_OK;
+}
+
+int gdfv_block_set_conserved(int ctx, int blk, const double* U) {
+    Context* c = get_ctx(ctx);
+    int st = check_ready(c, blk);
+    if (st) return st;
+    if (!U || blk < 0) return fail(c, GDFV_ERR_ARG, "bad argument");
+    if (read_ctl(c)) return GDFV_ERR_CUDA;
+    const HostBlock& b = c->blocks[blk];
+    long long n = (long long)b.n[0] * b.n[1] * b.n[2];
+    double* dst = c->U[c->h_ctl->step & 1];
+    for (int q = 0; q < c->nq; ++q)
+        CK(cudaMemcpyAsync(dst + q * c->total + b.offset, U + q * n, sizeof(double) * n, cudaMemcpyHostToDevice,
+                           c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->signal_valid = false;
+    return GDFV_OK;
+}
+
+int gdfv_block_get_conserved(int ctx, int blk, double* U) {
+    Context* c = get_ctx(ctx);
+    int st = check_ready(c, blk);
+    if (st) return st;
+    if (!U || blk < 0) return fail(c, GDFV_ERR_ARG, "bad argument");
+    if (read_ctl(c)) return GDFV_ERR_CUDA;
+    const HostBlock& b = c->blocks[blk];
+    long long n = (long long)b.n[0] * b.n[1] * b.n[2];
+    const double* src = c->U[c->h_ctl->step & 1];
+    for (int q = 0; q < c->nq; ++q)
+        CK(cudaMemcpyAsync(U + q * n, src + q * c->total + b.offset, sizeof(double) * n, cudaMemcpyDeviceToHost,
+                           c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return GDFV_OK;
+}
+
+int gdfv_block_get_flow(int ctx, int blk, double* out) {
+    Context* c = get_ctx(ctx);
+    int st = check_ready(c, blk);
+    if (st) return st;
+    if (!out || blk < 0) return fail(c, GDFV_ERR_ARG, "bad argument");
+    if (read_ctl(c)) return GDFV_ERR_CUDA;
+    const HostBlock& b = c->blocks[blk];
+    long long n = (long long)b.n[0] * b.n[1] * b.n[2];
+    double* d_out = nullptr;
+    CK(cudaMalloc(&d_out, sizeof(double) * 12 * n));
+    decode_kernel<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(c->U[c->h_ctl->step & 1], c->total, b.offset,
+                                                                       n, c->P, d_out);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, d_out, sizeof(double) * 12 * n, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(d_out);
+    if (e != cudaSuccess) return cuda_fail(c, e, "get_flow");
+    return GDFV_OK;
+}
+
+int gdfv_run(int ctx, int max_steps, double max_time, int* steps_taken) {
+    Context* c = get_ctx(ctx);
+    int st = check_ready(c, -1);
+    if (st) return st;
+    if (steps_taken) *steps_taken = 0;
+    if (max_steps <= 0) return GDFV_OK;
+    if (!c->signal_valid) {
+        if ((st = scan_signal(c)) != GDFV_OK) return st;
+    }
+    if (read_ctl(c)) return GDFV_ERR_CUDA;
+    if (c->h_ctl->status != ST_OK) return fail(c, GDFV_ERR_STATE, "a previous run failed; reset the state");
+    const int start_step = c->h_ctl->step;
+    c->h_ctl->step_limit = start_step + max_steps;
+    c->h_ctl->max_time = max_time;
+    c->h_ctl->halted = 0;
+    c->h_ctl->steps_done = 0;
+    if (write_ctl(c)) return GDFV_ERR_CUDA;
+    if (!c->graph) {
+        if ((st = build_graph(c)) != GDFV_OK) return st;
+    }
+    // Replay the captured steps in batches sized to what is left, reading the
+    // control record back after each batch.  Steps past the halt are no-ops.
+    const long long slot_budget = (long long)(c->cfg.max_attempts + 1) * (max_steps + 1) + 2 * c->graph_steps;
+    long long launched = 0;
+    while (!c->h_ctl->halted && c->h_ctl->status == ST_OK && launched < slot_budget) {
+        long long remaining = (long long)c->h_ctl->step_limit - c->h_ctl->step;
+        if (max_time > 0.0 && c->h_ctl->dt_global > 0.0) {
+            double est = std::ceil((max_time - c->h_ctl->time) / c->h_ctl->dt_global) + 1.0;
+            if (est < (double)remaining) remaining = (long long)std::max(1.0, est);
+        }
+        if (c->h_ctl->retrying) remaining += 1;
+        int graphs = (int)std::min<long long>(64, std::max<long long>(1, (remaining + c->graph_steps - 1) / c->graph_steps));
+        for (int g = 0; g < graphs; ++g) CK(cudaGraphLaunch(c->graph, c->stream));
+        launched += (long long)graphs * c->graph_steps;
+        if (read_ctl(c)) return GDFV_ERR_CUDA;
+    }
+    if (steps_taken) *steps_taken = c->h_ctl->step - start_step;
+    if (c->h_ctl->status == ST_TOO_MANY_BAD_CELLS)
+        return fail(c, GDFV_ERR_BAD_CELLS, "Too many bad cells during explicit gasdynamic update.");
+    if (c->h_ctl->status == ST_DECODE_FAILED)
+        return fail(c, GDFV_ERR_STEP_FAILED, "Explicit update failed after max_attempts_for_step attempts.");
+    return GDFV_OK;
+}
+
+int gdfv_get_time(int ctx, double* out5, int* step) {
+    Context* c = get_ctx(ctx);
+    int st = check_ready(c, -1);
+    if (st) return st;
+    if (read_ctl(c)) return GDFV_ERR_CUDA;
+    if (out5) {
+        out5[0] = c->h_ctl->time; out5[1] = c->h_ctl->dt_global; out5[2] = c->h_ctl->c_h;
+        out5[3] = c->h_ctl->cfl_max; out5[4] = c->h_ctl->dt_allow;
+    }
+    if (step) *step = c->h_ctl->step;
+    return GDFV_OK;
+}
+
+int gdfv_set_time(int ctx, double time, int step, double dt_global) {
+    Context* c = get_ctx(ctx);
+    int st = check_ready(c, -1);
+    if (st) return st;
+    if (step < 0 || !(dt_global > 0)) return fail(c, GDFV_ERR_ARG, "bad time state");
+    if (read_ctl(c)) return GDFV_ERR_CUDA;
+    int old_parity = c->h_ctl->step & 1;
+    if ((step & 1) != old_parity) {
+        CK(cudaMemcpyAsync(c->U[step & 1], c->U[old_parity], sizeof(double) * c->nq * c->total,
+                           cudaMemcpyDeviceToDevice, c->stream));
+    }
+    c->h_ctl->time = time;
+    c->h_ctl->step = step;
+    c->h_ctl->dt_global = dt_global;
+    c->h_ctl->status = ST_OK;
+    c->h_ctl->halted = 0;
+    c->h_ctl->attempt = 0;
+    c->h_ctl->retrying = 0;
+    if (write_ctl(c)) return GDFV_ERR_CUDA;
+    c->signal_valid = false;
+    return GDFV_OK;
+}
+
+int gdfv_residual(int ctx, const double* U_dev, double* R_dev) {
+    Context* c = get_ctx(ctx);
+    int st = check_ready(c, -1);
+    if (st) return st;
+    if (!U_dev || !R_dev) return fail(c, GDFV_ERR_ARG, "null pointer");
+    StageArgs A = stage_args(c);
+    A.U_in = U_dev;
+    A.R_out = R_dev;
+    CK(launch_stage(c, 0, A));
+    CK(cudaStreamSynchronize(c->stream));
+    return GDFV_OK;
+}
+
+int gdfv_state_device_ptr(int ctx, double** U_dev) {
+    Context* c = get_ctx(ctx);
+    int st = check_ready(c, -1);
+    if (st) return st;
+    if (!U_dev) return fail(c, GDFV_ERR_ARG, "null pointer");
+    if (read_ctl(c)) return GDFV_ERR_CUDA;
+    *U_dev = c->U[c->h_ctl->step & 1];
+    return GDFV_OK;
+}
+
+int gdfv_set_stream(int ctx, void* stream) {
+    Context* c = get_ctx(ctx);
+    if (!c) return fail(nullptr, GDFV_ERR_ARG, "bad context");
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    c->stream = (cudaStream_t)stream;
+    c->own_stream = false;
+    if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
+    return GDFV_OK;
+}
+
+int gdfv_time_stages(int ctx, int reps, double* ms) {
+    Context* c = get_ctx(ctx);
+    int st = check_ready(c, -1);
+    if (st) return st;
+    if (reps < 1 || !ms) return fail(c, GDFV_ERR_ARG, "bad argument");
+    if (!c->signal_valid && (st = scan_signal(c)) != GDFV_OK) return st;
+    if (read_ctl(c)) return GDFV_ERR_CUDA;
+    Control saved = *c->h_ctl;
+    // a step that cannot halt: the kernels run, the step counter does not move
+    c->h_ctl->step_limit = INT_MAX;
+    c->h_ctl->max_time = 0.0;
+    c->h_ctl->halted = 0;
+    c->h_ctl->n_fail = 0;
+    c->h_ctl->n_invalid1 = 0;
+    if (write_ctl(c)) return GDFV_ERR_CUDA;
+    StageArgs A = stage_args(c);
+    cudaEvent_t e0, e1, e2;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventCreate(&e2));
+    float t1 = 0, t2 = 0;
+    for (int r = 0; r < reps + 1; ++r) {
+        CK(cudaEventRecord(e0, c->stream));
+        CK(launch_stage(c, 1, A));
+        CK(cudaEventRecord(e1, c->stream));
+        CK(launch_stage(c, 2, A));
+        CK(cudaEventRecord(e2, c->stream));
+        CK(cudaEventSynchronize(e2));
+        float a = 0, b = 0;
+        CK(cudaEventElapsedTime(&a, e0, e1));
+        CK(cudaEventElapsedTime(&b, e1, e2));
+        if (r > 0) { t1 += a; t2 += b; }  // first repetition is a warm-up
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaEventDestroy(e2);
+    ms[0] = t1 / reps;
+    ms[1] = t2 / reps;
+    // stage 2 wrote the other buffer; the current state and the controller are untouched
+    *c->h_ctl = saved;
+    if (write_ctl(c)) return GDFV_ERR_CUDA;
+    c->signal_valid = false;  // the timed corrector stages overwrote the signal maxima
+    return GDFV_OK;
+}
+
+int gdfv_last_error(int ctx, char* buf, int n) {
+    if (!buf || n <= 0) return GDFV_ERR_ARG;
+    Context* c = get_ctx(ctx);
+    std::snprintf(buf, (size_t)n, "%s", c ? c->err.c_str() : g_err.c_str());
+    return GDFV_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,285 @@
+"""Host-side solver API over libgdfv, in the vocabulary of the reference's
+job scripts (e4/prep.lua, e4/configoptions.lua, e4/bc.lua, e4/fluidblock.lua):
+
+    cfg = Config(flux_calculator="ausmdv")          # config.flux_calculator = "ausmdv"
+    sim = Simulation(cfg, gas=IdealGas(R=287.1, gamma=1.4))
+    inflow = FlowState(p=5e3, T=220.0, velx=891.8)   # FlowState:new{p=,T=,velx=}
+    blk = sim.add_block(nic, njc, nkc, dx, dy, dz,
+                        bcList={"west": InFlowBC_Supersonic(inflow),
+                                "east": OutFlowBC_SimpleExtrapolate()})
+    sim.set_flow_rhoT(blk, rho, vel, T)
+    sim.run(max_time=..., max_step=...)
+
+Option names and accepted values are the reference's (e4/globalconfig.d:1858-2004),
+boundary-condition classes keep the reference's names.  Every call goes through
+the C ABI in include/gdfv.h.
+"""
+import numpy as np
+
+from ._lib import GDFV_OK, GdfvError, check, ffi, lib
+
+FACE_INDEX = {"west": 0, "iminus": 0, "east": 1, "iplus": 1, "south": 2, "jminus": 2,
+              "north": 3, "jplus": 3, "bottom": 4, "kminus": 4, "top": 5, "kplus": 5}
+FACE_NAMES = ["west", "east", "south", "north", "bottom", "top"]
+
+_STR_KEYS = ("flux_calculator", "gasdynamic_update_scheme", "thermo_interpolator", "flux_precision")
+_INT_KEYS = ("interpolation_order", "dimensions", "MHD", "divergence_cleaning", "apply_limiter",
+             "extrema_clipping", "apply_entropy_fix", "interpolate_in_local_frame", "stringent_cfl",
+             "cfl_count", "max_attempts_for_step", "max_invalid_cells", "fixed_time_step",
+             "n_ghost_cell_layers", "glm_reference_indexing", "tile_kchunk")
+_DBL_KEYS = ("cfl_value", "dt_init", "dt_max", "epsilon_van_albada", "divB_damping_length",
+             "flowstate_limits_max_velocity", "flowstate_limits_max_temp", "flowstate_limits_min_temp")
+
+
+class Config:
+    """Solver options.  Defaults are the reference's (e4/globalconfig.d:927-1299)
+    except flux_calculator, whose reference default (adaptive_hanel_ausmdv) is not
+    on this path; ausmdv is used instead."""
+
+    def __init__(self, **kw):
+        self.flux_calculator = "ausmdv"
+        self.gasdynamic_update_scheme = "predictor_corrector"
+        self.thermo_interpolator = "rhou"
+        self.flux_precision = "fp64"
+        self.interpolation_order = 2
+        self.dimensions = 3
+        self.MHD = False
+        self.divergence_cleaning = False
+        self.apply_limiter = True
+        self.extrema_clipping = True
+        self.apply_entropy_fix = True
+        self.interpolate_in_local_frame = True
+        self.stringent_cfl = False
+        self.cfl_count = 10
+        self.max_attempts_for_step = 3
+        self.max_invalid_cells = 0
+        self.fixed_time_step = False
+        self.n_ghost_cell_layers = 2
+        self.glm_reference_indexing = True
+        self.tile_kchunk = 0
+        self.cfl_value = 0.5
+        self.dt_init = 1.0e-3
+        self.dt_max = 1.0e-3
+        self.epsilon_van_albada = 1.0e-12
+        self.divB_damping_length = 1.0
+        self.flowstate_limits_max_velocity = 30000.0
+        self.flowstate_limits_max_temp = 50000.0
+        self.flowstate_limits_min_temp = 0.0
+        for k, v in kw.items():
+            if not hasattr(self, k):
+                raise KeyError(f"unknown config option {k}")
+            setattr(self, k, v)
+
+
+class IdealGas:
+    """Ideal gas (src/gas/ideal_gas.d): R = R_universal / mMass."""
+
+    R_UNIVERSAL = 8.31451  # src/gas/physical_constants.d:13
+
+    def __init__(self, R=None, gamma=1.4, mMass=None):
+        if R is None:
+            if mMass is None:
+                raise ValueError("give R or mMass")
+            R = self.R_UNIVERSAL / mMass
+        self.R = float(R)
+        self.gamma = float(gamma)
+        self.Cv = self.R / (self.gamma - 1.0)
+
+
+class FlowState:
+    """Uniform flow state given by p and T (FlowState:new{p=,T=,velx=,...})."""
+
+    def __init__(self, p, T, velx=0.0, vely=0.0, velz=0.0, Bx=0.0, By=0.0, Bz=0.0, psi=0.0):
+        self.p, self.T = float(p), float(T)
+        self.vel = (float(velx), float(vely), float(velz))
+        self.B = (float(Bx), float(By), float(Bz))
+        self.psi = float(psi)
+
+    def as_array(self):
+        return np.array([self.p, self.T, *self.vel, *self.B, self.psi], dtype=np.float64)
+
+
+class WallBC_WithSlip:
+    name = "wall_with_slip"
+
+
+class OutFlowBC_SimpleExtrapolate:
+    name = "outflow_simple_extrapolate"
+
+    def __init__(self, xOrder=0):
+        self.xOrder = int(xOrder)
+
+
+class InFlowBC_Supersonic:
+    name = "inflow_supersonic"
+
+    def __init__(self, flowState):
+        self.flowState = flowState
+
+
+class ExchangeBC_FullFace:
+    name = "exchange_over_full_face"
+
+    def __init__(self, otherBlock, otherFace):
+        self.otherBlock = int(otherBlock)
+        self.otherFace = FACE_INDEX[otherFace] if isinstance(otherFace, str) else int(otherFace)
+
+
+class Simulation:
+    """One libgdfv context: configuration, blocks, and the time-marching state."""
+
+    def __init__(self, config=None, gas=None):
+        self.config = config or Config()
+        self.gas = gas or IdealGas(R=287.1, gamma=1.4)
+        self.L = lib()
+        self.ctx = self.L.gdfv_context_new()
+        if self.ctx < 0:
+            raise GdfvError(self.ctx, "could not create a context")
+        self.blocks = []
+        self._bcs = []
+        self._prepared = False
+
+    # ---------------------------------------------------------------- setup
+    def _apply_config(self):
+        c = self.config
+        L, h = self.L, self.ctx
+        for k in _STR_KEYS:
+            check(h, L.gdfv_config_set_str(h, k.encode(), str(getattr(c, k)).encode()))
+        for k in _INT_KEYS:
+            check(h, L.gdfv_config_set_int(h, k.encode(), int(getattr(c, k))))
+        for k in _DBL_KEYS:
+            check(h, L.gdfv_config_set_double(h, k.encode(), float(getattr(c, k))))
+        check(h, L.gdfv_config_set_double(h, b"R", self.gas.R))
+        check(h, L.gdfv_config_set_double(h, b"gamma", self.gas.gamma))
+
+    @property
+    def nq(self):
+        return 10 if self.config.MHD else 5
+
+    def add_block(self, nic, njc, nkc, dx, dy, dz, x0=0.0, y0=0.0, z0=0.0, bcList=None):
+        """A uniform Cartesian block; bcList maps face names to BC objects
+        (faces not listed are slip walls, as in e4/fluidblock.lua:102)."""
+        b = self.L.gdfv_block_new(self.ctx, nic, njc, nkc, dx, dy, dz, x0, y0, z0)
+        if b < 0:
+            check(self.ctx, b)
+        self.blocks.append((nic, njc, nkc))
+        self._bcs.append({})
+        for face, bc in (bcList or {}).items():
+            self.set_bc(b, face, bc)
+        return b
+
+    def set_bc(self, blk, face, bc):
+        f = FACE_INDEX[face] if isinstance(face, str) else int(face)
+        x_order, other, other_face = 0, -1, -1
+        inflow = ffi.NULL
+        if isinstance(bc, OutFlowBC_SimpleExtrapolate):
+            x_order = bc.xOrder
+        elif isinstance(bc, ExchangeBC_FullFace):
+            other, other_face = bc.otherBlock, bc.otherFace
+        elif isinstance(bc, InFlowBC_Supersonic):
+            arr = bc.flowState.as_array()
+            self._bcs[blk][f] = arr  # keep alive
+            inflow = ffi.cast("double*", arr.ctypes.data)
+        check(self.ctx, self.L.gdfv_block_set_bc(self.ctx, blk, f, bc.name.encode(), x_order, other,
+                                                  other_face, inflow))
+
+    def prepare(self):
+        if not self._prepared:
+            self._apply_config()
+            check(self.ctx, self.L.gdfv_prepare(self.ctx))
+            self._prepared = True
+
+    def ncells(self, blk):
+        nic, njc, nkc = self.blocks[blk]
+        return nic * njc * nkc
+
+    # ---------------------------------------------------------------- state
+    def set_flow_rhoT(self, blk, rho, vel, T, B=None, psi=None):
+        """Cell states from density, velocity and temperature (arrays shaped
+        (nkc, njc, nic) or broadcastable)."""
+        self.prepare()
+        nic, njc, nkc = self.blocks[blk]
+        shp = (nkc, njc, nic)
+        prim = np.zeros((9, nic * njc * nkc))
+        prim[0] = np.broadcast_to(rho, shp).ravel()
+        for c in range(3):
+            prim[1 + c] = np.broadcast_to(vel[c], shp).ravel()
+        prim[4] = np.broadcast_to(T, shp).ravel()
+        if B is not None:
+            for c in range(3):
+                prim[5 + c] = np.broadcast_to(B[c], shp).ravel()
+        if psi is not None:
+            prim[8] = np.broadcast_to(psi, shp).ravel()
+        prim = np.ascontiguousarray(prim)
+        check(self.ctx, self.L.gdfv_block_set_flow_rhoT(self.ctx, blk, ffi.cast("double*", prim.ctypes.data)))
+
+    def set_flowstate(self, blk, fs):
+        """Uniform initial state from a p,T FlowState."""
+        rho = fs.p / (fs.T * self.gas.R)
+        self.set_flow_rhoT(blk, rho, fs.vel, fs.T, B=fs.B, psi=fs.psi)
+
+    def get_conserved(self, blk):
+        self.prepare()
+        out = np.zeros((self.nq, self.ncells(blk)))
+        check(self.ctx, self.L.gdfv_block_get_conserved(self.ctx, blk, ffi.cast("double*", out.ctypes.data)))
+        return out
+
+    def set_conserved(self, blk, U):
+        self.prepare()
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        check(self.ctx, self.L.gdfv_block_set_conserved(self.ctx, blk, ffi.cast("double*", U.ctypes.data)))
+
+    def get_flow(self, blk):
+        self.prepare()
+        out = np.zeros((12, self.ncells(blk)))
+        check(self.ctx, self.L.gdfv_block_get_flow(self.ctx, blk, ffi.cast("double*", out.ctypes.data)))
+        names = ["rho", "vx", "vy", "vz", "u", "p", "T", "a", "Bx", "By", "Bz", "psi"]
+        return {k: out[q] for q, k in enumerate(names)}
+
+    # ---------------------------------------------------------------- marching
+    def run(self, max_step=1, max_time=0.0):
+        """Advance until max_step more steps or time >= max_time; returns steps taken."""
+        self.prepare()
+        taken = ffi.new("int*")
+        check(self.ctx, self.L.gdfv_run(self.ctx, int(max_step), float(max_time), taken))
+        return taken[0]
+
+    def time(self):
+        out = ffi.new("double[5]")
+        st = ffi.new("int*")
+        check(self.ctx, self.L.gdfv_get_time(self.ctx, out, st))
+        return dict(time=out[0], dt=out[1], c_h=out[2], cfl_max=out[3], dt_allow=out[4], step=st[0])
+
+    def set_time(self, time, step, dt_global):
+        check(self.ctx, self.L.gdfv_set_time(self.ctx, float(time), int(step), float(dt_global)))
+
+    def total_cells(self):
+        return int(self.L.gdfv_total_cells(self.ctx))
+
+    def residual(self, U_ptr, R_ptr):
+        """R(U) on device arrays [nq][total] given as integer device addresses."""
+        check(self.ctx, self.L.gdfv_residual(self.ctx, ffi.cast("double*", U_ptr), ffi.cast("double*", R_ptr)))
+
+    def state_ptr(self):
+        p = ffi.new("double**")
+        check(self.ctx, self.L.gdfv_state_device_ptr(self.ctx, p))
+        return int(ffi.cast("uintptr_t", p[0]))
+
+    def set_stream(self, stream_handle):
+        check(self.ctx, self.L.gdfv_set_stream(self.ctx, ffi.cast("void*", stream_handle)))
+
+    def time_stages(self, reps=10):
+        ms = ffi.new("double[2]")
+        check(self.ctx, self.L.gdfv_time_stages(self.ctx, int(reps), ms))
+        return ms[0], ms[1]
+
+    def close(self):
+        if getattr(self, "ctx", -1) >= 0:
+            self.L.gdfv_context_free(self.ctx)
+            self.ctx = -1
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

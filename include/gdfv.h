@@ -1,0 +1,128 @@
+/* gdfv.h -- C ABI of the B200 structured-grid finite-volume library (libgdfv.so).
+ *
+ * Drop-in boundary for the explicit structured-grid update that Eilmer-4 and
+ * chicken share.  Conventions follow the reference's loadable-library wrappers
+ * (src/gas/gas_cwrap.d): integer handles, plain pointers and sizes, status 0 on
+ * success and a negative value on error, never an exception across the ABI;
+ * the message of the last error is kept per context (gdfv_last_error).
+ *
+ * Arrays are structure-of-arrays, FP64, cell index i fastest:
+ *   conserved  [nq][ncells]  nq = 5 (mass, x/y/z-momentum, total energy) or 10 with MHD
+ *              (+ xB, yB, zB, psi, divB), e4/conservedquantities.d:148-197
+ *   flow       [12][ncells]  rho, vel.x, vel.y, vel.z, u, p, T, a, B.x, B.y, B.z, psi
+ *   rhoT state [9][ncells]   rho, vel.x, vel.y, vel.z, T, B.x, B.y, B.z, psi
+ * "Host" arguments are host memory; "device" arguments are device memory on the
+ * context's GPU (for example torch's data_ptr()).
+ */
+#ifndef GDFV_H
+#define GDFV_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+#define GDFV_OK 0
+#define GDFV_ERR_ARG (-1)          /* bad handle, key, value or size */
+#define GDFV_ERR_BAD_CELLS (-2)    /* too many invalid cells: the run stopped */
+#define GDFV_ERR_STEP_FAILED (-3)  /* decode failed on every attempt of a step */
+#define GDFV_ERR_CUDA (-4)         /* a CUDA call failed */
+#define GDFV_ERR_STATE (-5)        /* call out of order (e.g. before gdfv_prepare) */
+
+/* Face numbering of a structured block, src/geom/elements/nomenclature.d:12-19. */
+#define GDFV_WEST 0
+#define GDFV_EAST 1
+#define GDFV_SOUTH 2
+#define GDFV_NORTH 3
+#define GDFV_BOTTOM 4
+#define GDFV_TOP 5
+
+/* New context on the current CUDA device; returns a handle >= 0 or < 0.
+ * Replaces the global configuration object GlobalConfig (e4/globalconfig.d:927). */
+int gdfv_context_new(void);
+int gdfv_context_free(int ctx);
+
+/* Solver options by the reference's own JSON/Lua key names and values
+ * (e4/globalconfig.d:1858-2004 readers, :186-206 and :320-345 name->enum maps,
+ * '-' accepted for '_').  Strings: flux_calculator (ausmdv | hllc | hlle),
+ * gasdynamic_update_scheme (predictor_corrector | pc), thermo_interpolator (rhou),
+ * flux_precision (fp64 | fp32).  Integers: interpolation_order (2), dimensions (2|3),
+ * MHD, divergence_cleaning, apply_limiter, extrema_clipping, apply_entropy_fix,
+ * interpolate_in_local_frame (1), stringent_cfl, cfl_count, max_attempts_for_step,
+ * max_invalid_cells, fixed_time_step, n_ghost_cell_layers (2), glm_reference_indexing,
+ * tile_kchunk.  Doubles: cfl_value, dt_init, dt_max, epsilon_van_albada, R, gamma,
+ * divB_damping_length, flowstate_limits_max_velocity, flowstate_limits_max_temp,
+ * flowstate_limits_min_temp.  Unknown key or value: GDFV_ERR_ARG. */
+int gdfv_config_set_str(int ctx, const char* key, const char* value);
+int gdfv_config_set_int(int ctx, const char* key, long long value);
+int gdfv_config_set_double(int ctx, const char* key, double value);
+int gdfv_config_get_double(int ctx, const char* key, double* value);
+
+/* A uniform Cartesian structured block of nic x njc x nkc cells with origin
+ * (x0,y0,z0); returns the block id (>= 0).  Replaces SFluidBlock construction
+ * (e4/sfluidblock.d:440-700) for axis-aligned grids. */
+int gdfv_block_new(int ctx, int nic, int njc, int nkc, double dx, double dy, double dz,
+                   double x0, double y0, double z0);
+
+/* Boundary condition of one face, by the reference's BC type names:
+ *   "wall_with_slip"             WallBC_WithSlip (e4/bc.lua:733-757)
+ *   "outflow_simple_extrapolate" OutFlowBC_SimpleExtrapolate, x_order 0 or 1 (:1511-1530)
+ *   "inflow_supersonic"          InFlowBC_Supersonic; inflow = {p, T, vel.x, vel.y, vel.z,
+ *                                B.x, B.y, B.z, psi} as FlowState:new{p=,T=,...} (:1251-1280)
+ *   "exchange_over_full_face"    ExchangeBC_FullFace with orientation 0 onto the opposite
+ *                                face other_face of block other_blk (:1603)
+ * Ghost cells are never stored: the kernels synthesise them (ghost_cell_effect/*.d). */
+int gdfv_block_set_bc(int ctx, int blk, int face, const char* bc_type, int x_order,
+                      int other_blk, int other_face, const double* inflow);
+
+/* Validate the configuration and allocate device memory.  After this call
+ * blocks and options are frozen. */
+int gdfv_prepare(int ctx);
+
+/* Initial state from host rhoT arrays (e4/fvcell.d:511-583 encode_conserved after
+ * update_thermo_from_rhoT, ideal_gas.d:107-115). */
+int gdfv_block_set_flow_rhoT(int ctx, int blk, const double* rhoT_host);
+/* Conserved state of one block, host arrays. */
+int gdfv_block_set_conserved(int ctx, int blk, const double* U_host);
+int gdfv_block_get_conserved(int ctx, int blk, double* U_host);
+/* Decoded flow state of one block (e4/fvcell.d:586-822 decode_conserved), host array. */
+int gdfv_block_get_flow(int ctx, int blk, double* flow_host);
+/* Number of cells in one block, and in all blocks together. */
+long long gdfv_block_ncells(int ctx, int blk);
+long long gdfv_total_cells(int ctx);
+
+/* Time-march: take steps until max_steps more steps are done or time >= max_time
+ * (max_time <= 0: no time limit).  Replaces the loop of integrate_in_time
+ * (e4/simcore.d:1055-1366) around gasdynamic_explicit_increment_with_fixed_grid
+ * (e4/simcore_gasdynamic_step.d:904-1587) with determine_time_step_size (:60-160)
+ * and update_ch_for_divergence_cleaning (e4/simcore.d:1625-1648).  The dt rule, the
+ * retry with dt*0.2 and the bad-cell abort run on the device.
+ * Returns 0, GDFV_ERR_BAD_CELLS or GDFV_ERR_STEP_FAILED. */
+int gdfv_run(int ctx, int max_steps, double max_time, int* steps_taken);
+/* out5 = {time, dt_global, c_h, cfl_max, dt_allow}; step = steps taken so far. */
+int gdfv_get_time(int ctx, double* out5, int* step);
+/* Set the simulation time, step counter and dt_global (e.g. after a restart). */
+int gdfv_set_time(int ctx, double time, int step, double dt_global);
+
+/* Residual R(U) = dU/dt for every block, device arrays over all blocks ([nq][total]).
+ * One call = FluidBlock.applyPreReconAction + convective_flux_phase0
+ * (e4/sfluidblock.d:2188-2245) + FVCell.time_derivatives (e4/fvcell.d:824-856)
+ * on the state U.  Uses the context's current c_h. */
+int gdfv_residual(int ctx, const double* U_dev, double* R_dev);
+
+/* Device pointer of the current conserved state ([nq][total], borrowed, valid
+ * until the next gdfv_run), and of the context's CUDA stream. */
+int gdfv_state_device_ptr(int ctx, double** U_dev);
+int gdfv_set_stream(int ctx, void* cuda_stream);
+
+/* Kernel timing: run `reps` repetitions of each stage kernel on the current state
+ * without advancing it; ms[0] = stage 1, ms[1] = stage 2 average milliseconds per launch. */
+int gdfv_time_stages(int ctx, int reps, double* ms);
+
+/* Copy of the last error message of a context (NUL-terminated, truncated to n). */
+int gdfv_last_error(int ctx, char* buf, int n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GDFV_H */

@@ -1,0 +1,203 @@
+"""ctypes front end of the CPU oracle (liboracle.so).
+
+TEST INFRASTRUCTURE ONLY.  The oracle restates the Eilmer-4 explicit
+structured-grid update on the CPU (see fv_oracle.hpp / fv_oracle.cpp for the
+reference file:line of every function).  Only tests/, __graft_entry__.smoke()
+and bench.py's CPU-baseline leg may load it, and only as the checker.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+FLUX = {"ausmdv": 0, "hllc": 1, "hlle": 2}
+SCHEME = {"euler": 0, "pc": 1, "predictor_corrector": 1, "tvd_rk3": 2}
+BC = {"wall_with_slip": 0, "extrapolate": 1, "inflow_supersonic": 2, "exchange": 3}
+FACES = {"west": 0, "east": 1, "south": 2, "north": 3, "bottom": 4, "top": 5}
+
+
+def build():
+    """Compile liboracle.so in place (g++ with OpenMP)."""
+    subprocess.run(["make", "-s", "-C", _HERE, "liboracle.so"], check=True)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        L = ctypes.CDLL(path)
+        dp = ctypes.POINTER(ctypes.c_double)
+        L.orc_new.restype = ctypes.c_int
+        L.orc_set_int.argtypes = [ctypes.c_int, ctypes.c_char_p, ctypes.c_int]
+        L.orc_set_double.argtypes = [ctypes.c_int, ctypes.c_char_p, ctypes.c_double]
+        L.orc_add_block.argtypes = [ctypes.c_int] + [ctypes.c_int] * 3 + [ctypes.c_double] * 6
+        L.orc_set_bc.argtypes = [ctypes.c_int] * 7 + [dp]
+        L.orc_set_flow_rhoT.argtypes = [ctypes.c_int, ctypes.c_int, dp]
+        L.orc_run.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double]
+        L.orc_get_time.argtypes = [ctypes.c_int, dp, ctypes.POINTER(ctypes.c_int)]
+        L.orc_get_U.argtypes = [ctypes.c_int, ctypes.c_int, dp]
+        L.orc_set_U.argtypes = [ctypes.c_int, ctypes.c_int, dp]
+        L.orc_get_flow.argtypes = [ctypes.c_int, ctypes.c_int, dp]
+        L.orc_residual.argtypes = [ctypes.c_int, dp, dp]
+        L.orc_jvp_complex.argtypes = [ctypes.c_int, dp, dp, ctypes.c_double, dp]
+        L.orc_jvp_real.argtypes = [ctypes.c_int, dp, dp, ctypes.c_double, dp, dp]
+        L.orc_face_flux.argtypes = [ctypes.c_int, ctypes.c_int, dp, ctypes.c_double, dp]
+        L.orc_last_error.argtypes = [ctypes.c_int, ctypes.c_char_p, ctypes.c_int]
+        _LIB = L
+    return _LIB
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class OracleSim:
+    """One oracle simulation: a set of uniform Cartesian blocks."""
+
+    INT_KEYS = {"dimensions", "MHD", "divergence_cleaning", "apply_limiter", "extrema_clipping",
+                "apply_entropy_fix", "glm_reference_indexing", "stringent_cfl", "cfl_count",
+                "max_attempts_for_step", "max_invalid_cells", "chicken_compat"}
+
+    def __init__(self, **cfg):
+        self.L = lib()
+        self.h = self.L.orc_new()
+        self.blocks = []
+        self.mhd = bool(cfg.get("MHD", False))
+        for k, v in cfg.items():
+            self.set(k, v)
+
+    def set(self, key, value):
+        if key == "flux_calculator":
+            rc = self.L.orc_set_int(self.h, b"flux_calculator", FLUX[value])
+        elif key == "gasdynamic_update_scheme":
+            rc = self.L.orc_set_int(self.h, b"update_scheme", SCHEME[value.replace("-", "_")])
+        elif key in self.INT_KEYS:
+            rc = self.L.orc_set_int(self.h, key.encode(), int(value))
+        else:
+            rc = self.L.orc_set_double(self.h, key.encode(), float(value))
+        if rc != 0:
+            raise KeyError(key)
+
+    @property
+    def nq(self):
+        return 10 if self.mhd else 5
+
+    def add_block(self, nic, njc, nkc, dx, dy, dz, x0=0.0, y0=0.0, z0=0.0):
+        b = self.L.orc_add_block(self.h, nic, njc, nkc, dx, dy, dz, x0, y0, z0)
+        self.blocks.append((nic, njc, nkc))
+        return b
+
+    def set_bc(self, blk, face, kind, x_order=0, other_block=-1, other_face=-1, inflow=None):
+        """inflow: dict with p, T, vel=(3,), B=(3,), psi (FlowState:new{p=,T=,...})."""
+        arr = np.zeros(9)
+        if inflow is not None:
+            arr[0] = inflow["p"]
+            arr[1] = inflow["T"]
+            arr[2:5] = inflow.get("vel", (0.0, 0.0, 0.0))
+            arr[5:8] = inflow.get("B", (0.0, 0.0, 0.0))
+            arr[8] = inflow.get("psi", 0.0)
+        f = FACES[face] if isinstance(face, str) else face
+        of = FACES[other_face] if isinstance(other_face, str) else other_face
+        rc = self.L.orc_set_bc(self.h, blk, f, BC[kind], x_order, other_block, of, _p(arr))
+        if rc != 0:
+            raise ValueError("set_bc failed")
+
+    def set_flow_rhoT(self, blk, rho, vel, T, B=None, psi=None):
+        """Arrays shaped (nkc, njc, nic) (i fastest); vel (3, ...)."""
+        nic, njc, nkc = self.blocks[blk]
+        n = nic * njc * nkc
+        prim = np.zeros((9, n))
+        prim[0] = np.broadcast_to(rho, (nkc, njc, nic)).ravel()
+        for c in range(3):
+            prim[1 + c] = np.broadcast_to(vel[c], (nkc, njc, nic)).ravel()
+        prim[4] = np.broadcast_to(T, (nkc, njc, nic)).ravel()
+        if B is not None:
+            for c in range(3):
+                prim[5 + c] = np.broadcast_to(B[c], (nkc, njc, nic)).ravel()
+        if psi is not None:
+            prim[8] = np.broadcast_to(psi, (nkc, njc, nic)).ravel()
+        prim = np.ascontiguousarray(prim)
+        if self.L.orc_set_flow_rhoT(self.h, blk, _p(prim)) != 0:
+            raise ValueError("bad initial state")
+
+    def init(self):
+        self.L.orc_init(self.h)
+
+    def run(self, nsteps, max_time=0.0, fixed_dt=None):
+        rc = self.L.orc_run(self.h, int(nsteps), float(max_time), 1 if fixed_dt else 0,
+                            float(fixed_dt or 0.0))
+        return rc
+
+    def time(self):
+        out = np.zeros(5)
+        st = ctypes.c_int(0)
+        self.L.orc_get_time(self.h, _p(out), ctypes.byref(st))
+        return dict(time=out[0], dt=out[1], c_h=out[2], cfl_max=out[3], dt_allow=out[4], step=st.value)
+
+    def get_U(self, blk):
+        nic, njc, nkc = self.blocks[blk]
+        out = np.zeros((self.nq, nic * njc * nkc))
+        self.L.orc_get_U(self.h, blk, _p(out))
+        return out
+
+    def set_U(self, blk, U):
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        return self.L.orc_set_U(self.h, blk, _p(U))
+
+    def get_flow(self, blk):
+        nic, njc, nkc = self.blocks[blk]
+        out = np.zeros((12, nic * njc * nkc))
+        self.L.orc_get_flow(self.h, blk, _p(out))
+        names = ["rho", "vx", "vy", "vz", "u", "p", "T", "a", "Bx", "By", "Bz", "psi"]
+        return {k: out[q] for q, k in enumerate(names)}
+
+    def all_U(self):
+        return np.concatenate([self.get_U(b).ravel() for b in range(len(self.blocks))])
+
+    def residual(self, U):
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        R = np.zeros_like(U)
+        rc = self.L.orc_residual(self.h, _p(U), _p(R))
+        if rc != 0:
+            raise ValueError("residual failed")
+        return R
+
+    def jvp_complex(self, U, v, sigma=1.0e-30):
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        Jv = np.zeros_like(U)
+        if self.L.orc_jvp_complex(self.h, _p(U), _p(v), sigma, _p(Jv)) != 0:
+            raise ValueError("jvp failed")
+        return Jv
+
+    def jvp_real(self, U, v, sigma=0.0):
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        Jv = np.zeros_like(U)
+        used = np.zeros(1)
+        if self.L.orc_jvp_real(self.h, _p(U), _p(v), sigma, _p(Jv), _p(used)) != 0:
+            raise ValueError("jvp failed")
+        return Jv, used[0]
+
+    def face_flux(self, d, cells, length):
+        cells = np.ascontiguousarray(cells, dtype=np.float64).reshape(4, 12)
+        F = np.zeros(self.nq)
+        self.L.orc_face_flux(self.h, d, _p(cells), float(length), _p(F))
+        return F
+
+    def last_error(self):
+        buf = ctypes.create_string_buffer(512)
+        self.L.orc_last_error(self.h, buf, 512)
+        return buf.value.decode()
+
+    def __del__(self):
+        try:
+            self.L.orc_free(self.h)
+        except Exception:
+            pass

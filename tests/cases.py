@@ -1,0 +1,261 @@
+"""Seeded problem definitions shared by the parity tests, smoke() and bench.py.
+
+Each case is built identically on the CPU oracle (oracle/oracle.py) and on the
+CUDA library (gdfv.Simulation), so the two can be compared cell by cell.
+"""
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PKG = os.path.join(ROOT, "gdtk-rmhd_b200")
+if PKG not in sys.path:
+    sys.path.insert(0, PKG)
+
+R_AIR_CHICKEN = 287.1
+R_AIR_EILMER = 8.31451 / 28.96e-3   # ideal-air-gas-model.lua via species-database/air.lua
+R_HE = 8.31451 / 4.0026020e-3       # species-database/He.lua
+
+
+class Case:
+    """A problem: config, gas, blocks (dims, spacing, origin, BCs) and initial rhoT fields."""
+
+    def __init__(self, name, config, R, gamma):
+        self.name = name
+        self.config = dict(config)
+        self.R = R
+        self.gamma = gamma
+        self.blocks = []
+
+    def add_block(self, n, d, origin, bcs, rho, vel, T, B=None, psi=None):
+        self.blocks.append(dict(n=n, d=d, origin=origin, bcs=bcs, rho=rho, vel=vel, T=T, B=B, psi=psi))
+        return len(self.blocks) - 1
+
+    @property
+    def mhd(self):
+        return bool(self.config.get("MHD", False))
+
+    @property
+    def nq(self):
+        return 10 if self.mhd else 5
+
+    def total_cells(self):
+        return sum(int(np.prod(b["n"])) for b in self.blocks)
+
+
+def _noisy_rho(rng, rho, shape, amp=0.01):
+    return rho * (1.0 + amp * rng.standard_normal(shape))
+
+
+def c1_shock_box(n=32, seed=1234):
+    """32^3 cells of 1 mm, ideal air (R=287.1, gamma=1.4), ausmdv, PC, CFL 0.5;
+    x < 16 mm: p=1e5 T=300, else p=1e4 T=300; u=0; density noise 1%; extrapolate BCs."""
+    c = Case("c1", dict(flux_calculator="ausmdv"), R_AIR_CHICKEN, 1.4)
+    rng = np.random.default_rng(seed)
+    dx = 1.0e-3
+    x = (np.arange(n) + 0.5) * dx
+    p = np.where(x < 0.5 * n * dx, 1.0e5, 1.0e4)
+    T = 300.0
+    rho0 = np.broadcast_to(p / (R_AIR_CHICKEN * T), (n, n, n))
+    rho = _noisy_rho(rng, rho0, (n, n, n))
+    bcs = {f: ("outflow_simple_extrapolate", dict(x_order=0)) for f in
+           ("west", "east", "south", "north", "bottom", "top")}
+    c.add_block((n, n, n), (dx, dx, dx), (0, 0, 0), bcs, rho, (0.0, 0.0, 0.0), T)
+    return c
+
+
+def inflow_state_m3():
+    """M=3 ideal air, p=5e3 Pa, T=220 K."""
+    T = 220.0
+    a = np.sqrt(1.4 * R_AIR_CHICKEN * T)
+    return dict(p=5.0e3, T=T, vel=(3.0 * a, 0.0, 0.0))
+
+
+def c2_inflow_box(n=(256, 256, 256), flux="ausmdv", seed=4321, precision="fp64"):
+    """Single block, M=3 inflow on x-min, extrapolate outflow on x-max, slip walls
+    on y and z faces, inflow state everywhere plus 1% density noise (dx = 1 mm)."""
+    c = Case("c2", dict(flux_calculator=flux, flux_precision=precision), R_AIR_CHICKEN, 1.4)
+    rng = np.random.default_rng(seed)
+    inf = inflow_state_m3()
+    nic, njc, nkc = n
+    rho_inf = inf["p"] / (R_AIR_CHICKEN * inf["T"])
+    rho = _noisy_rho(rng, rho_inf, (nkc, njc, nic))
+    bcs = {"west": ("inflow_supersonic", dict(inflow=inf)),
+           "east": ("outflow_simple_extrapolate", dict(x_order=0)),
+           "south": ("wall_with_slip", {}), "north": ("wall_with_slip", {}),
+           "bottom": ("wall_with_slip", {}), "top": ("wall_with_slip", {})}
+    c.add_block(n, (1e-3, 1e-3, 1e-3), (0, 0, 0), bcs, rho, inf["vel"], inf["T"])
+    return c
+
+
+def multiblock_lattice(nb=(2, 2, 2), sizes=(16, 24, 32), seed=77, flux="ausmdv", precision="fp64", choices=None):
+    """Blocks on an nb lattice joined by full-face exchange; per-axis sizes drawn
+    from `sizes` by seed (chicken's lattice model: faces always match).  M=3 inflow
+    on the outer x-min faces, extrapolate on x-max, slip walls elsewhere."""
+    c = Case("multiblock", dict(flux_calculator=flux, flux_precision=precision), R_AIR_CHICKEN, 1.4)
+    rng = np.random.default_rng(seed)
+    sz = [rng.choice(sizes, nb[a]) if choices is None else np.array(choices[a]) for a in range(3)]
+    inf = inflow_state_m3()
+    rho_inf = inf["p"] / (R_AIR_CHICKEN * inf["T"])
+    dx = 1e-3
+    idx = {}
+    for bk in range(nb[2]):
+        for bj in range(nb[1]):
+            for bi in range(nb[0]):
+                idx[(bi, bj, bk)] = len(idx)
+    for bk in range(nb[2]):
+        for bj in range(nb[1]):
+            for bi in range(nb[0]):
+                n = (int(sz[0][bi]), int(sz[1][bj]), int(sz[2][bk]))
+                origin = (dx * sum(sz[0][:bi]), dx * sum(sz[1][:bj]), dx * sum(sz[2][:bk]))
+                bcs = {}
+                pos = (bi, bj, bk)
+                for a, (fm, fp) in enumerate((("west", "east"), ("south", "north"), ("bottom", "top"))):
+                    lo = list(pos); lo[a] -= 1
+                    hi = list(pos); hi[a] += 1
+                    if pos[a] > 0:
+                        bcs[fm] = ("exchange_over_full_face", dict(other=idx[tuple(lo)], other_face=fp))
+                    elif a == 0:
+                        bcs[fm] = ("inflow_supersonic", dict(inflow=inf))
+                    else:
+                        bcs[fm] = ("wall_with_slip", {})
+                    if pos[a] < nb[a] - 1:
+                        bcs[fp] = ("exchange_over_full_face", dict(other=idx[tuple(hi)], other_face=fm))
+                    elif a == 0:
+                        bcs[fp] = ("outflow_simple_extrapolate", dict(x_order=0))
+                    else:
+                        bcs[fp] = ("wall_with_slip", {})
+                rho = _noisy_rho(rng, rho_inf, (n[2], n[1], n[0]))
+                c.add_block(n, (dx, dx, dx), origin, bcs, rho, inf["vel"], inf["T"])
+    return c
+
+
+def sod_eilmer(nic=100):
+    """examples/eilmer/3D/sod-shock-tube/sg/sod.lua: 1 m x 0.1 m x 0.1 m, 100x2x2,
+    ideal air, ausmdv, slip walls everywhere (the default BC), max_time 0.6 ms."""
+    c = Case("sod", dict(flux_calculator="ausmdv"), R_AIR_EILMER, 1.4)
+    dx = 1.0 / nic
+    x = (np.arange(nic) + 0.5) * dx
+    p = np.where(x < 0.5, 1.0e5, 1.0e4)
+    T = np.where(x < 0.5, 348.4, 278.8)
+    rho = np.broadcast_to(p / (R_AIR_EILMER * T), (2, 2, nic))
+    T3 = np.broadcast_to(T, (2, 2, nic))
+    c.add_block((nic, 2, 2), (dx, 0.05, 0.05), (0, 0, 0), {}, rho, (0.0, 0.0, 0.0), T3)
+    return c
+
+
+def mhd_shock_tube(N=512):
+    """examples/eilmer/2D/MHDShockTube/MHDShockTube.lua (Dai & Woodward problem 3):
+    2D, two 256x3 blocks, hlle MHD without cleaning, stringent CFL, ideal He."""
+    c = Case("mhd_tube", dict(flux_calculator="hlle", MHD=1, divergence_cleaning=0, dimensions=2,
+                              stringent_cfl=1, cfl_value=0.5, dt_init=1e-5), R_HE, 5.0 / 3.0)
+    nic, njc = N // 2, 3
+    dx, dy = 0.5 / nic, 0.5 / 3
+    Bx = 5 / np.sqrt(4 * np.pi)
+    s4 = 1 / np.sqrt(4 * np.pi)
+    for side in (0, 1):
+        vel = (11.7106, -0.312542, -0.495260) if side == 0 else (-11.7106, 0.312542, -0.495260)
+        B = (Bx, s4, -s4) if side == 0 else (Bx, s4, s4)
+        rho, p = 1.0, 1.0
+        T = p / (rho * R_HE)
+        bcs = {"north": ("exchange_over_full_face", dict(other=side, other_face="south")),
+               "south": ("exchange_over_full_face", dict(other=side, other_face="north"))}
+        if side == 0:
+            bcs["west"] = ("outflow_simple_extrapolate", dict(x_order=1))
+            bcs["east"] = ("exchange_over_full_face", dict(other=1, other_face="west"))
+        else:
+            bcs["east"] = ("outflow_simple_extrapolate", dict(x_order=1))
+            bcs["west"] = ("exchange_over_full_face", dict(other=0, other_face="east"))
+        c.add_block((nic, njc, 1), (dx, dy, 1.0), (0.5 * side, 0, 0), bcs, rho, vel, T, B=B)
+    return c
+
+
+def orszag_tang(n=(512, 512, 4), seed=99, precision="fp64", cleaning=True):
+    """Ideal MHD Orszag-Tang vortex on [0,1]^2 x [0, 4/512], periodic on all faces,
+    gamma=5/3, rho=25/(36 pi), p=5/(12 pi), v=(-sin 2 pi y, sin 2 pi x, 0),
+    B=(-sin 2 pi y, sin 4 pi x, 0)/sqrt(4 pi), 1% density noise; hlle with GLM."""
+    R = 1.0
+    c = Case("orszag_tang", dict(flux_calculator="hlle", MHD=1, divergence_cleaning=int(cleaning),
+                                 stringent_cfl=1, flux_precision=precision, dt_init=1e-3, dt_max=1e-3),
+             R, 5.0 / 3.0)
+    nic, njc, nkc = n
+    dx, dy = 1.0 / nic, 1.0 / njc
+    dz = dx
+    rng = np.random.default_rng(seed)
+    x = (np.arange(nic) + 0.5) * dx
+    y = (np.arange(njc) + 0.5) * dy
+    X = np.broadcast_to(x[None, None, :], (nkc, njc, nic))
+    Y = np.broadcast_to(y[None, :, None], (nkc, njc, nic))
+    rho0 = 25.0 / (36.0 * np.pi)
+    p0 = 5.0 / (12.0 * np.pi)
+    rho = _noisy_rho(rng, rho0, (nkc, njc, nic))
+    T = p0 / (rho * R)
+    vel = (-np.sin(2 * np.pi * Y), np.sin(2 * np.pi * X), np.zeros_like(X))
+    B = (-np.sin(2 * np.pi * Y) / np.sqrt(4 * np.pi), np.sin(4 * np.pi * X) / np.sqrt(4 * np.pi), np.zeros_like(X))
+    bcs = {"west": ("exchange_over_full_face", dict(other=0, other_face="east")),
+           "east": ("exchange_over_full_face", dict(other=0, other_face="west")),
+           "south": ("exchange_over_full_face", dict(other=0, other_face="north")),
+           "north": ("exchange_over_full_face", dict(other=0, other_face="south")),
+           "bottom": ("exchange_over_full_face", dict(other=0, other_face="top")),
+           "top": ("exchange_over_full_face", dict(other=0, other_face="bottom"))}
+    c.add_block(n, (dx, dy, dz), (0, 0, 0), bcs, rho, vel, T, B=B)
+    return c
+
+
+# ---------------------------------------------------------------- builders
+_ORACLE_BC = {"wall_with_slip": "wall_with_slip", "outflow_simple_extrapolate": "extrapolate",
+              "inflow_supersonic": "inflow_supersonic", "exchange_over_full_face": "exchange"}
+
+
+def build_oracle(case):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import OracleSim
+    cfg = {k: v for k, v in case.config.items() if k != "flux_precision"}
+    s = OracleSim(R=case.R, gamma=case.gamma, **cfg)
+    for b in case.blocks:
+        s.add_block(*b["n"], *b["d"], *b["origin"])
+    for bi, b in enumerate(case.blocks):
+        for face, (kind, kw) in b["bcs"].items():
+            s.set_bc(bi, face, _ORACLE_BC[kind], x_order=kw.get("x_order", 0),
+                     other_block=kw.get("other", -1), other_face=kw.get("other_face", -1),
+                     inflow=kw.get("inflow"))
+        s.set_flow_rhoT(bi, b["rho"], b["vel"], b["T"], B=b["B"])
+    s.init()
+    return s
+
+
+def build_gpu(case, **extra_config):
+    import gdfv
+    cfg = gdfv.Config(**{**case.config, **extra_config})
+    sim = gdfv.Simulation(cfg, gas=gdfv.IdealGas(R=case.R, gamma=case.gamma))
+    for b in case.blocks:
+        sim.add_block(*b["n"], *b["d"], *b["origin"])
+    for bi, b in enumerate(case.blocks):
+        for face, (kind, kw) in b["bcs"].items():
+            if kind == "wall_with_slip":
+                bc = gdfv.WallBC_WithSlip()
+            elif kind == "outflow_simple_extrapolate":
+                bc = gdfv.OutFlowBC_SimpleExtrapolate(xOrder=kw.get("x_order", 0))
+            elif kind == "inflow_supersonic":
+                inf = kw["inflow"]
+                bc = gdfv.InFlowBC_Supersonic(gdfv.FlowState(p=inf["p"], T=inf["T"], velx=inf["vel"][0],
+                                                             vely=inf["vel"][1], velz=inf["vel"][2]))
+            else:
+                bc = gdfv.ExchangeBC_FullFace(kw["other"], kw["other_face"])
+            sim.set_bc(bi, face, bc)
+    sim.prepare()
+    for bi, b in enumerate(case.blocks):
+        sim.set_flow_rhoT(bi, b["rho"], b["vel"], b["T"], B=b["B"])
+    return sim
+
+
+def rel_err_per_cell(x, ref):
+    """max over cells of |x - ref| / max(|ref|, scale), scale = max |ref| of the variable
+    times 1e-3 (a floor for variables that pass through zero, e.g. momentum)."""
+    scale = np.max(np.abs(ref)) * 1e-3 + 1e-300
+    return float(np.max(np.abs(x - ref) / np.maximum(np.abs(ref), scale)))
+
+
+def rel_l2(x, ref):
+    return float(np.linalg.norm(x - ref) / (np.linalg.norm(ref) + 1e-300))

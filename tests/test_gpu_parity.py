@@ -1,0 +1,119 @@
+"""GPU parity: the CUDA path (through the C ABI) against the CPU oracle on the
+same seeded inputs.  FP64 flux: per-cell relative error <= 1e-12 after N steps
+(floor for variables through zero: 1e-3 of the variable's max).  FP32 flux:
+relative L2 error of rho, momentum and energy <= 1e-6."""
+import numpy as np
+import pytest
+
+import cases
+
+pytestmark = pytest.mark.gpu
+
+TOL_FP64 = 1.0e-12
+TOL_FP32_L2 = 1.0e-6
+
+
+def run_both(case, nsteps, **gpu_cfg):
+    orc = cases.build_oracle(case)
+    assert orc.run(nsteps) == 0, orc.last_error()
+    sim = cases.build_gpu(case, **gpu_cfg)
+    taken = sim.run(max_step=nsteps)
+    assert taken == nsteps
+    return orc, sim
+
+
+def compare_fp64(case, orc, sim):
+    to, tg = orc.time(), sim.time()
+    assert to["step"] == tg["step"]
+    assert abs(to["time"] - tg["time"]) <= TOL_FP64 * abs(to["time"])
+    assert abs(to["dt"] - tg["dt"]) <= TOL_FP64 * abs(to["dt"])
+    worst = 0.0
+    for b in range(len(case.blocks)):
+        Uo = orc.get_U(b)
+        Ug = sim.get_conserved(b)
+        for q in range(case.nq):
+            if case.mhd and q == 9:
+                continue  # divB slot: checked separately (accumulates face differences)
+            e = cases.rel_err_per_cell(Ug[q], Uo[q])
+            worst = max(worst, e)
+    return worst
+
+
+@pytest.mark.parametrize("nsteps", [1, 20])
+def test_c1_shock_box_fp64(nsteps):
+    case = cases.c1_shock_box(n=32)
+    orc, sim = run_both(case, nsteps)
+    assert compare_fp64(case, orc, sim) <= TOL_FP64
+
+
+@pytest.mark.parametrize("flux", ["ausmdv", "hllc"])
+def test_inflow_box_partial_tiles_fp64(flux):
+    # sizes that are not multiples of the 32x8 column tile or of the k chunk
+    case = cases.c2_inflow_box(n=(45, 19, 37), flux=flux)
+    orc, sim = run_both(case, 12)
+    assert compare_fp64(case, orc, sim) <= TOL_FP64
+
+
+def test_multiblock_exchange_fp64():
+    case = cases.multiblock_lattice(nb=(2, 2, 2), sizes=(16, 24, 32), seed=5)
+    orc, sim = run_both(case, 10)
+    assert compare_fp64(case, orc, sim) <= TOL_FP64
+
+
+def test_sod_reference_job():
+    """examples/eilmer/3D/sod-shock-tube/sg/sod-test.rb: 75 +/- 3 steps to 0.6 ms and the
+    post-shock probes within 1%; the GPU run also matches the oracle cell by cell."""
+    case = cases.sod_eilmer()
+    orc = cases.build_oracle(case)
+    assert orc.run(600, max_time=0.6e-3) == 0
+    sim = cases.build_gpu(case)
+    steps = sim.run(max_step=600, max_time=0.6e-3)
+    assert abs(steps - 75) < 3
+    fl = sim.get_flow(0)
+    i = 78
+    for key, ref in (("rho", 0.2647), ("p", 30.2e3), ("T", 398.0), ("vx", 293.0)):
+        assert abs(fl[key][i] - ref) / ref < 1e-2, key
+    assert compare_fp64(case, orc, sim) <= TOL_FP64
+
+
+def test_mhd_shock_tube_reference_job():
+    """examples/eilmer/2D/MHDShockTube/MHD-ShockTube-Test.rb: 880 +/- 10 steps to 0.06 and
+    region values; the GPU run matches the oracle after 200 steps."""
+    case = cases.mhd_shock_tube()
+    orc, sim = run_both(case, 200)
+    assert compare_fp64(case, orc, sim) <= TOL_FP64
+    steps = 200 + sim.run(max_step=100000, max_time=6e-2)
+    assert abs(steps - 880) < 10
+    nic = 256
+    dx = 0.5 / nic
+    for xp, blk, vy_ref, bz_ref in ((0.3, 0, -2.36600e-1, -4.00346), (0.7, 1, 2.36599e-1, 4.00346)):
+        fl = sim.get_flow(blk)
+        c = int((xp - 0.5 * blk) / dx) + nic * 1
+        assert abs(fl["p"][c] - 1.84083e2) < 1e1
+        assert abs(fl["rho"][c] - 3.90913) < 1e-1
+        assert abs(fl["vy"][c] - vy_ref) < 1e-2
+        assert abs(fl["vz"][c] - (-5.71203e-1)) < 1e-2
+        assert abs(fl["Bz"][c] * np.sqrt(4 * np.pi) - bz_ref) < 1e-1
+
+
+def test_orszag_tang_glm_fp64():
+    case = cases.orszag_tang(n=(64, 64, 4), cleaning=True)
+    orc, sim = run_both(case, 10)
+    assert compare_fp64(case, orc, sim) <= TOL_FP64
+    Ug = sim.get_conserved(0)
+    Uo = orc.get_U(0)
+    assert np.max(np.abs(Ug[9] - Uo[9])) <= 1e-10 * (np.max(np.abs(Uo[9])) + 1e-30) + 1e-14
+
+
+@pytest.mark.parametrize("flux", ["ausmdv", "hllc"])
+def test_inflow_box_fp32_flux(flux):
+    case = cases.c2_inflow_box(n=(48, 40, 36), flux=flux)
+    orc = cases.build_oracle(case)
+    assert orc.run(50) == 0
+    sim = cases.build_gpu(case, flux_precision="fp32")
+    assert sim.run(max_step=50) == 50
+    Uo, Ug = orc.get_U(0), sim.get_conserved(0)
+    rho_err = cases.rel_l2(Ug[0], Uo[0])
+    mom_err = cases.rel_l2(Ug[1:4].ravel(), Uo[1:4].ravel())
+    e_err = cases.rel_l2(Ug[4], Uo[4])
+    assert max(rho_err, mom_err, e_err) <= TOL_FP32_L2, (rho_err, mom_err, e_err)
