@@ -1,0 +1,301 @@
+#!/usr/bin/env python
+"""Benchmark of the explicit structured-grid FV update on B200.
+
+Workload (one GPU): single block 256x256x256 ideal air (R=287.1, gamma=1.4), M=3
+supersonic inflow (p=5e3 Pa, T=220 K) on x-min, extrapolate outflow on x-max, slip
+walls on y/z, 1% seeded density noise, AUSMDV flux, l2r2 van Albada, predictor-
+corrector.  A step is one full predictor-corrector step over all cells (with the
+device-resident dt rule).  `value` is Mcell-updates/s of the FP32-flux / FP64-update
+form; the plain FP64 form is timed beside it and both final states are compared
+(relative L2 of rho, momentum, energy).
+
+`--impl reference` times the reference's own CPU path: the compiled chicken solver
+(oracle/_ref/chkn-run, TVD-RK3 AUSMDV, OpenMP over blocks) when it is present,
+else the CPU oracle port (OpenMP over cells), on a bounded sample of the workload.
+
+Multi-GPU (torchrun): every rank advances its own replica of the workload (the path
+partitions into independent blocks; no collective on the data path), timed on the
+device, max over ranks; value = all cells*steps / that time.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "gdtk-rmhd_b200"))
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+METRIC = "Mcell-updates/s, FP32-flux vs FP64 plain at <=1e-6 rel L2 rho; adjoint/fwd time"
+UNIT = "Mcell-updates/s"
+BYTES_STAGE1 = 80    # read U0 (5 x 8 B), write dU0 (5 x 8 B) per cell
+BYTES_STAGE2 = 120   # read U0 and dU0, write U2 per cell
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for n, v in zip(names, s[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+def cpu_oracle_baseline(cells_target=96, steps=24):
+    """CPU oracle port (OpenMP over cells) on a bounded sample: 96^3 cells of the same workload."""
+    import cases
+    n = cells_target
+    case = cases.c2_inflow_box(n=(n, n, n))
+    orc = cases.build_oracle(case)
+    orc.run(1)  # warm
+    t0 = time.perf_counter()
+    rc = orc.run(steps)
+    dt = time.perf_counter() - t0
+    cores = len(os.sched_getaffinity(0))
+    return dict(value=n ** 3 * steps / dt / 1e6, unit=UNIT, cores=cores, kind="port",
+                sample=f"CPU oracle (restatement of the Eilmer-4 path, OpenMP over cells), {n}^3 cells of the "
+                       f"same M=3 inflow box, {steps} predictor-corrector steps, rc={rc}")
+
+
+def chicken_baseline(steps, warmup):
+    """The reference's chicken CPU build, if oracle/_ref holds it."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "chkn-run")
+    if not os.path.exists(exe):
+        return None
+    try:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import chicken_job
+    except Exception:
+        return None
+    return chicken_job.bench(exe, steps=steps, warmup=warmup)
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    res = chicken_baseline(args.steps, args.warmup)
+    if res is None:
+        base = cpu_oracle_baseline()
+        res = dict(value=base["value"], cpu_baseline=base)
+    line = {
+        "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "higher_is_better": True, "impl": "reference",
+        "cpu_baseline": res["cpu_baseline"],
+        "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "config": {"workload": "M=3 inflow box 256^3 (bounded CPU sample)", "flux_calculator": "ausmdv"},
+        "data": "synthetic",
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--size", type=int, default=256)
+    ap.add_argument("--flux", default="ausmdv", choices=["ausmdv", "hllc"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-case", action="store_true",
+                    help="small case for ncu captures: 128^3, warmup steps then exit")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+    import torch.distributed as dist
+
+    import cases
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    n = 128 if args.profile_case else args.size
+    shape = (n, n, n)
+    stream = torch.cuda.Stream()  # a capturable (non-default) stream shared with the library
+
+    def make(prec):
+        case = cases.c2_inflow_box(n=shape, flux=args.flux, precision=prec, seed=4321)
+        sim = cases.build_gpu(case)
+        sim.set_stream(stream.cuda_stream)
+        return case, sim
+
+    if args.profile_case:
+        for prec in ("fp32", "fp64"):
+            _, sim = make(prec)
+            sim.run(max_step=max(3, args.warmup))
+        torch.cuda.synchronize()
+        return 0
+
+    cells = n ** 3
+    results = {}
+    sims = {}
+    for prec in ("fp32", "fp64"):
+        case, sim = make(prec)
+        sims[prec] = (case, sim)
+        sim.run(max_step=args.warmup)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        sampler = ClockSampler(local)
+        with sampler:
+            e0.record(stream)
+            taken = sim.run(max_step=args.steps)
+            e1.record(stream)
+            torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        if world > 1:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+            dist.barrier()
+        results[prec] = dict(ms=ms, taken=taken, clocks=sampler.summary())
+
+    # accuracy of the FP32-flux form against the plain FP64 form after the same steps
+    Uf = sims["fp32"][1].get_conserved(0)
+    Ud = sims["fp64"][1].get_conserved(0)
+    err = dict(rho=cases.rel_l2(Uf[0], Ud[0]), momentum=cases.rel_l2(Uf[1:4].ravel(), Ud[1:4].ravel()),
+               energy=cases.rel_l2(Uf[4], Ud[4]))
+
+    # roofline of the dominant kernel (corrector stage) of the FP32-flux form, live
+    sim32 = sims["fp32"][1]
+    st1, st2 = sim32.time_stages(reps=10)
+    peak, peak_kind = measured_peaks()
+    ach2 = BYTES_STAGE2 * cells / (st2 * 1e-3) / 1e9
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "stage2_fp32_traffic.json")
+    if os.path.exists(tf):
+        with open(tf) as f:
+            tr = json.load(f)
+        traffic = tr.get("bytes_per_cell", 0) * cells if tr.get("bytes_per_cell") else None
+
+    # end to end through the public API: host state in, K steps, host state out
+    case32, _ = sims["fp32"]
+    _, sim_e2e = make("fp32")
+    U_host = torch.from_numpy(sim_e2e.get_conserved(0)).pin_memory()
+    U_np = U_host.numpy()
+    sim_e2e.run(max_step=args.warmup)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    sim_e2e.set_conserved(0, U_np)
+    sim_e2e.run(max_step=args.steps)
+    out = sim_e2e.get_conserved(0)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    state_bytes = U_np.nbytes
+    e2e_val = world * cells * args.steps / e2e_s / 1e6
+
+    steps = args.steps
+    val32 = world * cells * steps / (results["fp32"]["ms"] * 1e-3) / 1e6
+    val64 = world * cells * steps / (results["fp64"]["ms"] * 1e-3) / 1e6
+    line = {
+        "metric": METRIC,
+        "value": val32,
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": steps,
+        "warmup": args.warmup,
+        "ms_per_step": results["fp32"]["ms"] / steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 flux / f64 state",
+        "data": "synthetic (seeded 1% density noise)",
+        "config": {"workload": f"M=3 inflow box {n}^3, {args.flux}, l2r2 van Albada, predictor-corrector",
+                   "cells": cells, "flux_calculator": args.flux, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (state 671 MB per buffer)"},
+        "fp64_plain": {"value": val64, "ms_per_step": results["fp64"]["ms"] / steps},
+        "fp32_over_fp64": val32 / val64,
+        "rel_l2_vs_fp64": err,
+        "adjoint_over_forward": None,
+        "roofline": {"bound": "hbm", "kernel": "stage_kernel<2,float> (corrector)", "achieved": ach2,
+                     "peak": peak, "unit": "GB/s", "frac": ach2 / peak, "traffic": traffic,
+                     "peak_source": peak_kind, "algorithmic_bytes_per_cell": BYTES_STAGE2,
+                     "stage_ms": [st1, st2]},
+        "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": state_bytes / steps,
+                "d2h_bytes_per_step": (state_bytes + 64 * steps) / steps,
+                "how": "gdfv_block_set_conserved from pinned host memory, gdfv_run of all steps, "
+                       "gdfv_block_get_conserved back to host, wall clock"},
+        "gpu_launches": 4 * steps,
+        "clocks": results["fp32"]["clocks"],
+        "clocks_fp64": results["fp64"]["clocks"],
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_oracle_baseline()
+        except Exception as e:  # the baseline is reported, never required
+            line["cpu_baseline"] = {"error": str(e)}
+    if world > 1:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

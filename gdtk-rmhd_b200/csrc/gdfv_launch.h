@@ -7,6 +7,10 @@
 
 namespace gdfv {
 
+// Rows of cells per column tile (the tile is 32 x TJ columns) of each flux precision.
+constexpr int TJ_FP64 = 4;
+constexpr int TJ_FP32 = 8;
+
 // Launch one stage (0 = residual only, 1 = predictor, 2 = corrector) over A.n_tiles tiles.
 cudaError_t launch_stage_fp64(int stage, int flux, bool mhd, const StageArgs& A, cudaStream_t s);
 cudaError_t launch_stage_fp32(int stage, int flux, bool mhd, const StageArgs& A, cudaStream_t s);

@@ -427,9 +427,10 @@ int do_prepare(Context* c) {
         // tile table: TI x TJ columns, k chunks
         int kc = g.tile_kchunk > 0 ? g.tile_kchunk : std::min(hb.n[2], 32);
         if (g.dims == 2) kc = 1;
+        const int TJ = g.precision == 0 ? TJ_FP64 : TJ_FP32;
         for (int k0 = 0; k0 < hb.n[2]; k0 += kc)
             for (int j0 = 0; j0 < hb.n[1]; j0 += TJ)
-                for (int i0 = 0; i0 < hb.n[0]; i0 += TI) {
+                for (int i0 = 0; i0 < hb.n[0]; i0 += 32) {
                     TileDesc t{};
                     t.block = (int)b; t.i0 = i0; t.j0 = j0; t.k0 = k0; t.k1 = std::min(k0 + kc, hb.n[2]);
                     tiles.push_back(t);
@@ -586,7 +587,7 @@ int gdfv_config_set_int(int ctx, const char* key, long long value) {
     else if (k == "n_ghost_cell_layers") { if (v != 2) return fail(c, GDFV_ERR_ARG, "n_ghost_cell_layers must be 2"); }
     else if (k == "interpolate_in_local_frame") { if (v != 1) return fail(c, GDFV_ERR_ARG, "interpolate_in_local_frame must be true"); }
     else if (k == "dimensions") g.dims = v;
-    else if (k == "mhd") g.mhd = v != 0;
+    else if (k == "MHD" || k == "mhd") g.mhd = v != 0;
     else if (k == "divergence_cleaning") g.divergence_cleaning = v != 0;
     else if (k == "apply_limiter") g.apply_limiter = v != 0;
     else if (k == "extrema_clipping") g.extrema_clipping = v != 0;

@@ -2,30 +2,35 @@
 // l2r2 reconstruction, interface flux, residual assembly, RK stage update,
 // decode checks and the CFL signal reduction, in one pass over HBM.
 //
-// Work decomposition (2.5D blocking): a CTA owns a TI x TJ column tile of one
-// block and marches in k over [k0, k1).  Decoded cell states live in a
-// 4-plane shared-memory ring (planes k-1..k+2 for the k-faces) plus a
-// cross-shaped halo for the current plane (x/y neighbours for the i- and
-// j-faces).  Cells outside the block are synthesised by the boundary
+// Work decomposition (2.5D blocking): a CTA owns a 32 x TJ column tile of one
+// block and marches in k over [k0, k1).  Decoded cell states of the planes
+// k, k+1, k+2 sit in a 3-slot shared-memory ring of padded planes (2-cell
+// halo in i and j).  Cells outside the block are synthesised by the boundary
 // condition of the face they lie beyond (e4/bc/ghost_cell_effect/*), so no
-// ghost storage exists in HBM and the inter-block exchange is a direct read of
-// the neighbour's conserved state.
+// ghost storage exists in HBM and the inter-block exchange is a direct read
+// of the neighbour's conserved state.
+//
+// Reconstruction is done once per cell and direction: on a uniform grid the
+// van Albada limiter that e4/onedinterp.d:357-386 evaluates for the left state
+// of face c+1/2 (delLminus, del) and for the right state of face c-1/2
+// (del, delRplus) is the same expression of the same two scaled differences,
+// so one evaluation gives both interface values of cell c bit for bit.
+//
+// Per plane: phase A loads the leading plane and the current plane's halo,
+// phase B reconstructs (i and j directions through shared memory, k in
+// registers of the column's owner thread), phase C evaluates the interface
+// fluxes, phase D assembles the residual and the stage update.  The CTA has
+// 32*(TJ+1) threads: one per column plus one warp that balances phases B/C.
 //
 // Stage semantics (e4/simcore_gasdynamic_step.d:1245-1333, predictor-corrector):
 //   stage 1: dU0 = R(U0);  U1 = U0 + dt*dU0 is decoded and checked, not stored
 //   stage 2: U1 is recomputed on the fly from (U0, dU0) for every loaded cell,
 //            dU1 = R(U1);   U2 = U0 + dt*(0.5*dU0 + 0.5*dU1)  -> stored
-// giving 5 passes of the state per step.  The update arithmetic is written
-// with round-to-nearest intrinsics so that it is not contracted into FMAs.
+// giving 5 passes of the state per step.
 #pragma once
 #include "gdfv_device.cuh"
 
 namespace gdfv {
-
-constexpr int TI = 32;
-constexpr int TJ = 8;
-constexpr int NT = TI * TJ;
-constexpr int NHALO = 4 * TJ + 4 * TI;
 
 struct StageArgs {
     const BlockDesc* blocks;
@@ -44,6 +49,29 @@ struct StageArgs {
     int max_invalid_cells;
 };
 
+// Compile-time geometry of the tile and of the shared-memory layout.
+template <class R, bool MHD, int TJ_>
+struct Geo {
+    static constexpr int TI = 32, TJ = TJ_;
+    static constexpr int NCOL = TI * TJ;
+    static constexpr int NT = 32 * (TJ + 1);
+    static constexpr int PW = TI + 4, PH = TJ + 4, PLANE = PW * PH;  // padded plane
+    static constexpr int NPV = MHD ? 10 : 6;   // rho, v0, v1, v2, u, a, [B0, B1, B2, psi]
+    static constexpr int NRS = MHD ? 9 : 5;    // vn, vt1, vt2, rho, u, [Bn, Bt1, Bt2, psi]
+    static constexpr int NQ = MHD ? 10 : 5;
+    static constexpr int NRI = (TI + 2) * TJ, NRJ = TI * (TJ + 2);
+    static constexpr int NFI = (TI + 1) * TJ, NFJ = TI * (TJ + 1);
+    static constexpr int O_RING = 0;
+    static constexpr int O_RI = O_RING + 3 * NPV * PLANE;
+    static constexpr int O_RJ = O_RI + 2 * NRS * NRI;
+    static constexpr int O_FI = O_RJ + 2 * NRS * NRJ;
+    static constexpr int O_FJ = O_FI + NQ * NFI;
+    static constexpr int O_END = O_FJ + NQ * NFJ;
+    static constexpr size_t bytes = sizeof(R) * (size_t)O_END;
+    // the extra warp takes the first EXTRA items of each flat list, the column threads the rest
+    static constexpr int EXTRA = 3 * 32;
+};
+
 template <class R>
 struct CellR {
     R rho, v[3], u, a, B[3], psi;
@@ -53,57 +81,19 @@ __device__ __forceinline__ long long cell_index(const BlockDesc& B, int i, int j
     return (long long)i + (long long)B.n[0] * ((long long)j + (long long)B.n[1] * (long long)k);
 }
 
-// Read the conserved vector of one cell (stage 2: U1 = U0 + dt*dU0, psi damped) and decode it.
-template <int STAGE>
-__device__ __forceinline__ int fetch_decode(const StageArgs& A, const double* Uin, const BlockDesc& B,
-                                            long long cell, double dt, double damp, Prim<double>& s) {
-    const int nq = A.P.nq;
-    double U[10];
-    const long long g = B.offset + cell;
-#pragma unroll
-    for (int q = 0; q < 10; ++q) {
-        if (q < nq) U[q] = __ldg(Uin + (long long)q * A.total + g);
-    }
-    if (STAGE == 2) {
-#pragma unroll
-        for (int q = 0; q < 10; ++q) {
-            if (q < nq) U[q] = d_add(U[q], d_mul(dt, __ldg(A.dU0 + (long long)q * A.total + g)));
-        }
-        if (A.P.mhd && A.P.divergence_cleaning) U[PSI] = d_mul(U[PSI], damp);
-    }
-    double p, T;
-    return decode(A.P, U, s, p, T);
-}
+// Where the state of block cell (i,j,k) comes from.
+enum : int { SRC_CELL = 0, SRC_MIRROR = 1, SRC_EXTRAP1_G0 = 2, SRC_EXTRAP1_G1 = 3, SRC_INFLOW = 4 };
+struct CellSrc {
+    const BlockDesc* blk;  // block holding the source cell(s)
+    long long c0, c1;      // source cell (and the depth-1 cell for xOrder 1)
+    int kind, axis, inflow;
+};
 
-// extrapolate_copy.d:171-201 linearly_extrapolate_flowstate; fields the
-// reference leaves stale (a, psi) come from the boundary cell `edge`.
-__device__ __forceinline__ void extrapolate(const NumParams& P, const Prim<double>& f0, const Prim<double>& f1,
-                                            const Prim<double>& edge, Prim<double>& f2) {
-    f2 = edge;
-    f2.rho = 2.0 * f1.rho - f0.rho;
-    f2.u = 2.0 * f1.u - f0.u;
-#pragma unroll
-    for (int c = 0; c < 3; ++c) f2.v[c] = 2.0 * f1.v[c] - f0.v[c];
-    if (P.mhd) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) f2.B[c] = 2.0 * f1.B[c] - f0.B[c];
-    }
-}
-
-// Flow state of block cell (i,j,k); at most one index may lie outside the block,
-// in which case the boundary condition of that face supplies a ghost state.
-__device__ __forceinline__ void negate_axis(Prim<double>& s, int axis) {
-    if (axis == 0) s.v[0] = -(s.v[0]);
-    else if (axis == 1) s.v[1] = -(s.v[1]);
-    else s.v[2] = -(s.v[2]);
-}
-
-// Flow state of block cell (i,j,k); at most one index may lie outside the block,
-// in which case the boundary condition of that face supplies a ghost state.
-template <int STAGE>
-__device__ Prim<double> load_cell(const StageArgs& A, const double* Uin, int blk, int i, int j, int k,
-                                  double dt, double damp) {
-    const BlockDesc& B = A.blocks[blk];
+// At most one index may lie outside the block; the boundary condition of that
+// face supplies the ghost (e4/bc/ghost_cell_effect/*.d).
+__device__ __forceinline__ CellSrc resolve(const StageArgs& A, const BlockDesc& B, int i, int j, int k) {
+    CellSrc s;
+    s.blk = &B; s.c1 = -1; s.kind = SRC_CELL; s.axis = 0; s.inflow = 0;
     const int n0 = B.n[0], n1 = B.n[1], n2 = B.n[2];
     int axis = -1, face = 0, depth = 0;
     if (i < 0) { axis = 0; face = 0; depth = -1 - i; }
@@ -112,58 +102,140 @@ __device__ Prim<double> load_cell(const StageArgs& A, const double* Uin, int blk
     else if (j >= n1) { axis = 1; face = 3; depth = j - n1; }
     else if (k < 0) { axis = 2; face = 4; depth = -1 - k; }
     else if (k >= n2) { axis = 2; face = 5; depth = k - n2; }
-    Prim<double> s;
-    if (axis < 0) {
-        fetch_decode<STAGE>(A, Uin, B, cell_index(B, i, j, k), dt, damp, s);
-        return s;
-    }
+    if (axis < 0) { s.c0 = cell_index(B, i, j, k); return s; }
+    s.axis = axis;
     const int type = B.bc_type[face];
     const bool plus = face & 1;
-    // index of the interior cell at depth m from this face, same cross indices
+    const int nax = axis == 0 ? n0 : (axis == 1 ? n1 : n2);
     auto at_depth = [&](int m) -> long long {
-        int a = plus ? (B.n[axis] - 1 - m) : m;
+        int a = plus ? (nax - 1 - m) : m;
         return cell_index(B, axis == 0 ? a : i, axis == 1 ? a : j, axis == 2 ? a : k);
     };
     if (type == BC_SLIP_WALL) {
-        // internal_copy_then_reflect.d:111-150: mirror cell n into ghost n, negate normal velocity
-        fetch_decode<STAGE>(A, Uin, B, at_depth(depth), dt, damp, s);
-        negate_axis(s, axis);
-        if (A.P.mhd) {
-            // :140-143 dipole field written into slip-wall ghosts with |x| < 0.4136
+        s.kind = SRC_MIRROR;            // internal_copy_then_reflect.d:111-150
+        s.c0 = at_depth(depth);
+    } else if (type == BC_EXTRAPOLATE) {
+        if (B.bc_xorder[face] == 0) {   // extrapolate_copy.d:124-147
+            s.c0 = at_depth(0);
+        } else {                        // extrapolate_copy.d:148-168
+            s.kind = depth == 0 ? SRC_EXTRAP1_G0 : SRC_EXTRAP1_G1;
+            s.c0 = at_depth(0);
+            s.c1 = at_depth(1);
+        }
+    } else if (type == BC_INFLOW) {     // flow_state_copy.d:92-107
+        s.kind = SRC_INFLOW;
+        s.c0 = -1;
+        s.inflow = B.bc_inflow[face];
+    } else {                            // full_face_copy.d: partner's interior cell n from its face
+        const BlockDesc& O = A.blocks[B.bc_other[face]];
+        const int of = B.bc_other_face[face];
+        const int onax = axis == 0 ? O.n[0] : (axis == 1 ? O.n[1] : O.n[2]);
+        int a = (of & 1) ? (onax - 1 - depth) : depth;
+        s.blk = &O;
+        s.c0 = cell_index(O, axis == 0 ? a : i, axis == 1 ? a : j, axis == 2 ? a : k);
+    }
+    return s;
+}
+
+// Conserved vector of one cell: stage 2 forms U1 = U0 + dt*dU0 (psi damped).
+template <int STAGE, int NQ>
+__device__ __forceinline__ void fetch_U(const StageArgs& A, const double* Uin, const BlockDesc& B, long long c,
+                                        double dt, double damp, double* U) {
+    const long long g = B.offset + c;
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) U[q] = __ldg(Uin + (long long)q * A.total + g);
+    if (STAGE == 2) {
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) U[q] = d_add(U[q], d_mul(dt, __ldg(A.dU0 + (long long)q * A.total + g)));
+        if (NQ == 10 && A.P.divergence_cleaning) U[PSI] = d_mul(U[PSI], damp);
+    }
+}
+
+// Decode for the state loader.  FAST (FP32-flux variant): the reciprocal of rho
+// from a float estimate refined by one FP64 Newton step, and a float square root
+// for a, which the float flux arithmetic consumes anyway.
+template <bool FAST, bool MHD>
+__device__ __forceinline__ void decode_prim(const NumParams& P, const double* U, Prim<double>& s) {
+    double rho = U[MASS];
+    double dinv;
+    if (FAST) {
+        double r0 = (double)__frcp_rn((float)rho);
+        dinv = r0 * (2.0 - rho * r0);
+    } else {
+        dinv = 1.0 / rho;
+    }
+    s.rho = rho;
+    s.v[0] = U[XMOM] * dinv;
+    s.v[1] = U[YMOM] * dinv;
+    s.v[2] = U[ZMOM] * dinv;
+    double rE = U[TOTENERGY];
+    if (MHD) {
+        s.B[0] = U[XB]; s.B[1] = U[YB]; s.B[2] = U[ZB]; s.psi = U[PSI];
+        double me = 0.5 * (s.B[0] * s.B[0] + s.B[1] * s.B[1] + s.B[2] * s.B[2]);
+        rE = rE - me;
+    } else {
+        s.B[0] = s.B[1] = s.B[2] = 0.0; s.psi = 0.0;
+    }
+    double u = rE * dinv;
+    double ke = 0.5 * (s.v[0] * s.v[0] + s.v[1] * s.v[1] + s.v[2] * s.v[2]);
+    u = u - ke;
+    s.u = u;
+    double T = u * P.gas.Cvinv;
+    if (FAST) s.a = (double)sqrtf((float)(P.gas.gamma * P.gas.R * T));
+    else s.a = sqrt(P.gas.gamma * P.gas.R * T);
+}
+
+// extrapolate_copy.d:171-201 linearly_extrapolate_flowstate; fields the
+// reference leaves stale (a, psi) come from the boundary cell `edge`.
+template <bool MHD>
+__device__ __forceinline__ void extrapolate(const Prim<double>& f0, const Prim<double>& f1, const Prim<double>& edge,
+                                            Prim<double>& f2) {
+    f2 = edge;
+    f2.rho = 2.0 * f1.rho - f0.rho;
+    f2.u = 2.0 * f1.u - f0.u;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) f2.v[c] = 2.0 * f1.v[c] - f0.v[c];
+    if (MHD) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) f2.B[c] = 2.0 * f1.B[c] - f0.B[c];
+    }
+}
+
+// Finish a ghost/interior state from the decoded source cell(s).
+template <bool FAST, bool MHD>
+__device__ __forceinline__ void finish_cell(const StageArgs& A, const CellSrc& s, const double* U0, const double* U1,
+                                            int i, int j, Prim<double>& out) {
+    if (s.kind == SRC_INFLOW) {
+        const InflowState& in = A.inflow[s.inflow];
+        out.rho = in.rho; out.u = in.u; out.a = in.a; out.psi = in.psi;
+        out.v[0] = in.vel[0]; out.v[1] = in.vel[1]; out.v[2] = in.vel[2];
+        out.B[0] = in.B[0]; out.B[1] = in.B[1]; out.B[2] = in.B[2];
+        return;
+    }
+    decode_prim<FAST, MHD>(A.P, U0, out);
+    if (s.kind == SRC_MIRROR) {
+        if (s.axis == 0) out.v[0] = -(out.v[0]);
+        else if (s.axis == 1) out.v[1] = -(out.v[1]);
+        else out.v[2] = -(out.v[2]);
+        if (MHD) {
+            // internal_copy_then_reflect.d:140-143 dipole field in slip-wall ghosts with |x| < 0.4136
+            const BlockDesc& B = *s.blk;
             double x = B.x0 + ((double)i + 0.5) * B.len[0];
             double y = B.y0 + ((double)j + 0.5) * B.len[1];
             if (x > -0.4136 && x < 0.4136) {
                 double r = pow(pow(pow(x + 0., 2.0) + pow(y + 0.0, 2.0), 0.5), 5.0);
                 double cc = ((0.1) * pow(0.82 / 2, 3.0)) / (2 * r);
-                s.B[0] = -cc * (2 * pow(x + 0., 2.0) - pow(y + 0.0, 2.0));
-                s.B[1] = -cc * (3 * (x + 0.) * (y + 0.0));
+                out.B[0] = -cc * (2 * pow(x + 0., 2.0) - pow(y + 0.0, 2.0));
+                out.B[1] = -cc * (3 * (x + 0.) * (y + 0.0));
             }
         }
-    } else if (type == BC_EXTRAPOLATE) {
-        if (B.bc_xorder[face] == 0) {
-            fetch_decode<STAGE>(A, Uin, B, at_depth(0), dt, damp, s);  // extrapolate_copy.d:124-147
-        } else {
-            Prim<double> e, f1, g0;
-            fetch_decode<STAGE>(A, Uin, B, at_depth(0), dt, damp, e);
-            fetch_decode<STAGE>(A, Uin, B, at_depth(1), dt, damp, f1);
-            extrapolate(A.P, f1, e, e, g0);
-            if (depth == 0) s = g0;
-            else extrapolate(A.P, e, g0, e, s);
-        }
-    } else if (type == BC_INFLOW) {
-        const InflowState& in = A.inflow[B.bc_inflow[face]];
-        s.rho = in.rho; s.u = in.u; s.a = in.a; s.psi = in.psi;
-        s.v[0] = in.vel[0]; s.v[1] = in.vel[1]; s.v[2] = in.vel[2];
-        s.B[0] = in.B[0]; s.B[1] = in.B[1]; s.B[2] = in.B[2];
-    } else {
-        // full_face_copy.d: ghost n <- the partner block's interior cell n from its face
-        const BlockDesc& O = A.blocks[B.bc_other[face]];
-        const int of = B.bc_other_face[face];
-        int a = (of & 1) ? (O.n[axis] - 1 - depth) : depth;
-        fetch_decode<STAGE>(A, Uin, O, cell_index(O, axis == 0 ? a : i, axis == 1 ? a : j, axis == 2 ? a : k),
-                            dt, damp, s);
+    } else if (s.kind == SRC_EXTRAP1_G0 || s.kind == SRC_EXTRAP1_G1) {
+        Prim<double> e = out, f1, g0;
+        decode_prim<FAST, MHD>(A.P, U1, f1);
+        extrapolate<MHD>(f1, e, e, g0);
+        if (s.kind == SRC_EXTRAP1_G0) out = g0;
+        else extrapolate<MHD>(e, g0, e, out);
     }
-    return s;
 }
 
 template <class R, int NPV>
@@ -200,51 +272,85 @@ __device__ __forceinline__ void get_prim(const R* base, int stride, int idx, Cel
     }
 }
 
-// One interface: l2r2 reconstruction (e4/onedinterp.d:751-989, rhou, local
-// frame, EOS fallback of :44-74), then compute_interface_flux_interior
-// (e4/fluxcalc.d:54-187) for a fixed grid.  Fg receives the flux in the
-// global frame.
+// Prim-array variable of reconstructed scalar s in direction D (face-local order
+// vn, vt1, vt2, rho, u, Bn, Bt1, Bt2, psi).
+template <int D>
+__device__ __forceinline__ constexpr int prim_var(int s) {
+    return s == 0 ? 1 + D : s == 1 ? 1 + (D + 1) % 3 : s == 2 ? 1 + (D + 2) % 3 : s == 3 ? 0 : s == 4 ? 4
+         : s == 5 ? 6 + D : s == 6 ? 6 + (D + 1) % 3 : s == 7 ? 6 + (D + 2) % 3 : 9;
+}
+
+// Gather the reconstructed scalars of direction D from a prim array.
+template <class R, int NRS, int D>
+__device__ __forceinline__ void gather(const R* base, int stride, int idx, R* q) {
+#pragma unroll
+    for (int s = 0; s < NRS; ++s) q[s] = base[prim_var<D>(s) * stride + idx];
+}
+
+// One cell, one direction: both interface values of every reconstructed scalar
+// (e4/onedinterp.d:338-386 with beta = 1 and equal lengths).  qm[s]: value at
+// the cell's minus face (right state there), qp[s]: at its plus face (left state).
+// psi is reconstructed only with divergence cleaning (onedinterp.d:783-786).
+template <class R, int NRS, bool MHD>
+__device__ __forceinline__ void recon_cell(const R* w, const NumParams& P, const R* qm1, const R* q0, const R* qp1,
+                                           R* qm, R* qp) {
+    const R t = w[W_TOC];
+    const R aL0 = w[W_AL0], aR0 = w[W_AR0], len = w[W_LENL0], w3 = w[W_TWOL];
+#pragma unroll
+    for (int s = 0; s < NRS; ++s) {
+        if (MHD && s == 8 && !P.divergence_cleaning) { qm[s] = q0[s]; qp[s] = q0[s]; continue; }
+        R dm = (q0[s] - qm1[s]) * t;
+        R dp = (qp1[s] - q0[s]) * t;
+        R sl = R(1.0);
+        if (P.apply_limiter) {
+            const R eps = R(P.eps_van_albada);
+            sl = (dm * dp + rabs(dm * dp) + eps) / (dm * dm + dp * dp + eps);
+        }
+        R vp = q0[s] + sl * aL0 * (dp * w3 + dm * len);
+        R vm = q0[s] - sl * aR0 * (dp * len + dm * w3);
+        if (P.extrema_clipping) {
+            vp = clip_to_limits(vp, q0[s], qp1[s]);
+            vm = clip_to_limits(vm, qm1[s], q0[s]);
+        }
+        qp[s] = vp;
+        qm[s] = vm;
+    }
+}
+
+// Interface flux from reconstructed left/right scalars (face-local frame)
+// plus the centre states of the two adjacent cells for the EOS fallback
+// (e4/onedinterp.d:44-74) and the sound speed (the rhou update keeps it).
+// Then compute_interface_flux_interior (e4/fluxcalc.d:54-187) for a fixed grid.
+// Fg receives the flux in the global frame.
 template <class R, bool MHD, int FLUX, int D>
-__device__ __forceinline__ void face_flux(const NumParams& P, const R* w, R c_h,
-                                          const CellR<R>& c1, const CellR<R>& c0, const CellR<R>& d0,
-                                          const CellR<R>& d1, R* Fg) {
+__device__ __forceinline__ void face_flux(const NumParams& P, R c_h, const R* qL, const R* qR,
+                                          const CellR<R>& cL, const CellR<R>& cR, R* Fg) {
     constexpr int NQ = MHD ? 10 : 5;
     constexpr int ax[3] = {D, (D + 1) % 3, (D + 2) % 3};
-    FaceState<R> L, Rr;
-    R vL[3], vR[3], BL[3], BR[3];
-#pragma unroll
-    for (int m = 0; m < 3; ++m) l2r2(w, P, c1.v[ax[m]], c0.v[ax[m]], d0.v[ax[m]], d1.v[ax[m]], vL[m], vR[m]);
-    L.psi = c0.psi; Rr.psi = d0.psi;
-    if (MHD) {
-#pragma unroll
-        for (int m = 0; m < 3; ++m) l2r2(w, P, c1.B[ax[m]], c0.B[ax[m]], d0.B[ax[m]], d1.B[ax[m]], BL[m], BR[m]);
-        if (P.divergence_cleaning) l2r2(w, P, c1.psi, c0.psi, d0.psi, d1.psi, L.psi, Rr.psi);
-    }
-    R rL, rR, uL, uR;
-    l2r2(w, P, c1.rho, c0.rho, d0.rho, d1.rho, rL, rR);
-    l2r2(w, P, c1.u, c0.u, d0.u, d1.u, uL, uR);
     const R Rg = R(P.gas.R), Cvinv = R(P.gas.Cvinv);
-    // update_thermo_from_rhou, falling back to the cell-centre state on failure
-    if (uL <= R(0.0) || rL <= R(0.0)) {
-        L.rho = c0.rho; L.u = c0.u; L.p = c0.rho * Rg * (c0.u * Cvinv); L.psi = c0.psi;
+    FaceState<R> L, Rr;
+    if (qL[4] <= R(0.0) || qL[3] <= R(0.0)) {
+        L.rho = cL.rho; L.u = cL.u; L.p = cL.rho * Rg * (cL.u * Cvinv); L.psi = cL.psi;
 #pragma unroll
-        for (int m = 0; m < 3; ++m) { L.v[m] = c0.v[ax[m]]; L.B[m] = c0.B[ax[m]]; }
+        for (int m = 0; m < 3; ++m) { L.v[m] = cL.v[ax[m]]; L.B[m] = cL.B[ax[m]]; }
     } else {
-        L.rho = rL; L.u = uL; L.p = rL * Rg * (uL * Cvinv);
+        L.rho = qL[3]; L.u = qL[4]; L.p = qL[3] * Rg * (qL[4] * Cvinv);
 #pragma unroll
-        for (int m = 0; m < 3; ++m) { L.v[m] = vL[m]; L.B[m] = MHD ? BL[m] : R(0); }
+        for (int m = 0; m < 3; ++m) { L.v[m] = qL[m]; L.B[m] = MHD ? qL[5 + m] : R(0); }
+        L.psi = MHD ? qL[8] : R(0);
     }
-    if (uR <= R(0.0) || rR <= R(0.0)) {
-        Rr.rho = d0.rho; Rr.u = d0.u; Rr.p = d0.rho * Rg * (d0.u * Cvinv); Rr.psi = d0.psi;
+    if (qR[4] <= R(0.0) || qR[3] <= R(0.0)) {
+        Rr.rho = cR.rho; Rr.u = cR.u; Rr.p = cR.rho * Rg * (cR.u * Cvinv); Rr.psi = cR.psi;
 #pragma unroll
-        for (int m = 0; m < 3; ++m) { Rr.v[m] = d0.v[ax[m]]; Rr.B[m] = d0.B[ax[m]]; }
+        for (int m = 0; m < 3; ++m) { Rr.v[m] = cR.v[ax[m]]; Rr.B[m] = cR.B[ax[m]]; }
     } else {
-        Rr.rho = rR; Rr.u = uR; Rr.p = rR * Rg * (uR * Cvinv);
+        Rr.rho = qR[3]; Rr.u = qR[4]; Rr.p = qR[3] * Rg * (qR[4] * Cvinv);
 #pragma unroll
-        for (int m = 0; m < 3; ++m) { Rr.v[m] = vR[m]; Rr.B[m] = MHD ? BR[m] : R(0); }
+        for (int m = 0; m < 3; ++m) { Rr.v[m] = qR[m]; Rr.B[m] = MHD ? qR[5 + m] : R(0); }
+        Rr.psi = MHD ? qR[8] : R(0);
     }
-    L.a = c0.a;   // the rhou update leaves the cell-centre sound speed in place
-    Rr.a = d0.a;
+    L.a = cL.a;
+    Rr.a = cR.a;
     R F[NQ];
     if (FLUX == FLUX_AUSMDV) ausmdv(P, L, Rr, F);
     else if (FLUX == FLUX_HLLC) hllc(P, L, Rr, F);
@@ -274,38 +380,56 @@ __device__ __forceinline__ void face_flux(const NumParams& P, const R* w, R c_h,
     }
 }
 
-template <class R, bool MHD>
-struct StageSmem {
-    static constexpr int NPV = MHD ? 10 : 6;
-    static constexpr int NQ = MHD ? 10 : 5;
-    static constexpr int NFI = (TI + 1) * TJ;
-    static constexpr int NFJ = TI * (TJ + 1);
-    static constexpr size_t bytes = sizeof(R) * (size_t)(4 * NPV * NT + NPV * NHALO + NQ * NFI + NQ * NFJ);
-};
+// Load the state of up to two cells per thread: resolve, issue every global
+// load, then decode (keeps the loads in flight together).
+template <int STAGE, bool FAST, bool MHD, int NQ>
+__device__ __forceinline__ void load_pair(const StageArgs& A, const double* Uin, const BlockDesc& B, double dt,
+                                          double damp, int n, const int* ci, const int* cj, const int* ck,
+                                          Prim<double>* out) {
+    CellSrc s[2];
+    double U0[2][NQ], U1[2][NQ];
+#pragma unroll
+    for (int m = 0; m < 2; ++m) {
+        if (m < n) {
+            s[m] = resolve(A, B, ci[m], cj[m], ck[m]);
+            if (s[m].kind != SRC_INFLOW) fetch_U<STAGE, NQ>(A, Uin, *s[m].blk, s[m].c0, dt, damp, U0[m]);
+            if (s[m].c1 >= 0) fetch_U<STAGE, NQ>(A, Uin, *s[m].blk, s[m].c1, dt, damp, U1[m]);
+        }
+    }
+#pragma unroll
+    for (int m = 0; m < 2; ++m) {
+        if (m < n) finish_cell<FAST, MHD>(A, s[m], U0[m], U1[m], ci[m], cj[m], out[m]);
+    }
+}
 
 // STAGE 0: residual only (R_out = dUdt of U_in).  STAGE 1/2: predictor / corrector.
-template <int STAGE, class R, bool MHD, int FLUX>
-__global__ void __launch_bounds__(NT, MHD ? 1 : 2) stage_kernel(StageArgs A) {
-    using SM = StageSmem<R, MHD>;
-    constexpr int NPV = SM::NPV;
-    constexpr int NQ = SM::NQ;
+template <int STAGE, class R, bool MHD, int FLUX, int TJ>
+__global__ void __launch_bounds__(32 * (TJ + 1), (sizeof(R) == 4 && !MHD) ? 2 : 1) stage_kernel(StageArgs A) {
+    using G = Geo<R, MHD, TJ>;
+    constexpr int TI = G::TI, NT = G::NT, NCOL = G::NCOL, PW = G::PW, PLANE = G::PLANE;
+    constexpr int NPV = G::NPV, NRS = G::NRS, NQ = G::NQ;
+    constexpr int NRI = G::NRI, NRJ = G::NRJ, NFI = G::NFI, NFJ = G::NFJ;
+    constexpr bool FAST = sizeof(R) == 4;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    R* ring = reinterpret_cast<R*>(smem_raw);        // [4][NPV][NT]
-    R* halo = ring + 4 * NPV * NT;                    // [NPV][NHALO]
-    R* fI = halo + NPV * NHALO;                       // [NQ][NFI]
-    R* fJ = fI + NQ * SM::NFI;                        // [NQ][NFJ]
+    R* sm = reinterpret_cast<R*>(smem_raw);
+    R* ring = sm + G::O_RING;   // [3][NPV][PLANE]
+    R* RI = sm + G::O_RI;       // [2*NRS][NRI]  (q-, q+) per cell, i direction, cells -1..TI
+    R* RJ = sm + G::O_RJ;       // [2*NRS][NRJ]  j direction, rows -1..TJ
+    R* FI = sm + G::O_FI;       // [NQ][NFI]
+    R* FJ = sm + G::O_FJ;       // [NQ][NFJ]
     __shared__ double s_red[NT / 32];
+    __shared__ R w[3][W_N];
 
     const Control* ctl = A.ctl;
     int parity = 0;
-    double dt = 0.0, c_h = 0.0;
+    double dt = 0.0;
     if (STAGE != 0) {
         if (ctl->halted || ctl->status != ST_OK) return;
         if (STAGE == 2 && (ctl->n_fail > 0 || ctl->n_invalid1 > A.max_invalid_cells)) return;
         parity = ctl->step & 1;
         dt = ctl->dt_global;
     }
-    c_h = ctl->c_h;
+    const double c_h = ctl->c_h;
     const double* Uin = (STAGE == 0) ? A.U_in : A.Ubuf[parity];
     double* Uout = A.Ubuf[parity ^ 1];
     double damp = 1.0;
@@ -319,130 +443,205 @@ __global__ void __launch_bounds__(NT, MHD ? 1 : 2) stage_kernel(StageArgs A) {
     const TileDesc t = A.tiles[blockIdx.x];
     const int blk = t.block;
     const BlockDesc& B = A.blocks[blk];
+    const NumParams& P = A.P;
     const int ni_t = min(TI, B.n[0] - t.i0);
     const int nj_t = min(TJ, B.n[1] - t.j0);
     const int tid = threadIdx.x;
+    const bool owner = tid < NCOL;                 // owns column (ti, tj)
     const int ti = tid % TI, tj = tid / TI;
-    const bool active = (ti < ni_t) && (tj < nj_t);
-    const bool has_k = (A.P.dims == 3);
-    const NumParams& P = A.P;
-
-    // reconstruction weights of this block, shared by the CTA (kept out of registers)
-    __shared__ R w[3][W_N];
+    const bool active = owner && ti < ni_t && tj < nj_t;
+    const int pidx = (ti + 2) + PW * (tj + 2);     // own cell in a padded plane
+    const bool has_k = (P.dims == 3);
     if (tid < 3 * W_N) w[tid / W_N][tid % W_N] = (R)B.w[tid / W_N][tid % W_N];
     const R c_hR = (R)c_h;
+    __syncthreads();
 
-    // Prologue: interior states of planes k0-2 .. k0+1.
-    const int kfirst = has_k ? t.k0 - 2 : t.k0;
-    const int klast = has_k ? t.k0 + 2 : t.k0 + 1;
-    if (active) {
-        for (int kk = kfirst; kk < klast; ++kk) {
-            Prim<double> s = load_cell<STAGE>(A, Uin, blk, t.i0 + ti, t.j0 + tj, kk, dt, damp);
-            put_prim<R, NPV>(ring + (kk & 3) * NPV * NT, NT, tid, s);
-        }
-    }
-    R fB[NQ];
+    auto slot = [&](int kk) -> R* { return ring + (((kk % 3) + 3) % 3) * NPV * PLANE; };
+
+    R kq_prev_p[NRS];        // k-direction q+ of the current plane (left state of its top face)
+    R fB[NQ];                // flux through the bottom face of the owner's cell
 #pragma unroll
     for (int q = 0; q < NQ; ++q) fB[q] = R(0);
-    __syncthreads();
-    if (active && has_k) {
-        CellR<R> c[4];
 #pragma unroll
-        for (int m = 0; m < 4; ++m) get_prim<R, NPV>(ring + ((t.k0 - 2 + m) & 3) * NPV * NT, NT, tid, c[m]);
-        face_flux<R, MHD, FLUX, 2>(P, w[2], c_hR, c[0], c[1], c[2], c[3], fB);
+    for (int s = 0; s < NRS; ++s) kq_prev_p[s] = R(0);
+
+    // ---------------- prologue: planes k0-2 .. k0+1 (k0 only in 2D)
+    if (has_k) {
+        int ci[2] = {t.i0 + ti, t.i0 + ti}, cj[2] = {t.j0 + tj, t.j0 + tj};
+        if (active) {
+            Prim<double> pr[2];
+            int ck[2] = {t.k0 - 2, t.k0 - 1};
+            load_pair<STAGE, FAST, MHD, NQ>(A, Uin, B, dt, damp, 2, ci, cj, ck, pr);
+            put_prim<R, NPV>(slot(t.k0 - 2), PLANE, pidx, pr[0]);
+            put_prim<R, NPV>(slot(t.k0 - 1), PLANE, pidx, pr[1]);
+            int ck2[2] = {t.k0, 0};
+            load_pair<STAGE, FAST, MHD, NQ>(A, Uin, B, dt, damp, 1, ci, cj, ck2, pr);
+            put_prim<R, NPV>(slot(t.k0), PLANE, pidx, pr[0]);
+            // q+ of plane k0-1 (left state of face k0-1/2); own column only
+            R qm1[NRS], q0[NRS], qp1[NRS], qm[NRS];
+            gather<R, NRS, 2>(slot(t.k0 - 2), PLANE, pidx, qm1);
+            gather<R, NRS, 2>(slot(t.k0 - 1), PLANE, pidx, q0);
+            gather<R, NRS, 2>(slot(t.k0), PLANE, pidx, qp1);
+            recon_cell<R, NRS, MHD>(w[2], P, qm1, q0, qp1, qm, kq_prev_p);
+            // plane k0+1 replaces k0-2 in the ring
+            int ck3[2] = {t.k0 + 1, 0};
+            load_pair<STAGE, FAST, MHD, NQ>(A, Uin, B, dt, damp, 1, ci, cj, ck3, pr);
+            put_prim<R, NPV>(slot(t.k0 + 1), PLANE, pidx, pr[0]);
+            R qkm[NRS], qkp[NRS];
+            gather<R, NRS, 2>(slot(t.k0 - 1), PLANE, pidx, qm1);
+            gather<R, NRS, 2>(slot(t.k0), PLANE, pidx, q0);
+            gather<R, NRS, 2>(slot(t.k0 + 1), PLANE, pidx, qp1);
+            recon_cell<R, NRS, MHD>(w[2], P, qm1, q0, qp1, qkm, qkp);
+            CellR<R> cL, cR;
+            get_prim<R, NPV>(slot(t.k0 - 1), PLANE, pidx, cL);
+            get_prim<R, NPV>(slot(t.k0), PLANE, pidx, cR);
+            face_flux<R, MHD, FLUX, 2>(P, c_hR, kq_prev_p, qkm, cL, cR, fB);
+#pragma unroll
+            for (int s = 0; s < NRS; ++s) kq_prev_p[s] = qkp[s];
+        }
+    } else {
+        if (active) {
+            int ci[2] = {t.i0 + ti, 0}, cj[2] = {t.j0 + tj, 0}, ck[2] = {t.k0, 0};
+            Prim<double> pr[2];
+            load_pair<STAGE, FAST, MHD, NQ>(A, Uin, B, dt, damp, 1, ci, cj, ck, pr);
+            put_prim<R, NPV>(slot(t.k0), PLANE, pidx, pr[0]);
+        }
     }
-    __syncthreads();
 
     double sig_max = 0.0;
     const double Ai = B.area[0], Aj = B.area[1], Ak = B.area[2];
-    const int nfi = (ni_t + 1) * nj_t;
-    const int nfj = ni_t * (nj_t + 1);
     const int nh = 4 * nj_t + 4 * ni_t;
+    const int f0 = owner ? G::EXTRA + tid : tid - NCOL;   // flat-list start and stride
+    const int fstride = owner ? NCOL : 32;
+    const int fend = owner ? 0x7fffffff : G::EXTRA;
 
     for (int k = t.k0; k < t.k1; ++k) {
-        // leading plane (k+2) interior and the halo of the current plane k
-        if (active && has_k) {
-            Prim<double> s = load_cell<STAGE>(A, Uin, blk, t.i0 + ti, t.j0 + tj, k + 2, dt, damp);
-            put_prim<R, NPV>(ring + ((k + 2) & 3) * NPV * NT, NT, tid, s);
-        }
-        for (int h = tid; h < nh; h += NT) {
-            int hi, hj;
-            if (h < 4 * nj_t) {
-                int side = h / (2 * nj_t), rem = h % (2 * nj_t);
-                int col = rem / nj_t, row = rem % nj_t;
-                hi = side == 0 ? col - 2 : ni_t + col;
-                hj = row;
-            } else {
-                int h2 = h - 4 * nj_t;
-                int side = h2 / (2 * ni_t), rem = h2 % (2 * ni_t);
-                int row = rem / ni_t, col = rem % ni_t;
-                hj = side == 0 ? row - 2 : nj_t + row;
-                hi = col;
+        R* cur = slot(k);
+        // ---------------- phase A: leading plane k+2 (owners) and the halo of plane k
+        {
+            int ci[2], cj[2], ck[2], dst[2];
+            R* dplane[2];
+            int n = 0;
+            if (active && has_k) {
+                ci[n] = t.i0 + ti; cj[n] = t.j0 + tj; ck[n] = k + 2; dst[n] = pidx; dplane[n] = slot(k + 2); ++n;
             }
-            Prim<double> s = load_cell<STAGE>(A, Uin, blk, t.i0 + hi, t.j0 + hj, k, dt, damp);
-            put_prim<R, NPV>(halo, NHALO, h, s);
+            const int h = owner ? tid + 32 : tid - NCOL;   // the extra warp takes halo items 0..31
+            if (h < nh) {
+                int hi, hj;
+                if (h < 4 * nj_t) {
+                    int side = h / (2 * nj_t), rem = h % (2 * nj_t);
+                    int col = rem / nj_t, row = rem % nj_t;
+                    hi = side == 0 ? col - 2 : ni_t + col;
+                    hj = row;
+                } else {
+                    int h2 = h - 4 * nj_t;
+                    int side = h2 / (2 * ni_t), rem = h2 % (2 * ni_t);
+                    int row = rem / ni_t, col = rem % ni_t;
+                    hj = side == 0 ? row - 2 : nj_t + row;
+                    hi = col;
+                }
+                ci[n] = t.i0 + hi; cj[n] = t.j0 + hj; ck[n] = k; dst[n] = (hi + 2) + PW * (hj + 2); dplane[n] = cur; ++n;
+            }
+            if (n > 0) {
+                Prim<double> pr[2];
+                load_pair<STAGE, FAST, MHD, NQ>(A, Uin, B, dt, damp, n, ci, cj, ck, pr);
+                put_prim<R, NPV>(dplane[0], PLANE, dst[0], pr[0]);
+                if (n > 1) put_prim<R, NPV>(dplane[1], PLANE, dst[1], pr[1]);
+            }
         }
         __syncthreads();
 
-        const R* plane = ring + (k & 3) * NPV * NT;
-        auto cell_at = [&](int ci, int cj, CellR<R>& c) {
-            if (ci >= 0 && ci < ni_t && cj >= 0 && cj < nj_t) {
-                get_prim<R, NPV>(plane, NT, ci + TI * cj, c);
-            } else if (ci < 0 || ci >= ni_t) {
-                int side = ci < 0 ? 0 : 1;
-                int col = side == 0 ? ci + 2 : ci - ni_t;
-                get_prim<R, NPV>(halo, NHALO, side * 2 * nj_t + col * nj_t + cj, c);
+        // ---------------- phase B: reconstruction
+        R kq_m[NRS], kq_p[NRS];
+        if (active && has_k) {
+            R qm1[NRS], q0[NRS], qp1[NRS];
+            gather<R, NRS, 2>(cur, PLANE, pidx, qm1);
+            gather<R, NRS, 2>(slot(k + 1), PLANE, pidx, q0);
+            gather<R, NRS, 2>(slot(k + 2), PLANE, pidx, qp1);
+            recon_cell<R, NRS, MHD>(w[2], P, qm1, q0, qp1, kq_m, kq_p);
+        }
+        for (int f = f0; f < NRI + NRJ && f < fend; f += fstride) {
+            R qm1[NRS], q0[NRS], qp1[NRS], qm[NRS], qp[NRS];
+            if (f < NRI) {
+                const int row = f / (TI + 2), ci = f % (TI + 2) - 1;   // cells -1..TI
+                if (row >= nj_t || ci > ni_t) continue;
+                const int p = (ci + 2) + PW * (row + 2);
+                gather<R, NRS, 0>(cur, PLANE, p - 1, qm1);
+                gather<R, NRS, 0>(cur, PLANE, p, q0);
+                gather<R, NRS, 0>(cur, PLANE, p + 1, qp1);
+                recon_cell<R, NRS, MHD>(w[0], P, qm1, q0, qp1, qm, qp);
+#pragma unroll
+                for (int s = 0; s < NRS; ++s) { RI[s * NRI + f] = qm[s]; RI[(NRS + s) * NRI + f] = qp[s]; }
             } else {
-                int side = cj < 0 ? 0 : 1;
-                int row = side == 0 ? cj + 2 : cj - nj_t;
-                get_prim<R, NPV>(halo, NHALO, 4 * nj_t + side * 2 * ni_t + row * ni_t + ci, c);
+                const int g = f - NRI;
+                const int cj = g / TI - 1, col = g % TI;               // rows -1..TJ
+                if (col >= ni_t || cj > nj_t) continue;
+                const int p = (col + 2) + PW * (cj + 2);
+                gather<R, NRS, 1>(cur, PLANE, p - PW, qm1);
+                gather<R, NRS, 1>(cur, PLANE, p, q0);
+                gather<R, NRS, 1>(cur, PLANE, p + PW, qp1);
+                recon_cell<R, NRS, MHD>(w[1], P, qm1, q0, qp1, qm, qp);
+#pragma unroll
+                for (int s = 0; s < NRS; ++s) { RJ[s * NRJ + g] = qm[s]; RJ[(NRS + s) * NRJ + g] = qp[s]; }
             }
-        };
+        }
+        __syncthreads();
 
+        // ---------------- phase C: interface fluxes
         R fT[NQ];
 #pragma unroll
         for (int q = 0; q < NQ; ++q) fT[q] = R(0);
         if (active && has_k) {
-            CellR<R> c[4];
+            CellR<R> cL, cR;
+            get_prim<R, NPV>(cur, PLANE, pidx, cL);
+            get_prim<R, NPV>(slot(k + 1), PLANE, pidx, cR);
+            face_flux<R, MHD, FLUX, 2>(P, c_hR, kq_prev_p, kq_m, cL, cR, fT);
 #pragma unroll
-            for (int m = 0; m < 4; ++m) get_prim<R, NPV>(ring + ((k - 1 + m) & 3) * NPV * NT, NT, tid, c[m]);
-            face_flux<R, MHD, FLUX, 2>(P, w[2], c_hR, c[0], c[1], c[2], c[3], fT);
+            for (int s = 0; s < NRS; ++s) kq_prev_p[s] = kq_p[s];
         }
-        for (int f = tid; f < nfi + nfj; f += NT) {
-            CellR<R> c[4];
-            R F[NQ];
-            if (f < nfi) {
-                int row = f / (ni_t + 1), fi = f % (ni_t + 1);
+        for (int f = f0; f < NFI + NFJ && f < fend; f += fstride) {
+            R qL[NRS], qR[NRS], F[NQ];
+            CellR<R> cL, cR;
+            if (f < NFI) {
+                const int row = f / (TI + 1), fi = f % (TI + 1);       // faces 0..TI
+                if (row >= nj_t || fi > ni_t) continue;
+                const int rl = fi + (TI + 2) * row;                    // RI index of cell fi-1
 #pragma unroll
-                for (int m = 0; m < 4; ++m) cell_at(fi - 2 + m, row, c[m]);
-                face_flux<R, MHD, FLUX, 0>(P, w[0], c_hR, c[0], c[1], c[2], c[3], F);
-                const int idx = fi + (TI + 1) * row;
+                for (int s = 0; s < NRS; ++s) { qL[s] = RI[(NRS + s) * NRI + rl]; qR[s] = RI[s * NRI + rl + 1]; }
+                const int p = (fi + 2) + PW * (row + 2);
+                get_prim<R, NPV>(cur, PLANE, p - 1, cL);
+                get_prim<R, NPV>(cur, PLANE, p, cR);
+                face_flux<R, MHD, FLUX, 0>(P, c_hR, qL, qR, cL, cR, F);
 #pragma unroll
-                for (int q = 0; q < NQ; ++q) fI[q * SM::NFI + idx] = F[q];
+                for (int q = 0; q < NQ; ++q) FI[q * NFI + f] = F[q];
             } else {
-                int f2 = f - nfi;
-                int fj = f2 / ni_t, col = f2 % ni_t;
+                const int g = f - NFI;
+                const int fj = g / TI, col = g % TI;                   // faces 0..TJ
+                if (col >= ni_t || fj > nj_t) continue;
+                const int rl = col + TI * fj;                          // RJ index of row fj-1
 #pragma unroll
-                for (int m = 0; m < 4; ++m) cell_at(col, fj - 2 + m, c[m]);
-                face_flux<R, MHD, FLUX, 1>(P, w[1], c_hR, c[0], c[1], c[2], c[3], F);
-                const int idx = col + TI * fj;
+                for (int s = 0; s < NRS; ++s) { qL[s] = RJ[(NRS + s) * NRJ + rl]; qR[s] = RJ[s * NRJ + rl + TI]; }
+                const int p = (col + 2) + PW * (fj + 2);
+                get_prim<R, NPV>(cur, PLANE, p - PW, cL);
+                get_prim<R, NPV>(cur, PLANE, p, cR);
+                face_flux<R, MHD, FLUX, 1>(P, c_hR, qL, qR, cL, cR, F);
 #pragma unroll
-                for (int q = 0; q < NQ; ++q) fJ[q * SM::NFJ + idx] = F[q];
+                for (int q = 0; q < NQ; ++q) FJ[q * NFJ + g] = F[q];
             }
         }
         __syncthreads();
 
+        // ---------------- phase D: residual (e4/fvcell.d:824-856, faces W, E, S, N, B, T) and update
         if (active) {
-            // e4/fvcell.d:824-856 time_derivatives: faces W, E, S, N, B, T
             const long long cell = cell_index(B, t.i0 + ti, t.j0 + tj, k);
             const long long g = B.offset + cell;
             double dU[NQ];
 #pragma unroll
             for (int q = 0; q < NQ; ++q) {
-                double FW = (double)fI[q * SM::NFI + ti + (TI + 1) * tj];
-                double FE = (double)fI[q * SM::NFI + ti + 1 + (TI + 1) * tj];
-                double FS = (double)fJ[q * SM::NFJ + ti + TI * tj];
-                double FN = (double)fJ[q * SM::NFJ + ti + TI * (tj + 1)];
+                double FW = (double)FI[q * NFI + ti + (TI + 1) * tj];
+                double FE = (double)FI[q * NFI + ti + 1 + (TI + 1) * tj];
+                double FS = (double)FJ[q * NFJ + ti + TI * tj];
+                double FN = (double)FJ[q * NFJ + ti + TI * (tj + 1)];
                 double si = 0.0;
                 si = __dsub_rn(si, d_mul(FW, -Ai));
                 si = __dsub_rn(si, d_mul(FE, Ai));
@@ -460,7 +659,7 @@ __global__ void __launch_bounds__(NT, MHD ? 1 : 2) stage_kernel(StageArgs A) {
             } else {
                 double U[10];
 #pragma unroll
-                for (int q = 0; q < NQ; ++q) U[q] = Uin[(long long)q * A.total + g];
+                for (int q = 0; q < NQ; ++q) U[q] = __ldg(Uin + (long long)q * A.total + g);
                 if (STAGE == 1) {
 #pragma unroll
                     for (int q = 0; q < NQ; ++q) {
@@ -470,7 +669,7 @@ __global__ void __launch_bounds__(NT, MHD ? 1 : 2) stage_kernel(StageArgs A) {
                 } else {
 #pragma unroll
                     for (int q = 0; q < NQ; ++q) {
-                        double d0 = A.dU0[(long long)q * A.total + g];
+                        double d0 = __ldg(A.dU0 + (long long)q * A.total + g);
                         U[q] = d_add(U[q], d_mul(dt, d_add(d_mul(0.5, d0), d_mul(0.5, dU[q]))));
                     }
                 }
@@ -498,7 +697,6 @@ __global__ void __launch_bounds__(NT, MHD ? 1 : 2) stage_kernel(StageArgs A) {
         }
 #pragma unroll
         for (int q = 0; q < NQ; ++q) fB[q] = fT[q];
-        __syncthreads();
     }
 
     if (STAGE == 2) {

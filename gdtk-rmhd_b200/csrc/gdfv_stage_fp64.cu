@@ -7,19 +7,20 @@ namespace gdfv {
 
 namespace {
 using Real = double;
+constexpr int TJ = TJ_FP64;
 
 template <int STAGE, bool MHD, int FLUX>
 cudaError_t launch_one(const StageArgs& A, cudaStream_t s) {
-    const size_t smem = StageSmem<Real, MHD>::bytes;
-    stage_kernel<STAGE, Real, MHD, FLUX><<<A.n_tiles, NT, smem, s>>>(A);
+    using G = Geo<Real, MHD, TJ>;
+    stage_kernel<STAGE, Real, MHD, FLUX, TJ><<<A.n_tiles, G::NT, G::bytes, s>>>(A);
     return cudaGetLastError();
 }
 
 template <int STAGE, bool MHD, int FLUX>
 cudaError_t configure_one() {
-    return cudaFuncSetAttribute(stage_kernel<STAGE, Real, MHD, FLUX>,
+    return cudaFuncSetAttribute(stage_kernel<STAGE, Real, MHD, FLUX, TJ>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)StageSmem<Real, MHD>::bytes);
+                                (int)Geo<Real, MHD, TJ>::bytes);
 }
 
 template <int STAGE>

@@ -250,11 +250,46 @@ def build_gpu(case, **extra_config):
     return sim
 
 
+def build_pair(case, **extra_config):
+    """Oracle and GPU simulation started from the same conserved state: the oracle
+    encodes the rhoT initial state (e4/fvcell.d:511-583), both sides then decode
+    that U0, so the comparison starts from identical inputs."""
+    orc = build_oracle(case)
+    sim = build_gpu(case, **extra_config)
+    for b in range(len(case.blocks)):
+        U0 = orc.get_U(b)
+        assert orc.set_U(b, U0) == 0
+        sim.set_conserved(b, U0)
+    return orc, sim
+
+
 def rel_err_per_cell(x, ref):
     """max over cells of |x - ref| / max(|ref|, scale), scale = max |ref| of the variable
     times 1e-3 (a floor for variables that pass through zero, e.g. momentum)."""
     scale = np.max(np.abs(ref)) * 1e-3 + 1e-300
     return float(np.max(np.abs(x - ref) / np.maximum(np.abs(ref), scale)))
+
+
+def cell_errors(U, Uref, mhd):
+    """Per-cell relative errors of the conserved vector, by group:
+    mass and total energy per cell; momentum and B as vectors per cell (|dm|/|m|),
+    with a floor of 1e-3 of the field maximum of the group's magnitude for cells
+    where it passes through zero; psi likewise.  Returns {group: max over cells}."""
+    out = {}
+
+    def vec(a, b):
+        d = np.sqrt(np.sum((a - b) ** 2, axis=0))
+        m = np.sqrt(np.sum(b ** 2, axis=0))
+        floor = 1e-3 * np.max(m) + 1e-300
+        return float(np.max(d / np.maximum(m, floor)))
+
+    out["mass"] = float(np.max(np.abs(U[0] - Uref[0]) / np.abs(Uref[0])))
+    out["momentum"] = vec(U[1:4], Uref[1:4])
+    out["energy"] = float(np.max(np.abs(U[4] - Uref[4]) / np.abs(Uref[4])))
+    if mhd:
+        out["B"] = vec(U[5:8], Uref[5:8])
+        out["psi"] = vec(U[8:9], Uref[8:9])
+    return out
 
 
 def rel_l2(x, ref):

@@ -1,6 +1,7 @@
 """GPU parity: the CUDA path (through the C ABI) against the CPU oracle on the
 same seeded inputs.  FP64 flux: per-cell relative error <= 1e-12 after N steps
-(floor for variables through zero: 1e-3 of the variable's max).  FP32 flux:
+(cases.cell_errors: mass and energy per cell, momentum and B as per-cell vectors,
+floor 1e-3 of the field maximum where a group passes through zero).  FP32 flux:
 relative L2 error of rho, momentum and energy <= 1e-6."""
 import numpy as np
 import pytest
@@ -14,9 +15,8 @@ TOL_FP32_L2 = 1.0e-6
 
 
 def run_both(case, nsteps, **gpu_cfg):
-    orc = cases.build_oracle(case)
+    orc, sim = cases.build_pair(case, **gpu_cfg)
     assert orc.run(nsteps) == 0, orc.last_error()
-    sim = cases.build_gpu(case, **gpu_cfg)
     taken = sim.run(max_step=nsteps)
     assert taken == nsteps
     return orc, sim
@@ -29,13 +29,8 @@ def compare_fp64(case, orc, sim):
     assert abs(to["dt"] - tg["dt"]) <= TOL_FP64 * abs(to["dt"])
     worst = 0.0
     for b in range(len(case.blocks)):
-        Uo = orc.get_U(b)
-        Ug = sim.get_conserved(b)
-        for q in range(case.nq):
-            if case.mhd and q == 9:
-                continue  # divB slot: checked separately (accumulates face differences)
-            e = cases.rel_err_per_cell(Ug[q], Uo[q])
-            worst = max(worst, e)
+        errs = cases.cell_errors(sim.get_conserved(b), orc.get_U(b), case.mhd)
+        worst = max(worst, max(errs.values()))
     return worst
 
 
@@ -64,9 +59,8 @@ def test_sod_reference_job():
     """examples/eilmer/3D/sod-shock-tube/sg/sod-test.rb: 75 +/- 3 steps to 0.6 ms and the
     post-shock probes within 1%; the GPU run also matches the oracle cell by cell."""
     case = cases.sod_eilmer()
-    orc = cases.build_oracle(case)
+    orc, sim = cases.build_pair(case)
     assert orc.run(600, max_time=0.6e-3) == 0
-    sim = cases.build_gpu(case)
     steps = sim.run(max_step=600, max_time=0.6e-3)
     assert abs(steps - 75) < 3
     fl = sim.get_flow(0)
@@ -108,9 +102,8 @@ def test_orszag_tang_glm_fp64():
 @pytest.mark.parametrize("flux", ["ausmdv", "hllc"])
 def test_inflow_box_fp32_flux(flux):
     case = cases.c2_inflow_box(n=(48, 40, 36), flux=flux)
-    orc = cases.build_oracle(case)
+    orc, sim = cases.build_pair(case, flux_precision="fp32")
     assert orc.run(50) == 0
-    sim = cases.build_gpu(case, flux_precision="fp32")
     assert sim.run(max_step=50) == 50
     Uo, Ug = orc.get_U(0), sim.get_conserved(0)
     rho_err = cases.rel_l2(Ug[0], Uo[0])
