@@ -201,10 +201,24 @@ __device__ __forceinline__ void extrapolate(const Prim<double>& f0, const Prim<d
     }
 }
 
-// Finish a ghost/interior state from the decoded source cell(s).
-template <bool FAST, bool MHD>
-__device__ __forceinline__ void finish_cell(const StageArgs& A, const CellSrc& s, const double* U0, const double* U1,
-                                            int i, int j, Prim<double>& out) {
+// Finish a ghost/interior state from the decoded source cell; the depth-1 cell of
+// an xOrder=1 extrapolation is fetched here (rare path).
+template <int STAGE, bool FAST, bool MHD, int NQ>
+__device__ __noinline__ void finish_extrap1(const StageArgs& A, const double* Uin, const CellSrc& s, double dt,
+                                            double damp, Prim<double>& out) {
+    double U1[NQ];
+    fetch_U<STAGE, NQ>(A, Uin, *s.blk, s.c1, dt, damp, U1);
+    Prim<double> e = out, f1, g0;
+    decode_prim<FAST, MHD>(A.P, U1, f1);
+    extrapolate<MHD>(f1, e, e, g0);
+    if (s.kind == SRC_EXTRAP1_G0) out = g0;
+    else extrapolate<MHD>(e, g0, e, out);
+}
+
+template <int STAGE, bool FAST, bool MHD, int NQ>
+__device__ __forceinline__ void finish_cell(const StageArgs& A, const double* Uin, const CellSrc& s,
+                                            const double* U0, int i, int j, double dt, double damp,
+                                            Prim<double>& out) {
     if (s.kind == SRC_INFLOW) {
         const InflowState& in = A.inflow[s.inflow];
         out.rho = in.rho; out.u = in.u; out.a = in.a; out.psi = in.psi;
@@ -230,11 +244,7 @@ __device__ __forceinline__ void finish_cell(const StageArgs& A, const CellSrc& s
             }
         }
     } else if (s.kind == SRC_EXTRAP1_G0 || s.kind == SRC_EXTRAP1_G1) {
-        Prim<double> e = out, f1, g0;
-        decode_prim<FAST, MHD>(A.P, U1, f1);
-        extrapolate<MHD>(f1, e, e, g0);
-        if (s.kind == SRC_EXTRAP1_G0) out = g0;
-        else extrapolate<MHD>(e, g0, e, out);
+        finish_extrap1<STAGE, FAST, MHD, NQ>(A, Uin, s, dt, damp, out);
     }
 }
 
@@ -287,30 +297,39 @@ __device__ __forceinline__ void gather(const R* base, int stride, int idx, R* q)
     for (int s = 0; s < NRS; ++s) q[s] = base[prim_var<D>(s) * stride + idx];
 }
 
+// Clip q to the range of A and B (src/nm/limiters.d:41-50).  The FP64 path keeps
+// the reference's comparisons; the float path uses min/max (the same value for
+// every non-NaN input up to the sign of a zero result).
+__device__ __forceinline__ double clip_fast(double q, double A, double B) { return clip_to_limits(q, A, B); }
+__device__ __forceinline__ float clip_fast(float q, float A, float B) {
+    return fminf(fmaxf(q, fminf(A, B)), fmaxf(A, B));
+}
+
 // One cell, one direction: both interface values of every reconstructed scalar
 // (e4/onedinterp.d:338-386 with beta = 1 and equal lengths).  qm[s]: value at
 // the cell's minus face (right state there), qp[s]: at its plus face (left state).
 // psi is reconstructed only with divergence cleaning (onedinterp.d:783-786).
-template <class R, int NRS, bool MHD>
+// OPT = 1: apply_limiter and extrema_clipping known to be on (the defaults).
+template <class R, int NRS, bool MHD, int OPT>
 __device__ __forceinline__ void recon_cell(const R* w, const NumParams& P, const R* qm1, const R* q0, const R* qp1,
                                            R* qm, R* qp) {
     const R t = w[W_TOC];
     const R aL0 = w[W_AL0], aR0 = w[W_AR0], len = w[W_LENL0], w3 = w[W_TWOL];
+    const bool lim = OPT == 1 ? true : (bool)P.apply_limiter;
+    const bool clip = OPT == 1 ? true : (bool)P.extrema_clipping;
+    const R eps = R(P.eps_van_albada);
 #pragma unroll
     for (int s = 0; s < NRS; ++s) {
         if (MHD && s == 8 && !P.divergence_cleaning) { qm[s] = q0[s]; qp[s] = q0[s]; continue; }
         R dm = (q0[s] - qm1[s]) * t;
         R dp = (qp1[s] - q0[s]) * t;
         R sl = R(1.0);
-        if (P.apply_limiter) {
-            const R eps = R(P.eps_van_albada);
-            sl = (dm * dp + rabs(dm * dp) + eps) / (dm * dm + dp * dp + eps);
-        }
+        if (lim) sl = (dm * dp + rabs(dm * dp) + eps) / (dm * dm + dp * dp + eps);
         R vp = q0[s] + sl * aL0 * (dp * w3 + dm * len);
         R vm = q0[s] - sl * aR0 * (dp * len + dm * w3);
-        if (P.extrema_clipping) {
-            vp = clip_to_limits(vp, q0[s], qp1[s]);
-            vm = clip_to_limits(vm, qm1[s], q0[s]);
+        if (clip) {
+            vp = clip_fast(vp, q0[s], qp1[s]);
+            vm = clip_fast(vm, qm1[s], q0[s]);
         }
         qp[s] = vp;
         qm[s] = vm;
@@ -387,23 +406,22 @@ __device__ __forceinline__ void load_pair(const StageArgs& A, const double* Uin,
                                           double damp, int n, const int* ci, const int* cj, const int* ck,
                                           Prim<double>* out) {
     CellSrc s[2];
-    double U0[2][NQ], U1[2][NQ];
+    double U0[2][NQ];
 #pragma unroll
     for (int m = 0; m < 2; ++m) {
         if (m < n) {
             s[m] = resolve(A, B, ci[m], cj[m], ck[m]);
             if (s[m].kind != SRC_INFLOW) fetch_U<STAGE, NQ>(A, Uin, *s[m].blk, s[m].c0, dt, damp, U0[m]);
-            if (s[m].c1 >= 0) fetch_U<STAGE, NQ>(A, Uin, *s[m].blk, s[m].c1, dt, damp, U1[m]);
         }
     }
 #pragma unroll
     for (int m = 0; m < 2; ++m) {
-        if (m < n) finish_cell<FAST, MHD>(A, s[m], U0[m], U1[m], ci[m], cj[m], out[m]);
+        if (m < n) finish_cell<STAGE, FAST, MHD, NQ>(A, Uin, s[m], U0[m], ci[m], cj[m], dt, damp, out[m]);
     }
 }
 
 // STAGE 0: residual only (R_out = dUdt of U_in).  STAGE 1/2: predictor / corrector.
-template <int STAGE, class R, bool MHD, int FLUX, int TJ>
+template <int STAGE, class R, bool MHD, int FLUX, int TJ, int OPT>
 __global__ void __launch_bounds__(32 * (TJ + 1), (sizeof(R) == 4 && !MHD) ? 2 : 1) stage_kernel(StageArgs A) {
     using G = Geo<R, MHD, TJ>;
     constexpr int TI = G::TI, NT = G::NT, NCOL = G::NCOL, PW = G::PW, PLANE = G::PLANE;
@@ -482,7 +500,7 @@ __global__ void __launch_bounds__(32 * (TJ + 1), (sizeof(R) == 4 && !MHD) ? 2 : 
             gather<R, NRS, 2>(slot(t.k0 - 2), PLANE, pidx, qm1);
             gather<R, NRS, 2>(slot(t.k0 - 1), PLANE, pidx, q0);
             gather<R, NRS, 2>(slot(t.k0), PLANE, pidx, qp1);
-            recon_cell<R, NRS, MHD>(w[2], P, qm1, q0, qp1, qm, kq_prev_p);
+            recon_cell<R, NRS, MHD, OPT>(w[2], P, qm1, q0, qp1, qm, kq_prev_p);
             // plane k0+1 replaces k0-2 in the ring
             int ck3[2] = {t.k0 + 1, 0};
             load_pair<STAGE, FAST, MHD, NQ>(A, Uin, B, dt, damp, 1, ci, cj, ck3, pr);
@@ -491,7 +509,7 @@ __global__ void __launch_bounds__(32 * (TJ + 1), (sizeof(R) == 4 && !MHD) ? 2 : 
             gather<R, NRS, 2>(slot(t.k0 - 1), PLANE, pidx, qm1);
             gather<R, NRS, 2>(slot(t.k0), PLANE, pidx, q0);
             gather<R, NRS, 2>(slot(t.k0 + 1), PLANE, pidx, qp1);
-            recon_cell<R, NRS, MHD>(w[2], P, qm1, q0, qp1, qkm, qkp);
+            recon_cell<R, NRS, MHD, OPT>(w[2], P, qm1, q0, qp1, qkm, qkp);
             CellR<R> cL, cR;
             get_prim<R, NPV>(slot(t.k0 - 1), PLANE, pidx, cL);
             get_prim<R, NPV>(slot(t.k0), PLANE, pidx, cR);
@@ -558,7 +576,7 @@ __global__ void __launch_bounds__(32 * (TJ + 1), (sizeof(R) == 4 && !MHD) ? 2 : 
             gather<R, NRS, 2>(cur, PLANE, pidx, qm1);
             gather<R, NRS, 2>(slot(k + 1), PLANE, pidx, q0);
             gather<R, NRS, 2>(slot(k + 2), PLANE, pidx, qp1);
-            recon_cell<R, NRS, MHD>(w[2], P, qm1, q0, qp1, kq_m, kq_p);
+            recon_cell<R, NRS, MHD, OPT>(w[2], P, qm1, q0, qp1, kq_m, kq_p);
         }
         for (int f = f0; f < NRI + NRJ && f < fend; f += fstride) {
             R qm1[NRS], q0[NRS], qp1[NRS], qm[NRS], qp[NRS];
@@ -569,7 +587,7 @@ __global__ void __launch_bounds__(32 * (TJ + 1), (sizeof(R) == 4 && !MHD) ? 2 : 
                 gather<R, NRS, 0>(cur, PLANE, p - 1, qm1);
                 gather<R, NRS, 0>(cur, PLANE, p, q0);
                 gather<R, NRS, 0>(cur, PLANE, p + 1, qp1);
-                recon_cell<R, NRS, MHD>(w[0], P, qm1, q0, qp1, qm, qp);
+                recon_cell<R, NRS, MHD, OPT>(w[0], P, qm1, q0, qp1, qm, qp);
 #pragma unroll
                 for (int s = 0; s < NRS; ++s) { RI[s * NRI + f] = qm[s]; RI[(NRS + s) * NRI + f] = qp[s]; }
             } else {
@@ -580,7 +598,7 @@ __global__ void __launch_bounds__(32 * (TJ + 1), (sizeof(R) == 4 && !MHD) ? 2 : 
                 gather<R, NRS, 1>(cur, PLANE, p - PW, qm1);
                 gather<R, NRS, 1>(cur, PLANE, p, q0);
                 gather<R, NRS, 1>(cur, PLANE, p + PW, qp1);
-                recon_cell<R, NRS, MHD>(w[1], P, qm1, q0, qp1, qm, qp);
+                recon_cell<R, NRS, MHD, OPT>(w[1], P, qm1, q0, qp1, qm, qp);
 #pragma unroll
                 for (int s = 0; s < NRS; ++s) { RJ[s * NRJ + g] = qm[s]; RJ[(NRS + s) * NRJ + g] = qp[s]; }
             }
@@ -636,6 +654,19 @@ __global__ void __launch_bounds__(32 * (TJ + 1), (sizeof(R) == 4 && !MHD) ? 2 : 
             const long long cell = cell_index(B, t.i0 + ti, t.j0 + tj, k);
             const long long g = B.offset + cell;
             double dU[NQ];
+            if (FAST) {
+                // float path: differences of opposite faces in float (same-signed,
+                // nearly equal fluxes subtract exactly), accumulation in FP64
+                const double Vi = B.vol_inv;
+#pragma unroll
+                for (int q = 0; q < NQ; ++q) {
+                    R dI = FI[q * NFI + ti + (TI + 1) * tj] - FI[q * NFI + ti + 1 + (TI + 1) * tj];
+                    R dJ = FJ[q * NFJ + ti + TI * tj] - FJ[q * NFJ + ti + TI * (tj + 1)];
+                    double si = (double)dI * Ai + (double)dJ * Aj;
+                    if (has_k) si += (double)(fB[q] - fT[q]) * Ak;
+                    dU[q] = Vi * si;
+                }
+            } else
 #pragma unroll
             for (int q = 0; q < NQ; ++q) {
                 double FW = (double)FI[q * NFI + ti + (TI + 1) * tj];

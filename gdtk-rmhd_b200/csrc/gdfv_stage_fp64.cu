@@ -12,13 +12,21 @@ constexpr int TJ = TJ_FP64;
 template <int STAGE, bool MHD, int FLUX>
 cudaError_t launch_one(const StageArgs& A, cudaStream_t s) {
     using G = Geo<Real, MHD, TJ>;
-    stage_kernel<STAGE, Real, MHD, FLUX, TJ><<<A.n_tiles, G::NT, G::bytes, s>>>(A);
+    // defaults (limiter and extrema clipping on) take the specialised path
+    if (A.P.apply_limiter && A.P.extrema_clipping)
+        stage_kernel<STAGE, Real, MHD, FLUX, TJ, 1><<<A.n_tiles, G::NT, G::bytes, s>>>(A);
+    else
+        stage_kernel<STAGE, Real, MHD, FLUX, TJ, 0><<<A.n_tiles, G::NT, G::bytes, s>>>(A);
     return cudaGetLastError();
 }
 
 template <int STAGE, bool MHD, int FLUX>
 cudaError_t configure_one() {
-    return cudaFuncSetAttribute(stage_kernel<STAGE, Real, MHD, FLUX, TJ>,
+    cudaError_t e = cudaFuncSetAttribute(stage_kernel<STAGE, Real, MHD, FLUX, TJ, 0>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)Geo<Real, MHD, TJ>::bytes);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(stage_kernel<STAGE, Real, MHD, FLUX, TJ, 1>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)Geo<Real, MHD, TJ>::bytes);
 }
