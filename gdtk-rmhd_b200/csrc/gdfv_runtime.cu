@@ -524,6 +524,46 @@ int build_graph(Context* c) {
     return GDFV_OK;
 }
 
+// Read-only view of a context for gdfv_step_noalloc (gdfv_noalloc.cu).
+struct NoallocView {
+    int prepared, precision, flux, mhd, nblocks, max_invalid_cells;
+    long long total;
+    int nq, n_tiles;
+    const BlockDesc* d_blocks;
+    const TileDesc* d_tiles;
+    const InflowState* d_inflow;
+    NumParams P;
+    double c_h;
+    cudaStream_t stream;
+};
+
+bool noalloc_view(int ctx, NoallocView* v) {
+    Context* c = get_ctx(ctx);
+    if (!c || !v) return false;
+    v->prepared = c->prepared;
+    v->precision = c->cfg.precision;
+    v->flux = c->cfg.flux;
+    v->mhd = c->cfg.mhd;
+    v->nblocks = (int)c->blocks.size();
+    v->max_invalid_cells = c->cfg.max_invalid_cells;
+    v->total = c->total;
+    v->nq = c->nq;
+    v->n_tiles = c->n_tiles;
+    v->d_blocks = c->d_blocks;
+    v->d_tiles = c->d_tiles;
+    v->d_inflow = c->d_inflow;
+    v->P = c->P;
+    v->c_h = c->h_ctl ? c->h_ctl->c_h : 0.0;
+    v->stream = c->stream;
+    return true;
+}
+
+void noalloc_set_error(int ctx, const std::string& msg) {
+    Context* c = get_ctx(ctx);
+    if (c) c->err = msg;
+    else g_err = msg;
+}
+
 }  // namespace gdfv
 
 // ====================================================================== C ABI

@@ -119,6 +119,25 @@ int gdfv_set_stream(int ctx, void* cuda_stream);
  * without advancing it; ms[0] = stage 1, ms[1] = stage 2 average milliseconds per launch. */
 int gdfv_time_stages(int ctx, int reps, double* ms);
 
+/* One predictor-corrector step of size dt from U_in_dev to U_out_dev (device arrays
+ * [nq][total], distinct), allocating no device memory.  This entry point has no
+ * counterpart in the reference.  It is for callers that cannot call cudaMalloc: an
+ * application whose device memory belongs to its own pool allocator, or a real-time
+ * loop that cannot accept cudaMalloc's latency and implicit synchronisation.  The
+ * step's scratch (predictor derivative, step-control record, signal maxima) lives in
+ * one fixed device array that the library reserves on every GPU it is loaded on and
+ * keeps until exit: nq * total cells must not exceed GDFV_NOALLOC_MAX_VALUES and the
+ * blocks must not exceed GDFV_NOALLOC_MAX_BLOCKS, else GDFV_ERR_ARG.  All calls share
+ * that array, so calls whose kernels overlap on the GPU race; calls made one after
+ * another on the context's stream are safe.  The first call on a device looks up the
+ * array's address; make it before any stream capture starts on that device.  MHD runs
+ * use the c_h of the context's last gdfv_run.  n_bad_cells (may be NULL) receives the
+ * decode failures plus invalid cells; a decode failure returns GDFV_ERR_STEP_FAILED
+ * (no retry is attempted). */
+#define GDFV_NOALLOC_MAX_VALUES 4194304LL
+#define GDFV_NOALLOC_MAX_BLOCKS 1024
+int gdfv_step_noalloc(int ctx, const double* U_in_dev, double* U_out_dev, double dt, int* n_bad_cells);
+
 /* Copy of the last error message of a context (NUL-terminated, truncated to n). */
 int gdfv_last_error(int ctx, char* buf, int n);
 
