@@ -95,6 +95,17 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(self.samples)}
 
 
+def max_over_ranks(value, device="cpu"):
+    """Max of a per-rank timing over all ranks (identity without a process group)."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(value)
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def cpu_oracle_baseline(cells_target=96, steps=24):
     """CPU oracle port (OpenMP over cells) on a bounded sample: 96^3 cells of the same workload."""
     import cases
@@ -208,11 +219,8 @@ def main():
             taken = sim.run(max_step=args.steps)
             e1.record(stream)
             torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1)
+        ms = max_over_ranks(e0.elapsed_time(e1), device="cuda")
         if world > 1:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
             dist.barrier()
         results[prec] = dict(ms=ms, taken=taken, clocks=sampler.summary())
 

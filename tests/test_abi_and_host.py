@@ -1,0 +1,101 @@
+"""CPU checks of the boundary: libgdfv.so loads, exports every entry point the
+header declares, and takes the reference's option and BC names (no GPU needed
+for configuration calls); the oracle library loads; the multi-rank timing
+reduction works over gloo with two ranks."""
+import ctypes
+import os
+
+import pytest
+
+import gdfv
+from gdfv._lib import GDFV_ERR_ARG, GDFV_OK, LIBPATH, check, ffi, last_error
+
+
+def test_library_exports_every_declared_symbol():
+    syms = gdfv.exported_symbols()
+    assert len(syms) >= 20
+    raw = ctypes.CDLL(LIBPATH)
+    for s in syms:
+        assert hasattr(raw, s), s          # dlsym
+        getattr(gdfv.lib(), s)             # and the cffi binding
+
+
+def test_config_accepts_reference_names_and_rejects_others():
+    L = gdfv.lib()
+    h = L.gdfv_context_new()
+    assert h >= 0
+    for key, val in (("flux_calculator", "ausmdv"), ("flux_calculator", "hllc"), ("flux_calculator", "hlle"),
+                     ("gasdynamic_update_scheme", "predictor-corrector"), ("gasdynamic_update_scheme", "pc"),
+                     ("thermo_interpolator", "rhou"), ("flux_precision", "fp32")):
+        assert L.gdfv_config_set_str(h, key.encode(), val.encode()) == GDFV_OK, (key, val)
+    for key, val in (("flux_calculator", "roe"), ("gasdynamic_update_scheme", "tvd_rk3"),
+                     ("thermo_interpolator", "pT"), ("no_such_option", "x")):
+        assert L.gdfv_config_set_str(h, key.encode(), val.encode()) == GDFV_ERR_ARG
+        assert len(last_error(h)) > 0
+    for key, val in (("interpolation_order", 2), ("MHD", 1), ("divergence_cleaning", 1), ("cfl_count", 10),
+                     ("max_attempts_for_step", 3), ("n_ghost_cell_layers", 2), ("dimensions", 3)):
+        assert L.gdfv_config_set_int(h, key.encode(), val) == GDFV_OK, key
+    assert L.gdfv_config_set_int(h, b"interpolation_order", 3) == GDFV_ERR_ARG
+    assert L.gdfv_config_set_int(h, b"cfl_count", 0) == GDFV_ERR_ARG
+    for key in ("cfl_value", "dt_init", "dt_max", "epsilon_van_albada", "R", "gamma", "divB_damping_length"):
+        assert L.gdfv_config_set_double(h, key.encode(), 0.5) == GDFV_OK, key
+    v = ffi.new("double*")
+    check(h, L.gdfv_config_get_double(h, b"cfl_value", v))
+    assert v[0] == 0.5
+    assert L.gdfv_context_free(h) == GDFV_OK
+    assert L.gdfv_context_free(h) == GDFV_ERR_ARG
+
+
+def test_blocks_and_boundary_names():
+    L = gdfv.lib()
+    h = L.gdfv_context_new()
+    assert L.gdfv_block_new(h, 0, 4, 4, 1.0, 1.0, 1.0, 0, 0, 0) < 0
+    b = L.gdfv_block_new(h, 8, 4, 4, 1e-3, 1e-3, 1e-3, 0, 0, 0)
+    assert b == 0
+    inflow = ffi.new("double[9]", [5e3, 220.0, 890.0, 0, 0, 0, 0, 0, 0])
+    for face, name in ((0, b"inflow_supersonic"), (1, b"outflow_simple_extrapolate"), (2, b"wall_with_slip"),
+                       (3, b"exchange_over_full_face")):
+        assert L.gdfv_block_set_bc(h, b, face, name, 0, 0, 2, inflow) == GDFV_OK
+    assert L.gdfv_block_set_bc(h, b, 4, b"wall_no_slip_fixed_t", 0, -1, -1, ffi.NULL) == GDFV_ERR_ARG
+    assert L.gdfv_block_set_bc(h, b, 7, b"wall_with_slip", 0, -1, -1, ffi.NULL) == GDFV_ERR_ARG
+    assert L.gdfv_block_ncells(h, b) == 128
+    assert L.gdfv_total_cells(h) == 128
+    L.gdfv_context_free(h)
+
+
+def test_oracle_library_loads():
+    from oracle import lib as orc_lib
+    L = orc_lib()
+    assert L.orc_new() >= 0
+
+
+def _ranks_worker(rank, world, port, q):
+    import torch.distributed as dist
+    import bench
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    q.put((rank, bench.max_over_ranks(10.0 + rank)))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_max_over_ranks_gloo_world2():
+    import socket
+    import sys
+    import torch.multiprocessing as mp
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    if root not in sys.path:
+        sys.path.insert(0, root)
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_ranks_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=120) for _ in range(2))
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    assert res == {0: 11.0, 1: 11.0}
