@@ -135,6 +135,49 @@ def chicken_baseline(steps, warmup):
     return chicken_job.bench(exe, steps=steps, warmup=warmup)
 
 
+def adjoint_over_forward(nsteps=50, checkpoint_every=10, shape=(128, 128, 64)):
+    """Adjoint configuration: 128x128x64 M=3 inflow box (FP64, ausmdv), J = pressure
+    integral over the y-min wall after 50 steps, gradient w.r.t. U0 and the inflow
+    state through the checkpointed rollout (every 10 steps).  Returns the ratio of
+    the backward time (recomputation + adjoint steps) to the forward time of the
+    same 50 steps run by gdfv_run, both with CUDA events on the device."""
+    import torch
+    import cases
+    from gdfv.autograd import rollout
+    from test_gpu_adjoint import wall_pressure
+    case = cases.c2_inflow_box(n=shape)
+    inf = cases.inflow_state_m3()
+    sim = cases.build_gpu(case)
+    stream = torch.cuda.Stream()
+    sim.set_stream(stream.cuda_stream)
+    U0 = torch.from_numpy(sim.get_conserved(0)).cuda()
+    sim.run(max_step=2)
+    sim.set_conserved(0, U0.cpu().numpy())
+    sim.set_time(0.0, 0, sim.config.dt_init)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sim.run(max_step=nsteps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    fwd_ms = e0.elapsed_time(e1)
+    theta = torch.tensor([inf["p"], inf["T"], inf["vel"][0]], dtype=torch.float64, requires_grad=True)
+    U0r = U0.clone().requires_grad_(True)
+    with torch.cuda.stream(stream):
+        UN = rollout(sim, U0r, theta, nsteps, checkpoint_every)
+        J = wall_pressure(case, UN, case.R)
+    torch.cuda.synchronize()
+    b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    b0.record()
+    J.backward()
+    b1.record()
+    torch.cuda.synchronize()
+    adj_ms = b0.elapsed_time(b1)
+    return dict(ratio=adj_ms / fwd_ms, forward_ms=fwd_ms, adjoint_ms=adj_ms, steps=nsteps,
+                checkpoint_every=checkpoint_every, workload=f"M=3 inflow box {shape[0]}x{shape[1]}x{shape[2]} FP64",
+                dJ_dp_inflow=float(theta.grad[0]), grad_U0_norm=float(U0r.grad.norm()))
+
+
 def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -293,6 +336,12 @@ def main():
         "clocks": results["fp32"]["clocks"],
         "clocks_fp64": results["fp64"]["clocks"],
     }
+    try:
+        adj = adjoint_over_forward()
+        line["adjoint_over_forward"] = adj["ratio"]
+        line["adjoint"] = adj
+    except Exception as e:  # reported, never required for the throughput line
+        line["adjoint"] = {"error": str(e)}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_oracle_baseline()

@@ -237,11 +237,18 @@ struct Context {
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;
     bool signal_valid = false;
+    int n_inflow = 0;
+    double* adj_scratch = nullptr;     // adjoint work arrays, allocated on first use
+    long long adj_scratch_n = 0;
+    Control* step_ctl = nullptr;       // control record of gdfv_step_dt
+    unsigned long long* step_maxsig = nullptr;
+    double* step_lastsig = nullptr;
 
     ~Context() {
         if (graph) cudaGraphExecDestroy(graph);
         for (void* p : {(void*)U[0], (void*)U[1], (void*)dU0, (void*)d_blocks, (void*)d_tiles, (void*)d_inflow,
-                        (void*)d_ctl, (void*)d_maxsig, (void*)d_lastsig, (void*)d_bad})
+                        (void*)d_ctl, (void*)d_maxsig, (void*)d_lastsig, (void*)d_bad, (void*)adj_scratch,
+                        (void*)step_ctl, (void*)step_maxsig, (void*)step_lastsig})
             if (p) cudaFree(p);
         if (h_ctl) cudaFreeHost(h_ctl);
         if (own_stream && stream) cudaStreamDestroy(stream);
@@ -439,6 +446,7 @@ int do_prepare(Context* c) {
     }
     c->total = off;
     c->n_tiles = (int)tiles.size();
+    c->n_inflow = (int)inflows.size();
     NumParams& P = c->P;
     P.gas.R = g.R; P.gas.gamma = g.gamma; P.gas.Cv = Cv; P.gas.Cvinv = 1.0 / Cv;
     P.eps_van_albada = g.eps_van_albada;
@@ -562,6 +570,65 @@ void noalloc_set_error(int ctx, const std::string& msg) {
     Context* c = get_ctx(ctx);
     if (c) c->err = msg;
     else g_err = msg;
+}
+
+// Host view of a context for the adjoint (gdfv_adjoint.cu).
+struct AdjView {
+    int prepared, flux, mhd, precision, nblocks, ninflow, dims;
+    long long total;
+    const BlockDesc* d_blocks;
+    const InflowState* d_inflow;
+    NumParams P;
+    cudaStream_t stream;
+    std::vector<BlockDesc> h_blocks;
+    double** scratch;
+    long long* scratch_n;
+};
+
+bool adjoint_view(int ctx, AdjView* v) {
+    Context* c = get_ctx(ctx);
+    if (!c || !v) return false;
+    v->prepared = c->prepared;
+    v->flux = c->cfg.flux;
+    v->mhd = c->cfg.mhd;
+    v->precision = c->cfg.precision;
+    v->nblocks = (int)c->blocks.size();
+    v->ninflow = c->n_inflow;
+    v->dims = c->cfg.dims;
+    v->total = c->total;
+    v->d_blocks = c->d_blocks;
+    v->d_inflow = c->d_inflow;
+    v->P = c->P;
+    v->stream = c->stream;
+    v->h_blocks = c->h_blocks;
+    v->scratch = &c->adj_scratch;
+    v->scratch_n = &c->adj_scratch_n;
+    return true;
+}
+
+void adjoint_set_error(int ctx, const std::string& msg) {
+    Context* c = get_ctx(ctx);
+    if (c) c->err = msg;
+    else g_err = msg;
+}
+
+// U1 = U0 + dt*dU0 with the predictor's rounding (no contraction), MHD psi not damped:
+// used only for the Euler adjoint.
+__global__ void predictor_state_kernel(const double* U0, const double* dU0, double dt, long long n, double* U1) {
+    long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (x < n) U1[x] = __dadd_rn(U0[x], __dmul_rn(dt, dU0[x]));
+}
+
+// Resets the control record of a single fixed-dt step.
+__global__ void step_dt_begin_kernel(Control* c, unsigned long long* maxsig, int nblocks, double dt, double c_h) {
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) maxsig[b] = 0ull;
+    if (threadIdx.x == 0) {
+        c->time = 0.0; c->dt_global = dt; c->c_h = c_h; c->cfl_max = 0.0; c->dt_allow = 0.0;
+        c->max_time = 0.0; c->t0 = 0.0; c->first_bad_cell = LLONG_MAX;
+        c->step = 0; c->step_limit = 1; c->status = ST_OK; c->halted = 0;
+        c->n_fail = 0; c->n_invalid1 = 0; c->n_invalid2 = 0;
+        c->attempt = 0; c->retrying = 0; c->steps_done = 0;
+    }
 }
 
 }  // namespace gdfv
@@ -918,6 +985,43 @@ int gdfv_residual(int ctx, const double* U_dev, double* R_dev) {
     A.R_out = R_dev;
     CK(launch_stage(c, 0, A));
     CK(cudaStreamSynchronize(c->stream));
+    return GDFV_OK;
+}
+
+int gdfv_step_dt(int ctx, const double* U_in_dev, double* U_out_dev, double dt, double* U1_out_dev) {
+    Context* c = get_ctx(ctx);
+    int st = check_ready(c, -1);
+    if (st) return st;
+    if (!U_in_dev || !U_out_dev || U_in_dev == U_out_dev || !(dt > 0.0))
+        return fail(c, GDFV_ERR_ARG, "gdfv_step_dt needs distinct input/output arrays and dt > 0");
+    if (!c->step_ctl) {
+        CK(cudaMalloc(&c->step_ctl, sizeof(Control)));
+        CK(cudaMalloc(&c->step_maxsig, sizeof(unsigned long long) * c->blocks.size()));
+        CK(cudaMalloc(&c->step_lastsig, sizeof(double) * c->blocks.size()));
+    }
+    if (read_ctl(c)) return GDFV_ERR_CUDA;
+    StageArgs A = stage_args(c);
+    A.Ubuf[0] = const_cast<double*>(U_in_dev);
+    A.Ubuf[1] = U_out_dev;
+    A.ctl = c->step_ctl;
+    A.max_signal = c->step_maxsig;
+    A.last_signal = c->step_lastsig;
+    step_dt_begin_kernel<<<1, 256, 0, c->stream>>>(c->step_ctl, c->step_maxsig, (int)c->blocks.size(), dt,
+                                                   c->h_ctl->c_h);
+    CK(cudaGetLastError());
+    CK(launch_stage(c, 1, A));
+    if (U1_out_dev) {
+        long long n = (long long)c->nq * c->total;
+        predictor_state_kernel<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(U_in_dev, c->dU0, dt, n, U1_out_dev);
+        CK(cudaGetLastError());
+    }
+    CK(launch_stage(c, 2, A));
+    Control h{};
+    CK(cudaMemcpyAsync(&h, c->step_ctl, sizeof(Control), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (h.n_fail > 0) return fail(c, GDFV_ERR_STEP_FAILED, "gdfv_step_dt: a cell failed to decode");
+    if (h.n_invalid1 > c->cfg.max_invalid_cells || h.n_invalid2 > c->cfg.max_invalid_cells)
+        return fail(c, GDFV_ERR_BAD_CELLS, "gdfv_step_dt: too many bad cells");
     return GDFV_OK;
 }
 

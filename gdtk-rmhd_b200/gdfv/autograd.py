@@ -1,0 +1,150 @@
+"""torch.autograd wrappers over the hand-written adjoint kernels.
+
+* `residual(sim, U)`: R(U) with backward = gdfv_residual_vjp.
+* `rollout(sim, U0, theta, nsteps, checkpoint_every)`: nsteps predictor-corrector
+  steps of the GPU solver from U0, differentiable in U0 and in the supersonic-
+  inflow state theta = (p, T, vel.x).  The forward records each step's dt and
+  keeps a copy of the state every `checkpoint_every` steps; the backward
+  recomputes each segment from its checkpoint (gdfv_step_dt, bit-identical to
+  the forward steps) and applies the adjoint of the predictor-corrector step
+  (e4/simcore_gasdynamic_step.d:1245-1333):
+      U1 = U0 + dt R(U0),  U2 = U0 + dt (R(U0)/2 + R(U1)/2)
+      mu  = J(U1)^T (dt/2 lam)
+      lam <- lam + mu + J(U0)^T (dt/2 lam + dt mu)
+  with dt frozen at its forward value (the CFL rule is not differentiated).
+Tensors are float64 on the simulation's device, shaped [nq, total cells].
+"""
+import torch
+
+from ._lib import check, ffi
+
+
+def _p(t):
+    return ffi.cast("double*", t.data_ptr())
+
+
+def vjp(sim, U, W):
+    """G = (dR/dU)^T W and the inflow-state cotangents [n_inflow, 6]."""
+    U = U.contiguous()
+    W = W.contiguous()
+    G = torch.empty_like(U)
+    n_in = max(1, getattr(sim, "n_inflow", 1))
+    gin = torch.zeros((n_in, 6), dtype=torch.float64)
+    torch.cuda.current_stream().synchronize()
+    check(sim.ctx, sim.L.gdfv_residual_vjp(sim.ctx, _p(U), _p(W), _p(G), ffi.cast("double*", gin.data_ptr())))
+    return G, gin
+
+
+def residual_eval(sim, U):
+    U = U.contiguous()
+    R = torch.empty_like(U)
+    torch.cuda.current_stream().synchronize()
+    sim.residual(U.data_ptr(), R.data_ptr())
+    return R
+
+
+def step_dt(sim, U, dt, with_predictor=False):
+    """One step of the given dt; with_predictor also returns U1 = U + dt R(U)."""
+    U = U.contiguous()
+    out = torch.empty_like(U)
+    U1 = torch.empty_like(U) if with_predictor else None
+    torch.cuda.current_stream().synchronize()
+    check(sim.ctx, sim.L.gdfv_step_dt(sim.ctx, _p(U), _p(out), float(dt), _p(U1) if with_predictor else ffi.NULL))
+    return (out, U1) if with_predictor else out
+
+
+class Residual(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, U, sim):
+        ctx.sim = sim
+        ctx.save_for_backward(U)
+        return residual_eval(sim, U)
+
+    @staticmethod
+    def backward(ctx, gR):
+        (U,) = ctx.saved_tensors
+        G, _ = vjp(ctx.sim, U, gR)
+        return G, None
+
+
+def residual(sim, U):
+    return Residual.apply(U, sim)
+
+
+def inflow_chain(sim, theta, gprim):
+    """d/d(p, T, vel.x) of an inflow ghost state (FlowState:new{p=,T=}: rho = p/(R T),
+    u = Cv T, a = sqrt(gamma R T)) from its cotangent (rho, vx, vy, vz, u, a)."""
+    p, T, _ = [float(x) for x in theta]
+    R, g = sim.gas.R, sim.gas.gamma
+    Cv = R / (g - 1.0)
+    a = (g * R * T) ** 0.5
+    gr, gvx, _, _, gu, ga = [float(x) for x in gprim]
+    dp = gr / (R * T)
+    dT = gr * (-p / (R * T * T)) + gu * Cv + ga * g * R / (2.0 * a)
+    return torch.tensor([dp, dT, gvx], dtype=torch.float64)
+
+
+class Rollout(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, U0, theta, sim, nsteps, checkpoint_every):
+        U0 = U0.contiguous()
+        dts, ckpts = [], {0: U0.clone()}
+        sim.set_time(0.0, 0, sim.config.dt_init)
+        torch.cuda.current_stream().synchronize()
+        state = _state_view(sim)
+        state.copy_(U0)
+        torch.cuda.synchronize()
+        for n in range(nsteps):
+            sim.run(max_step=1)
+            dts.append(sim.time()["dt"])
+            if (n + 1) % checkpoint_every == 0 and n + 1 < nsteps:
+                ckpts[n + 1] = _state_view(sim).clone()
+        UN = _state_view(sim).clone()
+        ctx.sim, ctx.dts, ctx.ckpts, ctx.k = sim, dts, ckpts, checkpoint_every
+        ctx.theta = theta.detach().clone()
+        return UN
+
+    @staticmethod
+    def backward(ctx, gUN):
+        sim, dts, ckpts, K = ctx.sim, ctx.dts, ctx.ckpts, ctx.k
+        lam = gUN.contiguous().clone()
+        gin = None
+        n_total = len(dts)
+        for s0 in reversed(range(0, n_total, K)):
+            s1 = min(s0 + K, n_total)
+            states, preds = [ckpts[s0]], []
+            for n in range(s0, s1):
+                nxt, U1 = step_dt(sim, states[-1], dts[n], with_predictor=True)
+                preds.append(U1)
+                if n < s1 - 1:
+                    states.append(nxt)
+            for n in reversed(range(s0, s1)):
+                U0, dt = states[n - s0], dts[n]
+                U1 = preds[n - s0]
+                a = lam * (0.5 * dt)
+                mu, g1 = vjp(sim, U1, a)
+                b = a + mu * dt
+                g0, g0i = vjp(sim, U0, b)
+                lam = lam + mu + g0
+                gin = (g1 + g0i) if gin is None else gin + g1 + g0i
+        gtheta = inflow_chain(sim, ctx.theta, gin[0]).to(ctx.theta.device)
+        return lam, gtheta, None, None, None
+
+
+def _state_view(sim):
+    """The library's current state buffer as a torch tensor (no copy)."""
+    return _from_ptr(sim.state_ptr(), (sim.nq, sim.total_cells()))
+
+
+def _from_ptr(ptr, shape):
+    import numpy as np
+    numel = int(np.prod(shape))
+
+    class _Holder:
+        __cuda_array_interface__ = {"shape": (numel,), "typestr": "<f8", "data": (ptr, False), "version": 3}
+
+    return torch.as_tensor(_Holder(), device="cuda").view(*shape)
+
+
+def rollout(sim, U0, theta, nsteps, checkpoint_every=10):
+    return Rollout.apply(U0, theta, sim, int(nsteps), int(checkpoint_every))

@@ -138,6 +138,7 @@ class Simulation:
         self.blocks = []
         self._bcs = []
         self._prepared = False
+        self.n_inflow = 0   # supersonic-inflow faces, in the order the library numbers them
 
     # ---------------------------------------------------------------- setup
     def _apply_config(self):
@@ -180,6 +181,7 @@ class Simulation:
             arr = bc.flowState.as_array()
             self._bcs[blk][f] = arr  # keep alive
             inflow = ffi.cast("double*", arr.ctypes.data)
+            self.n_inflow += 1
         check(self.ctx, self.L.gdfv_block_set_bc(self.ctx, blk, f, bc.name.encode(), x_order, other,
                                                   other_face, inflow))
 

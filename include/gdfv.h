@@ -110,6 +110,22 @@ int gdfv_set_time(int ctx, double time, int step, double dt_global);
  * on the state U.  Uses the context's current c_h. */
 int gdfv_residual(int ctx, const double* U_dev, double* R_dev);
 
+/* Vector-Jacobian product of the residual: G = (dR/dU)^T W at the state U, device
+ * arrays [nq][total] over all blocks (the adjoint of gdfv_residual, hand-written:
+ * reverse of decode_conserved, interp_l2r2 and ausmdv, with the branches of the
+ * primal values).  g_inflow_host (may be NULL) receives, per supersonic-inflow face
+ * state in the order the faces were defined, the cotangent of its ghost state
+ * (rho, vel.x, vel.y, vel.z, u, a), 6 doubles each.  3D Euler with
+ * flux_calculator=ausmdv.  It is the transpose of the Jacobian-vector products of
+ * e4/steadystate_core.d:1870-2060 (evalJacobianVecProd), which it is checked against. */
+int gdfv_residual_vjp(int ctx, const double* U_dev, const double* W_dev, double* G_dev, double* g_inflow_host);
+
+/* One predictor-corrector step of a given dt from U_in_dev to U_out_dev (device arrays
+ * [nq][total], distinct), without the dt rule: the recomputation step of a
+ * checkpointed adjoint, bit-identical to the step gdfv_run took with that dt.
+ * U1_out_dev (may be NULL) receives the predictor state U1 = U0 + dt R(U0). */
+int gdfv_step_dt(int ctx, const double* U_in_dev, double* U_out_dev, double dt, double* U1_out_dev);
+
 /* Device pointer of the current conserved state ([nq][total], borrowed, valid
  * until the next gdfv_run), and of the context's CUDA stream. */
 int gdfv_state_device_ptr(int ctx, double** U_dev);

@@ -72,20 +72,29 @@ def inflow_state_m3():
     return dict(p=5.0e3, T=T, vel=(3.0 * a, 0.0, 0.0))
 
 
-def c2_inflow_box(n=(256, 256, 256), flux="ausmdv", seed=4321, precision="fp64"):
+def c2_inflow_box(n=(256, 256, 256), flux="ausmdv", seed=4321, precision="fp64", noise_all=False):
     """Single block, M=3 inflow on x-min, extrapolate outflow on x-max, slip walls
-    on y and z faces, inflow state everywhere plus 1% density noise (dx = 1 mm)."""
+    on y and z faces, inflow state everywhere plus 1% density noise (dx = 1 mm).
+    noise_all: also 1% noise on T and on the velocity components, so that no
+    reconstructed field is exactly uniform (limiters away from their kinks)."""
     c = Case("c2", dict(flux_calculator=flux, flux_precision=precision), R_AIR_CHICKEN, 1.4)
     rng = np.random.default_rng(seed)
     inf = inflow_state_m3()
     nic, njc, nkc = n
+    shp = (nkc, njc, nic)
     rho_inf = inf["p"] / (R_AIR_CHICKEN * inf["T"])
-    rho = _noisy_rho(rng, rho_inf, (nkc, njc, nic))
+    rho = _noisy_rho(rng, rho_inf, shp)
+    T, vel = inf["T"], inf["vel"]
+    if noise_all:
+        T = inf["T"] * (1.0 + 0.01 * rng.standard_normal(shp))
+        u = inf["vel"][0]
+        vel = (u * (1.0 + 0.01 * rng.standard_normal(shp)), 0.01 * u * rng.standard_normal(shp),
+               0.01 * u * rng.standard_normal(shp))
     bcs = {"west": ("inflow_supersonic", dict(inflow=inf)),
            "east": ("outflow_simple_extrapolate", dict(x_order=0)),
            "south": ("wall_with_slip", {}), "north": ("wall_with_slip", {}),
            "bottom": ("wall_with_slip", {}), "top": ("wall_with_slip", {})}
-    c.add_block(n, (1e-3, 1e-3, 1e-3), (0, 0, 0), bcs, rho, inf["vel"], inf["T"])
+    c.add_block(n, (1e-3, 1e-3, 1e-3), (0, 0, 0), bcs, rho, vel, T)
     return c
 
 
