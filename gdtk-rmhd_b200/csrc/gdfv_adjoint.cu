@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "../../include/gdfv.h"
+#include "gdfv_internal.h"
 #include "gdfv_launch.h"
 
 namespace gdfv {
@@ -286,8 +287,13 @@ struct AdjArgs {
     double* gU;        // [nq][total]
     double* gInflow;   // [ninflow][6]
     const long long* face_off;  // [3][nblocks+1] prefix counts of faces per direction
+    double* lam;       // [nq][total] adjoint state of a fused step (modes 1, 2)
+    double* bbuf;      // [nq][total] b = dt/2 lam + dt mu (mode 1 writes, mode 2 is its W)
+    double w_scale;    // W enters scaled by this
+    double dt;
     long long total;
     int nblocks;
+    int mode;          // 0: gU = result; 1: mu -> bbuf, lam += mu; 2: lam += result
     NumParams P;
 };
 
@@ -390,7 +396,7 @@ __global__ void __launch_bounds__(128, 3) adj_face_kernel(AdjArgs a) {
         adj_load(a, s[m], c[m]);
     }
     // cotangent of the face flux: F enters R_right with +A/V and R_left with -A/V
-    const double AV = B.area[D] * B.vol_inv;
+    const double AV = B.area[D] * B.vol_inv * a.w_scale;
     const int nD = B.n[D];
     const int idxD = D == 0 ? i : (D == 1 ? j : k);
     const bool leftIn = idxD - 1 >= 0, rightIn = idxD < nD;
@@ -476,71 +482,68 @@ __global__ void adj_decode_back_kernel(AdjArgs a) {
     double gu = gp[4] + gp[5] * gR * a.P.gas.Cvinv / (2.0 * aa);
     double gv0 = gp[1] - gu * v0, gv1 = gp[2] - gu * v1, gv2 = gp[3] - gu * v2;
     double gdinv = gu * U[4] + gv0 * U[1] + gv1 * U[2] + gv2 * U[3];
-    a.gU[0 * a.total + g] = gp[0] - gdinv * dinv * dinv;
-    a.gU[1 * a.total + g] = gv0 * dinv;
-    a.gU[2 * a.total + g] = gv1 * dinv;
-    a.gU[3 * a.total + g] = gv2 * dinv;
-    a.gU[4 * a.total + g] = gu * dinv;
+    const double r[5] = {gp[0] - gdinv * dinv * dinv, gv0 * dinv, gv1 * dinv, gv2 * dinv, gu * dinv};
+    if (a.mode == 0) {
+        for (int q = 0; q < 5; ++q) a.gU[q * a.total + g] = r[q];
+    } else if (a.mode == 1) {
+        // predictor-corrector adjoint, first product: r = mu = J(U1)^T (dt/2 lam)
+        for (int q = 0; q < 5; ++q) {
+            const double l = a.lam[q * a.total + g];
+            a.bbuf[q * a.total + g] = 0.5 * a.dt * l + a.dt * r[q];
+            a.lam[q * a.total + g] = l + r[q];
+        }
+    } else {
+        // second product: r = J(U0)^T b
+        for (int q = 0; q < 5; ++q) a.lam[q * a.total + g] += r[q];
+    }
 }
 
 }  // namespace
-
-// Host view of a context (gdfv_runtime.cu).
-struct AdjView {
-    int prepared, flux, mhd, precision, nblocks, ninflow, dims;
-    long long total;
-    const BlockDesc* d_blocks;
-    const InflowState* d_inflow;
-    NumParams P;
-    cudaStream_t stream;
-    std::vector<BlockDesc> h_blocks;
-    double** scratch;       // context-owned lazily allocated adjoint buffers
-    long long* scratch_n;
-};
-bool adjoint_view(int ctx, AdjView* v);
-void adjoint_set_error(int ctx, const std::string& msg);
 
 }  // namespace gdfv
 
 using namespace gdfv;
 
-extern "C" int gdfv_residual_vjp(int ctx, const double* U_dev, const double* W_dev, double* G_dev,
-                                 double* g_inflow_host) {
-    AdjView v;
-    if (!adjoint_view(ctx, &v)) return GDFV_ERR_ARG;
-    if (!v.prepared) { adjoint_set_error(ctx, "call gdfv_prepare first"); return GDFV_ERR_STATE; }
+namespace {
+
+bool vjp_supported(int ctx, const AdjView& v) {
+    if (!v.prepared) { adjoint_set_error(ctx, "call gdfv_prepare first"); return false; }
     if (v.mhd || v.flux != FLUX_AUSMDV || v.dims != 3) {
-        adjoint_set_error(ctx, "gdfv_residual_vjp supports the 3D Euler path with flux_calculator=ausmdv");
-        return GDFV_ERR_ARG;
+        adjoint_set_error(ctx, "the adjoint supports the 3D Euler path with flux_calculator=ausmdv");
+        return false;
     }
-    if (!U_dev || !W_dev || !G_dev) { adjoint_set_error(ctx, "null pointer"); return GDFV_ERR_ARG; }
+    return true;
+}
+
+// Scratch layout: P [6][total] | gP [6][total] | b [5][total] | face offsets [3][nblocks+1]
+// | inflow cotangents [ninflow][6].  Face offsets are uploaded once per allocation.
+cudaError_t vjp_setup(const AdjView& v, AdjArgs& a, std::vector<long long>& off) {
     const long long total = v.total;
-    // buffers: P [6][total], gP [6][total], face offsets, inflow cotangents
-    const long long need = 12 * total + 3 * (v.nblocks + 1) + 6 * (long long)v.ninflow + 8;
+    const long long need = 17 * total + 3 * (v.nblocks + 1) + 6 * (long long)v.ninflow + 8;
     cudaError_t e = cudaSuccess;
     if (*v.scratch_n < need) {
         if (*v.scratch) cudaFree(*v.scratch);
         *v.scratch = nullptr;
         *v.scratch_n = 0;
+        *v.scratch_ready = 0;
         e = cudaMalloc((void**)v.scratch, sizeof(double) * need);
-        if (e != cudaSuccess) { adjoint_set_error(ctx, cudaGetErrorString(e)); return GDFV_ERR_CUDA; }
+        if (e != cudaSuccess) return e;
         *v.scratch_n = need;
     }
     double* base = *v.scratch;
-    AdjArgs a{};
+    a = AdjArgs{};
     a.blocks = v.d_blocks;
     a.inflow = v.d_inflow;
-    a.U = U_dev;
-    a.W = W_dev;
     a.Pp = base;
     a.gP = base + 6 * total;
-    a.face_off = reinterpret_cast<const long long*>(base + 12 * total);
-    a.gInflow = base + 12 * total + 3 * (v.nblocks + 1);
-    a.gU = G_dev;
+    a.bbuf = base + 12 * total;
+    a.face_off = reinterpret_cast<const long long*>(base + 17 * total);
+    a.gInflow = base + 17 * total + 3 * (v.nblocks + 1);
     a.total = total;
     a.nblocks = v.nblocks;
     a.P = v.P;
-    std::vector<long long> off(3 * (v.nblocks + 1), 0);
+    a.w_scale = 1.0;
+    off.assign(3 * (v.nblocks + 1), 0);
     for (int d = 0; d < 3; ++d) {
         for (int b = 0; b < v.nblocks; ++b) {
             const BlockDesc& B = v.h_blocks[b];
@@ -548,13 +551,20 @@ extern "C" int gdfv_residual_vjp(int ctx, const double* U_dev, const double* W_d
             off[d * (v.nblocks + 1) + b + 1] = off[d * (v.nblocks + 1) + b] + nf;
         }
     }
-    e = cudaMemcpyAsync((void*)a.face_off, off.data(), sizeof(long long) * off.size(), cudaMemcpyHostToDevice, v.stream);
-    if (e == cudaSuccess && v.ninflow > 0) e = cudaMemsetAsync(a.gInflow, 0, sizeof(double) * 6 * v.ninflow, v.stream);
-    const int nt = 256;
-    if (e == cudaSuccess) {
-        adj_decode_kernel<<<(unsigned)((total + nt - 1) / nt), nt, 0, v.stream>>>(a);
-        e = cudaGetLastError();
+    if (!*v.scratch_ready) {
+        e = cudaMemcpy((void*)a.face_off, off.data(), sizeof(long long) * off.size(), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return e;
+        *v.scratch_ready = 1;
     }
+    return cudaSuccess;
+}
+
+// decode, the three face sweeps (cotangents scattered onto gP) and the reverse decode.
+cudaError_t enqueue_vjp(const AdjView& v, const AdjArgs& a, const std::vector<long long>& off) {
+    const int nt = 256;
+    const long long total = v.total;
+    adj_decode_kernel<<<(unsigned)((total + nt - 1) / nt), nt, 0, v.stream>>>(a);
+    cudaError_t e = cudaGetLastError();
     for (int d = 0; d < 3 && e == cudaSuccess; ++d) {
         long long nf = off[d * (v.nblocks + 1) + v.nblocks];
         const unsigned nb = (unsigned)((nf + 127) / 128);  // 128-thread CTAs, 3 per SM by registers
@@ -567,9 +577,60 @@ extern "C" int gdfv_residual_vjp(int ctx, const double* U_dev, const double* W_d
         adj_decode_back_kernel<<<(unsigned)((total + nt - 1) / nt), nt, 0, v.stream>>>(a);
         e = cudaGetLastError();
     }
+    return e;
+}
+
+}  // namespace
+
+extern "C" int gdfv_residual_vjp(int ctx, const double* U_dev, const double* W_dev, double* G_dev,
+                                 double* g_inflow_host) {
+    AdjView v;
+    if (!adjoint_view(ctx, &v)) return GDFV_ERR_ARG;
+    if (!vjp_supported(ctx, v)) return v.prepared ? GDFV_ERR_ARG : GDFV_ERR_STATE;
+    if (!U_dev || !W_dev || !G_dev) { adjoint_set_error(ctx, "null pointer"); return GDFV_ERR_ARG; }
+    AdjArgs a;
+    std::vector<long long> off;
+    cudaError_t e = vjp_setup(v, a, off);
+    a.U = U_dev;
+    a.W = W_dev;
+    a.gU = G_dev;
+    a.mode = 0;
+    if (e == cudaSuccess && v.ninflow > 0) e = cudaMemsetAsync(a.gInflow, 0, sizeof(double) * 6 * v.ninflow, v.stream);
+    if (e == cudaSuccess) e = enqueue_vjp(v, a, off);
     if (e == cudaSuccess && g_inflow_host && v.ninflow > 0)
         e = cudaMemcpyAsync(g_inflow_host, a.gInflow, sizeof(double) * 6 * v.ninflow, cudaMemcpyDeviceToHost, v.stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(v.stream);
+    if (e != cudaSuccess) { adjoint_set_error(ctx, cudaGetErrorString(e)); return GDFV_ERR_CUDA; }
+    return GDFV_OK;
+}
+
+extern "C" int gdfv_step_adjoint(int ctx, const double* U0_dev, const double* U1_dev, double dt, double* lam_dev,
+                                 double* g_inflow_dev) {
+    AdjView v;
+    if (!adjoint_view(ctx, &v)) return GDFV_ERR_ARG;
+    if (!vjp_supported(ctx, v)) return v.prepared ? GDFV_ERR_ARG : GDFV_ERR_STATE;
+    if (!U0_dev || !U1_dev || !lam_dev || (v.ninflow > 0 && !g_inflow_dev) || !(dt > 0.0)) {
+        adjoint_set_error(ctx, "gdfv_step_adjoint needs U0, U1, lam (and g_inflow with inflow faces) and dt > 0");
+        return GDFV_ERR_ARG;
+    }
+    AdjArgs a;
+    std::vector<long long> off;
+    cudaError_t e = vjp_setup(v, a, off);
+    if (v.ninflow > 0) a.gInflow = g_inflow_dev;
+    a.lam = lam_dev;
+    a.dt = dt;
+    // mu = J(U1)^T (dt/2 lam); b = dt/2 lam + dt mu; lam += mu
+    a.U = U1_dev;
+    a.W = lam_dev;
+    a.w_scale = 0.5 * dt;
+    a.mode = 1;
+    if (e == cudaSuccess) e = enqueue_vjp(v, a, off);
+    // lam += J(U0)^T b
+    a.U = U0_dev;
+    a.W = a.bbuf;
+    a.w_scale = 1.0;
+    a.mode = 2;
+    if (e == cudaSuccess) e = enqueue_vjp(v, a, off);
     if (e != cudaSuccess) { adjoint_set_error(ctx, cudaGetErrorString(e)); return GDFV_ERR_CUDA; }
     return GDFV_OK;
 }

@@ -1,0 +1,26 @@
+// Host-side views of a context shared between the translation units of libgdfv.so.
+#pragma once
+#include <string>
+#include <vector>
+#include <cuda_runtime.h>
+#include "gdfv_device.cuh"
+
+namespace gdfv {
+
+// What the adjoint (gdfv_adjoint.cu) needs of a context (gdfv_runtime.cu).
+struct AdjView {
+    int prepared, flux, mhd, precision, nblocks, ninflow, dims;
+    long long total;
+    const BlockDesc* d_blocks;
+    const InflowState* d_inflow;
+    NumParams P;
+    cudaStream_t stream;
+    std::vector<BlockDesc> h_blocks;
+    double** scratch;       // context-owned, lazily allocated adjoint buffers
+    long long* scratch_n;
+    int* scratch_ready;     // 1 once the face offsets in the scratch are uploaded
+};
+bool adjoint_view(int ctx, AdjView* v);
+void adjoint_set_error(int ctx, const std::string& msg);
+
+}  // namespace gdfv

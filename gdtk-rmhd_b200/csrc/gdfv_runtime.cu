@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "../../include/gdfv.h"
+#include "gdfv_internal.h"
 #include "gdfv_launch.h"
 
 namespace gdfv {
@@ -239,6 +240,7 @@ struct Context {
     bool signal_valid = false;
     int n_inflow = 0;
     double* adj_scratch = nullptr;     // adjoint work arrays, allocated on first use
+    int adj_ready = 0;
     long long adj_scratch_n = 0;
     Control* step_ctl = nullptr;       // control record of gdfv_step_dt
     unsigned long long* step_maxsig = nullptr;
@@ -572,19 +574,6 @@ void noalloc_set_error(int ctx, const std::string& msg) {
     else g_err = msg;
 }
 
-// Host view of a context for the adjoint (gdfv_adjoint.cu).
-struct AdjView {
-    int prepared, flux, mhd, precision, nblocks, ninflow, dims;
-    long long total;
-    const BlockDesc* d_blocks;
-    const InflowState* d_inflow;
-    NumParams P;
-    cudaStream_t stream;
-    std::vector<BlockDesc> h_blocks;
-    double** scratch;
-    long long* scratch_n;
-};
-
 bool adjoint_view(int ctx, AdjView* v) {
     Context* c = get_ctx(ctx);
     if (!c || !v) return false;
@@ -603,6 +592,7 @@ bool adjoint_view(int ctx, AdjView* v) {
     v->h_blocks = c->h_blocks;
     v->scratch = &c->adj_scratch;
     v->scratch_n = &c->adj_scratch_n;
+    v->scratch_ready = &c->adj_ready;
     return true;
 }
 
@@ -629,6 +619,12 @@ __global__ void step_dt_begin_kernel(Control* c, unsigned long long* maxsig, int
         c->n_fail = 0; c->n_invalid1 = 0; c->n_invalid2 = 0;
         c->attempt = 0; c->retrying = 0; c->steps_done = 0;
     }
+}
+
+// Sets the dt of the next step of a gdfv_steps_dt chain; failure counts carry over.
+__global__ void step_dt_next_kernel(Control* c, double dt) {
+    c->dt_global = dt;
+    c->step = 0;
 }
 
 }  // namespace gdfv
@@ -1022,6 +1018,56 @@ int gdfv_step_dt(int ctx, const double* U_in_dev, double* U_out_dev, double dt, 
     if (h.n_fail > 0) return fail(c, GDFV_ERR_STEP_FAILED, "gdfv_step_dt: a cell failed to decode");
     if (h.n_invalid1 > c->cfg.max_invalid_cells || h.n_invalid2 > c->cfg.max_invalid_cells)
         return fail(c, GDFV_ERR_BAD_CELLS, "gdfv_step_dt: too many bad cells");
+    return GDFV_OK;
+}
+
+int gdfv_steps_dt(int ctx, const double* U_in_dev, double* const* U_out_dev, double* const* U1_out_dev,
+                  const double* dts, int n) {
+    Context* c = get_ctx(ctx);
+    int st = check_ready(c, -1);
+    if (st) return st;
+    if (!U_in_dev || !U_out_dev || !dts || n < 1)
+        return fail(c, GDFV_ERR_ARG, "gdfv_steps_dt needs U_in, n >= 1 output arrays and their dts");
+    for (int m = 0; m < n; ++m) {
+        const double* src = m == 0 ? U_in_dev : U_out_dev[m - 1];
+        if (!U_out_dev[m] || U_out_dev[m] == src || !(dts[m] > 0.0))
+            return fail(c, GDFV_ERR_ARG, "gdfv_steps_dt: each step needs a distinct output array and dt > 0");
+    }
+    if (!c->step_ctl) {
+        CK(cudaMalloc(&c->step_ctl, sizeof(Control)));
+        CK(cudaMalloc(&c->step_maxsig, sizeof(unsigned long long) * c->blocks.size()));
+        CK(cudaMalloc(&c->step_lastsig, sizeof(double) * c->blocks.size()));
+    }
+    if (read_ctl(c)) return GDFV_ERR_CUDA;
+    StageArgs A = stage_args(c);
+    A.ctl = c->step_ctl;
+    A.max_signal = c->step_maxsig;
+    A.last_signal = c->step_lastsig;
+    const long long nvals = (long long)c->nq * c->total;
+    for (int m = 0; m < n; ++m) {
+        const double* src = m == 0 ? U_in_dev : U_out_dev[m - 1];
+        A.Ubuf[0] = const_cast<double*>(src);
+        A.Ubuf[1] = U_out_dev[m];
+        if (m == 0)
+            step_dt_begin_kernel<<<1, 256, 0, c->stream>>>(c->step_ctl, c->step_maxsig, (int)c->blocks.size(),
+                                                           dts[0], c->h_ctl->c_h);
+        else
+            step_dt_next_kernel<<<1, 1, 0, c->stream>>>(c->step_ctl, dts[m]);
+        CK(cudaGetLastError());
+        CK(launch_stage(c, 1, A));
+        if (U1_out_dev && U1_out_dev[m]) {
+            predictor_state_kernel<<<(unsigned)((nvals + 255) / 256), 256, 0, c->stream>>>(src, c->dU0, dts[m], nvals,
+                                                                                          U1_out_dev[m]);
+            CK(cudaGetLastError());
+        }
+        CK(launch_stage(c, 2, A));
+    }
+    Control h{};
+    CK(cudaMemcpyAsync(&h, c->step_ctl, sizeof(Control), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (h.n_fail > 0) return fail(c, GDFV_ERR_STEP_FAILED, "gdfv_steps_dt: a cell failed to decode");
+    if (h.n_invalid1 > c->cfg.max_invalid_cells || h.n_invalid2 > c->cfg.max_invalid_cells)
+        return fail(c, GDFV_ERR_BAD_CELLS, "gdfv_steps_dt: too many bad cells");
     return GDFV_OK;
 }
 

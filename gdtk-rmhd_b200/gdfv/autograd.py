@@ -5,9 +5,9 @@
   steps of the GPU solver from U0, differentiable in U0 and in the supersonic-
   inflow state theta = (p, T, vel.x).  The forward records each step's dt and
   keeps a copy of the state every `checkpoint_every` steps; the backward
-  recomputes each segment from its checkpoint (gdfv_step_dt, bit-identical to
+  recomputes each segment from its checkpoint (gdfv_steps_dt, bit-identical to
   the forward steps) and applies the adjoint of the predictor-corrector step
-  (e4/simcore_gasdynamic_step.d:1245-1333):
+  (gdfv_step_adjoint; the step is e4/simcore_gasdynamic_step.d:1245-1333):
       U1 = U0 + dt R(U0),  U2 = U0 + dt (R(U0)/2 + R(U1)/2)
       mu  = J(U1)^T (dt/2 lam)
       lam <- lam + mu + J(U0)^T (dt/2 lam + dt mu)
@@ -51,6 +51,24 @@ def step_dt(sim, U, dt, with_predictor=False):
     torch.cuda.current_stream().synchronize()
     check(sim.ctx, sim.L.gdfv_step_dt(sim.ctx, _p(U), _p(out), float(dt), _p(U1) if with_predictor else ffi.NULL))
     return (out, U1) if with_predictor else out
+
+
+def steps_dt(sim, U, dts, outs, preds):
+    """Chain of fixed-dt steps from U: outs[m] after step m, preds[m] its predictor
+    state (one host synchronisation at the end)."""
+    n = len(dts)
+    po = ffi.new("double*[]", [_p(t) for t in outs[:n]])
+    pp = ffi.new("double*[]", [_p(t) for t in preds[:n]])
+    pd = ffi.new("double[]", [float(d) for d in dts])
+    torch.cuda.current_stream().synchronize()
+    check(sim.ctx, sim.L.gdfv_steps_dt(sim.ctx, _p(U.contiguous()), po, pp, pd, n))
+
+
+def step_adjoint(sim, U0, U1, dt, lam, gin):
+    """lam <- (dU2/dU0)^T lam for the predictor-corrector step U0 -> U2 of frozen dt
+    (U1 its predictor state), in place; inflow cotangents added into gin [n_inflow, 6]
+    on the device.  Enqueued without a host synchronisation."""
+    check(sim.ctx, sim.L.gdfv_step_adjoint(sim.ctx, _p(U0), _p(U1), float(dt), _p(lam), _p(gin)))
 
 
 class Residual(torch.autograd.Function):
@@ -108,26 +126,18 @@ class Rollout(torch.autograd.Function):
     def backward(ctx, gUN):
         sim, dts, ckpts, K = ctx.sim, ctx.dts, ctx.ckpts, ctx.k
         lam = gUN.contiguous().clone()
-        gin = None
+        gin = torch.zeros((max(1, getattr(sim, "n_inflow", 1)), 6), dtype=torch.float64, device=lam.device)
         n_total = len(dts)
+        outs = [torch.empty_like(lam) for _ in range(min(K, n_total))]
+        preds = [torch.empty_like(lam) for _ in range(min(K, n_total))]
         for s0 in reversed(range(0, n_total, K)):
             s1 = min(s0 + K, n_total)
-            states, preds = [ckpts[s0]], []
-            for n in range(s0, s1):
-                nxt, U1 = step_dt(sim, states[-1], dts[n], with_predictor=True)
-                preds.append(U1)
-                if n < s1 - 1:
-                    states.append(nxt)
+            steps_dt(sim, ckpts[s0], dts[s0:s1], outs, preds)
             for n in reversed(range(s0, s1)):
-                U0, dt = states[n - s0], dts[n]
-                U1 = preds[n - s0]
-                a = lam * (0.5 * dt)
-                mu, g1 = vjp(sim, U1, a)
-                b = a + mu * dt
-                g0, g0i = vjp(sim, U0, b)
-                lam = lam + mu + g0
-                gin = (g1 + g0i) if gin is None else gin + g1 + g0i
-        gtheta = inflow_chain(sim, ctx.theta, gin[0]).to(ctx.theta.device)
+                U0 = ckpts[s0] if n == s0 else outs[n - s0 - 1]
+                step_adjoint(sim, U0, preds[n - s0], dts[n], lam, gin)
+        torch.cuda.synchronize()
+        gtheta = inflow_chain(sim, ctx.theta, gin[0].cpu()).to(ctx.theta.device)
         return lam, gtheta, None, None, None
 
 

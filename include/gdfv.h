@@ -126,6 +126,25 @@ int gdfv_residual_vjp(int ctx, const double* U_dev, const double* W_dev, double*
  * U1_out_dev (may be NULL) receives the predictor state U1 = U0 + dt R(U0). */
 int gdfv_step_dt(int ctx, const double* U_in_dev, double* U_out_dev, double dt, double* U1_out_dev);
 
+/* n steps of gdfv_step_dt in a chain: step m takes dts[m] from the previous output
+ * (U_in_dev for m = 0) to U_out_dev[m]; U1_out_dev (may be NULL, or hold NULL
+ * entries) receives the predictor states.  The recomputation of one checkpoint
+ * segment, with one host synchronisation at the end; a failed step is reported
+ * then (the steps after it do not write).  No reference counterpart: the
+ * reference has no adjoint of the time-accurate solver. */
+int gdfv_steps_dt(int ctx, const double* U_in_dev, double* const* U_out_dev, double* const* U1_out_dev,
+                  const double* dts, int n);
+
+/* Adjoint of one predictor-corrector step of frozen dt at the states U0 (step start)
+ * and U1 (its predictor state): lam <- lam + mu + (dR/dU(U0))^T (dt/2 lam + dt mu)
+ * with mu = (dR/dU(U1))^T (dt/2 lam), in place on the device array lam [nq][total].
+ * The inflow ghost-state cotangents of both products are added into g_inflow_dev
+ * (device, [n_inflow][6], caller-zeroed).  Enqueued on the context's stream with
+ * no host synchronisation.  Same scope as gdfv_residual_vjp; no reference
+ * counterpart. */
+int gdfv_step_adjoint(int ctx, const double* U0_dev, const double* U1_dev, double dt, double* lam_dev,
+                      double* g_inflow_dev);
+
 /* Device pointer of the current conserved state ([nq][total], borrowed, valid
  * until the next gdfv_run), and of the context's CUDA stream. */
 int gdfv_state_device_ptr(int ctx, double** U_dev);

@@ -154,3 +154,35 @@ def test_rollout_gradients_smooth_configuration():
     derivative is 3e-4) is roundoff in J, not truncation."""
     _rollout_fd_check(dict(apply_limiter=False, extrema_clipping=False), ((1e-6, 1e-4), (1e-7, 2e-5)),
                       ((1e-6, 1e-4), (1e-7, 2e-5)))
+
+
+def test_step_chain_and_fused_step_adjoint():
+    """gdfv_steps_dt equals repeated gdfv_step_dt bit for bit (states and predictor
+    states), and gdfv_step_adjoint equals the predictor-corrector adjoint composed
+    from two gdfv_residual_vjp products, inflow cotangents included."""
+    from gdfv.autograd import step_adjoint, step_dt, steps_dt, vjp
+    case = cases.c2_inflow_box(n=(24, 16, 12), noise_all=True)
+    _, sim = cases.build_pair(case)
+    U0 = torch.from_numpy(sim.get_conserved(0)).cuda()
+    dts = [3.0e-7, 2.5e-7, 3.5e-7]
+    outs = [torch.empty_like(U0) for _ in dts]
+    preds = [torch.empty_like(U0) for _ in dts]
+    steps_dt(sim, U0, dts, outs, preds)
+    U = U0
+    for m, dt in enumerate(dts):
+        nxt, U1 = step_dt(sim, U, dt, with_predictor=True)
+        assert torch.equal(nxt, outs[m]) and torch.equal(U1, preds[m])
+        U = nxt
+    rng = np.random.default_rng(11)
+    lam0 = torch.from_numpy(rng.standard_normal(tuple(U0.shape))).cuda()
+    dt = dts[0]
+    a = lam0 * (0.5 * dt)
+    mu, g1 = vjp(sim, preds[0], a)
+    g0, g0i = vjp(sim, U0, a + mu * dt)
+    want, want_in = lam0 + mu + g0, g1 + g0i
+    lam = lam0.clone()
+    gin = torch.zeros((sim.n_inflow, 6), dtype=torch.float64, device=lam.device)
+    step_adjoint(sim, U0, preds[0], dt, lam, gin)
+    torch.cuda.synchronize()
+    assert torch.allclose(lam, want, rtol=1e-13, atol=1e-13 * float(want.abs().max()))
+    assert np.allclose(gin.cpu().numpy(), want_in.numpy(), rtol=1e-12, atol=1e-12 * float(want_in.abs().max()))
