@@ -8,8 +8,14 @@
 namespace gdfv {
 
 // Rows of cells per column tile (the tile is 32 x TJ columns) of each flux precision.
-constexpr int TJ_FP64 = 4;
-constexpr int TJ_FP32 = 8;
+#ifndef GDFV_TJ_FP64
+#define GDFV_TJ_FP64 4
+#endif
+#ifndef GDFV_TJ_FP32
+#define GDFV_TJ_FP32 8
+#endif
+constexpr int TJ_FP64 = GDFV_TJ_FP64;
+constexpr int TJ_FP32 = GDFV_TJ_FP32;
 
 // Launch one stage (0 = residual only, 1 = predictor, 2 = corrector) over A.n_tiles tiles.
 cudaError_t launch_stage_fp64(int stage, int flux, bool mhd, const StageArgs& A, cudaStream_t s);

@@ -153,9 +153,9 @@ __device__ __forceinline__ void fetch_U(const StageArgs& A, const double* Uin, c
 
 // Decode for the state loader.  FAST (FP32-flux variant): the reciprocal of rho
 // from a float estimate refined by one FP64 Newton step, and a float square root
-// for a, which the float flux arithmetic consumes anyway.
+// for a, which the float flux arithmetic consumes anyway.  gR = gamma*R.
 template <bool FAST, bool MHD>
-__device__ __forceinline__ void decode_prim(const NumParams& P, const double* U, Prim<double>& s) {
+__device__ __forceinline__ void decode_prim_g(double Cvinv, double gR, const double* U, Prim<double>& s) {
     double rho = U[MASS];
     double dinv;
     if (FAST) {
@@ -180,9 +180,14 @@ __device__ __forceinline__ void decode_prim(const NumParams& P, const double* U,
     double ke = 0.5 * (s.v[0] * s.v[0] + s.v[1] * s.v[1] + s.v[2] * s.v[2]);
     u = u - ke;
     s.u = u;
-    double T = u * P.gas.Cvinv;
-    if (FAST) s.a = (double)sqrtf((float)(P.gas.gamma * P.gas.R * T));
-    else s.a = sqrt(P.gas.gamma * P.gas.R * T);
+    double T = u * Cvinv;
+    if (FAST) s.a = (double)sqrtf((float)(gR * T));
+    else s.a = sqrt(gR * T);
+}
+
+template <bool FAST, bool MHD>
+__device__ __forceinline__ void decode_prim(const NumParams& P, const double* U, Prim<double>& s) {
+    decode_prim_g<FAST, MHD>(P.gas.Cvinv, P.gas.gamma * P.gas.R, U, s);
 }
 
 // extrapolate_copy.d:171-201 linearly_extrapolate_flowstate; fields the
@@ -201,18 +206,27 @@ __device__ __forceinline__ void extrapolate(const Prim<double>& f0, const Prim<d
     }
 }
 
-// Finish a ghost/interior state from the decoded source cell; the depth-1 cell of
-// an xOrder=1 extrapolation is fetched here (rare path).
+// Ghost of an xOrder=1 extrapolation from the decoded boundary cell e and the
+// depth-1 cell at global index g1 (rare path, kept out of line).  Everything
+// is passed by value so that no caller state needs an address.
 template <int STAGE, bool FAST, bool MHD, int NQ>
-__device__ __noinline__ void finish_extrap1(const StageArgs& A, const double* Uin, const CellSrc& s, double dt,
-                                            double damp, Prim<double>& out) {
+__device__ __noinline__ Prim<double> extrap1_ghost(const double* Uin, const double* dU0, long long total, long long g1,
+                                                   double dt, double damp, int damp_psi, double Cvinv, double gR,
+                                                   Prim<double> e, int depth0) {
     double U1[NQ];
-    fetch_U<STAGE, NQ>(A, Uin, *s.blk, s.c1, dt, damp, U1);
-    Prim<double> e = out, f1, g0;
-    decode_prim<FAST, MHD>(A.P, U1, f1);
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) U1[q] = __ldg(Uin + (long long)q * total + g1);
+    if (STAGE == 2) {
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) U1[q] = d_add(U1[q], d_mul(dt, __ldg(dU0 + (long long)q * total + g1)));
+        if (NQ == 10 && damp_psi) U1[PSI] = d_mul(U1[PSI], damp);
+    }
+    Prim<double> f1, g0, out;
+    decode_prim_g<FAST, MHD>(Cvinv, gR, U1, f1);
     extrapolate<MHD>(f1, e, e, g0);
-    if (s.kind == SRC_EXTRAP1_G0) out = g0;
-    else extrapolate<MHD>(e, g0, e, out);
+    if (depth0) return g0;
+    extrapolate<MHD>(e, g0, e, out);
+    return out;
 }
 
 template <int STAGE, bool FAST, bool MHD, int NQ>
@@ -244,7 +258,9 @@ __device__ __forceinline__ void finish_cell(const StageArgs& A, const double* Ui
             }
         }
     } else if (s.kind == SRC_EXTRAP1_G0 || s.kind == SRC_EXTRAP1_G1) {
-        finish_extrap1<STAGE, FAST, MHD, NQ>(A, Uin, s, dt, damp, out);
+        out = extrap1_ghost<STAGE, FAST, MHD, NQ>(Uin, A.dU0, A.total, s.blk->offset + s.c1, dt, damp,
+                                                  A.P.divergence_cleaning, A.P.gas.Cvinv, A.P.gas.gamma * A.P.gas.R,
+                                                  out, s.kind == SRC_EXTRAP1_G0);
     }
 }
 
@@ -421,8 +437,13 @@ __device__ __forceinline__ void load_pair(const StageArgs& A, const double* Uin,
 }
 
 // STAGE 0: residual only (R_out = dUdt of U_in).  STAGE 1/2: predictor / corrector.
+// Resident CTAs per SM the FP32 Euler kernels are compiled for (register budget).
+#ifndef GDFV_MINB_FP32
+#define GDFV_MINB_FP32 2
+#endif
+
 template <int STAGE, class R, bool MHD, int FLUX, int TJ, int OPT>
-__global__ void __launch_bounds__(32 * (TJ + 1), (sizeof(R) == 4 && !MHD) ? 2 : 1) stage_kernel(StageArgs A) {
+__global__ void __launch_bounds__(32 * (TJ + 1), (sizeof(R) == 4 && !MHD) ? GDFV_MINB_FP32 : 1) stage_kernel(StageArgs A) {
     using G = Geo<R, MHD, TJ>;
     constexpr int TI = G::TI, NT = G::NT, NCOL = G::NCOL, PW = G::PW, PLANE = G::PLANE;
     constexpr int NPV = G::NPV, NRS = G::NRS, NQ = G::NQ;

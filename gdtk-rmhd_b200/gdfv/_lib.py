@@ -13,7 +13,8 @@ from cffi import FFI
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _REPO = os.path.dirname(os.path.dirname(_HERE))
 HEADER = os.path.join(_REPO, "include", "gdfv.h")
-LIBPATH = os.path.join(_HERE, "libgdfv.so")
+# GDFV_LIBRARY selects another build of the same library (e.g. other tile sizes)
+LIBPATH = os.environ.get("GDFV_LIBRARY") or os.path.join(_HERE, "libgdfv.so")
 
 GDFV_OK = 0
 GDFV_ERR_ARG = -1
