@@ -326,45 +326,69 @@ __device__ __forceinline__ float clip_fast(float q, float A, float B) {
 // the cell's minus face (right state there), qp[s]: at its plus face (left state).
 // psi is reconstructed only with divergence cleaning (onedinterp.d:783-786).
 // OPT = 1: apply_limiter and extrema_clipping known to be on (the defaults).
+// The float path with OPT = 1 works on raw differences a = q0-qm1, b = qp1-q0
+// with the length factors folded into per-direction constants wf (the same
+// expressions: dm = a*t, dp = b*t, so the limiter is (ab+|ab|+eps/t^2)/(a^2+b^2+eps/t^2)).
+enum : int { WF_EPS = 0, WF_P1, WF_P2, WF_R1, WF_R2, WF_N };
 template <class R, int NRS, bool MHD, int OPT>
-__device__ __forceinline__ void recon_cell(const R* w, const NumParams& P, const R* qm1, const R* q0, const R* qp1,
-                                           R* qm, R* qp) {
-    const R t = w[W_TOC];
-    const R aL0 = w[W_AL0], aR0 = w[W_AR0], len = w[W_LENL0], w3 = w[W_TWOL];
-    const bool lim = OPT == 1 ? true : (bool)P.apply_limiter;
-    const bool clip = OPT == 1 ? true : (bool)P.extrema_clipping;
-    const R eps = R(P.eps_van_albada);
+__device__ __forceinline__ void recon_cell(const R* w, const R* wf, const NumParams& P, const R* qm1, const R* q0,
+                                           const R* qp1, R* qm, R* qp) {
+    if constexpr (sizeof(R) == 4 && OPT == 1) {
+        const R e = wf[WF_EPS], P1 = wf[WF_P1], P2 = wf[WF_P2], R1 = wf[WF_R1], R2 = wf[WF_R2];
 #pragma unroll
-    for (int s = 0; s < NRS; ++s) {
-        if (MHD && s == 8 && !P.divergence_cleaning) { qm[s] = q0[s]; qp[s] = q0[s]; continue; }
-        R dm = (q0[s] - qm1[s]) * t;
-        R dp = (qp1[s] - q0[s]) * t;
-        R sl = R(1.0);
-        if (lim) sl = (dm * dp + rabs(dm * dp) + eps) / (dm * dm + dp * dp + eps);
-        R vp = q0[s] + sl * aL0 * (dp * w3 + dm * len);
-        R vm = q0[s] - sl * aR0 * (dp * len + dm * w3);
-        if (clip) {
-            vp = clip_fast(vp, q0[s], qp1[s]);
-            vm = clip_fast(vm, qm1[s], q0[s]);
+        for (int s = 0; s < NRS; ++s) {
+            if (MHD && s == 8 && !P.divergence_cleaning) { qm[s] = q0[s]; qp[s] = q0[s]; continue; }
+            const R a = q0[s] - qm1[s];
+            const R b = qp1[s] - q0[s];
+            const R ab = a * b;
+            const R sl = (ab + rabs(ab) + e) / (a * a + b * b + e);
+            const R vp = q0[s] + sl * (P1 * b + P2 * a);
+            const R vm = q0[s] - sl * (R1 * b + R2 * a);
+            qp[s] = clip_fast(vp, q0[s], qp1[s]);
+            qm[s] = clip_fast(vm, qm1[s], q0[s]);
         }
-        qp[s] = vp;
-        qm[s] = vm;
+    } else {
+        const R t = w[W_TOC];
+        const R aL0 = w[W_AL0], aR0 = w[W_AR0], len = w[W_LENL0], w3 = w[W_TWOL];
+        const bool lim = OPT == 1 ? true : (bool)P.apply_limiter;
+        const bool clip = OPT == 1 ? true : (bool)P.extrema_clipping;
+        const R eps = R(P.eps_van_albada);
+#pragma unroll
+        for (int s = 0; s < NRS; ++s) {
+            if (MHD && s == 8 && !P.divergence_cleaning) { qm[s] = q0[s]; qp[s] = q0[s]; continue; }
+            R dm = (q0[s] - qm1[s]) * t;
+            R dp = (qp1[s] - q0[s]) * t;
+            R sl = R(1.0);
+            if (lim) sl = (dm * dp + rabs(dm * dp) + eps) / (dm * dm + dp * dp + eps);
+            R vp = q0[s] + sl * aL0 * (dp * w3 + dm * len);
+            R vm = q0[s] - sl * aR0 * (dp * len + dm * w3);
+            if (clip) {
+                vp = clip_fast(vp, q0[s], qp1[s]);
+                vm = clip_fast(vm, qm1[s], q0[s]);
+            }
+            qp[s] = vp;
+            qm[s] = vm;
+        }
     }
 }
 
 // Interface flux from reconstructed left/right scalars (face-local frame)
-// plus the centre states of the two adjacent cells for the EOS fallback
-// (e4/onedinterp.d:44-74) and the sound speed (the rhou update keeps it).
+// plus the centre states of the two adjacent cells (prim arrays pl/pr, entries
+// il/ir, variable stride `stride`): their sound speed is kept (the rhou update
+// does not change it) and their full state is the EOS fallback
+// (e4/onedinterp.d:44-74), read only when a reconstructed state fails.
 // Then compute_interface_flux_interior (e4/fluxcalc.d:54-187) for a fixed grid.
 // Fg receives the flux in the global frame.
-template <class R, bool MHD, int FLUX, int D>
-__device__ __forceinline__ void face_flux(const NumParams& P, R c_h, const R* qL, const R* qR,
-                                          const CellR<R>& cL, const CellR<R>& cR, R* Fg) {
+template <class R, bool MHD, int FLUX, int D, int NPV>
+__device__ __forceinline__ void face_flux(const NumParams& P, R c_h, const R* qL, const R* qR, const R* pl, int il,
+                                          const R* pr, int ir, int stride, R* Fg) {
     constexpr int NQ = MHD ? 10 : 5;
     constexpr int ax[3] = {D, (D + 1) % 3, (D + 2) % 3};
     const R Rg = R(P.gas.R), Cvinv = R(P.gas.Cvinv);
     FaceState<R> L, Rr;
     if (qL[4] <= R(0.0) || qL[3] <= R(0.0)) {
+        CellR<R> cL;
+        get_prim<R, NPV>(pl, stride, il, cL);
         L.rho = cL.rho; L.u = cL.u; L.p = cL.rho * Rg * (cL.u * Cvinv); L.psi = cL.psi;
 #pragma unroll
         for (int m = 0; m < 3; ++m) { L.v[m] = cL.v[ax[m]]; L.B[m] = cL.B[ax[m]]; }
@@ -375,6 +399,8 @@ __device__ __forceinline__ void face_flux(const NumParams& P, R c_h, const R* qL
         L.psi = MHD ? qL[8] : R(0);
     }
     if (qR[4] <= R(0.0) || qR[3] <= R(0.0)) {
+        CellR<R> cR;
+        get_prim<R, NPV>(pr, stride, ir, cR);
         Rr.rho = cR.rho; Rr.u = cR.u; Rr.p = cR.rho * Rg * (cR.u * Cvinv); Rr.psi = cR.psi;
 #pragma unroll
         for (int m = 0; m < 3; ++m) { Rr.v[m] = cR.v[ax[m]]; Rr.B[m] = cR.B[ax[m]]; }
@@ -384,8 +410,8 @@ __device__ __forceinline__ void face_flux(const NumParams& P, R c_h, const R* qL
         for (int m = 0; m < 3; ++m) { Rr.v[m] = qR[m]; Rr.B[m] = MHD ? qR[5 + m] : R(0); }
         Rr.psi = MHD ? qR[8] : R(0);
     }
-    L.a = cL.a;
-    Rr.a = cR.a;
+    L.a = pl[5 * stride + il];
+    Rr.a = pr[5 * stride + ir];
     R F[NQ];
     if (FLUX == FLUX_AUSMDV) ausmdv(P, L, Rr, F);
     else if (FLUX == FLUX_HLLC) hllc(P, L, Rr, F);
@@ -415,28 +441,28 @@ __device__ __forceinline__ void face_flux(const NumParams& P, R c_h, const R* qL
     }
 }
 
-// Load the state of up to two cells per thread: resolve, issue every global
-// load, then decode (keeps the loads in flight together).
+// Load the state of up to two cells per thread (on[m] says which): resolve, issue
+// every global load, then decode (keeps the loads in flight together).
 template <int STAGE, bool FAST, bool MHD, int NQ>
-__device__ __forceinline__ void load_pair(const StageArgs& A, const double* Uin, const BlockDesc& B, double dt,
-                                          double damp, int n, const int* ci, const int* cj, const int* ck,
-                                          Prim<double>* out) {
+__device__ __forceinline__ void load_two(const StageArgs& A, const double* Uin, const BlockDesc& B, double dt,
+                                         double damp, bool on0, bool on1, const int* ci, const int* cj, const int* ck,
+                                         Prim<double>* out) {
     CellSrc s[2];
     double U0[2][NQ];
+    const bool on[2] = {on0, on1};
 #pragma unroll
     for (int m = 0; m < 2; ++m) {
-        if (m < n) {
+        if (on[m]) {
             s[m] = resolve(A, B, ci[m], cj[m], ck[m]);
             if (s[m].kind != SRC_INFLOW) fetch_U<STAGE, NQ>(A, Uin, *s[m].blk, s[m].c0, dt, damp, U0[m]);
         }
     }
 #pragma unroll
     for (int m = 0; m < 2; ++m) {
-        if (m < n) finish_cell<STAGE, FAST, MHD, NQ>(A, Uin, s[m], U0[m], ci[m], cj[m], dt, damp, out[m]);
+        if (on[m]) finish_cell<STAGE, FAST, MHD, NQ>(A, Uin, s[m], U0[m], ci[m], cj[m], dt, damp, out[m]);
     }
 }
 
-// STAGE 0: residual only (R_out = dUdt of U_in).  STAGE 1/2: predictor / corrector.
 // Resident CTAs per SM the FP32 Euler kernels are compiled for (register budget).
 #ifndef GDFV_MINB_FP32
 #define GDFV_MINB_FP32 2
@@ -458,6 +484,7 @@ __global__ void __launch_bounds__(32 * (TJ + 1), (sizeof(R) == 4 && !MHD) ? GDFV
     R* FJ = sm + G::O_FJ;       // [NQ][NFJ]
     __shared__ double s_red[NT / 32];
     __shared__ R w[3][W_N];
+    __shared__ R wf[3][WF_N];
 
     const Control* ctl = A.ctl;
     int parity = 0;
@@ -492,6 +519,15 @@ __global__ void __launch_bounds__(32 * (TJ + 1), (sizeof(R) == 4 && !MHD) ? GDFV
     const int pidx = (ti + 2) + PW * (tj + 2);     // own cell in a padded plane
     const bool has_k = (P.dims == 3);
     if (tid < 3 * W_N) w[tid / W_N][tid % W_N] = (R)B.w[tid / W_N][tid % W_N];
+    if (tid < 3) {
+        const double* bw = B.w[tid];
+        const double tc = bw[W_TOC];
+        wf[tid][WF_EPS] = (R)(P.eps_van_albada / (tc * tc));
+        wf[tid][WF_P1] = (R)(bw[W_AL0] * tc * bw[W_TWOL]);
+        wf[tid][WF_P2] = (R)(bw[W_AL0] * tc * bw[W_LENL0]);
+        wf[tid][WF_R1] = (R)(bw[W_AR0] * tc * bw[W_LENL0]);
+        wf[tid][WF_R2] = (R)(bw[W_AR0] * tc * bw[W_TWOL]);
+    }
     const R c_hR = (R)c_h;
     __syncthreads();
 
@@ -510,31 +546,29 @@ __global__ void __launch_bounds__(32 * (TJ + 1), (sizeof(R) == 4 && !MHD) ? GDFV
         if (active) {
             Prim<double> pr[2];
             int ck[2] = {t.k0 - 2, t.k0 - 1};
-            load_pair<STAGE, FAST, MHD, NQ>(A, Uin, B, dt, damp, 2, ci, cj, ck, pr);
+            load_two<STAGE, FAST, MHD, NQ>(A, Uin, B, dt, damp, true, true, ci, cj, ck, pr);
             put_prim<R, NPV>(slot(t.k0 - 2), PLANE, pidx, pr[0]);
             put_prim<R, NPV>(slot(t.k0 - 1), PLANE, pidx, pr[1]);
             int ck2[2] = {t.k0, 0};
-            load_pair<STAGE, FAST, MHD, NQ>(A, Uin, B, dt, damp, 1, ci, cj, ck2, pr);
+            load_two<STAGE, FAST, MHD, NQ>(A, Uin, B, dt, damp, true, false, ci, cj, ck2, pr);
             put_prim<R, NPV>(slot(t.k0), PLANE, pidx, pr[0]);
             // q+ of plane k0-1 (left state of face k0-1/2); own column only
             R qm1[NRS], q0[NRS], qp1[NRS], qm[NRS];
             gather<R, NRS, 2>(slot(t.k0 - 2), PLANE, pidx, qm1);
             gather<R, NRS, 2>(slot(t.k0 - 1), PLANE, pidx, q0);
             gather<R, NRS, 2>(slot(t.k0), PLANE, pidx, qp1);
-            recon_cell<R, NRS, MHD, OPT>(w[2], P, qm1, q0, qp1, qm, kq_prev_p);
+            recon_cell<R, NRS, MHD, OPT>(w[2], wf[2], P, qm1, q0, qp1, qm, kq_prev_p);
             // plane k0+1 replaces k0-2 in the ring
             int ck3[2] = {t.k0 + 1, 0};
-            load_pair<STAGE, FAST, MHD, NQ>(A, Uin, B, dt, damp, 1, ci, cj, ck3, pr);
+            load_two<STAGE, FAST, MHD, NQ>(A, Uin, B, dt, damp, true, false, ci, cj, ck3, pr);
             put_prim<R, NPV>(slot(t.k0 + 1), PLANE, pidx, pr[0]);
             R qkm[NRS], qkp[NRS];
             gather<R, NRS, 2>(slot(t.k0 - 1), PLANE, pidx, qm1);
             gather<R, NRS, 2>(slot(t.k0), PLANE, pidx, q0);
             gather<R, NRS, 2>(slot(t.k0 + 1), PLANE, pidx, qp1);
-            recon_cell<R, NRS, MHD, OPT>(w[2], P, qm1, q0, qp1, qkm, qkp);
-            CellR<R> cL, cR;
-            get_prim<R, NPV>(slot(t.k0 - 1), PLANE, pidx, cL);
-            get_prim<R, NPV>(slot(t.k0), PLANE, pidx, cR);
-            face_flux<R, MHD, FLUX, 2>(P, c_hR, kq_prev_p, qkm, cL, cR, fB);
+            recon_cell<R, NRS, MHD, OPT>(w[2], wf[2], P, qm1, q0, qp1, qkm, qkp);
+            face_flux<R, MHD, FLUX, 2, NPV>(P, c_hR, kq_prev_p, qkm, slot(t.k0 - 1), pidx, slot(t.k0), pidx, PLANE,
+                                            fB);
 #pragma unroll
             for (int s = 0; s < NRS; ++s) kq_prev_p[s] = qkp[s];
         }
@@ -542,14 +576,37 @@ __global__ void __launch_bounds__(32 * (TJ + 1), (sizeof(R) == 4 && !MHD) ? GDFV
         if (active) {
             int ci[2] = {t.i0 + ti, 0}, cj[2] = {t.j0 + tj, 0}, ck[2] = {t.k0, 0};
             Prim<double> pr[2];
-            load_pair<STAGE, FAST, MHD, NQ>(A, Uin, B, dt, damp, 1, ci, cj, ck, pr);
+            load_two<STAGE, FAST, MHD, NQ>(A, Uin, B, dt, damp, true, false, ci, cj, ck, pr);
             put_prim<R, NPV>(slot(t.k0), PLANE, pidx, pr[0]);
         }
     }
 
     double sig_max = 0.0;
     const double Ai = B.area[0], Aj = B.area[1], Ak = B.area[2];
+    // halo cell of this thread in every plane (4 columns beside, 4 rows above/below
+    // the tile; the extra warp takes items 0..31); the same for all planes
     const int nh = 4 * nj_t + 4 * ni_t;
+    const int h = owner ? tid + 32 : tid - NCOL;
+    const bool h_on = h < nh;
+    int h_ci = 0, h_cj = 0, h_dst = 0;
+    if (h_on) {
+        int hi, hj;
+        if (h < 4 * nj_t) {
+            int side = h / (2 * nj_t), rem = h % (2 * nj_t);
+            int col = rem / nj_t, row = rem % nj_t;
+            hi = side == 0 ? col - 2 : ni_t + col;
+            hj = row;
+        } else {
+            int h2 = h - 4 * nj_t;
+            int side = h2 / (2 * ni_t), rem = h2 % (2 * ni_t);
+            int row = rem / ni_t, col = rem % ni_t;
+            hj = side == 0 ? row - 2 : nj_t + row;
+            hi = col;
+        }
+        h_ci = t.i0 + hi;
+        h_cj = t.j0 + hj;
+        h_dst = (hi + 2) + PW * (hj + 2);
+    }
     const int f0 = owner ? G::EXTRA + tid : tid - NCOL;   // flat-list start and stride
     const int fstride = owner ? NCOL : 32;
     const int fend = owner ? 0x7fffffff : G::EXTRA;
@@ -558,34 +615,13 @@ __global__ void __launch_bounds__(32 * (TJ + 1), (sizeof(R) == 4 && !MHD) ? GDFV
         R* cur = slot(k);
         // ---------------- phase A: leading plane k+2 (owners) and the halo of plane k
         {
-            int ci[2], cj[2], ck[2], dst[2];
-            R* dplane[2];
-            int n = 0;
-            if (active && has_k) {
-                ci[n] = t.i0 + ti; cj[n] = t.j0 + tj; ck[n] = k + 2; dst[n] = pidx; dplane[n] = slot(k + 2); ++n;
-            }
-            const int h = owner ? tid + 32 : tid - NCOL;   // the extra warp takes halo items 0..31
-            if (h < nh) {
-                int hi, hj;
-                if (h < 4 * nj_t) {
-                    int side = h / (2 * nj_t), rem = h % (2 * nj_t);
-                    int col = rem / nj_t, row = rem % nj_t;
-                    hi = side == 0 ? col - 2 : ni_t + col;
-                    hj = row;
-                } else {
-                    int h2 = h - 4 * nj_t;
-                    int side = h2 / (2 * ni_t), rem = h2 % (2 * ni_t);
-                    int row = rem / ni_t, col = rem % ni_t;
-                    hj = side == 0 ? row - 2 : nj_t + row;
-                    hi = col;
-                }
-                ci[n] = t.i0 + hi; cj[n] = t.j0 + hj; ck[n] = k; dst[n] = (hi + 2) + PW * (hj + 2); dplane[n] = cur; ++n;
-            }
-            if (n > 0) {
+            const bool lead = active && has_k;
+            int ci[2] = {t.i0 + ti, h_ci}, cj[2] = {t.j0 + tj, h_cj}, ck[2] = {k + 2, k};
+            if (lead || h_on) {
                 Prim<double> pr[2];
-                load_pair<STAGE, FAST, MHD, NQ>(A, Uin, B, dt, damp, n, ci, cj, ck, pr);
-                put_prim<R, NPV>(dplane[0], PLANE, dst[0], pr[0]);
-                if (n > 1) put_prim<R, NPV>(dplane[1], PLANE, dst[1], pr[1]);
+                load_two<STAGE, FAST, MHD, NQ>(A, Uin, B, dt, damp, lead, h_on, ci, cj, ck, pr);
+                if (lead) put_prim<R, NPV>(slot(k + 2), PLANE, pidx, pr[0]);
+                if (h_on) put_prim<R, NPV>(cur, PLANE, h_dst, pr[1]);
             }
         }
         __syncthreads();
@@ -597,7 +633,7 @@ __global__ void __launch_bounds__(32 * (TJ + 1), (sizeof(R) == 4 && !MHD) ? GDFV
             gather<R, NRS, 2>(cur, PLANE, pidx, qm1);
             gather<R, NRS, 2>(slot(k + 1), PLANE, pidx, q0);
             gather<R, NRS, 2>(slot(k + 2), PLANE, pidx, qp1);
-            recon_cell<R, NRS, MHD, OPT>(w[2], P, qm1, q0, qp1, kq_m, kq_p);
+            recon_cell<R, NRS, MHD, OPT>(w[2], wf[2], P, qm1, q0, qp1, kq_m, kq_p);
         }
         for (int f = f0; f < NRI + NRJ && f < fend; f += fstride) {
             R qm1[NRS], q0[NRS], qp1[NRS], qm[NRS], qp[NRS];
@@ -608,7 +644,7 @@ __global__ void __launch_bounds__(32 * (TJ + 1), (sizeof(R) == 4 && !MHD) ? GDFV
                 gather<R, NRS, 0>(cur, PLANE, p - 1, qm1);
                 gather<R, NRS, 0>(cur, PLANE, p, q0);
                 gather<R, NRS, 0>(cur, PLANE, p + 1, qp1);
-                recon_cell<R, NRS, MHD, OPT>(w[0], P, qm1, q0, qp1, qm, qp);
+                recon_cell<R, NRS, MHD, OPT>(w[0], wf[0], P, qm1, q0, qp1, qm, qp);
 #pragma unroll
                 for (int s = 0; s < NRS; ++s) { RI[s * NRI + f] = qm[s]; RI[(NRS + s) * NRI + f] = qp[s]; }
             } else {
@@ -619,7 +655,7 @@ __global__ void __launch_bounds__(32 * (TJ + 1), (sizeof(R) == 4 && !MHD) ? GDFV
                 gather<R, NRS, 1>(cur, PLANE, p - PW, qm1);
                 gather<R, NRS, 1>(cur, PLANE, p, q0);
                 gather<R, NRS, 1>(cur, PLANE, p + PW, qp1);
-                recon_cell<R, NRS, MHD, OPT>(w[1], P, qm1, q0, qp1, qm, qp);
+                recon_cell<R, NRS, MHD, OPT>(w[1], wf[1], P, qm1, q0, qp1, qm, qp);
 #pragma unroll
                 for (int s = 0; s < NRS; ++s) { RJ[s * NRJ + g] = qm[s]; RJ[(NRS + s) * NRJ + g] = qp[s]; }
             }
@@ -631,16 +667,12 @@ __global__ void __launch_bounds__(32 * (TJ + 1), (sizeof(R) == 4 && !MHD) ? GDFV
 #pragma unroll
         for (int q = 0; q < NQ; ++q) fT[q] = R(0);
         if (active && has_k) {
-            CellR<R> cL, cR;
-            get_prim<R, NPV>(cur, PLANE, pidx, cL);
-            get_prim<R, NPV>(slot(k + 1), PLANE, pidx, cR);
-            face_flux<R, MHD, FLUX, 2>(P, c_hR, kq_prev_p, kq_m, cL, cR, fT);
+            face_flux<R, MHD, FLUX, 2, NPV>(P, c_hR, kq_prev_p, kq_m, cur, pidx, slot(k + 1), pidx, PLANE, fT);
 #pragma unroll
             for (int s = 0; s < NRS; ++s) kq_prev_p[s] = kq_p[s];
         }
         for (int f = f0; f < NFI + NFJ && f < fend; f += fstride) {
             R qL[NRS], qR[NRS], F[NQ];
-            CellR<R> cL, cR;
             if (f < NFI) {
                 const int row = f / (TI + 1), fi = f % (TI + 1);       // faces 0..TI
                 if (row >= nj_t || fi > ni_t) continue;
@@ -648,9 +680,7 @@ __global__ void __launch_bounds__(32 * (TJ + 1), (sizeof(R) == 4 && !MHD) ? GDFV
 #pragma unroll
                 for (int s = 0; s < NRS; ++s) { qL[s] = RI[(NRS + s) * NRI + rl]; qR[s] = RI[s * NRI + rl + 1]; }
                 const int p = (fi + 2) + PW * (row + 2);
-                get_prim<R, NPV>(cur, PLANE, p - 1, cL);
-                get_prim<R, NPV>(cur, PLANE, p, cR);
-                face_flux<R, MHD, FLUX, 0>(P, c_hR, qL, qR, cL, cR, F);
+                face_flux<R, MHD, FLUX, 0, NPV>(P, c_hR, qL, qR, cur, p - 1, cur, p, PLANE, F);
 #pragma unroll
                 for (int q = 0; q < NQ; ++q) FI[q * NFI + f] = F[q];
             } else {
@@ -661,9 +691,7 @@ __global__ void __launch_bounds__(32 * (TJ + 1), (sizeof(R) == 4 && !MHD) ? GDFV
 #pragma unroll
                 for (int s = 0; s < NRS; ++s) { qL[s] = RJ[(NRS + s) * NRJ + rl]; qR[s] = RJ[s * NRJ + rl + TI]; }
                 const int p = (col + 2) + PW * (fj + 2);
-                get_prim<R, NPV>(cur, PLANE, p - PW, cL);
-                get_prim<R, NPV>(cur, PLANE, p, cR);
-                face_flux<R, MHD, FLUX, 1>(P, c_hR, qL, qR, cL, cR, F);
+                face_flux<R, MHD, FLUX, 1, NPV>(P, c_hR, qL, qR, cur, p - PW, cur, p, PLANE, F);
 #pragma unroll
                 for (int q = 0; q < NQ; ++q) FJ[q * NFJ + g] = F[q];
             }
