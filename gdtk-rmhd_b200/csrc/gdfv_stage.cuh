@@ -372,6 +372,68 @@ __device__ __forceinline__ void recon_cell(const R* w, const R* wf, const NumPar
     }
 }
 
+// AUSMDV (e4/fluxcalc.d:477-651) for the float-flux ideal-gas variant.  The
+// ideal-gas identities p/rho = (gamma-1) e and H = e + p/rho + ke = gamma e + ke
+// replace the divisions of the general form: alpha = 2 e_L/(e_L + e_R), the
+// supersonic pressure split p*du/u is p or 0 by the sign of u.  Velocity
+// components are face-local (normal, tangent 1, tangent 2).
+__device__ __forceinline__ void ausmdv_f(float g, float gm1, bool efix, float rL, float uL, float vL, float wL,
+                                         float eL, float aL, float rR, float uR, float vR, float wR, float eR, float aR,
+                                         float* F) {
+    const float pL = rL * (gm1 * eL), pR = rR * (gm1 * eR);
+    const float keL = 0.5f * (uL * uL + vL * vL + wL * wL);
+    const float keR = 0.5f * (uR * uR + vR * vR + wR * wR);
+    const float HL = g * eL + keL, HR = g * eR + keR;
+    const float isum = 1.0f / (eL + eR);
+    const float alphaL = 2.0f * eL * isum, alphaR = 2.0f * eR * isum;
+    const float am = fmaxf(aL, aR), iam = 1.0f / am;
+    const float ML = uL * iam, MR = uR * iam;
+    const float duL = 0.5f * (uL + fabsf(uL)), duR = 0.5f * (uR - fabsf(uR));
+    float pLplus, uLplus, pRminus, uRminus;
+    if (fabsf(ML) <= 1.0f) {
+        pLplus = pL * (ML + 1.0f) * (ML + 1.0f) * (2.0f - ML) * 0.25f;
+        uLplus = alphaL * ((uL + am) * (uL + am) * (0.25f * iam) - duL) + duL;
+    } else {
+        pLplus = uL > 0.0f ? pL : 0.0f;
+        uLplus = duL;
+    }
+    if (fabsf(MR) <= 1.0f) {
+        pRminus = pR * (MR - 1.0f) * (MR - 1.0f) * (2.0f + MR) * 0.25f;
+        uRminus = alphaR * (-(uR - am) * (uR - am) * (0.25f * iam) - duR) + duR;
+    } else {
+        pRminus = uR < 0.0f ? pR : 0.0f;
+        uRminus = duR;
+    }
+    const float ru_half = uLplus * rL + uRminus * rR;
+    const float p_half = pLplus + pRminus;
+    const float dp = 10.0f * fabsf(pL - pR) / fminf(pL, pR);
+    const float sw = 0.5f * fminf(1.0f, dp);
+    const float ru2_AUSMV = uLplus * rL * uL + uRminus * rR * uR;
+    const float ru2_AUSMD = 0.5f * (ru_half * (uL + uR) - fabsf(ru_half) * (uR - uL));
+    const float ru2_half = (0.5f + sw) * ru2_AUSMV + (0.5f - sw) * ru2_AUSMD;
+    const bool up = ru_half >= 0.0f;
+    F[0] = ru_half;
+    F[1] = ru2_half + p_half;
+    F[2] = ru_half * (up ? vL : vR);
+    F[3] = ru_half * (up ? wL : wR);
+    F[4] = ru_half * (up ? HL : HR);
+    if (efix) {
+        const float C_EFIX = 0.125f;
+        const bool caseA = ((uL - aL) < 0.0f) && ((uR - aR) > 0.0f);
+        const bool caseB = ((uL + aL) < 0.0f) && ((uR + aR) > 0.0f);
+        float d_ua = 0.0f;
+        if (caseA && !caseB) d_ua = C_EFIX * ((uR - aR) - (uL - aL));
+        if (caseB && !caseA) d_ua = C_EFIX * ((uR + aR) - (uL + aL));
+        if (d_ua != 0.0f) {
+            F[0] -= d_ua * (rR - rL);
+            F[1] -= d_ua * (rR * uR - rL * uL);
+            F[2] -= d_ua * (rR * vR - rL * vL);
+            F[3] -= d_ua * (rR * wR - rL * wL);
+            F[4] -= d_ua * (rR * HR - rL * HL);
+        }
+    }
+}
+
 // Interface flux from reconstructed left/right scalars (face-local frame)
 // plus the centre states of the two adjacent cells (prim arrays pl/pr, entries
 // il/ir, variable stride `stride`): their sound speed is kept (the rhou update
@@ -384,6 +446,27 @@ __device__ __forceinline__ void face_flux(const NumParams& P, R c_h, const R* qL
                                           const R* pr, int ir, int stride, R* Fg) {
     constexpr int NQ = MHD ? 10 : 5;
     constexpr int ax[3] = {D, (D + 1) % 3, (D + 2) % 3};
+    if constexpr (sizeof(R) == 4 && !MHD && FLUX == FLUX_AUSMDV) {
+        float rL = qL[3], uL = qL[0], vL = qL[1], wL = qL[2], eL = qL[4];
+        float rR = qR[3], uR = qR[0], vR = qR[1], wR = qR[2], eR = qR[4];
+        if (eL <= 0.0f || rL <= 0.0f) {   // e4/onedinterp.d:44-74: the cell-centre state
+            rL = pl[il]; uL = pl[(1 + ax[0]) * stride + il]; vL = pl[(1 + ax[1]) * stride + il];
+            wL = pl[(1 + ax[2]) * stride + il]; eL = pl[4 * stride + il];
+        }
+        if (eR <= 0.0f || rR <= 0.0f) {
+            rR = pr[ir]; uR = pr[(1 + ax[0]) * stride + ir]; vR = pr[(1 + ax[1]) * stride + ir];
+            wR = pr[(1 + ax[2]) * stride + ir]; eR = pr[4 * stride + ir];
+        }
+        const float g = (float)P.gas.gamma;
+        float F[5];
+        ausmdv_f(g, g - 1.0f, P.apply_entropy_fix, rL, uL, vL, wL, eL, pl[5 * stride + il], rR, uR, vR, wR, eR,
+                 pr[5 * stride + ir], F);
+        Fg[MASS] = F[0];
+        Fg[TOTENERGY] = F[4];
+#pragma unroll
+        for (int m = 0; m < 3; ++m) Fg[XMOM + ax[m]] = F[1 + m];
+        return;
+    }
     const R Rg = R(P.gas.R), Cvinv = R(P.gas.Cvinv);
     FaceState<R> L, Rr;
     if (qL[4] <= R(0.0) || qL[3] <= R(0.0)) {
@@ -439,6 +522,52 @@ __device__ __forceinline__ void face_flux(const NumParams& P, R c_h, const R* qL
         Fg[PSI] = F[PSI];
         Fg[DIVB] = F[DIVB];
     }
+}
+
+// Phase-D decode of the float-flux variant: as decode() (e4/fvcell.d:586-822 with
+// ideal_gas.d:98-139), with the reciprocal of rho from a float estimate and one
+// FP64 Newton step and a float square root for a.  Only the checks and the
+// signal frequency consume it; the stored state is the FP64 update itself.
+__device__ __forceinline__ int decode_fast(const NumParams& P, const double* U, Prim<double>& s, double& p,
+                                           double& T) {
+    double rho = U[MASS];
+    if (!(rho > 0.0)) return 1;
+    s.rho = rho;
+    double dinv;
+    if (rho > 1.0e-30 && rho < 1.0e30) {
+        const double r0 = (double)__frcp_rn((float)rho);
+        dinv = r0 * (2.0 - rho * r0);
+    } else {
+        dinv = 1.0 / rho;
+    }
+    s.v[0] = U[XMOM] * dinv;
+    s.v[1] = U[YMOM] * dinv;
+    s.v[2] = U[ZMOM] * dinv;
+    s.B[0] = s.B[1] = s.B[2] = 0.0; s.psi = 0.0;
+    double u = U[TOTENERGY] * dinv - 0.5 * (s.v[0] * s.v[0] + s.v[1] * s.v[1] + s.v[2] * s.v[2]);
+    s.u = u;
+    if (u <= 0.0) return 2;
+    T = u * P.gas.Cvinv;
+    p = rho * P.gas.R * T;
+    if (T <= 0.0) return 2;
+    s.a = (double)sqrtf((float)(P.gas.gamma * P.gas.R * T));
+    return 0;
+}
+
+// signal_frequency (e4/fvcell.d:975-1059) for the float-flux Euler variant with the
+// reciprocal cell lengths precomputed (FP64 products instead of divisions).
+__device__ __forceinline__ double signal_fast(const NumParams& P, const double* inv_len, const Prim<double>& s) {
+    const double un_E = fabs(s.v[0]), un_N = fabs(s.v[1]);
+    const double un_T = (P.dims == 3) ? fabs(s.v[2]) : 0.0;
+    if (P.stringent_cfl) {
+        double un_max = fmax(un_N, un_E);
+        double inv_min = fmax(inv_len[0], inv_len[1]);
+        if (P.dims == 3) { un_max = fmax(un_max, un_T); inv_min = fmax(inv_min, inv_len[2]); }
+        return (un_max + s.a) * inv_min;
+    }
+    double sig = fmax((un_N + s.a) * inv_len[1], (un_E + s.a) * inv_len[0]);
+    if (P.dims == 3) sig = fmax(sig, (un_T + s.a) * inv_len[2]);
+    return fmax(sig, 0.0);
 }
 
 // Load the state of up to two cells per thread (on[m] says which): resolve, issue
@@ -583,6 +712,8 @@ __global__ void __launch_bounds__(32 * (TJ + 1), (sizeof(R) == 4 && !MHD) ? GDFV
 
     double sig_max = 0.0;
     const double Ai = B.area[0], Aj = B.area[1], Ak = B.area[2];
+    double inv_len[3] = {0.0, 0.0, 0.0};
+    if (FAST && !MHD && STAGE == 2) { inv_len[0] = 1.0 / B.len[0]; inv_len[1] = 1.0 / B.len[1]; inv_len[2] = 1.0 / B.len[2]; }
     // halo cell of this thread in every plane (4 columns beside, 4 rows above/below
     // the tile; the extra warp takes items 0..31); the same for all planes
     const int nh = 4 * nj_t + 4 * ni_t;
@@ -760,7 +891,7 @@ __global__ void __launch_bounds__(32 * (TJ + 1), (sizeof(R) == 4 && !MHD) ? GDFV
                 }
                 Prim<double> s;
                 double p, T;
-                int st = decode(P, U, s, p, T);
+                int st = (FAST && !MHD) ? decode_fast(P, U, s, p, T) : decode(P, U, s, p, T);
                 if (st != 0) {
                     atomicAdd(&A.ctl->n_fail, 1);
                     atomicMin(reinterpret_cast<unsigned long long*>(&A.ctl->first_bad_cell),
@@ -768,7 +899,7 @@ __global__ void __launch_bounds__(32 * (TJ + 1), (sizeof(R) == 4 && !MHD) ? GDFV
                 } else {
                     if (!check_data(P, s, p, T)) atomicAdd(STAGE == 1 ? &A.ctl->n_invalid1 : &A.ctl->n_invalid2, 1);
                     if (STAGE == 2) {
-                        double sig = signal_frequency(P, B, s);
+                        double sig = (FAST && !MHD) ? signal_fast(P, inv_len, s) : signal_frequency(P, B, s);
                         sig_max = fmax(sig_max, sig);
                         if (cell == (long long)B.n[0] * B.n[1] * B.n[2] - 1) A.last_signal[blk] = sig;
                     }
