@@ -72,7 +72,8 @@ struct Control {
     int step, step_limit, status, halted;
     int n_fail;                // decode failures in the current attempt (retry)
     int n_invalid1, n_invalid2;  // check_data failures after stage 1 / stage 2 (abort)
-    int attempt, retrying, steps_done, pad1_[2];
+    int attempt, retrying, steps_done;
+    unsigned int tile_next, tile_done;  // work queue of a persistent stage launch (0 between launches)
 };
 
 // ---------------------------------------------------------------- state structs

@@ -7,6 +7,22 @@
 
 namespace gdfv {
 
+// What the allocation-free step (gdfv_noalloc.cu) needs of a context.
+struct NoallocView {
+    int prepared, precision, flux, mhd, nblocks, max_invalid_cells;
+    long long total;
+    int nq, n_tiles;
+    const BlockDesc* d_blocks;
+    const TileDesc* d_tiles;
+    const InflowState* d_inflow;
+    NumParams P;
+    double c_h;
+    cudaStream_t stream;
+    int persistent;
+};
+bool noalloc_view(int ctx, NoallocView* v);
+void noalloc_set_error(int ctx, const std::string& msg);
+
 // What the adjoint (gdfv_adjoint.cu) needs of a context (gdfv_runtime.cu).
 struct AdjView {
     int prepared, flux, mhd, precision, nblocks, ninflow, dims;

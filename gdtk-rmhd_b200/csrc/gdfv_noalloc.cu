@@ -28,24 +28,10 @@
 #include <string>
 
 #include "../../include/gdfv.h"
+#include "gdfv_internal.h"
 #include "gdfv_launch.h"
 
 namespace gdfv {
-
-// Host access to the context (defined in gdfv_runtime.cu).
-struct NoallocView {
-    int prepared, precision, flux, mhd, nblocks, max_invalid_cells;
-    long long total;
-    int nq, n_tiles;
-    const BlockDesc* d_blocks;
-    const TileDesc* d_tiles;
-    const InflowState* d_inflow;
-    NumParams P;
-    double c_h;
-    cudaStream_t stream;
-};
-bool noalloc_view(int ctx, NoallocView* v);
-void noalloc_set_error(int ctx, const std::string& msg);
 
 namespace {
 
@@ -75,6 +61,7 @@ __global__ void noalloc_begin_kernel(Control* c, unsigned long long* maxsig, int
         c->step = 0; c->step_limit = 1; c->status = ST_OK; c->halted = 0;
         c->n_fail = 0; c->n_invalid1 = 0; c->n_invalid2 = 0;
         c->attempt = 0; c->retrying = 0; c->steps_done = 0;
+        c->tile_next = 0; c->tile_done = 0;
     }
 }
 
@@ -135,6 +122,7 @@ extern "C" int gdfv_step_noalloc(int ctx, const double* U_in_dev, double* U_out_
     A.P = v.P;
     A.n_tiles = v.n_tiles;
     A.max_invalid_cells = v.max_invalid_cells;
+    A.persistent = v.persistent;
 
     noalloc_begin_kernel<<<1, 256, 0, v.stream>>>(ctl, maxsig, v.nblocks, dt, v.c_h);
     e = cudaGetLastError();

@@ -206,6 +206,8 @@ struct Config {
     int stringent_cfl = 0, cfl_count = 10, max_attempts = 3, max_invalid_cells = 0;
     int fixed_time_step = 0;
     int tile_kchunk = 0;  // 0: chosen per block
+    int persistent = 0;   // 1: stage kernels as a resident grid taking tiles from a queue
+    int autotune = 0;     // time tile shapes and the launch form on the first run, keep the fastest
     double cfl_value = 0.5, dt_init = 1.0e-3, dt_max = 1.0e-3;
     double eps_van_albada = 1.0e-12, R = 287.1, gamma = 1.4, divB_damping_length = 1.0;
     double max_velocity = 30000.0, max_temp = 50000.0, min_temp = 0.0;
@@ -239,6 +241,9 @@ struct Context {
     int graph_steps = 0;
     bool signal_valid = false;
     int n_inflow = 0;
+    size_t tiles_cap = 0;              // capacity of d_tiles (entries)
+    bool tuned = false;
+    double tune_ms = 0.0;              // stage-1 + stage-2 time of the tuned configuration
     double* adj_scratch = nullptr;     // adjoint work arrays, allocated on first use
     int adj_ready = 0;
     long long adj_scratch_n = 0;
@@ -308,6 +313,7 @@ StageArgs stage_args(Context* c) {
     A.P = c->P;
     A.n_tiles = c->n_tiles;
     A.max_invalid_cells = c->cfg.max_invalid_cells;
+    A.persistent = c->cfg.persistent;
     return A;
 }
 
@@ -361,6 +367,32 @@ void fill_weights(double len, double* w) {
     w[W_TOR] = 2.0 / (lenR1 + lenR0);
     w[W_TWOL] = (2.0 * lenL0 + lenL1);
     w[W_TWOR] = (2.0 * lenR0 + lenR1);
+}
+
+// Tile table over all blocks: 32 x TJ columns and kchunk planes per tile (0: the
+// block's nkc up to 32).  Ordered by decreasing work (cells), so that a grid
+// taking tiles in order -- the hardware's CTA order, or the persistent stride --
+// starts the long tiles of uneven blocks first.
+void build_tiles(Context* c, int kchunk, std::vector<TileDesc>& tiles) {
+    tiles.clear();
+    const int TJ = c->cfg.precision == 0 ? TJ_FP64 : TJ_FP32;
+    for (size_t b = 0; b < c->blocks.size(); ++b) {
+        const HostBlock& hb = c->blocks[b];
+        int kc = kchunk > 0 ? kchunk : std::min(hb.n[2], 32);
+        if (c->cfg.dims == 2) kc = 1;
+        for (int k0 = 0; k0 < hb.n[2]; k0 += kc)
+            for (int j0 = 0; j0 < hb.n[1]; j0 += TJ)
+                for (int i0 = 0; i0 < hb.n[0]; i0 += 32) {
+                    TileDesc t{};
+                    t.block = (int)b; t.i0 = i0; t.j0 = j0; t.k0 = k0; t.k1 = std::min(k0 + kc, hb.n[2]);
+                    tiles.push_back(t);
+                }
+    }
+    auto work = [&](const TileDesc& t) {
+        const HostBlock& hb = c->blocks[t.block];
+        return (long long)std::min(32, hb.n[0] - t.i0) * std::min(TJ, hb.n[1] - t.j0) * (t.k1 - t.k0);
+    };
+    std::stable_sort(tiles.begin(), tiles.end(), [&](const TileDesc& a, const TileDesc& b) { return work(a) > work(b); });
 }
 
 int do_prepare(Context* c) {
@@ -433,20 +465,10 @@ int do_prepare(Context* c) {
             }
         }
         c->h_blocks.push_back(B);
-        // tile table: TI x TJ columns, k chunks
-        int kc = g.tile_kchunk > 0 ? g.tile_kchunk : std::min(hb.n[2], 32);
-        if (g.dims == 2) kc = 1;
-        const int TJ = g.precision == 0 ? TJ_FP64 : TJ_FP32;
-        for (int k0 = 0; k0 < hb.n[2]; k0 += kc)
-            for (int j0 = 0; j0 < hb.n[1]; j0 += TJ)
-                for (int i0 = 0; i0 < hb.n[0]; i0 += 32) {
-                    TileDesc t{};
-                    t.block = (int)b; t.i0 = i0; t.j0 = j0; t.k0 = k0; t.k1 = std::min(k0 + kc, hb.n[2]);
-                    tiles.push_back(t);
-                }
         off += (long long)hb.n[0] * hb.n[1] * hb.n[2];
     }
     c->total = off;
+    build_tiles(c, g.tile_kchunk, tiles);
     c->n_tiles = (int)tiles.size();
     c->n_inflow = (int)inflows.size();
     NumParams& P = c->P;
@@ -485,6 +507,7 @@ int do_prepare(Context* c) {
     CK(cudaMalloc(&c->d_blocks, sizeof(BlockDesc) * c->h_blocks.size()));
     CK(cudaMemcpy(c->d_blocks, c->h_blocks.data(), sizeof(BlockDesc) * c->h_blocks.size(), cudaMemcpyHostToDevice));
     CK(cudaMalloc(&c->d_tiles, sizeof(TileDesc) * tiles.size()));
+    c->tiles_cap = tiles.size();
     CK(cudaMemcpy(c->d_tiles, tiles.data(), sizeof(TileDesc) * tiles.size(), cudaMemcpyHostToDevice));
     CK(cudaMalloc(&c->d_inflow, sizeof(InflowState) * std::max<size_t>(1, inflows.size())));
     if (!inflows.empty())
@@ -535,17 +558,6 @@ int build_graph(Context* c) {
 }
 
 // Read-only view of a context for gdfv_step_noalloc (gdfv_noalloc.cu).
-struct NoallocView {
-    int prepared, precision, flux, mhd, nblocks, max_invalid_cells;
-    long long total;
-    int nq, n_tiles;
-    const BlockDesc* d_blocks;
-    const TileDesc* d_tiles;
-    const InflowState* d_inflow;
-    NumParams P;
-    double c_h;
-    cudaStream_t stream;
-};
 
 bool noalloc_view(int ctx, NoallocView* v) {
     Context* c = get_ctx(ctx);
@@ -565,6 +577,7 @@ bool noalloc_view(int ctx, NoallocView* v) {
     v->P = c->P;
     v->c_h = c->h_ctl ? c->h_ctl->c_h : 0.0;
     v->stream = c->stream;
+    v->persistent = c->cfg.persistent;
     return true;
 }
 
@@ -618,6 +631,7 @@ __global__ void step_dt_begin_kernel(Control* c, unsigned long long* maxsig, int
         c->step = 0; c->step_limit = 1; c->status = ST_OK; c->halted = 0;
         c->n_fail = 0; c->n_invalid1 = 0; c->n_invalid2 = 0;
         c->attempt = 0; c->retrying = 0; c->steps_done = 0;
+        c->tile_next = 0; c->tile_done = 0;
     }
 }
 
@@ -702,6 +716,8 @@ int gdfv_config_set_int(int ctx, const char* key, long long value) {
     else if (k == "max_invalid_cells") g.max_invalid_cells = v;
     else if (k == "fixed_time_step") g.fixed_time_step = v != 0;
     else if (k == "tile_kchunk") { if (v < 0) return fail(c, GDFV_ERR_ARG, "tile_kchunk >= 0"); g.tile_kchunk = v; }
+    else if (k == "persistent") g.persistent = v != 0;
+    else if (k == "autotune") g.autotune = v != 0;
     else return fail(c, GDFV_ERR_ARG, "unknown integer option: " + k);
     return GDFV_OK;
 }
@@ -738,6 +754,10 @@ int gdfv_config_get_double(int ctx, const char* key, double* value) {
     else if (k == "R" || k == "r") *value = g.R;
     else if (k == "gamma") *value = g.gamma;
     else if (k == "divB_damping_length" || k == "divb_damping_length") *value = g.divB_damping_length;
+    else if (k == "tile_kchunk") *value = g.tile_kchunk;
+    else if (k == "persistent") *value = g.persistent;
+    else if (k == "autotune") *value = g.autotune;
+    else if (k == "autotune_stage_ms") *value = c->tune_ms;
     else return fail(c, GDFV_ERR_ARG, "unknown real option: " + k);
     return GDFV_OK;
 }
@@ -891,6 +911,97 @@ int gdfv_block_get_flow(int ctx, int blk, double* out) {
     return GDFV_OK;
 }
 
+}  // extern "C"
+
+namespace gdfv {
+
+int upload_tiles(Context* c, const std::vector<TileDesc>& tiles) {
+    CK(cudaStreamSynchronize(c->stream));
+    if (tiles.size() > c->tiles_cap) {
+        if (c->d_tiles) cudaFree(c->d_tiles);
+        c->d_tiles = nullptr;
+        c->tiles_cap = 0;
+        CK(cudaMalloc(&c->d_tiles, sizeof(TileDesc) * tiles.size()));
+        c->tiles_cap = tiles.size();
+    }
+    CK(cudaMemcpy(c->d_tiles, tiles.data(), sizeof(TileDesc) * tiles.size(), cudaMemcpyHostToDevice));
+    c->n_tiles = (int)tiles.size();
+    if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }  // captured the old table
+    return GDFV_OK;
+}
+
+// Autotuner: for each tile k-chunk and launch form (persistent grid or one CTA
+// per tile), time stage 1 + stage 2 on the current state and keep the fastest.
+// The trial steps use a scratch control record with dt = 0 and write only the
+// idle state buffer and dU0, so the solution is not changed.
+int autotune(Context* c) {
+    if (!c->step_ctl) {
+        CK(cudaMalloc(&c->step_ctl, sizeof(Control)));
+        CK(cudaMalloc(&c->step_maxsig, sizeof(unsigned long long) * c->blocks.size()));
+        CK(cudaMalloc(&c->step_lastsig, sizeof(double) * c->blocks.size()));
+    }
+    if (read_ctl(c)) return GDFV_ERR_CUDA;
+    const int parity = c->h_ctl->step & 1;
+    const double c_h = c->h_ctl->c_h > 0.0 ? c->h_ctl->c_h : 1.0;
+    int maxk = 1;
+    for (const HostBlock& hb : c->blocks) maxk = std::max(maxk, hb.n[2]);
+    std::vector<int> kcs;
+    if (c->cfg.dims == 2) kcs.push_back(1);
+    else
+        for (int kc : {8, 16, 32, 64, 128})
+            if (kc <= maxk || kcs.empty()) kcs.push_back(kc);
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    double best = 1e30;
+    int best_kc = c->cfg.tile_kchunk, best_p = c->cfg.persistent;
+    std::vector<TileDesc> tiles;
+    cudaError_t e = cudaSuccess;
+    const int reps = 3;
+    for (int kc : kcs) {
+        build_tiles(c, kc, tiles);
+        int st = upload_tiles(c, tiles);
+        if (st) { cudaEventDestroy(e0); cudaEventDestroy(e1); return st; }
+        for (int pers = 1; pers >= 0 && e == cudaSuccess; --pers) {
+            StageArgs A = stage_args(c);
+            A.Ubuf[0] = c->U[parity];
+            A.Ubuf[1] = c->U[parity ^ 1];
+            A.ctl = c->step_ctl;
+            A.max_signal = c->step_maxsig;
+            A.last_signal = c->step_lastsig;
+            A.persistent = pers;
+            step_dt_begin_kernel<<<1, 256, 0, c->stream>>>(c->step_ctl, c->step_maxsig, (int)c->blocks.size(), 0.0, c_h);
+            e = cudaGetLastError();
+            for (int r = -1; r < reps && e == cudaSuccess; ++r) {
+                if (r == 0) e = cudaEventRecord(e0, c->stream);
+                if (e == cudaSuccess) e = launch_stage(c, 1, A);
+                if (e == cudaSuccess) e = launch_stage(c, 2, A);
+            }
+            if (e == cudaSuccess) e = cudaEventRecord(e1, c->stream);
+            if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+            float ms = 0.0f;
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+            if (e == cudaSuccess && ms / reps < best) { best = ms / reps; best_kc = kc; best_p = pers; }
+        }
+        if (e != cudaSuccess) break;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (e != cudaSuccess) return cuda_fail(c, e, "autotune");
+    c->cfg.tile_kchunk = best_kc;
+    c->cfg.persistent = best_p;
+    build_tiles(c, best_kc, tiles);
+    int st = upload_tiles(c, tiles);
+    if (st) return st;
+    c->tuned = true;
+    c->tune_ms = best;
+    return GDFV_OK;
+}
+
+}  // namespace gdfv
+
+extern "C" {
+
 int gdfv_run(int ctx, int max_steps, double max_time, int* steps_taken) {
     Context* c = get_ctx(ctx);
     int st = check_ready(c, -1);
@@ -899,6 +1010,9 @@ int gdfv_run(int ctx, int max_steps, double max_time, int* steps_taken) {
     if (max_steps <= 0) return GDFV_OK;
     if (!c->signal_valid) {
         if ((st = scan_signal(c)) != GDFV_OK) return st;
+    }
+    if (c->cfg.autotune && !c->tuned) {
+        if ((st = autotune(c)) != GDFV_OK) return st;
     }
     if (read_ctl(c)) return GDFV_ERR_CUDA;
     if (c->h_ctl->status != ST_OK) return fail(c, GDFV_ERR_STATE, "a previous run failed; reset the state");

@@ -47,6 +47,8 @@ struct StageArgs {
     NumParams P;
     int n_tiles;
     int max_invalid_cells;
+    int persistent;           // grid of resident CTAs striding over the tiles
+    int pad_;
 };
 
 // Compile-time geometry of the tile and of the shared-memory layout.
@@ -597,7 +599,9 @@ __device__ __forceinline__ void load_two(const StageArgs& A, const double* Uin, 
 #define GDFV_MINB_FP32 2
 #endif
 
-template <int STAGE, class R, bool MHD, int FLUX, int TJ, int OPT>
+// PERS = 1: persistent grid over the tile queue; 0: one CTA per tile (no
+// state carried between tiles, so the compiler keeps fewer values live).
+template <int STAGE, class R, bool MHD, int FLUX, int TJ, int OPT, int PERS>
 __global__ void __launch_bounds__(32 * (TJ + 1), (sizeof(R) == 4 && !MHD) ? GDFV_MINB_FP32 : 1) stage_kernel(StageArgs A) {
     using G = Geo<R, MHD, TJ>;
     constexpr int TI = G::TI, NT = G::NT, NCOL = G::NCOL, PW = G::PW, PLANE = G::PLANE;
@@ -635,290 +639,315 @@ __global__ void __launch_bounds__(32 * (TJ + 1), (sizeof(R) == 4 && !MHD) ? GDFV
         damp = exp(-(c_h2 / c_p2) * dt);
     }
 
-    const TileDesc t = A.tiles[blockIdx.x];
-    const int blk = t.block;
-    const BlockDesc& B = A.blocks[blk];
-    const NumParams& P = A.P;
-    const int ni_t = min(TI, B.n[0] - t.i0);
-    const int nj_t = min(TJ, B.n[1] - t.j0);
-    const int tid = threadIdx.x;
-    const bool owner = tid < NCOL;                 // owns column (ti, tj)
-    const int ti = tid % TI, tj = tid / TI;
-    const bool active = owner && ti < ni_t && tj < nj_t;
-    const int pidx = (ti + 2) + PW * (tj + 2);     // own cell in a padded plane
-    const bool has_k = (P.dims == 3);
-    if (tid < 3 * W_N) w[tid / W_N][tid % W_N] = (R)B.w[tid / W_N][tid % W_N];
-    if (tid < 3) {
-        const double* bw = B.w[tid];
-        const double tc = bw[W_TOC];
-        wf[tid][WF_EPS] = (R)(P.eps_van_albada / (tc * tc));
-        wf[tid][WF_P1] = (R)(bw[W_AL0] * tc * bw[W_TWOL]);
-        wf[tid][WF_P2] = (R)(bw[W_AL0] * tc * bw[W_LENL0]);
-        wf[tid][WF_R1] = (R)(bw[W_AR0] * tc * bw[W_LENL0]);
-        wf[tid][WF_R2] = (R)(bw[W_AR0] * tc * bw[W_TWOL]);
+    // Tiles of the block table (ordered by decreasing work).  One CTA per tile, or
+    // a persistent grid whose CTAs take tiles from a queue in the control record
+    // (one atomic ticket per tile; the last CTA to finish resets the queue).
+    __shared__ int s_tile;
+    Control* qctl = const_cast<Control*>(ctl);
+    int tix = blockIdx.x;
+    if (PERS) {
+        if (threadIdx.x == 0) s_tile = (int)atomicAdd(&qctl->tile_next, 1u);
+        __syncthreads();
+        tix = s_tile;
     }
-    const R c_hR = (R)c_h;
-    __syncthreads();
-
-    auto slot = [&](int kk) -> R* { return ring + (((kk % 3) + 3) % 3) * NPV * PLANE; };
-
-    R kq_prev_p[NRS];        // k-direction q+ of the current plane (left state of its top face)
-    R fB[NQ];                // flux through the bottom face of the owner's cell
-#pragma unroll
-    for (int q = 0; q < NQ; ++q) fB[q] = R(0);
-#pragma unroll
-    for (int s = 0; s < NRS; ++s) kq_prev_p[s] = R(0);
-
-    // ---------------- prologue: planes k0-2 .. k0+1 (k0 only in 2D)
-    if (has_k) {
-        int ci[2] = {t.i0 + ti, t.i0 + ti}, cj[2] = {t.j0 + tj, t.j0 + tj};
-        if (active) {
-            Prim<double> pr[2];
-            int ck[2] = {t.k0 - 2, t.k0 - 1};
-            load_two<STAGE, FAST, MHD, NQ>(A, Uin, B, dt, damp, true, true, ci, cj, ck, pr);
-            put_prim<R, NPV>(slot(t.k0 - 2), PLANE, pidx, pr[0]);
-            put_prim<R, NPV>(slot(t.k0 - 1), PLANE, pidx, pr[1]);
-            int ck2[2] = {t.k0, 0};
-            load_two<STAGE, FAST, MHD, NQ>(A, Uin, B, dt, damp, true, false, ci, cj, ck2, pr);
-            put_prim<R, NPV>(slot(t.k0), PLANE, pidx, pr[0]);
-            // q+ of plane k0-1 (left state of face k0-1/2); own column only
-            R qm1[NRS], q0[NRS], qp1[NRS], qm[NRS];
-            gather<R, NRS, 2>(slot(t.k0 - 2), PLANE, pidx, qm1);
-            gather<R, NRS, 2>(slot(t.k0 - 1), PLANE, pidx, q0);
-            gather<R, NRS, 2>(slot(t.k0), PLANE, pidx, qp1);
-            recon_cell<R, NRS, MHD, OPT>(w[2], wf[2], P, qm1, q0, qp1, qm, kq_prev_p);
-            // plane k0+1 replaces k0-2 in the ring
-            int ck3[2] = {t.k0 + 1, 0};
-            load_two<STAGE, FAST, MHD, NQ>(A, Uin, B, dt, damp, true, false, ci, cj, ck3, pr);
-            put_prim<R, NPV>(slot(t.k0 + 1), PLANE, pidx, pr[0]);
-            R qkm[NRS], qkp[NRS];
-            gather<R, NRS, 2>(slot(t.k0 - 1), PLANE, pidx, qm1);
-            gather<R, NRS, 2>(slot(t.k0), PLANE, pidx, q0);
-            gather<R, NRS, 2>(slot(t.k0 + 1), PLANE, pidx, qp1);
-            recon_cell<R, NRS, MHD, OPT>(w[2], wf[2], P, qm1, q0, qp1, qkm, qkp);
-            face_flux<R, MHD, FLUX, 2, NPV>(P, c_hR, kq_prev_p, qkm, slot(t.k0 - 1), pidx, slot(t.k0), pidx, PLANE,
-                                            fB);
-#pragma unroll
-            for (int s = 0; s < NRS; ++s) kq_prev_p[s] = qkp[s];
+    while (tix < A.n_tiles) {
+        const TileDesc t = A.tiles[tix];
+        const int blk = t.block;
+        const BlockDesc& B = A.blocks[blk];
+        const NumParams& P = A.P;
+        const int ni_t = min(TI, B.n[0] - t.i0);
+        const int nj_t = min(TJ, B.n[1] - t.j0);
+        const int tid = threadIdx.x;
+        const bool owner = tid < NCOL;                 // owns column (ti, tj)
+        const int ti = tid % TI, tj = tid / TI;
+        const bool active = owner && ti < ni_t && tj < nj_t;
+        const int pidx = (ti + 2) + PW * (tj + 2);     // own cell in a padded plane
+        const bool has_k = (P.dims == 3);
+        if (tid < 3 * W_N) w[tid / W_N][tid % W_N] = (R)B.w[tid / W_N][tid % W_N];
+        if (tid < 3) {
+            const double* bw = B.w[tid];
+            const double tc = bw[W_TOC];
+            wf[tid][WF_EPS] = (R)(P.eps_van_albada / (tc * tc));
+            wf[tid][WF_P1] = (R)(bw[W_AL0] * tc * bw[W_TWOL]);
+            wf[tid][WF_P2] = (R)(bw[W_AL0] * tc * bw[W_LENL0]);
+            wf[tid][WF_R1] = (R)(bw[W_AR0] * tc * bw[W_LENL0]);
+            wf[tid][WF_R2] = (R)(bw[W_AR0] * tc * bw[W_TWOL]);
         }
-    } else {
-        if (active) {
-            int ci[2] = {t.i0 + ti, 0}, cj[2] = {t.j0 + tj, 0}, ck[2] = {t.k0, 0};
-            Prim<double> pr[2];
-            load_two<STAGE, FAST, MHD, NQ>(A, Uin, B, dt, damp, true, false, ci, cj, ck, pr);
-            put_prim<R, NPV>(slot(t.k0), PLANE, pidx, pr[0]);
-        }
-    }
+        const R c_hR = (R)c_h;
+        __syncthreads();
 
-    double sig_max = 0.0;
-    const double Ai = B.area[0], Aj = B.area[1], Ak = B.area[2];
-    double inv_len[3] = {0.0, 0.0, 0.0};
-    if (FAST && !MHD && STAGE == 2) { inv_len[0] = 1.0 / B.len[0]; inv_len[1] = 1.0 / B.len[1]; inv_len[2] = 1.0 / B.len[2]; }
-    // halo cell of this thread in every plane (4 columns beside, 4 rows above/below
-    // the tile; the extra warp takes items 0..31); the same for all planes
-    const int nh = 4 * nj_t + 4 * ni_t;
-    const int h = owner ? tid + 32 : tid - NCOL;
-    const bool h_on = h < nh;
-    int h_ci = 0, h_cj = 0, h_dst = 0;
-    if (h_on) {
-        int hi, hj;
-        if (h < 4 * nj_t) {
-            int side = h / (2 * nj_t), rem = h % (2 * nj_t);
-            int col = rem / nj_t, row = rem % nj_t;
-            hi = side == 0 ? col - 2 : ni_t + col;
-            hj = row;
-        } else {
-            int h2 = h - 4 * nj_t;
-            int side = h2 / (2 * ni_t), rem = h2 % (2 * ni_t);
-            int row = rem / ni_t, col = rem % ni_t;
-            hj = side == 0 ? row - 2 : nj_t + row;
-            hi = col;
-        }
-        h_ci = t.i0 + hi;
-        h_cj = t.j0 + hj;
-        h_dst = (hi + 2) + PW * (hj + 2);
-    }
-    const int f0 = owner ? G::EXTRA + tid : tid - NCOL;   // flat-list start and stride
-    const int fstride = owner ? NCOL : 32;
-    const int fend = owner ? 0x7fffffff : G::EXTRA;
+        auto slot = [&](int kk) -> R* { return ring + (((kk % 3) + 3) % 3) * NPV * PLANE; };
 
-    for (int k = t.k0; k < t.k1; ++k) {
-        R* cur = slot(k);
-        // ---------------- phase A: leading plane k+2 (owners) and the halo of plane k
-        {
-            const bool lead = active && has_k;
-            int ci[2] = {t.i0 + ti, h_ci}, cj[2] = {t.j0 + tj, h_cj}, ck[2] = {k + 2, k};
-            if (lead || h_on) {
+        R kq_prev_p[NRS];        // k-direction q+ of the current plane (left state of its top face)
+        R fB[NQ];                // flux through the bottom face of the owner's cell
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) fB[q] = R(0);
+#pragma unroll
+        for (int s = 0; s < NRS; ++s) kq_prev_p[s] = R(0);
+
+        // ---------------- prologue: planes k0-2 .. k0+1 (k0 only in 2D)
+        if (has_k) {
+            int ci[2] = {t.i0 + ti, t.i0 + ti}, cj[2] = {t.j0 + tj, t.j0 + tj};
+            if (active) {
                 Prim<double> pr[2];
-                load_two<STAGE, FAST, MHD, NQ>(A, Uin, B, dt, damp, lead, h_on, ci, cj, ck, pr);
-                if (lead) put_prim<R, NPV>(slot(k + 2), PLANE, pidx, pr[0]);
-                if (h_on) put_prim<R, NPV>(cur, PLANE, h_dst, pr[1]);
+                int ck[2] = {t.k0 - 2, t.k0 - 1};
+                load_two<STAGE, FAST, MHD, NQ>(A, Uin, B, dt, damp, true, true, ci, cj, ck, pr);
+                put_prim<R, NPV>(slot(t.k0 - 2), PLANE, pidx, pr[0]);
+                put_prim<R, NPV>(slot(t.k0 - 1), PLANE, pidx, pr[1]);
+                int ck2[2] = {t.k0, 0};
+                load_two<STAGE, FAST, MHD, NQ>(A, Uin, B, dt, damp, true, false, ci, cj, ck2, pr);
+                put_prim<R, NPV>(slot(t.k0), PLANE, pidx, pr[0]);
+                // q+ of plane k0-1 (left state of face k0-1/2); own column only
+                R qm1[NRS], q0[NRS], qp1[NRS], qm[NRS];
+                gather<R, NRS, 2>(slot(t.k0 - 2), PLANE, pidx, qm1);
+                gather<R, NRS, 2>(slot(t.k0 - 1), PLANE, pidx, q0);
+                gather<R, NRS, 2>(slot(t.k0), PLANE, pidx, qp1);
+                recon_cell<R, NRS, MHD, OPT>(w[2], wf[2], P, qm1, q0, qp1, qm, kq_prev_p);
+                // plane k0+1 replaces k0-2 in the ring
+                int ck3[2] = {t.k0 + 1, 0};
+                load_two<STAGE, FAST, MHD, NQ>(A, Uin, B, dt, damp, true, false, ci, cj, ck3, pr);
+                put_prim<R, NPV>(slot(t.k0 + 1), PLANE, pidx, pr[0]);
+                R qkm[NRS], qkp[NRS];
+                gather<R, NRS, 2>(slot(t.k0 - 1), PLANE, pidx, qm1);
+                gather<R, NRS, 2>(slot(t.k0), PLANE, pidx, q0);
+                gather<R, NRS, 2>(slot(t.k0 + 1), PLANE, pidx, qp1);
+                recon_cell<R, NRS, MHD, OPT>(w[2], wf[2], P, qm1, q0, qp1, qkm, qkp);
+                face_flux<R, MHD, FLUX, 2, NPV>(P, c_hR, kq_prev_p, qkm, slot(t.k0 - 1), pidx, slot(t.k0), pidx, PLANE,
+                                                fB);
+#pragma unroll
+                for (int s = 0; s < NRS; ++s) kq_prev_p[s] = qkp[s];
+            }
+        } else {
+            if (active) {
+                int ci[2] = {t.i0 + ti, 0}, cj[2] = {t.j0 + tj, 0}, ck[2] = {t.k0, 0};
+                Prim<double> pr[2];
+                load_two<STAGE, FAST, MHD, NQ>(A, Uin, B, dt, damp, true, false, ci, cj, ck, pr);
+                put_prim<R, NPV>(slot(t.k0), PLANE, pidx, pr[0]);
             }
         }
-        __syncthreads();
 
-        // ---------------- phase B: reconstruction
-        R kq_m[NRS], kq_p[NRS];
-        if (active && has_k) {
-            R qm1[NRS], q0[NRS], qp1[NRS];
-            gather<R, NRS, 2>(cur, PLANE, pidx, qm1);
-            gather<R, NRS, 2>(slot(k + 1), PLANE, pidx, q0);
-            gather<R, NRS, 2>(slot(k + 2), PLANE, pidx, qp1);
-            recon_cell<R, NRS, MHD, OPT>(w[2], wf[2], P, qm1, q0, qp1, kq_m, kq_p);
-        }
-        for (int f = f0; f < NRI + NRJ && f < fend; f += fstride) {
-            R qm1[NRS], q0[NRS], qp1[NRS], qm[NRS], qp[NRS];
-            if (f < NRI) {
-                const int row = f / (TI + 2), ci = f % (TI + 2) - 1;   // cells -1..TI
-                if (row >= nj_t || ci > ni_t) continue;
-                const int p = (ci + 2) + PW * (row + 2);
-                gather<R, NRS, 0>(cur, PLANE, p - 1, qm1);
-                gather<R, NRS, 0>(cur, PLANE, p, q0);
-                gather<R, NRS, 0>(cur, PLANE, p + 1, qp1);
-                recon_cell<R, NRS, MHD, OPT>(w[0], wf[0], P, qm1, q0, qp1, qm, qp);
-#pragma unroll
-                for (int s = 0; s < NRS; ++s) { RI[s * NRI + f] = qm[s]; RI[(NRS + s) * NRI + f] = qp[s]; }
+        double sig_max = 0.0;
+        const double Ai = B.area[0], Aj = B.area[1], Ak = B.area[2];
+        double inv_len[3] = {0.0, 0.0, 0.0};
+        if (FAST && !MHD && STAGE == 2) { inv_len[0] = 1.0 / B.len[0]; inv_len[1] = 1.0 / B.len[1]; inv_len[2] = 1.0 / B.len[2]; }
+        // halo cell of this thread in every plane (4 columns beside, 4 rows above/below
+        // the tile; the extra warp takes items 0..31); the same for all planes
+        const int nh = 4 * nj_t + 4 * ni_t;
+        const int h = owner ? tid + 32 : tid - NCOL;
+        const bool h_on = h < nh;
+        int h_ci = 0, h_cj = 0, h_dst = 0;
+        if (h_on) {
+            int hi, hj;
+            if (h < 4 * nj_t) {
+                int side = h / (2 * nj_t), rem = h % (2 * nj_t);
+                int col = rem / nj_t, row = rem % nj_t;
+                hi = side == 0 ? col - 2 : ni_t + col;
+                hj = row;
             } else {
-                const int g = f - NRI;
-                const int cj = g / TI - 1, col = g % TI;               // rows -1..TJ
-                if (col >= ni_t || cj > nj_t) continue;
-                const int p = (col + 2) + PW * (cj + 2);
-                gather<R, NRS, 1>(cur, PLANE, p - PW, qm1);
-                gather<R, NRS, 1>(cur, PLANE, p, q0);
-                gather<R, NRS, 1>(cur, PLANE, p + PW, qp1);
-                recon_cell<R, NRS, MHD, OPT>(w[1], wf[1], P, qm1, q0, qp1, qm, qp);
-#pragma unroll
-                for (int s = 0; s < NRS; ++s) { RJ[s * NRJ + g] = qm[s]; RJ[(NRS + s) * NRJ + g] = qp[s]; }
+                int h2 = h - 4 * nj_t;
+                int side = h2 / (2 * ni_t), rem = h2 % (2 * ni_t);
+                int row = rem / ni_t, col = rem % ni_t;
+                hj = side == 0 ? row - 2 : nj_t + row;
+                hi = col;
             }
+            h_ci = t.i0 + hi;
+            h_cj = t.j0 + hj;
+            h_dst = (hi + 2) + PW * (hj + 2);
         }
-        __syncthreads();
+        const int f0 = owner ? G::EXTRA + tid : tid - NCOL;   // flat-list start and stride
+        const int fstride = owner ? NCOL : 32;
+        const int fend = owner ? 0x7fffffff : G::EXTRA;
 
-        // ---------------- phase C: interface fluxes
-        R fT[NQ];
-#pragma unroll
-        for (int q = 0; q < NQ; ++q) fT[q] = R(0);
-        if (active && has_k) {
-            face_flux<R, MHD, FLUX, 2, NPV>(P, c_hR, kq_prev_p, kq_m, cur, pidx, slot(k + 1), pidx, PLANE, fT);
-#pragma unroll
-            for (int s = 0; s < NRS; ++s) kq_prev_p[s] = kq_p[s];
-        }
-        for (int f = f0; f < NFI + NFJ && f < fend; f += fstride) {
-            R qL[NRS], qR[NRS], F[NQ];
-            if (f < NFI) {
-                const int row = f / (TI + 1), fi = f % (TI + 1);       // faces 0..TI
-                if (row >= nj_t || fi > ni_t) continue;
-                const int rl = fi + (TI + 2) * row;                    // RI index of cell fi-1
-#pragma unroll
-                for (int s = 0; s < NRS; ++s) { qL[s] = RI[(NRS + s) * NRI + rl]; qR[s] = RI[s * NRI + rl + 1]; }
-                const int p = (fi + 2) + PW * (row + 2);
-                face_flux<R, MHD, FLUX, 0, NPV>(P, c_hR, qL, qR, cur, p - 1, cur, p, PLANE, F);
-#pragma unroll
-                for (int q = 0; q < NQ; ++q) FI[q * NFI + f] = F[q];
-            } else {
-                const int g = f - NFI;
-                const int fj = g / TI, col = g % TI;                   // faces 0..TJ
-                if (col >= ni_t || fj > nj_t) continue;
-                const int rl = col + TI * fj;                          // RJ index of row fj-1
-#pragma unroll
-                for (int s = 0; s < NRS; ++s) { qL[s] = RJ[(NRS + s) * NRJ + rl]; qR[s] = RJ[s * NRJ + rl + TI]; }
-                const int p = (col + 2) + PW * (fj + 2);
-                face_flux<R, MHD, FLUX, 1, NPV>(P, c_hR, qL, qR, cur, p - PW, cur, p, PLANE, F);
-#pragma unroll
-                for (int q = 0; q < NQ; ++q) FJ[q * NFJ + g] = F[q];
+        for (int k = t.k0; k < t.k1; ++k) {
+            R* cur = slot(k);
+            // ---------------- phase A: leading plane k+2 (owners) and the halo of plane k
+            {
+                const bool lead = active && has_k;
+                int ci[2] = {t.i0 + ti, h_ci}, cj[2] = {t.j0 + tj, h_cj}, ck[2] = {k + 2, k};
+                if (lead || h_on) {
+                    Prim<double> pr[2];
+                    load_two<STAGE, FAST, MHD, NQ>(A, Uin, B, dt, damp, lead, h_on, ci, cj, ck, pr);
+                    if (lead) put_prim<R, NPV>(slot(k + 2), PLANE, pidx, pr[0]);
+                    if (h_on) put_prim<R, NPV>(cur, PLANE, h_dst, pr[1]);
+                }
             }
-        }
-        __syncthreads();
+            __syncthreads();
 
-        // ---------------- phase D: residual (e4/fvcell.d:824-856, faces W, E, S, N, B, T) and update
-        if (active) {
-            const long long cell = cell_index(B, t.i0 + ti, t.j0 + tj, k);
-            const long long g = B.offset + cell;
-            double dU[NQ];
-            if (FAST) {
-                // float path: differences of opposite faces in float (same-signed,
-                // nearly equal fluxes subtract exactly), accumulation in FP64
-                const double Vi = B.vol_inv;
+            // ---------------- phase B: reconstruction
+            R kq_m[NRS], kq_p[NRS];
+            if (active && has_k) {
+                R qm1[NRS], q0[NRS], qp1[NRS];
+                gather<R, NRS, 2>(cur, PLANE, pidx, qm1);
+                gather<R, NRS, 2>(slot(k + 1), PLANE, pidx, q0);
+                gather<R, NRS, 2>(slot(k + 2), PLANE, pidx, qp1);
+                recon_cell<R, NRS, MHD, OPT>(w[2], wf[2], P, qm1, q0, qp1, kq_m, kq_p);
+            }
+            for (int f = f0; f < NRI + NRJ && f < fend; f += fstride) {
+                R qm1[NRS], q0[NRS], qp1[NRS], qm[NRS], qp[NRS];
+                if (f < NRI) {
+                    const int row = f / (TI + 2), ci = f % (TI + 2) - 1;   // cells -1..TI
+                    if (row >= nj_t || ci > ni_t) continue;
+                    const int p = (ci + 2) + PW * (row + 2);
+                    gather<R, NRS, 0>(cur, PLANE, p - 1, qm1);
+                    gather<R, NRS, 0>(cur, PLANE, p, q0);
+                    gather<R, NRS, 0>(cur, PLANE, p + 1, qp1);
+                    recon_cell<R, NRS, MHD, OPT>(w[0], wf[0], P, qm1, q0, qp1, qm, qp);
+#pragma unroll
+                    for (int s = 0; s < NRS; ++s) { RI[s * NRI + f] = qm[s]; RI[(NRS + s) * NRI + f] = qp[s]; }
+                } else {
+                    const int g = f - NRI;
+                    const int cj = g / TI - 1, col = g % TI;               // rows -1..TJ
+                    if (col >= ni_t || cj > nj_t) continue;
+                    const int p = (col + 2) + PW * (cj + 2);
+                    gather<R, NRS, 1>(cur, PLANE, p - PW, qm1);
+                    gather<R, NRS, 1>(cur, PLANE, p, q0);
+                    gather<R, NRS, 1>(cur, PLANE, p + PW, qp1);
+                    recon_cell<R, NRS, MHD, OPT>(w[1], wf[1], P, qm1, q0, qp1, qm, qp);
+#pragma unroll
+                    for (int s = 0; s < NRS; ++s) { RJ[s * NRJ + g] = qm[s]; RJ[(NRS + s) * NRJ + g] = qp[s]; }
+                }
+            }
+            __syncthreads();
+
+            // ---------------- phase C: interface fluxes
+            R fT[NQ];
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) fT[q] = R(0);
+            if (active && has_k) {
+                face_flux<R, MHD, FLUX, 2, NPV>(P, c_hR, kq_prev_p, kq_m, cur, pidx, slot(k + 1), pidx, PLANE, fT);
+#pragma unroll
+                for (int s = 0; s < NRS; ++s) kq_prev_p[s] = kq_p[s];
+            }
+            for (int f = f0; f < NFI + NFJ && f < fend; f += fstride) {
+                R qL[NRS], qR[NRS], F[NQ];
+                if (f < NFI) {
+                    const int row = f / (TI + 1), fi = f % (TI + 1);       // faces 0..TI
+                    if (row >= nj_t || fi > ni_t) continue;
+                    const int rl = fi + (TI + 2) * row;                    // RI index of cell fi-1
+#pragma unroll
+                    for (int s = 0; s < NRS; ++s) { qL[s] = RI[(NRS + s) * NRI + rl]; qR[s] = RI[s * NRI + rl + 1]; }
+                    const int p = (fi + 2) + PW * (row + 2);
+                    face_flux<R, MHD, FLUX, 0, NPV>(P, c_hR, qL, qR, cur, p - 1, cur, p, PLANE, F);
+#pragma unroll
+                    for (int q = 0; q < NQ; ++q) FI[q * NFI + f] = F[q];
+                } else {
+                    const int g = f - NFI;
+                    const int fj = g / TI, col = g % TI;                   // faces 0..TJ
+                    if (col >= ni_t || fj > nj_t) continue;
+                    const int rl = col + TI * fj;                          // RJ index of row fj-1
+#pragma unroll
+                    for (int s = 0; s < NRS; ++s) { qL[s] = RJ[(NRS + s) * NRJ + rl]; qR[s] = RJ[s * NRJ + rl + TI]; }
+                    const int p = (col + 2) + PW * (fj + 2);
+                    face_flux<R, MHD, FLUX, 1, NPV>(P, c_hR, qL, qR, cur, p - PW, cur, p, PLANE, F);
+#pragma unroll
+                    for (int q = 0; q < NQ; ++q) FJ[q * NFJ + g] = F[q];
+                }
+            }
+            __syncthreads();
+
+            // ---------------- phase D: residual (e4/fvcell.d:824-856, faces W, E, S, N, B, T) and update
+            if (active) {
+                const long long cell = cell_index(B, t.i0 + ti, t.j0 + tj, k);
+                const long long g = B.offset + cell;
+                double dU[NQ];
+                if (FAST) {
+                    // float path: differences of opposite faces in float (same-signed,
+                    // nearly equal fluxes subtract exactly), accumulation in FP64
+                    const double Vi = B.vol_inv;
+#pragma unroll
+                    for (int q = 0; q < NQ; ++q) {
+                        R dI = FI[q * NFI + ti + (TI + 1) * tj] - FI[q * NFI + ti + 1 + (TI + 1) * tj];
+                        R dJ = FJ[q * NFJ + ti + TI * tj] - FJ[q * NFJ + ti + TI * (tj + 1)];
+                        double si = (double)dI * Ai + (double)dJ * Aj;
+                        if (has_k) si += (double)(fB[q] - fT[q]) * Ak;
+                        dU[q] = Vi * si;
+                    }
+                } else
 #pragma unroll
                 for (int q = 0; q < NQ; ++q) {
-                    R dI = FI[q * NFI + ti + (TI + 1) * tj] - FI[q * NFI + ti + 1 + (TI + 1) * tj];
-                    R dJ = FJ[q * NFJ + ti + TI * tj] - FJ[q * NFJ + ti + TI * (tj + 1)];
-                    double si = (double)dI * Ai + (double)dJ * Aj;
-                    if (has_k) si += (double)(fB[q] - fT[q]) * Ak;
-                    dU[q] = Vi * si;
-                }
-            } else
-#pragma unroll
-            for (int q = 0; q < NQ; ++q) {
-                double FW = (double)FI[q * NFI + ti + (TI + 1) * tj];
-                double FE = (double)FI[q * NFI + ti + 1 + (TI + 1) * tj];
-                double FS = (double)FJ[q * NFJ + ti + TI * tj];
-                double FN = (double)FJ[q * NFJ + ti + TI * (tj + 1)];
-                double si = 0.0;
-                si = __dsub_rn(si, d_mul(FW, -Ai));
-                si = __dsub_rn(si, d_mul(FE, Ai));
-                si = __dsub_rn(si, d_mul(FS, -Aj));
-                si = __dsub_rn(si, d_mul(FN, Aj));
-                if (has_k) {
-                    si = __dsub_rn(si, d_mul((double)fB[q], -Ak));
-                    si = __dsub_rn(si, d_mul((double)fT[q], Ak));
-                }
-                dU[q] = d_add(d_mul(B.vol_inv, si), 0.0);
-            }
-            if (STAGE == 0) {
-#pragma unroll
-                for (int q = 0; q < NQ; ++q) A.R_out[(long long)q * A.total + g] = dU[q];
-            } else {
-                double U[10];
-#pragma unroll
-                for (int q = 0; q < NQ; ++q) U[q] = __ldg(Uin + (long long)q * A.total + g);
-                if (STAGE == 1) {
-#pragma unroll
-                    for (int q = 0; q < NQ; ++q) {
-                        A.dU0[(long long)q * A.total + g] = dU[q];
-                        U[q] = d_add(U[q], d_mul(dt, dU[q]));
+                    double FW = (double)FI[q * NFI + ti + (TI + 1) * tj];
+                    double FE = (double)FI[q * NFI + ti + 1 + (TI + 1) * tj];
+                    double FS = (double)FJ[q * NFJ + ti + TI * tj];
+                    double FN = (double)FJ[q * NFJ + ti + TI * (tj + 1)];
+                    double si = 0.0;
+                    si = __dsub_rn(si, d_mul(FW, -Ai));
+                    si = __dsub_rn(si, d_mul(FE, Ai));
+                    si = __dsub_rn(si, d_mul(FS, -Aj));
+                    si = __dsub_rn(si, d_mul(FN, Aj));
+                    if (has_k) {
+                        si = __dsub_rn(si, d_mul((double)fB[q], -Ak));
+                        si = __dsub_rn(si, d_mul((double)fT[q], Ak));
                     }
-                } else {
+                    dU[q] = d_add(d_mul(B.vol_inv, si), 0.0);
+                }
+                if (STAGE == 0) {
 #pragma unroll
-                    for (int q = 0; q < NQ; ++q) {
-                        double d0 = __ldg(A.dU0 + (long long)q * A.total + g);
-                        U[q] = d_add(U[q], d_mul(dt, d_add(d_mul(0.5, d0), d_mul(0.5, dU[q]))));
+                    for (int q = 0; q < NQ; ++q) A.R_out[(long long)q * A.total + g] = dU[q];
+                } else {
+                    double U[10];
+#pragma unroll
+                    for (int q = 0; q < NQ; ++q) U[q] = __ldg(Uin + (long long)q * A.total + g);
+                    if (STAGE == 1) {
+#pragma unroll
+                        for (int q = 0; q < NQ; ++q) {
+                            A.dU0[(long long)q * A.total + g] = dU[q];
+                            U[q] = d_add(U[q], d_mul(dt, dU[q]));
+                        }
+                    } else {
+#pragma unroll
+                        for (int q = 0; q < NQ; ++q) {
+                            double d0 = __ldg(A.dU0 + (long long)q * A.total + g);
+                            U[q] = d_add(U[q], d_mul(dt, d_add(d_mul(0.5, d0), d_mul(0.5, dU[q]))));
+                        }
                     }
-                }
-                if (MHD && P.divergence_cleaning) U[PSI] = d_mul(U[PSI], damp);
-                if (STAGE == 2) {
-#pragma unroll
-                    for (int q = 0; q < NQ; ++q) Uout[(long long)q * A.total + g] = U[q];
-                }
-                Prim<double> s;
-                double p, T;
-                int st = (FAST && !MHD) ? decode_fast(P, U, s, p, T) : decode(P, U, s, p, T);
-                if (st != 0) {
-                    atomicAdd(&A.ctl->n_fail, 1);
-                    atomicMin(reinterpret_cast<unsigned long long*>(&A.ctl->first_bad_cell),
-                              (unsigned long long)g);
-                } else {
-                    if (!check_data(P, s, p, T)) atomicAdd(STAGE == 1 ? &A.ctl->n_invalid1 : &A.ctl->n_invalid2, 1);
+                    if (MHD && P.divergence_cleaning) U[PSI] = d_mul(U[PSI], damp);
                     if (STAGE == 2) {
-                        double sig = (FAST && !MHD) ? signal_fast(P, inv_len, s) : signal_frequency(P, B, s);
-                        sig_max = fmax(sig_max, sig);
-                        if (cell == (long long)B.n[0] * B.n[1] * B.n[2] - 1) A.last_signal[blk] = sig;
+#pragma unroll
+                        for (int q = 0; q < NQ; ++q) Uout[(long long)q * A.total + g] = U[q];
+                    }
+                    Prim<double> s;
+                    double p, T;
+                    int st = (FAST && !MHD) ? decode_fast(P, U, s, p, T) : decode(P, U, s, p, T);
+                    if (st != 0) {
+                        atomicAdd(&A.ctl->n_fail, 1);
+                        atomicMin(reinterpret_cast<unsigned long long*>(&A.ctl->first_bad_cell),
+                                  (unsigned long long)g);
+                    } else {
+                        if (!check_data(P, s, p, T)) atomicAdd(STAGE == 1 ? &A.ctl->n_invalid1 : &A.ctl->n_invalid2, 1);
+                        if (STAGE == 2) {
+                            double sig = (FAST && !MHD) ? signal_fast(P, inv_len, s) : signal_frequency(P, B, s);
+                            sig_max = fmax(sig_max, sig);
+                            if (cell == (long long)B.n[0] * B.n[1] * B.n[2] - 1) A.last_signal[blk] = sig;
+                        }
                     }
                 }
+            }
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) fB[q] = fT[q];
+        }
+
+        if (STAGE == 2) {
+            // CTA max of the signal frequency -> one atomic per CTA (dt rule input)
+            for (int o = 16; o > 0; o >>= 1) sig_max = fmax(sig_max, __shfl_xor_sync(0xffffffffu, sig_max, o));
+            if ((tid & 31) == 0) s_red[tid >> 5] = sig_max;
+            __syncthreads();
+            if (tid == 0) {
+                double m = s_red[0];
+                for (int wv = 1; wv < NT / 32; ++wv) m = fmax(m, s_red[wv]);
+                atomicMax(&A.max_signal[blk], (unsigned long long)__double_as_longlong(m));
             }
         }
-#pragma unroll
-        for (int q = 0; q < NQ; ++q) fB[q] = fT[q];
-    }
-
-    if (STAGE == 2) {
-        // CTA max of the signal frequency -> one atomic per CTA (dt rule input)
-        for (int o = 16; o > 0; o >>= 1) sig_max = fmax(sig_max, __shfl_xor_sync(0xffffffffu, sig_max, o));
-        if ((tid & 31) == 0) s_red[tid >> 5] = sig_max;
+        if (!PERS) break;
         __syncthreads();
-        if (tid == 0) {
-            double m = s_red[0];
-            for (int wv = 1; wv < NT / 32; ++wv) m = fmax(m, s_red[wv]);
-            atomicMax(&A.max_signal[blk], (unsigned long long)__double_as_longlong(m));
+        if (threadIdx.x == 0) s_tile = (int)atomicAdd(&qctl->tile_next, 1u);
+        __syncthreads();
+        tix = s_tile;
+    }
+    if (PERS && threadIdx.x == 0) {
+        // every CTA has taken its last ticket before it counts itself done
+        if (atomicAdd(&qctl->tile_done, 1u) == gridDim.x - 1) {
+            atomicExch(&qctl->tile_next, 0u);
+            atomicExch(&qctl->tile_done, 0u);
         }
     }
 }

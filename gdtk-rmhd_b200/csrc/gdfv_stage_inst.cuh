@@ -1,0 +1,98 @@
+// gdfv_stage_inst.cuh -- launch and configuration of the stage-kernel
+// instantiations of one flux precision.  Included once by each precision's
+// translation unit, which defines GDFV_REAL, GDFV_TJ, GDFV_LAUNCH and
+// GDFV_CONFIGURE first.
+#include "gdfv_launch.h"
+
+namespace gdfv {
+
+namespace {
+using Real = GDFV_REAL;
+constexpr int TJ = GDFV_TJ;
+
+// Resident CTAs on the device (CTAs per SM x SMs) of the persistent
+// instantiation: the grid of the persistent launch.
+template <int STAGE, bool MHD, int FLUX>
+int& resident() {
+    static int v = 0;
+    return v;
+}
+
+template <int STAGE, bool MHD, int FLUX>
+cudaError_t launch_one(const StageArgs& A, cudaStream_t s) {
+    using G = Geo<Real, MHD, TJ>;
+    // defaults (limiter and extrema clipping on) take the specialised path, which
+    // also has the persistent form
+    if (A.P.apply_limiter && A.P.extrema_clipping) {
+        const int cap = resident<STAGE, MHD, FLUX>();
+        if (A.persistent && cap > 0)
+            stage_kernel<STAGE, Real, MHD, FLUX, TJ, 1, 1><<<cap < A.n_tiles ? cap : A.n_tiles, G::NT, G::bytes, s>>>(A);
+        else
+            stage_kernel<STAGE, Real, MHD, FLUX, TJ, 1, 0><<<A.n_tiles, G::NT, G::bytes, s>>>(A);
+    } else {
+        stage_kernel<STAGE, Real, MHD, FLUX, TJ, 0, 0><<<A.n_tiles, G::NT, G::bytes, s>>>(A);
+    }
+    return cudaGetLastError();
+}
+
+template <class K>
+cudaError_t set_smem(K k, size_t bytes) {
+    return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+template <int STAGE, bool MHD, int FLUX>
+cudaError_t configure_one(int n_sm) {
+    using G = Geo<Real, MHD, TJ>;
+    cudaError_t e = set_smem(stage_kernel<STAGE, Real, MHD, FLUX, TJ, 0, 0>, G::bytes);
+    if (e == cudaSuccess) e = set_smem(stage_kernel<STAGE, Real, MHD, FLUX, TJ, 1, 0>, G::bytes);
+    if (e == cudaSuccess) e = set_smem(stage_kernel<STAGE, Real, MHD, FLUX, TJ, 1, 1>, G::bytes);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, stage_kernel<STAGE, Real, MHD, FLUX, TJ, 1, 1>, G::NT,
+                                                      G::bytes);
+    if (e != cudaSuccess) return e;
+    resident<STAGE, MHD, FLUX>() = per_sm * n_sm;
+    return cudaSuccess;
+}
+
+template <int STAGE>
+cudaError_t launch_stage_t(int flux, bool mhd, const StageArgs& A, cudaStream_t s) {
+    if (mhd) {
+        if (flux == FLUX_HLLE) return launch_one<STAGE, true, FLUX_HLLE>(A, s);
+        return cudaErrorInvalidValue;
+    }
+    if (flux == FLUX_AUSMDV) return launch_one<STAGE, false, FLUX_AUSMDV>(A, s);
+    if (flux == FLUX_HLLC) return launch_one<STAGE, false, FLUX_HLLC>(A, s);
+    return cudaErrorInvalidValue;
+}
+
+template <int STAGE>
+cudaError_t configure_t(int n_sm) {
+    cudaError_t e;
+    if ((e = configure_one<STAGE, true, FLUX_HLLE>(n_sm)) != cudaSuccess) return e;
+    if ((e = configure_one<STAGE, false, FLUX_AUSMDV>(n_sm)) != cudaSuccess) return e;
+    return configure_one<STAGE, false, FLUX_HLLC>(n_sm);
+}
+}  // namespace
+
+cudaError_t GDFV_LAUNCH(int stage, int flux, bool mhd, const StageArgs& A, cudaStream_t s) {
+    if (A.n_tiles <= 0) return cudaSuccess;
+    switch (stage) {
+    case 0: return launch_stage_t<0>(flux, mhd, A, s);
+    case 1: return launch_stage_t<1>(flux, mhd, A, s);
+    case 2: return launch_stage_t<2>(flux, mhd, A, s);
+    }
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t GDFV_CONFIGURE() {
+    int dev = 0, n_sm = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    if ((e = configure_t<0>(n_sm)) != cudaSuccess) return e;
+    if ((e = configure_t<1>(n_sm)) != cudaSuccess) return e;
+    return configure_t<2>(n_sm);
+}
+
+}  // namespace gdfv

@@ -26,7 +26,7 @@ _STR_KEYS = ("flux_calculator", "gasdynamic_update_scheme", "thermo_interpolator
 _INT_KEYS = ("interpolation_order", "dimensions", "MHD", "divergence_cleaning", "apply_limiter",
              "extrema_clipping", "apply_entropy_fix", "interpolate_in_local_frame", "stringent_cfl",
              "cfl_count", "max_attempts_for_step", "max_invalid_cells", "fixed_time_step",
-             "n_ghost_cell_layers", "glm_reference_indexing", "tile_kchunk")
+             "n_ghost_cell_layers", "glm_reference_indexing", "tile_kchunk", "persistent", "autotune")
 _DBL_KEYS = ("cfl_value", "dt_init", "dt_max", "epsilon_van_albada", "divB_damping_length",
              "flowstate_limits_max_velocity", "flowstate_limits_max_temp", "flowstate_limits_min_temp")
 
@@ -56,7 +56,9 @@ class Config:
         self.fixed_time_step = False
         self.n_ghost_cell_layers = 2
         self.glm_reference_indexing = True
-        self.tile_kchunk = 0
+        self.tile_kchunk = 0          # planes per tile (0: the block's nkc up to 32)
+        self.persistent = False       # True: stage kernels as a resident grid over the tile queue
+        self.autotune = False         # time tile shapes and launch forms on the first run
         self.cfl_value = 0.5
         self.dt_init = 1.0e-3
         self.dt_max = 1.0e-3
@@ -274,6 +276,13 @@ class Simulation:
         ms = ffi.new("double[2]")
         check(self.ctx, self.L.gdfv_time_stages(self.ctx, int(reps), ms))
         return ms[0], ms[1]
+
+    def option(self, key):
+        """Current value of a numeric option as the library holds it (after an
+        autotuned run: tile_kchunk, persistent and autotune_stage_ms)."""
+        v = ffi.new("double*")
+        check(self.ctx, self.L.gdfv_config_get_double(self.ctx, key.encode(), v))
+        return v[0]
 
     def close(self):
         if getattr(self, "ctx", -1) >= 0:

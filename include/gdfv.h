@@ -52,7 +52,14 @@ int gdfv_context_free(int ctx);
  * max_invalid_cells, fixed_time_step, n_ghost_cell_layers (2), glm_reference_indexing,
  * tile_kchunk.  Doubles: cfl_value, dt_init, dt_max, epsilon_van_albada, R, gamma,
  * divB_damping_length, flowstate_limits_max_velocity, flowstate_limits_max_temp,
- * flowstate_limits_min_temp.  Unknown key or value: GDFV_ERR_ARG. */
+ * flowstate_limits_min_temp.  Unknown key or value: GDFV_ERR_ARG.
+ * Scheduling integers with no reference counterpart (results do not depend on them):
+ * tile_kchunk (planes per tile, 0: the block's nkc up to 32), persistent (1: each
+ * stage is one resident grid taking the tiles of all blocks from a queue; default 0:
+ * one CTA per tile),
+ * autotune (1: the first gdfv_run times the tile k-chunks and both launch forms and
+ * keeps the fastest).  gdfv_config_get_double also reads tile_kchunk, persistent,
+ * autotune and autotune_stage_ms (stage 1 + stage 2 time of the tuned choice). */
 int gdfv_config_set_str(int ctx, const char* key, const char* value);
 int gdfv_config_set_int(int ctx, const char* key, long long value);
 int gdfv_config_set_double(int ctx, const char* key, double value);

@@ -35,6 +35,11 @@ def test_config_accepts_reference_names_and_rejects_others():
     for key, val in (("interpolation_order", 2), ("MHD", 1), ("divergence_cleaning", 1), ("cfl_count", 10),
                      ("max_attempts_for_step", 3), ("n_ghost_cell_layers", 2), ("dimensions", 3)):
         assert L.gdfv_config_set_int(h, key.encode(), val) == GDFV_OK, key
+    for key, val in (("tile_kchunk", 16), ("persistent", 0), ("autotune", 1)):
+        assert L.gdfv_config_set_int(h, key.encode(), val) == GDFV_OK, key
+        check(h, L.gdfv_config_get_double(h, key.encode(), v := ffi.new("double*")))
+        assert v[0] == val
+    assert L.gdfv_config_set_int(h, b"tile_kchunk", -1) == GDFV_ERR_ARG
     assert L.gdfv_config_set_int(h, b"interpolation_order", 3) == GDFV_ERR_ARG
     assert L.gdfv_config_set_int(h, b"cfl_count", 0) == GDFV_ERR_ARG
     for key in ("cfl_value", "dt_init", "dt_max", "epsilon_van_albada", "R", "gamma", "divB_damping_length"):

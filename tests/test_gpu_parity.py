@@ -110,3 +110,42 @@ def test_inflow_box_fp32_flux(flux):
     mom_err = cases.rel_l2(Ug[1:4].ravel(), Uo[1:4].ravel())
     e_err = cases.rel_l2(Ug[4], Uo[4])
     assert max(rho_err, mom_err, e_err) <= TOL_FP32_L2, (rho_err, mom_err, e_err)
+
+
+def test_c3_lattice_uneven_blocks_fp64():
+    """64 blocks on a 4x4x4 lattice with per-axis sizes drawn by seed (the batched
+    multi-block configuration at sizes the oracle finishes in seconds): every stage
+    is one persistent launch over the tile table of all blocks."""
+    case = cases.multiblock_lattice(nb=(4, 4, 4), sizes=(16, 32, 48), seed=11)
+    orc, sim = run_both(case, 4, persistent=True)
+    assert sim.option("persistent") == 1
+    assert compare_fp64(case, orc, sim) <= TOL_FP64
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_schedule_does_not_change_results(precision):
+    """Tile k-chunk, launch form and the autotuner's choice change who computes a
+    face, not what is computed.  FP64 (no FMA contraction): the states after N
+    steps are bit-identical for every schedule.  Float flux (compiled with
+    contraction, which may differ between the inlined copies of a face evaluation):
+    every schedule is deterministic run to run, and schedules agree to float
+    rounding (rel L2 <= 1e-6)."""
+    case = cases.multiblock_lattice(nb=(3, 2, 2), sizes=(16, 40, 72), seed=12, precision=precision)
+    runs = {}
+    for name, extra in (("tile8", dict(persistent=False, tile_kchunk=8)), ("tile8b", dict(persistent=False, tile_kchunk=8)),
+                        ("tile0", dict(persistent=False)), ("tile5", dict(persistent=False, tile_kchunk=5)),
+                        ("pers0", dict(persistent=True)), ("pers8", dict(persistent=True, tile_kchunk=8)),
+                        ("tuned", dict(autotune=True))):
+        sim = cases.build_gpu(case, **extra)
+        assert sim.run(max_step=6) == 6
+        runs[name] = np.concatenate([sim.get_conserved(b) for b in range(len(case.blocks))], axis=1)
+        if name == "tuned":
+            assert sim.option("tile_kchunk") in (8, 16, 32, 64) and sim.option("autotune_stage_ms") > 0
+        sim.close()
+    assert np.array_equal(runs["tile8"], runs["tile8b"])
+    for name in ("tile0", "tile5", "pers0", "pers8", "tuned"):
+        if precision == "fp64":
+            assert np.array_equal(runs["tile8"], runs[name]), name
+        else:
+            for q in range(5):
+                assert cases.rel_l2(runs[name][q], runs["tile8"][q]) <= 1e-6, (name, q)
