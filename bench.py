@@ -140,7 +140,8 @@ def adjoint_over_forward(nsteps=50, checkpoint_every=10, shape=(128, 128, 64)):
     integral over the y-min wall after 50 steps, gradient w.r.t. U0 and the inflow
     state through the checkpointed rollout (every 10 steps).  Returns the ratio of
     the backward time (recomputation + adjoint steps) to the forward time of the
-    same 50 steps run by gdfv_run, both with CUDA events on the device."""
+    same 50 steps run by gdfv_run, both with CUDA events on the device and both
+    warm (a 10-step rollout and its backward run first)."""
     import torch
     import cases
     from gdfv.autograd import rollout
@@ -162,20 +163,120 @@ def adjoint_over_forward(nsteps=50, checkpoint_every=10, shape=(128, 128, 64)):
     torch.cuda.synchronize()
     fwd_ms = e0.elapsed_time(e1)
     theta = torch.tensor([inf["p"], inf["T"], inf["vel"][0]], dtype=torch.float64, requires_grad=True)
-    U0r = U0.clone().requires_grad_(True)
-    with torch.cuda.stream(stream):
-        UN = rollout(sim, U0r, theta, nsteps, checkpoint_every)
-        J = wall_pressure(case, UN, case.R)
-    torch.cuda.synchronize()
-    b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    b0.record()
-    J.backward()
-    b1.record()
-    torch.cuda.synchronize()
-    adj_ms = b0.elapsed_time(b1)
+    adj_ms = None
+    for rep in range(2):   # the first pass warms the adjoint (scratch allocation, face tables)
+        theta.grad = None
+        U0r = U0.clone().requires_grad_(True)
+        with torch.cuda.stream(stream):
+            UN = rollout(sim, U0r, theta, nsteps if rep else checkpoint_every, checkpoint_every)
+            J = wall_pressure(case, UN, case.R)
+        torch.cuda.synchronize()
+        b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        b0.record()
+        J.backward()
+        b1.record()
+        torch.cuda.synchronize()
+        adj_ms = b0.elapsed_time(b1)
     return dict(ratio=adj_ms / fwd_ms, forward_ms=fwd_ms, adjoint_ms=adj_ms, steps=nsteps,
                 checkpoint_every=checkpoint_every, workload=f"M=3 inflow box {shape[0]}x{shape[1]}x{shape[2]} FP64",
                 dJ_dp_inflow=float(theta.grad[0]), grad_U0_norm=float(U0r.grad.norm()))
+
+
+def _timed_run(sim, stream, steps):
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sim.run(max_step=steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def _l2_errors(Uf, Ud, mhd=False):
+    import cases
+    err = dict(rho=cases.rel_l2(Uf[0], Ud[0]), momentum=cases.rel_l2(Uf[1:4].ravel(), Ud[1:4].ravel()),
+               energy=cases.rel_l2(Uf[4], Ud[4]))
+    if mhd:
+        err["B"] = cases.rel_l2(Uf[5:8].ravel(), Ud[5:8].ravel())
+    return err
+
+
+def accuracy_leg(sims, n, flux, total_steps, stream):
+    """FP32-flux against plain FP64 on the M=3 inflow box after `total_steps` steps
+    from the same seeded state (both forms run their own dt rule)."""
+    import cases
+    out = {}
+    if sims is None:
+        sims = {}
+        for prec in ("fp32", "fp64"):
+            case = cases.c2_inflow_box(n=(n, n, n), flux=flux, precision=prec, seed=4321)
+            sim = cases.build_gpu(case)
+            sim.set_stream(stream.cuda_stream)
+            sims[prec] = sim
+    for prec, sim in sims.items():
+        done = sim.time()["step"]
+        if total_steps > done:
+            sim.run(max_step=total_steps - done)
+    Uf, Ud = sims["fp32"].get_conserved(0), sims["fp64"].get_conserved(0)
+    out["steps"] = total_steps
+    out["rel_l2_vs_fp64"] = _l2_errors(Uf, Ud)
+    out["time_fp32"], out["time_fp64"] = sims["fp32"].time()["time"], sims["fp64"].time()["time"]
+    return out
+
+
+def multiblock_leg(stream, steps=20, seed=2024):
+    """Batched multi-block configuration: 64 blocks on a 4x4x4 lattice with per-axis
+    sizes drawn by seed from {16,32,48,64,96,128}, full-face exchange inside, the M=3
+    inflow box's boundary conditions outside; FP32 flux; tiles and launch form chosen
+    by the autotuner on the first run."""
+    import cases
+    case = cases.multiblock_lattice(nb=(4, 4, 4), sizes=(16, 32, 48, 64, 96, 128), seed=seed, precision="fp32")
+    cells = sum(int(np.prod(b["n"])) for b in case.blocks)
+    sim = cases.build_gpu(case, autotune=True)
+    sim.set_stream(stream.cuda_stream)
+    sim.run(max_step=3)
+    ms = _timed_run(sim, stream, steps)
+    out = dict(workload=f"64-block lattice (4x4x4, sizes by seed {seed} from 16..128), FP32 flux",
+               cells=cells, steps=steps, value=cells * steps / (ms * 1e-3) / 1e6, unit=UNIT,
+               tile_kchunk=sim.option("tile_kchunk"), persistent=bool(sim.option("persistent")),
+               autotune_stage_ms=sim.option("autotune_stage_ms"))
+    sim.close()
+    return out
+
+
+def _max_divB(U, n, d):
+    """max |div B| by central differences of the cell-centred field (periodic)."""
+    nic, njc, nkc = n
+    Bx = U[5].reshape(nkc, njc, nic)
+    By = U[6].reshape(nkc, njc, nic)
+    div = (np.roll(Bx, -1, axis=2) - np.roll(Bx, 1, axis=2)) / (2 * d[0]) + \
+          (np.roll(By, -1, axis=1) - np.roll(By, 1, axis=1)) / (2 * d[1])
+    return float(np.abs(div).max())
+
+
+def mhd_leg(stream, steps=2000, n=(512, 512, 4), dt=8.0e-5):
+    """Ideal-MHD Orszag-Tang vortex (hlle + GLM divergence cleaning, periodic, gamma
+    5/3, 1% seeded density noise): plain FP64 and FP32-flux forms at one fixed dt
+    (so that both compare at the same times; 2000 x 8e-5 = 0.16), throughput over
+    the last 100 steps, error of the float form and max |div B| of both."""
+    import cases
+    out = dict(workload=f"Orszag-Tang {n[0]}x{n[1]}x{n[2]} hlle+GLM, fixed dt {dt}", steps=steps)
+    states = {}
+    cells = int(np.prod(n))
+    for prec in ("fp64", "fp32"):
+        case = cases.orszag_tang(n=n, precision=prec)
+        sim = cases.build_gpu(case, fixed_time_step=True, dt_init=dt, dt_max=dt)
+        sim.set_stream(stream.cuda_stream)
+        sim.run(max_step=steps - 100)
+        ms = _timed_run(sim, stream, 100)
+        out[f"value_{prec}"] = cells * 100 / (ms * 1e-3) / 1e6
+        states[prec] = sim.get_conserved(0)
+        out[f"max_divB_{prec}"] = _max_divB(states[prec], n, case.blocks[0]["d"])
+        out[f"time_{prec}"] = sim.time()["time"]
+        sim.close()
+    out["unit"] = UNIT
+    out["rel_l2_vs_fp64"] = _l2_errors(states["fp32"], states["fp64"], mhd=True)
+    return out
 
 
 def run_reference_arm(args):
@@ -207,6 +308,9 @@ def main():
     ap.add_argument("--size", type=int, default=256)
     ap.add_argument("--flux", default="ausmdv", choices=["ausmdv", "hllc"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--accuracy-steps", type=int, default=1000,
+                    help="steps after which the FP32 form is compared with FP64 (0: at the timed steps)")
+    ap.add_argument("--no-extra", action="store_true", help="skip the multi-block, MHD and adjoint legs")
     ap.add_argument("--profile-case", action="store_true",
                     help="small case for ncu captures: 128^3, warmup steps then exit")
     args = ap.parse_args()
@@ -268,10 +372,9 @@ def main():
         results[prec] = dict(ms=ms, taken=taken, clocks=sampler.summary())
 
     # accuracy of the FP32-flux form against the plain FP64 form after the same steps
-    Uf = sims["fp32"][1].get_conserved(0)
-    Ud = sims["fp64"][1].get_conserved(0)
-    err = dict(rho=cases.rel_l2(Uf[0], Ud[0]), momentum=cases.rel_l2(Uf[1:4].ravel(), Ud[1:4].ravel()),
-               energy=cases.rel_l2(Uf[4], Ud[4]))
+    acc_steps = max(args.accuracy_steps, args.warmup + args.steps)
+    acc = accuracy_leg({p: sims[p][1] for p in sims}, n, args.flux, acc_steps, stream)
+    err = acc["rel_l2_vs_fp64"]
 
     # roofline of the dominant kernel (corrector stage) of the FP32-flux form, live
     sim32 = sims["fp32"][1]
@@ -336,12 +439,24 @@ def main():
         "clocks": results["fp32"]["clocks"],
         "clocks_fp64": results["fp64"]["clocks"],
     }
-    try:
-        adj = adjoint_over_forward()
-        line["adjoint_over_forward"] = adj["ratio"]
-        line["adjoint"] = adj
-    except Exception as e:  # reported, never required for the throughput line
-        line["adjoint"] = {"error": str(e)}
+    line["accuracy"] = acc
+    if not args.no_extra:
+        for sim in list(sims.values()) + [(None, sim_e2e)]:
+            sim[1].close()
+        torch.cuda.empty_cache()
+        legs = [("adjoint", adjoint_over_forward),
+                ("accuracy_other_flux", lambda: accuracy_leg(None, n, "hllc" if args.flux == "ausmdv" else "ausmdv",
+                                                             acc_steps, stream)),
+                ("multiblock", lambda: multiblock_leg(stream)),
+                ("mhd", lambda: mhd_leg(stream))]
+        for name, fn in legs:
+            try:
+                line[name] = fn()
+            except Exception as e:  # reported, never required for the throughput line
+                line[name] = {"error": f"{type(e).__name__}: {e}"}
+            torch.cuda.empty_cache()
+        if isinstance(line.get("adjoint"), dict) and "ratio" in line["adjoint"]:
+            line["adjoint_over_forward"] = line["adjoint"]["ratio"]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_oracle_baseline()

@@ -120,6 +120,10 @@ class Rollout(torch.autograd.Function):
         UN = _state_view(sim).clone()
         ctx.sim, ctx.dts, ctx.ckpts, ctx.k = sim, dts, ckpts, checkpoint_every
         ctx.theta = theta.detach().clone()
+        # work arrays of the backward's segment recomputation, allocated with the checkpoints
+        m = min(checkpoint_every, nsteps)
+        ctx.outs = [torch.empty_like(U0) for _ in range(m)]
+        ctx.preds = [torch.empty_like(U0) for _ in range(m)]
         return UN
 
     @staticmethod
@@ -128,8 +132,7 @@ class Rollout(torch.autograd.Function):
         lam = gUN.contiguous().clone()
         gin = torch.zeros((max(1, getattr(sim, "n_inflow", 1)), 6), dtype=torch.float64, device=lam.device)
         n_total = len(dts)
-        outs = [torch.empty_like(lam) for _ in range(min(K, n_total))]
-        preds = [torch.empty_like(lam) for _ in range(min(K, n_total))]
+        outs, preds = ctx.outs, ctx.preds
         for s0 in reversed(range(0, n_total, K)):
             s1 = min(s0 + K, n_total)
             steps_dt(sim, ckpts[s0], dts[s0:s1], outs, preds)
@@ -137,6 +140,7 @@ class Rollout(torch.autograd.Function):
                 U0 = ckpts[s0] if n == s0 else outs[n - s0 - 1]
                 step_adjoint(sim, U0, preds[n - s0], dts[n], lam, gin)
         torch.cuda.synchronize()
+        ctx.outs = ctx.preds = None
         gtheta = inflow_chain(sim, ctx.theta, gin[0].cpu()).to(ctx.theta.device)
         return lam, gtheta, None, None, None
 

@@ -99,6 +99,21 @@ def test_orszag_tang_glm_fp64():
     assert np.max(np.abs(Ug[9] - Uo[9])) <= 1e-10 * (np.max(np.abs(Uo[9])) + 1e-30) + 1e-14
 
 
+@pytest.mark.parametrize("nsteps", [10, 100])
+def test_orszag_tang_fp32_flux(nsteps):
+    """Float-flux MHD (hlle + GLM) against the FP64 oracle on the Orszag-Tang vortex
+    at one fixed dt (both at the same times): float rounding, grown by the limiter
+    as the vortex steepens."""
+    case = cases.orszag_tang(n=(64, 64, 4), cleaning=True)
+    orc, sim = cases.build_pair(case, flux_precision="fp32", fixed_time_step=True, dt_init=5e-4, dt_max=5e-4)
+    assert orc.run(nsteps, fixed_dt=5e-4) == 0
+    assert sim.run(max_step=nsteps) == nsteps
+    Uo, Ug = orc.get_U(0), sim.get_conserved(0)
+    errs = [cases.rel_l2(Ug[0], Uo[0]), cases.rel_l2(Ug[1:4].ravel(), Uo[1:4].ravel()), cases.rel_l2(Ug[4], Uo[4]),
+            cases.rel_l2(Ug[5:8].ravel(), Uo[5:8].ravel())]
+    assert max(errs) <= (1e-6 if nsteps <= 10 else 1e-5), errs
+
+
 @pytest.mark.parametrize("flux", ["ausmdv", "hllc"])
 def test_inflow_box_fp32_flux(flux):
     case = cases.c2_inflow_box(n=(48, 40, 36), flux=flux)
