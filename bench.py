@@ -382,11 +382,13 @@ def main():
     peak, peak_kind = measured_peaks()
     ach2 = BYTES_STAGE2 * cells / (st2 * 1e-3) / 1e9
     traffic = None
-    tf = os.path.join(ROOT, "profiles", "stage2_fp32_traffic.json")
+    tf = os.path.join(ROOT, "profiles", "stage_kernel_fp32_128cube.md")
     if os.path.exists(tf):
+        import re
         with open(tf) as f:
-            tr = json.load(f)
-        traffic = tr.get("bytes_per_cell", 0) * cells if tr.get("bytes_per_cell") else None
+            m = re.search(r"stage2_dram_bytes_per_cell:\s*([0-9.]+)", f.read())
+        if m:   # ncu DRAM bytes per cell of the corrector at 128^3, scaled to this launch
+            traffic = float(m.group(1)) * cells
 
     # end to end through the public API: host state in, K steps, host state out
     case32, _ = sims["fp32"]
