@@ -284,9 +284,16 @@ def run_reference_arm(args):
     if rank != 0:
         return 0
     res = chicken_baseline(args.steps, args.warmup)
+    one_block = None
     if res is None:
         base = cpu_oracle_baseline()
         res = dict(value=base["value"], cpu_baseline=base)
+    else:
+        try:   # the same solver on one block: OpenMP over blocks leaves one core working
+            import chicken_job
+            one_block = chicken_job.bench(steps=10, warmup=2, n=64, nblk=(1, 1, 1))["cpu_baseline"]
+        except Exception as e:
+            one_block = {"error": str(e)}
     line = {
         "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "higher_is_better": True, "impl": "reference",
@@ -295,6 +302,8 @@ def run_reference_arm(args):
         "config": {"workload": "M=3 inflow box 256^3 (bounded CPU sample)", "flux_calculator": "ausmdv"},
         "data": "synthetic",
     }
+    if one_block is not None:
+        line["one_block"] = one_block
     print(json.dumps(line))
     return 0
 
@@ -460,10 +469,18 @@ def main():
         if isinstance(line.get("adjoint"), dict) and "ratio" in line["adjoint"]:
             line["adjoint_over_forward"] = line["adjoint"]["ratio"]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # the reference's own CPU build when present (kind "reference"), the oracle port beside it
         try:
-            line["cpu_baseline"] = cpu_oracle_baseline()
+            ref = chicken_baseline(10, 2)
         except Exception as e:  # the baseline is reported, never required
-            line["cpu_baseline"] = {"error": str(e)}
+            ref = None
+            line["cpu_baseline_reference_error"] = str(e)
+        try:
+            port = cpu_oracle_baseline()
+        except Exception as e:
+            port = {"error": str(e)}
+        line["cpu_baseline"] = ref["cpu_baseline"] if ref else port
+        line["cpu_baseline_port"] = port
     if world > 1:
         dist.destroy_process_group()
     if rank == 0:
