@@ -220,7 +220,8 @@ _ORACLE_BC = {"wall_with_slip": "wall_with_slip", "outflow_simple_extrapolate": 
 def build_oracle(case):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from oracle import OracleSim
-    cfg = {k: v for k, v in case.config.items() if k != "flux_precision"}
+    # the oracle takes the flow-state limits under their GlobalConfig field names
+    cfg = {k.replace("flowstate_limits_", ""): v for k, v in case.config.items() if k != "flux_precision"}
     s = OracleSim(R=case.R, gamma=case.gamma, **cfg)
     for b in case.blocks:
         s.add_block(*b["n"], *b["d"], *b["origin"])

@@ -164,3 +164,34 @@ def test_schedule_does_not_change_results(precision):
         else:
             for q in range(5):
                 assert cases.rel_l2(runs[name][q], runs["tile8"][q]) <= 1e-6, (name, q)
+
+
+@pytest.mark.parametrize("cfl,extra", [(1.6, {}), (4.0, {}), (400.0, {}),
+                                       (0.5, {"flowstate_limits_max_velocity": 1.0e-3})])
+def test_failed_step_retry_and_abort_match_oracle(cfl, extra):
+    """Failure paths of the step (e4/simcore_gasdynamic_step.d:991-1560) driven by an
+    unstable CFL: a decode failure retries the step with dt x 0.2 (up to
+    max_attempts_for_step), invalid cells abort.  GPU and oracle take the same path
+    to the same status, and bit-identical states when the step succeeds."""
+    import gdfv
+    case = cases.c1_shock_box(n=24)
+    case.config.update(cfl_value=cfl, dt_init=1.0, **extra)
+    orc, sim = cases.build_pair(case)
+    rc = orc.run(3)
+    try:
+        taken = sim.run(max_step=3)
+        code = 0
+    except gdfv.GdfvError as e:
+        taken, code = None, e.code
+    if rc == 0:
+        assert code == 0 and taken == 3
+        assert compare_fp64(case, orc, sim) <= TOL_FP64
+        t = sim.time()
+        retried = t["dt"] < 0.5 * min(t["dt_allow"], 1.0)
+        print(f"cfl {cfl}: ok, dt {t['dt']:.3e} dt_allow {t['dt_allow']:.3e} retried {retried}")
+    else:
+        from gdfv._lib import GDFV_ERR_BAD_CELLS, GDFV_ERR_STEP_FAILED
+        assert code != 0, (rc, code)
+        # oracle statuses: -3 too many bad cells, -2 failed after max attempts
+        assert code == (GDFV_ERR_BAD_CELLS if rc == -3 else GDFV_ERR_STEP_FAILED), (rc, code)
+        print(f"cfl {cfl}: status rc={rc} code={code}")
