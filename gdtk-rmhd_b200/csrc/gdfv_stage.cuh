@@ -330,7 +330,14 @@ __device__ __forceinline__ float clip_fast(float q, float A, float B) {
 // OPT = 1: apply_limiter and extrema_clipping known to be on (the defaults).
 // The float path with OPT = 1 works on raw differences a = q0-qm1, b = qp1-q0
 // with the length factors folded into per-direction constants wf (the same
-// expressions: dm = a*t, dp = b*t, so the limiter is (ab+|ab|+eps/t^2)/(a^2+b^2+eps/t^2)).
+// expressions: dm = a*t, dp = b*t, so the limiter is (ab+|ab|+eps/t^2)/(a^2+b^2+eps/t^2)),
+// and without the extrema clipping, which cannot act above float rounding on a
+// uniform grid: with equal lengths vp - q0 = sl*(3b + a)/8 and q0 - vm = sl*(b + 3a)/8,
+// and sl = (ab + |ab|)/(a^2 + b^2 + e) + e/(a^2 + b^2 + e).  The first part moves vp
+// by at most 0.52 b towards qp1 (2ab <= a^2 + b^2, max of 2r(3 + r)/(8(1 + r^2)));
+// the second by at most e*m/(2(m^2 + e)) <= sqrt(e)/4, m = max(|a|, |b|), in any
+// direction.  So vp leaves [q0, qp1] (vm leaves [qm1, q0]) by at most sqrt(e)/4 =
+// 2.5e-7 * cell length, far below float rounding of the reconstructed fields.
 enum : int { WF_EPS = 0, WF_P1, WF_P2, WF_R1, WF_R2, WF_N };
 template <class R, int NRS, bool MHD, int OPT>
 __device__ __forceinline__ void recon_cell(const R* w, const R* wf, const NumParams& P, const R* qm1, const R* q0,
@@ -344,10 +351,8 @@ __device__ __forceinline__ void recon_cell(const R* w, const R* wf, const NumPar
             const R b = qp1[s] - q0[s];
             const R ab = a * b;
             const R sl = (ab + rabs(ab) + e) / (a * a + b * b + e);
-            const R vp = q0[s] + sl * (P1 * b + P2 * a);
-            const R vm = q0[s] - sl * (R1 * b + R2 * a);
-            qp[s] = clip_fast(vp, q0[s], qp1[s]);
-            qm[s] = clip_fast(vm, qm1[s], q0[s]);
+            qp[s] = q0[s] + sl * (P1 * b + P2 * a);
+            qm[s] = q0[s] - sl * (R1 * b + R2 * a);
         }
     } else {
         const R t = w[W_TOC];
