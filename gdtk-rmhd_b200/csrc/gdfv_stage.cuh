@@ -55,6 +55,8 @@ struct StageArgs {
 template <class R, bool MHD, int TJ_>
 struct Geo {
     static constexpr int TI = 32, TJ = TJ_;
+    // the halo cells of a plane (4 TJ + 4 TI) are one item per thread of the 32 (TJ + 1)
+    static_assert(TJ_ >= 4, "column tiles need at least 4 rows");
     static constexpr int NCOL = TI * TJ;
     static constexpr int NT = 32 * (TJ + 1);
     static constexpr int PW = TI + 4, PH = TJ + 4, PLANE = PW * PH;  // padded plane
@@ -599,15 +601,20 @@ __device__ __forceinline__ void load_two(const StageArgs& A, const double* Uin, 
     }
 }
 
-// Resident CTAs per SM the FP32 Euler kernels are compiled for (register budget).
+// Resident CTAs per SM the Euler kernels of each flux precision are compiled for
+// (register budget; three float-flux CTAs also fill the shared memory).
 #ifndef GDFV_MINB_FP32
-#define GDFV_MINB_FP32 2
+#define GDFV_MINB_FP32 3
+#endif
+#ifndef GDFV_MINB_FP64
+#define GDFV_MINB_FP64 2
 #endif
 
 // PERS = 1: persistent grid over the tile queue; 0: one CTA per tile (no
 // state carried between tiles, so the compiler keeps fewer values live).
 template <int STAGE, class R, bool MHD, int FLUX, int TJ, int OPT, int PERS>
-__global__ void __launch_bounds__(32 * (TJ + 1), (sizeof(R) == 4 && !MHD) ? GDFV_MINB_FP32 : 1) stage_kernel(StageArgs A) {
+__global__ void __launch_bounds__(32 * (TJ + 1), MHD ? 1 : (sizeof(R) == 4 ? GDFV_MINB_FP32 : GDFV_MINB_FP64))
+    stage_kernel(StageArgs A) {
     using G = Geo<R, MHD, TJ>;
     constexpr int TI = G::TI, NT = G::NT, NCOL = G::NCOL, PW = G::PW, PLANE = G::PLANE;
     constexpr int NPV = G::NPV, NRS = G::NRS, NQ = G::NQ;
@@ -769,11 +776,18 @@ __global__ void __launch_bounds__(32 * (TJ + 1), (sizeof(R) == 4 && !MHD) ? GDFV
             {
                 const bool lead = active && has_k;
                 int ci[2] = {t.i0 + ti, h_ci}, cj[2] = {t.j0 + tj, h_cj}, ck[2] = {k + 2, k};
-                if (lead || h_on) {
+                // one cell at a time: the FP64 loads and decode of two cells in flight
+                // together cost more registers (spills, occupancy) than their overlap gains
+                if (lead) {
                     Prim<double> pr[2];
-                    load_two<STAGE, FAST, MHD, NQ>(A, Uin, B, dt, damp, lead, h_on, ci, cj, ck, pr);
-                    if (lead) put_prim<R, NPV>(slot(k + 2), PLANE, pidx, pr[0]);
-                    if (h_on) put_prim<R, NPV>(cur, PLANE, h_dst, pr[1]);
+                    load_two<STAGE, FAST, MHD, NQ>(A, Uin, B, dt, damp, true, false, ci, cj, ck, pr);
+                    put_prim<R, NPV>(slot(k + 2), PLANE, pidx, pr[0]);
+                }
+                if (h_on) {
+                    Prim<double> pr[2];
+                    int ci2[2] = {h_ci, 0}, cj2[2] = {h_cj, 0}, ck2[2] = {k, 0};
+                    load_two<STAGE, FAST, MHD, NQ>(A, Uin, B, dt, damp, true, false, ci2, cj2, ck2, pr);
+                    put_prim<R, NPV>(cur, PLANE, h_dst, pr[0]);
                 }
             }
             __syncthreads();
