@@ -17,6 +17,7 @@
 // derivative +1 at x = 0 as in src/ntypes/complex.d:944-955.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <string>
 #include <vector>
 
@@ -297,9 +298,7 @@ struct AdjArgs {
     NumParams P;
 };
 
-__global__ void adj_decode_kernel(AdjArgs a) {
-    long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (g >= a.total) return;
+__device__ __forceinline__ void decode_cell(const AdjArgs& a, long long g) {
     double u[5];
     for (int q = 0; q < 5; ++q) u[q] = a.U[q * a.total + g];
     Prim<double> s;
@@ -307,6 +306,11 @@ __global__ void adj_decode_kernel(AdjArgs a) {
     decode(a.P, u, s, p, T);
     double v[NP] = {s.rho, s.v[0], s.v[1], s.v[2], s.u, s.a};
     for (int m = 0; m < NP; ++m) { a.Pp[m * a.total + g] = v[m]; a.gP[m * a.total + g] = 0.0; }
+}
+
+__global__ void adj_decode_kernel(AdjArgs a) {
+    long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (g < a.total) decode_cell(a, g);
 }
 
 // Stencil cell state from P (with the ghost maps) and the reverse map of a cotangent.
@@ -371,29 +375,46 @@ __device__ void adj_scatter(const AdjArgs& a, const Src& s, const double* gc) {
     }
 }
 
+// Block and cell indices of face f of direction D (the face lies between cells
+// index-1 and index along D).
 template <int D>
-__global__ void __launch_bounds__(128, 3) adj_face_kernel(AdjArgs a) {
-    long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+__device__ __forceinline__ int face_coords(const AdjArgs& a, long long f, int& i, int& j, int& k) {
     const long long* off = a.face_off + D * (a.nblocks + 1);
-    if (f >= off[a.nblocks]) return;
     int b = 0;
     while (off[b + 1] <= f) ++b;
     const BlockDesc& B = a.blocks[b];
-    long long lf = f - off[b];
-    int nf0 = B.n[0] + (D == 0), nf1 = B.n[1] + (D == 1);
-    int i = (int)(lf % nf0);
-    int j = (int)((lf / nf0) % nf1);
-    int k = (int)(lf / ((long long)nf0 * nf1));
-    // stencil: cells at index-2, -1, 0, +1 along D (left cells below the face index)
-    int ci[4], cj[4], ck[4];
-    for (int m = 0; m < 4; ++m) {
-        ci[m] = i - (D == 0 ? 2 - m : 0); cj[m] = j - (D == 1 ? 2 - m : 0); ck[m] = k - (D == 2 ? 2 - m : 0);
-    }
-    Src s[4];
+    const long long lf = f - off[b];
+    const int nf0 = B.n[0] + (D == 0), nf1 = B.n[1] + (D == 1);
+    i = (int)(lf % nf0);
+    j = (int)((lf / nf0) % nf1);
+    k = (int)(lf / ((long long)nf0 * nf1));
+    return b;
+}
+
+// Source of stencil cell m (index -2, -1, 0, +1 along D from the face).
+template <int D>
+__device__ __forceinline__ Src stencil_src(const AdjArgs& a, const BlockDesc& B, int i, int j, int k, int m) {
+    return adj_resolve(a, B, i - (D == 0 ? 2 - m : 0), j - (D == 1 ? 2 - m : 0), k - (D == 2 ? 2 - m : 0));
+}
+
+// The reverse sweep of face f of direction D: cotangents gc[m] of the stencil
+// cells (added to), the kind of each stencil source and the inflow state the
+// stencil reaches (if any).  Only these small records stay live: the sources
+// themselves are resolved again when the cotangents are scattered.
+// rowid identifies the line of faces (block and the two other indices).
+template <int D>
+__device__ __forceinline__ void face_vjp(const AdjArgs& a, long long f, int* kind, int& inflow, double (*gc)[NP],
+                                         long long& rowid) {
+    int i, j, k;
+    const int b = face_coords<D>(a, f, i, j, k);
+    const BlockDesc& B = a.blocks[b];
+    rowid = (long long)b * 0x100000000ll + (D == 0 ? (long long)j + (long long)B.n[1] * k : (long long)i);
     double c[4][NP];
     for (int m = 0; m < 4; ++m) {
-        s[m] = adj_resolve(a, B, ci[m], cj[m], ck[m]);
-        adj_load(a, s[m], c[m]);
+        const Src sm = stencil_src<D>(a, B, i, j, k, m);
+        kind[m] = sm.kind;
+        if (sm.kind == SRC_INFLOW) inflow = sm.inflow;
+        adj_load(a, sm, c[m]);
     }
     // cotangent of the face flux: F enters R_right with +A/V and R_left with -A/V
     const double AV = B.area[D] * B.vol_inv * a.w_scale;
@@ -429,9 +450,6 @@ __global__ void __launch_bounds__(128, 3) adj_face_kernel(AdjArgs a) {
     // ---- reverse
     FS gL, gR;
     ausmdv_vjp(P, L, Rs, gF, gL, gR);
-    double gc[4][NP];
-    for (int m = 0; m < 4; ++m)
-        for (int q = 0; q < NP; ++q) gc[m][q] = 0.0;
     gc[1][5] += gL.a;
     gc[2][5] += gR.a;
     double gqL[5] = {0, 0, 0, 0, 0}, gqR[5] = {0, 0, 0, 0, 0};
@@ -462,13 +480,105 @@ __global__ void __launch_bounds__(128, 3) adj_face_kernel(AdjArgs a) {
         l2r2_rev(w, P, c[0][v], c[1][v], c[2][v], c[3][v], rec, gqL[sc], gqR[sc], gc[0][v], gc[1][v], gc[2][v],
                  gc[3][v]);
     }
-    for (int m = 0; m < 4; ++m) adj_scatter(a, s[m], gc[m]);
+}
+
+// Face f of direction D, one thread.  Along i (D = 0) the four faces whose
+// stencils share a cell are neighbouring lanes of one warp: their contributions
+// to that cell are summed with shuffles first, and one lane adds the sum
+// (same-address atomics from one warp would serialise).
+#ifndef GDFV_ADJ_MINB
+#define GDFV_ADJ_MINB 3
+#endif
+template <int D>
+__device__ __forceinline__ void face_thread(const AdjArgs& a, long long f) {
+    const long long* off = a.face_off + D * (a.nblocks + 1);
+    const bool act = f < off[a.nblocks];
+    int kind[4] = {SRC_INFLOW + 1, SRC_INFLOW + 1, SRC_INFLOW + 1, SRC_INFLOW + 1};
+    int inflow = -1;
+    double gc[4][NP];
+    for (int m = 0; m < 4; ++m)
+        for (int q = 0; q < NP; ++q) gc[m][q] = 0.0;
+    long long rowid = -1 - (long long)threadIdx.x;   // distinct for inactive lanes
+    if (act) face_vjp<D>(a, f, kind, inflow, gc, rowid);
+    if (D == 0) {
+        const unsigned full = 0xffffffffu;
+        const int lane = threadIdx.x & 31;
+        // source lane l + d holds the contribution of its stencil cell m to the
+        // cell of lane l (its own stencil cell 2): m = 0 at d = 2, m = 1 at d = 1, m = 3 at d = -1
+#pragma unroll
+        for (int t = 0; t < 3; ++t) {
+            const int m = t == 0 ? 0 : (t == 1 ? 1 : 3);
+            const int d = t == 0 ? 2 : (t == 1 ? 1 : -1);
+            const bool mine = act && kind[m] == SRC_CELL;
+            const int from = lane + d, to = lane - d;
+            const long long row_from = __shfl_sync(full, rowid, from & 31);
+            const int ok_from = __shfl_sync(full, (int)mine, from & 31);
+            const long long row_to = __shfl_sync(full, rowid, to & 31);
+            const bool recv = from >= 0 && from < 32 && act && ok_from && row_from == rowid;
+            const bool sent = to >= 0 && to < 32 && mine && row_to == rowid;
+#pragma unroll
+            for (int q = 0; q < NP; ++q) {
+                const double v = __shfl_sync(full, gc[m][q], from & 31);
+                if (recv) gc[2][q] += v;
+                if (sent) gc[m][q] = 0.0;
+            }
+            if (sent) kind[m] = SRC_INFLOW + 1;   // nothing left to scatter for this source
+        }
+    }
+    // Inflow ghost states are shared by every face along an inflow boundary: sum the
+    // warp's cotangents per inflow state (a face's stencil crosses at most one
+    // boundary face, so a lane carries at most one state), one atomic per state.
+    {
+        const unsigned full = 0xffffffffu;
+        int key = -1;
+        double vin[NP];
+#pragma unroll
+        for (int q = 0; q < NP; ++q) vin[q] = 0.0;
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            if (act && kind[m] == SRC_INFLOW) {
+                key = inflow;
+#pragma unroll
+                for (int q = 0; q < NP; ++q) vin[q] += gc[m][q];
+                kind[m] = SRC_INFLOW + 1;
+            }
+        }
+        if (__ballot_sync(full, key >= 0)) {
+            const unsigned grp = __match_any_sync(full, key);
+            const int lane = threadIdx.x & 31;
+#pragma unroll
+            for (int q = 0; q < NP; ++q) {
+                double acc = 0.0;
+                for (int src = 0; src < 32; ++src) {
+                    const double v = __shfl_sync(full, vin[q], src);
+                    if ((grp >> src) & 1u) acc += v;
+                }
+                vin[q] = acc;
+            }
+            if (key >= 0 && lane == __ffs(grp) - 1)
+                for (int q = 0; q < NP; ++q) atomicAdd(&a.gInflow[key * NP + q], vin[q]);
+        }
+    }
+    if (!act) return;
+    int i, j, k;
+    const int b = face_coords<D>(a, f, i, j, k);
+    const BlockDesc& B = a.blocks[b];
+    for (int m = 0; m < 4; ++m)
+        if (kind[m] <= SRC_INFLOW) adj_scatter(a, stencil_src<D>(a, B, i, j, k, m), gc[m]);
+}
+
+// All faces of the three directions in one launch: CTAs [0, nb0) take the i faces,
+// [nb0, nb0 + nb1) the j faces, the rest the k faces (128 faces per CTA).
+constexpr int FACE_CTA = 128;
+__global__ void __launch_bounds__(FACE_CTA, GDFV_ADJ_MINB) adj_faces_kernel(AdjArgs a, unsigned nb0, unsigned nb1) {
+    const unsigned bid = blockIdx.x;
+    if (bid < nb0) face_thread<0>(a, (long long)bid * FACE_CTA + threadIdx.x);
+    else if (bid < nb0 + nb1) face_thread<1>(a, (long long)(bid - nb0) * FACE_CTA + threadIdx.x);
+    else face_thread<2>(a, (long long)(bid - nb0 - nb1) * FACE_CTA + threadIdx.x);
 }
 
 // gU = (dP/dU)^T gP for P = decode(U) (e4/fvcell.d:586-822 with ideal_gas.d:98-139)
-__global__ void adj_decode_back_kernel(AdjArgs a) {
-    long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (g >= a.total) return;
+__device__ __forceinline__ void back_cell(const AdjArgs& a, long long g) {
     double U[5];
     for (int q = 0; q < 5; ++q) U[q] = a.U[q * a.total + g];
     double gp[NP];
@@ -496,6 +606,21 @@ __global__ void adj_decode_back_kernel(AdjArgs a) {
         // second product: r = J(U0)^T b
         for (int q = 0; q < 5; ++q) a.lam[q * a.total + g] += r[q];
     }
+}
+
+
+__global__ void adj_decode_back_kernel(AdjArgs a) {
+    long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (g < a.total) back_cell(a, g);
+}
+
+// The reverse decode of one product and the decode of the next, in one pass per
+// cell (the cell's cotangent gP is read, then cleared for the next product).
+__global__ void adj_back_decode_kernel(AdjArgs back, AdjArgs next) {
+    long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (g >= back.total) return;
+    back_cell(back, g);
+    decode_cell(next, g);
 }
 
 }  // namespace
@@ -565,12 +690,10 @@ cudaError_t enqueue_vjp(const AdjView& v, const AdjArgs& a, const std::vector<lo
     const long long total = v.total;
     adj_decode_kernel<<<(unsigned)((total + nt - 1) / nt), nt, 0, v.stream>>>(a);
     cudaError_t e = cudaGetLastError();
-    for (int d = 0; d < 3 && e == cudaSuccess; ++d) {
-        long long nf = off[d * (v.nblocks + 1) + v.nblocks];
-        const unsigned nb = (unsigned)((nf + 127) / 128);  // 128-thread CTAs, 3 per SM by registers
-        if (d == 0) adj_face_kernel<0><<<nb, 128, 0, v.stream>>>(a);
-        if (d == 1) adj_face_kernel<1><<<nb, 128, 0, v.stream>>>(a);
-        if (d == 2) adj_face_kernel<2><<<nb, 128, 0, v.stream>>>(a);
+    if (e == cudaSuccess) {
+        unsigned nb[3];
+        for (int d = 0; d < 3; ++d) nb[d] = (unsigned)((off[d * (v.nblocks + 1) + v.nblocks] + 127) / 128);
+        adj_faces_kernel<<<nb[0] + nb[1] + nb[2], FACE_CTA, 0, v.stream>>>(a, nb[0], nb[1]);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) {
@@ -604,6 +727,59 @@ extern "C" int gdfv_residual_vjp(int ctx, const double* U_dev, const double* W_d
     return GDFV_OK;
 }
 
+namespace {
+
+// A chain of products: the reverse decode of each product runs fused with the
+// decode of the next one (adj_back_decode_kernel); finish() ends the chain.
+struct VjpChain {
+    bool pending = false;
+    AdjArgs back{};
+    cudaError_t product(const AdjView& v, const AdjArgs& a, const std::vector<long long>& off) {
+        const int nt = 256;
+        const unsigned nb_cells = (unsigned)((v.total + nt - 1) / nt);
+        if (pending) adj_back_decode_kernel<<<nb_cells, nt, 0, v.stream>>>(back, a);
+        else adj_decode_kernel<<<nb_cells, nt, 0, v.stream>>>(a);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) {
+            unsigned nb[3];
+            for (int d = 0; d < 3; ++d) nb[d] = (unsigned)((off[d * (v.nblocks + 1) + v.nblocks] + 127) / 128);
+            adj_faces_kernel<<<nb[0] + nb[1] + nb[2], FACE_CTA, 0, v.stream>>>(a, nb[0], nb[1]);
+            e = cudaGetLastError();
+        }
+        back = a;
+        pending = true;
+        return e;
+    }
+    cudaError_t finish(const AdjView& v) {
+        if (!pending) return cudaSuccess;
+        pending = false;
+        const int nt = 256;
+        adj_decode_back_kernel<<<(unsigned)((v.total + nt - 1) / nt), nt, 0, v.stream>>>(back);
+        return cudaGetLastError();
+    }
+};
+
+// The adjoint of one predictor-corrector step, enqueued on v.stream:
+// mu = J(U1)^T (dt/2 lam); b = dt/2 lam + dt mu; lam += mu; then lam += J(U0)^T b.
+cudaError_t enqueue_step_adjoint(const AdjView& v, AdjArgs a, const std::vector<long long>& off, const double* U0,
+                                 const double* U1, double dt, double* lam, VjpChain& chain) {
+    a.lam = lam;
+    a.dt = dt;
+    a.U = U1;
+    a.W = lam;
+    a.w_scale = 0.5 * dt;
+    a.mode = 1;
+    cudaError_t e = chain.product(v, a, off);
+    a.U = U0;
+    a.W = a.bbuf;
+    a.w_scale = 1.0;
+    a.mode = 2;
+    if (e == cudaSuccess) e = chain.product(v, a, off);
+    return e;
+}
+
+}  // namespace
+
 extern "C" int gdfv_step_adjoint(int ctx, const double* U0_dev, const double* U1_dev, double dt, double* lam_dev,
                                  double* g_inflow_dev) {
     AdjView v;
@@ -617,20 +793,90 @@ extern "C" int gdfv_step_adjoint(int ctx, const double* U0_dev, const double* U1
     std::vector<long long> off;
     cudaError_t e = vjp_setup(v, a, off);
     if (v.ninflow > 0) a.gInflow = g_inflow_dev;
-    a.lam = lam_dev;
-    a.dt = dt;
-    // mu = J(U1)^T (dt/2 lam); b = dt/2 lam + dt mu; lam += mu
-    a.U = U1_dev;
-    a.W = lam_dev;
-    a.w_scale = 0.5 * dt;
-    a.mode = 1;
-    if (e == cudaSuccess) e = enqueue_vjp(v, a, off);
-    // lam += J(U0)^T b
-    a.U = U0_dev;
-    a.W = a.bbuf;
-    a.w_scale = 1.0;
-    a.mode = 2;
-    if (e == cudaSuccess) e = enqueue_vjp(v, a, off);
+    VjpChain chain;
+    if (e == cudaSuccess) e = enqueue_step_adjoint(v, a, off, U0_dev, U1_dev, dt, lam_dev, chain);
+    if (e == cudaSuccess) e = chain.finish(v);
     if (e != cudaSuccess) { adjoint_set_error(ctx, cudaGetErrorString(e)); return GDFV_ERR_CUDA; }
     return GDFV_OK;
+}
+
+extern "C" int gdfv_rollout_adjoint(int ctx, const double* const* ckpt_dev, int n_ckpt, const double* dts, int nsteps,
+                                    int checkpoint_every, double* const* work_dev, int last_ready, double* lam_dev,
+                                    double* g_inflow_dev) {
+    AdjView v;
+    if (!adjoint_view(ctx, &v)) return GDFV_ERR_ARG;
+    if (!vjp_supported(ctx, v)) return v.prepared ? GDFV_ERR_ARG : GDFV_ERR_STATE;
+    const int K = checkpoint_every;
+    if (!ckpt_dev || !dts || !work_dev || !lam_dev || (v.ninflow > 0 && !g_inflow_dev) || nsteps < 1 || K < 1 ||
+        K > 64 || n_ckpt != (nsteps + K - 1) / K) {
+        adjoint_set_error(ctx, "gdfv_rollout_adjoint: needs one checkpoint per segment of checkpoint_every (<= 64) "
+                               "steps, 4*checkpoint_every work arrays, lam (and g_inflow with inflow faces)");
+        return GDFV_ERR_ARG;
+    }
+    for (int m = 0; m < 4 * K; ++m)
+        if (!work_dev[m]) { adjoint_set_error(ctx, "gdfv_rollout_adjoint: null work array"); return GDFV_ERR_ARG; }
+    for (int m = 0; m < nsteps; ++m)
+        if (!(dts[m] > 0.0)) { adjoint_set_error(ctx, "gdfv_rollout_adjoint: dt must be > 0"); return GDFV_ERR_ARG; }
+    int st = steps_dt_prepare(ctx);
+    if (st) return st;
+    AdjArgs a;
+    std::vector<long long> off;
+    cudaError_t e = vjp_setup(v, a, off);
+    if (v.ninflow > 0) a.gInflow = g_inflow_dev;
+    cudaStream_t aux = context_aux_stream(ctx, 0);     // recomputation, lowest priority
+    AdjView vh = v;                                    // adjoint sweep, highest priority
+    vh.stream = context_aux_stream(ctx, 1);
+    if (e == cudaSuccess && (!aux || !vh.stream)) e = cudaErrorNotReady;
+    // Work arrays: two sets of (K states, K predictor states); segment s uses set
+    // (nseg-1-s) % 2.  The recomputation of segment s-1 (aux stream) runs while the
+    // adjoint of segment s (context stream) runs; events order the reuse of a set.
+    cudaEvent_t start = nullptr, rec_done[2] = {nullptr, nullptr}, adj_done[2] = {nullptr, nullptr};
+    for (cudaEvent_t* ev : {&start, &rec_done[0], &rec_done[1], &adj_done[0], &adj_done[1]})
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
+    const int nseg = n_ckpt;
+    auto seg_len = [&](int s) { return std::min(K, nsteps - s * K); };
+    bool first = true;
+    auto recompute = [&](int s, int p) -> cudaError_t {
+        // the state after a segment's last step is the next checkpoint: not recomputed
+        double* outs[64];
+        const int len = seg_len(s);
+        for (int m = 0; m < len; ++m) outs[m] = m < len - 1 ? work_dev[2 * K * p + m] : nullptr;
+        cudaError_t r = enqueue_steps_dt(ctx, aux, ckpt_dev[s], outs, work_dev + 2 * K * p + K,
+                                         dts + (size_t)s * K, len, first);
+        first = false;
+        if (r == cudaSuccess) r = cudaEventRecord(rec_done[p], aux);
+        return r;
+    };
+    if (e == cudaSuccess) e = cudaEventRecord(start, v.stream);   // inputs written on the context stream
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(aux, start, 0);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(vh.stream, start, 0);
+    VjpChain chain;
+    // the last segment's states and predictor states may come from the forward pass
+    if (e == cudaSuccess) e = last_ready ? cudaEventRecord(rec_done[0], aux) : recompute(nseg - 1, 0);
+    for (int idx = 0; idx < nseg && e == cudaSuccess; ++idx) {
+        const int s = nseg - 1 - idx, p = idx % 2, q = 1 - p;
+        if (s >= 1) {
+            if (idx >= 1) e = cudaStreamWaitEvent(aux, adj_done[q], 0);   // set q free again
+            if (e == cudaSuccess) e = recompute(s - 1, q);
+        }
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(vh.stream, rec_done[p], 0);
+        double* const* outs = work_dev + 2 * K * p;
+        double* const* preds = work_dev + 2 * K * p + K;
+        for (int n = seg_len(s) - 1; n >= 0 && e == cudaSuccess; --n) {
+            const double* U0 = n == 0 ? ckpt_dev[s] : outs[n - 1];
+            e = enqueue_step_adjoint(vh, a, off, U0, preds[n], dts[(size_t)s * K + n], lam_dev, chain);
+        }
+        // each segment ends its chain, so that every reader of the set precedes adj_done
+        if (e == cudaSuccess) e = chain.finish(vh);
+        if (e == cudaSuccess) e = cudaEventRecord(adj_done[p], vh.stream);
+    }
+    if (e == cudaSuccess) {
+        if (!first) st = steps_dt_status(ctx, aux);   // failure counters of the recomputed segments
+        else e = cudaStreamSynchronize(aux);
+        if (st == GDFV_OK && e == cudaSuccess) e = cudaStreamSynchronize(vh.stream);
+    }
+    for (cudaEvent_t ev : {start, rec_done[0], rec_done[1], adj_done[0], adj_done[1]})
+        if (ev) cudaEventDestroy(ev);
+    if (e != cudaSuccess) { adjoint_set_error(ctx, cudaGetErrorString(e)); return GDFV_ERR_CUDA; }
+    return st;
 }

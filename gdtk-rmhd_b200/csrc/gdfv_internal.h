@@ -39,4 +39,11 @@ struct AdjView {
 bool adjoint_view(int ctx, AdjView* v);
 void adjoint_set_error(int ctx, const std::string& msg);
 
+// Fixed-dt step chains (gdfv_runtime.cu), for the adjoint's recomputation.
+int steps_dt_prepare(int ctx);
+cudaError_t enqueue_steps_dt(int ctx, cudaStream_t stream, const double* U_in, double* const* U_out,
+                             double* const* U1_out, const double* dts, int n, bool fresh);
+int steps_dt_status(int ctx, cudaStream_t stream);
+cudaStream_t context_aux_stream(int ctx, int which);
+
 }  // namespace gdfv

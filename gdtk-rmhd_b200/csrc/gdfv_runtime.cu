@@ -247,6 +247,7 @@ struct Context {
     double* adj_scratch = nullptr;     // adjoint work arrays, allocated on first use
     int adj_ready = 0;
     long long adj_scratch_n = 0;
+    cudaStream_t aux_stream[2] = {nullptr, nullptr};  // lowest / highest priority streams of the rollout adjoint
     Control* step_ctl = nullptr;       // control record of gdfv_step_dt
     unsigned long long* step_maxsig = nullptr;
     double* step_lastsig = nullptr;
@@ -258,6 +259,8 @@ struct Context {
                         (void*)step_ctl, (void*)step_maxsig, (void*)step_lastsig})
             if (p) cudaFree(p);
         if (h_ctl) cudaFreeHost(h_ctl);
+        for (cudaStream_t s : aux_stream)
+            if (s) cudaStreamDestroy(s);
         if (own_stream && stream) cudaStreamDestroy(stream);
     }
 };
@@ -915,6 +918,88 @@ int gdfv_block_get_flow(int ctx, int blk, double* out) {
 
 namespace gdfv {
 
+// Scratch control record of the fixed-dt step chains, and the current c_h (host read).
+int steps_dt_prepare(int ctx) {
+    Context* c = get_ctx(ctx);
+    if (!c) return GDFV_ERR_ARG;
+    if (!c->step_ctl) {
+        CK(cudaMalloc(&c->step_ctl, sizeof(Control)));
+        CK(cudaMalloc(&c->step_maxsig, sizeof(unsigned long long) * c->blocks.size()));
+        CK(cudaMalloc(&c->step_lastsig, sizeof(double) * c->blocks.size()));
+    }
+    if (read_ctl(c)) return GDFV_ERR_CUDA;
+    return GDFV_OK;
+}
+
+// Enqueues n fixed-dt steps on `stream`: step m takes dts[m] from the previous output
+// (U_in for m = 0) to U_out[m]; U1_out[m] (optional) receives the predictor state.
+// fresh: reset the chain's failure counters (otherwise they accumulate over chains).
+// steps_dt_prepare must have run.  Uses the context's dU0 and scratch control record,
+// so at most one chain may be in flight per context.
+cudaError_t enqueue_steps_dt(int ctx, cudaStream_t stream, const double* U_in, double* const* U_out,
+                             double* const* U1_out, const double* dts, int n, bool fresh) {
+    Context* c = get_ctx(ctx);
+    if (!c || !c->step_ctl || !U_in || !U_out || !dts || n < 1) return cudaErrorInvalidValue;
+    for (int m = 0; m < n; ++m) {
+        const double* src = m == 0 ? U_in : U_out[m - 1];
+        // only the last step may omit its output (then only its predictor state is formed)
+        if ((!U_out[m] && m < n - 1) || U_out[m] == src || !(dts[m] > 0.0)) return cudaErrorInvalidValue;
+    }
+    StageArgs A = stage_args(c);
+    A.ctl = c->step_ctl;
+    A.max_signal = c->step_maxsig;
+    A.last_signal = c->step_lastsig;
+    for (int m = 0; m < n; ++m) {
+        const double* src = m == 0 ? U_in : U_out[m - 1];
+        A.Ubuf[0] = const_cast<double*>(src);
+        A.Ubuf[1] = U_out[m];
+        A.R_out = U1_out ? U1_out[m] : nullptr;   // the predictor stage writes U1 there
+        if (m == 0 && fresh)
+            step_dt_begin_kernel<<<1, 256, 0, stream>>>(c->step_ctl, c->step_maxsig, (int)c->blocks.size(), dts[0],
+                                                        c->h_ctl->c_h);
+        else
+            step_dt_next_kernel<<<1, 1, 0, stream>>>(c->step_ctl, dts[m]);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = c->cfg.precision == 0 ? launch_stage_fp64(1, c->cfg.flux, c->cfg.mhd, A, stream)
+                                                        : launch_stage_fp32(1, c->cfg.flux, c->cfg.mhd, A, stream);
+        A.R_out = nullptr;
+        if (e == cudaSuccess && U_out[m])
+            e = c->cfg.precision == 0 ? launch_stage_fp64(2, c->cfg.flux, c->cfg.mhd, A, stream)
+                                      : launch_stage_fp32(2, c->cfg.flux, c->cfg.mhd, A, stream);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+// Waits for `stream` and reports the failure counters of the chains run since the
+// last fresh start: 0, GDFV_ERR_STEP_FAILED or GDFV_ERR_BAD_CELLS (with the message).
+int steps_dt_status(int ctx, cudaStream_t stream) {
+    Context* c = get_ctx(ctx);
+    if (!c) return GDFV_ERR_ARG;
+    Control h{};
+    CK(cudaMemcpyAsync(&h, c->step_ctl, sizeof(Control), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    if (h.n_fail > 0) return fail(c, GDFV_ERR_STEP_FAILED, "fixed-dt step: a cell failed to decode");
+    if (h.n_invalid1 > c->cfg.max_invalid_cells || h.n_invalid2 > c->cfg.max_invalid_cells)
+        return fail(c, GDFV_ERR_BAD_CELLS, "fixed-dt step: too many bad cells");
+    return GDFV_OK;
+}
+
+// The context's extra streams (created on first use): which = 0 at the lowest
+// priority, 1 at the highest.
+cudaStream_t context_aux_stream(int ctx, int which) {
+    Context* c = get_ctx(ctx);
+    if (!c || which < 0 || which > 1) return nullptr;
+    if (!c->aux_stream[which]) {
+        int least = 0, greatest = 0;
+        if (cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess) return nullptr;
+        if (cudaStreamCreateWithPriority(&c->aux_stream[which], cudaStreamNonBlocking, which ? greatest : least) !=
+            cudaSuccess)
+            c->aux_stream[which] = nullptr;
+    }
+    return c->aux_stream[which];
+}
+
 int upload_tiles(Context* c, const std::vector<TileDesc>& tiles) {
     CK(cudaStreamSynchronize(c->stream));
     if (tiles.size() > c->tiles_cap) {
@@ -1140,48 +1225,25 @@ int gdfv_steps_dt(int ctx, const double* U_in_dev, double* const* U_out_dev, dou
     Context* c = get_ctx(ctx);
     int st = check_ready(c, -1);
     if (st) return st;
-    if (!U_in_dev || !U_out_dev || !dts || n < 1)
-        return fail(c, GDFV_ERR_ARG, "gdfv_steps_dt needs U_in, n >= 1 output arrays and their dts");
-    for (int m = 0; m < n; ++m) {
-        const double* src = m == 0 ? U_in_dev : U_out_dev[m - 1];
-        if (!U_out_dev[m] || U_out_dev[m] == src || !(dts[m] > 0.0))
-            return fail(c, GDFV_ERR_ARG, "gdfv_steps_dt: each step needs a distinct output array and dt > 0");
-    }
-    if (!c->step_ctl) {
-        CK(cudaMalloc(&c->step_ctl, sizeof(Control)));
-        CK(cudaMalloc(&c->step_maxsig, sizeof(unsigned long long) * c->blocks.size()));
-        CK(cudaMalloc(&c->step_lastsig, sizeof(double) * c->blocks.size()));
-    }
+    if ((st = steps_dt_prepare(ctx))) return st;
+    cudaError_t e = enqueue_steps_dt(ctx, c->stream, U_in_dev, U_out_dev, U1_out_dev, dts, n, true);
+    if (e == cudaErrorInvalidValue) return fail(c, GDFV_ERR_ARG, "gdfv_steps_dt needs U_in, n >= 1 distinct output arrays and dt > 0");
+    if (e != cudaSuccess) return cuda_fail(c, e, "gdfv_steps_dt");
+    return steps_dt_status(ctx, c->stream);
+}
+
+int gdfv_last_predictor_state(int ctx, const double* U0_dev, double* U1_out_dev) {
+    Context* c = get_ctx(ctx);
+    int st = check_ready(c, -1);
+    if (st) return st;
+    if (!U0_dev || !U1_out_dev || U0_dev == U1_out_dev)
+        return fail(c, GDFV_ERR_ARG, "gdfv_last_predictor_state needs distinct U0 and U1 arrays");
     if (read_ctl(c)) return GDFV_ERR_CUDA;
-    StageArgs A = stage_args(c);
-    A.ctl = c->step_ctl;
-    A.max_signal = c->step_maxsig;
-    A.last_signal = c->step_lastsig;
-    const long long nvals = (long long)c->nq * c->total;
-    for (int m = 0; m < n; ++m) {
-        const double* src = m == 0 ? U_in_dev : U_out_dev[m - 1];
-        A.Ubuf[0] = const_cast<double*>(src);
-        A.Ubuf[1] = U_out_dev[m];
-        if (m == 0)
-            step_dt_begin_kernel<<<1, 256, 0, c->stream>>>(c->step_ctl, c->step_maxsig, (int)c->blocks.size(),
-                                                           dts[0], c->h_ctl->c_h);
-        else
-            step_dt_next_kernel<<<1, 1, 0, c->stream>>>(c->step_ctl, dts[m]);
-        CK(cudaGetLastError());
-        CK(launch_stage(c, 1, A));
-        if (U1_out_dev && U1_out_dev[m]) {
-            predictor_state_kernel<<<(unsigned)((nvals + 255) / 256), 256, 0, c->stream>>>(src, c->dU0, dts[m], nvals,
-                                                                                          U1_out_dev[m]);
-            CK(cudaGetLastError());
-        }
-        CK(launch_stage(c, 2, A));
-    }
-    Control h{};
-    CK(cudaMemcpyAsync(&h, c->step_ctl, sizeof(Control), cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    if (h.n_fail > 0) return fail(c, GDFV_ERR_STEP_FAILED, "gdfv_steps_dt: a cell failed to decode");
-    if (h.n_invalid1 > c->cfg.max_invalid_cells || h.n_invalid2 > c->cfg.max_invalid_cells)
-        return fail(c, GDFV_ERR_BAD_CELLS, "gdfv_steps_dt: too many bad cells");
+    if (c->h_ctl->step < 1) return fail(c, GDFV_ERR_STATE, "no step taken yet");
+    const long long n = (long long)c->nq * c->total;
+    predictor_state_kernel<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(U0_dev, c->dU0, c->h_ctl->dt_global, n,
+                                                                               U1_out_dev);
+    CK(cudaGetLastError());
     return GDFV_OK;
 }
 

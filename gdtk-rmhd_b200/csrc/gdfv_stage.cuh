@@ -39,7 +39,7 @@ struct StageArgs {
     double* Ubuf[2];          // conserved state, ping-pong by step parity (SoA [nq][total])
     const double* U_in;       // stage 0 only: explicit input state
     double* dU0;              // stage-1 derivative (SoA)
-    double* R_out;            // stage 0 only: residual output
+    double* R_out;            // stage 0: residual output; stage 1 (FP64 flux): predictor state U1 (optional)
     Control* ctl;
     unsigned long long* max_signal;  // per block, bit pattern of a positive double
     double* last_signal;             // per block
@@ -911,6 +911,10 @@ __global__ void __launch_bounds__(32 * (TJ + 1), MHD ? 1 : (sizeof(R) == 4 ? GDF
                         for (int q = 0; q < NQ; ++q) {
                             A.dU0[(long long)q * A.total + g] = dU[q];
                             U[q] = d_add(U[q], d_mul(dt, dU[q]));
+                        }
+                        if (sizeof(R) == 8 && A.R_out) {   // U1 before the psi damping (FP64 adjoint recomputation)
+#pragma unroll
+                            for (int q = 0; q < NQ; ++q) A.R_out[(long long)q * A.total + g] = U[q];
                         }
                     } else {
 #pragma unroll

@@ -5,9 +5,11 @@
   steps of the GPU solver from U0, differentiable in U0 and in the supersonic-
   inflow state theta = (p, T, vel.x).  The forward records each step's dt and
   keeps a copy of the state every `checkpoint_every` steps; the backward
-  recomputes each segment from its checkpoint (gdfv_steps_dt, bit-identical to
-  the forward steps) and applies the adjoint of the predictor-corrector step
-  (gdfv_step_adjoint; the step is e4/simcore_gasdynamic_step.d:1245-1333):
+  (gdfv_rollout_adjoint) recomputes each segment from its checkpoint
+  (bit-identical to the forward steps) on a second stream while it applies the
+  adjoint of the predictor-corrector step (e4/simcore_gasdynamic_step.d:1245-1333)
+  to the segment after it; the last segment's states and predictor states are
+  kept by the forward as it takes the steps, so that segment is not recomputed:
       U1 = U0 + dt R(U0),  U2 = U0 + dt (R(U0)/2 + R(U1)/2)
       mu  = J(U1)^T (dt/2 lam)
       lam <- lam + mu + J(U0)^T (dt/2 lam + dt mu)
@@ -106,7 +108,13 @@ class Rollout(torch.autograd.Function):
     @staticmethod
     def forward(ctx, U0, theta, sim, nsteps, checkpoint_every):
         U0 = U0.contiguous()
+        K = checkpoint_every
         dts, ckpts = [], {0: U0.clone()}
+        # work arrays of the backward (two sets of K states and K predictor states);
+        # the first set keeps the last segment's steps as the forward takes them
+        work = [torch.empty_like(U0) for _ in range(4 * K)]
+        outs0, preds0 = work[:K], work[K:2 * K]
+        s_last = ((nsteps + K - 1) // K - 1) * K
         sim.set_time(0.0, 0, sim.config.dt_init)
         torch.cuda.current_stream().synchronize()
         state = _state_view(sim)
@@ -115,15 +123,20 @@ class Rollout(torch.autograd.Function):
         for n in range(nsteps):
             sim.run(max_step=1)
             dts.append(sim.time()["dt"])
-            if (n + 1) % checkpoint_every == 0 and n + 1 < nsteps:
+            if n >= s_last:
+                m = n - s_last
+                U0n = ckpts[s_last] if m == 0 else outs0[m - 1]
+                check(sim.ctx, sim.L.gdfv_last_predictor_state(sim.ctx, _p(U0n), _p(preds0[m])))
+                if n < nsteps - 1:
+                    outs0[m].copy_(_state_view(sim))
+                    torch.cuda.synchronize()
+            if (n + 1) % K == 0 and n + 1 < nsteps:
                 ckpts[n + 1] = _state_view(sim).clone()
+                torch.cuda.synchronize()
         UN = _state_view(sim).clone()
-        ctx.sim, ctx.dts, ctx.ckpts, ctx.k = sim, dts, ckpts, checkpoint_every
+        torch.cuda.synchronize()
+        ctx.sim, ctx.dts, ctx.ckpts, ctx.k, ctx.work = sim, dts, ckpts, K, work
         ctx.theta = theta.detach().clone()
-        # work arrays of the backward's segment recomputation, allocated with the checkpoints
-        m = min(checkpoint_every, nsteps)
-        ctx.outs = [torch.empty_like(U0) for _ in range(m)]
-        ctx.preds = [torch.empty_like(U0) for _ in range(m)]
         return UN
 
     @staticmethod
@@ -131,16 +144,13 @@ class Rollout(torch.autograd.Function):
         sim, dts, ckpts, K = ctx.sim, ctx.dts, ctx.ckpts, ctx.k
         lam = gUN.contiguous().clone()
         gin = torch.zeros((max(1, getattr(sim, "n_inflow", 1)), 6), dtype=torch.float64, device=lam.device)
-        n_total = len(dts)
-        outs, preds = ctx.outs, ctx.preds
-        for s0 in reversed(range(0, n_total, K)):
-            s1 = min(s0 + K, n_total)
-            steps_dt(sim, ckpts[s0], dts[s0:s1], outs, preds)
-            for n in reversed(range(s0, s1)):
-                U0 = ckpts[s0] if n == s0 else outs[n - s0 - 1]
-                step_adjoint(sim, U0, preds[n - s0], dts[n], lam, gin)
+        nseg = (len(dts) + K - 1) // K
+        pc = ffi.new("double*[]", [_p(ckpts[s * K]) for s in range(nseg)])
+        pw = ffi.new("double*[]", [_p(t) for t in ctx.work])
+        pd = ffi.new("double[]", [float(d) for d in dts])
         torch.cuda.synchronize()
-        ctx.outs = ctx.preds = None
+        check(sim.ctx, sim.L.gdfv_rollout_adjoint(sim.ctx, pc, nseg, pd, len(dts), K, pw, 1, _p(lam), _p(gin)))
+        ctx.work = None
         gtheta = inflow_chain(sim, ctx.theta, gin[0].cpu()).to(ctx.theta.device)
         return lam, gtheta, None, None, None
 

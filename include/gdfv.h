@@ -134,7 +134,8 @@ int gdfv_residual_vjp(int ctx, const double* U_dev, const double* W_dev, double*
 int gdfv_step_dt(int ctx, const double* U_in_dev, double* U_out_dev, double dt, double* U1_out_dev);
 
 /* n steps of gdfv_step_dt in a chain: step m takes dts[m] from the previous output
- * (U_in_dev for m = 0) to U_out_dev[m]; U1_out_dev (may be NULL, or hold NULL
+ * (U_in_dev for m = 0) to U_out_dev[m] (U_out_dev[n-1] may be NULL: the last step
+ * then forms only its predictor state); U1_out_dev (may be NULL, or hold NULL
  * entries) receives the predictor states.  The recomputation of one checkpoint
  * segment, with one host synchronisation at the end; a failed step is reported
  * then (the steps after it do not write).  No reference counterpart: the
@@ -151,6 +152,28 @@ int gdfv_steps_dt(int ctx, const double* U_in_dev, double* const* U_out_dev, dou
  * counterpart. */
 int gdfv_step_adjoint(int ctx, const double* U0_dev, const double* U1_dev, double dt, double* lam_dev,
                       double* g_inflow_dev);
+
+/* The whole backward of a checkpointed rollout of nsteps predictor-corrector steps:
+ * lam (device, [nq][total]) holds dJ/dU_N on entry and dJ/dU_0 on return, the inflow
+ * cotangents are added into g_inflow_dev.  ckpt_dev[s] is the state at step
+ * s*checkpoint_every (checkpoint_every <= 64; n_ckpt = ceil(nsteps/checkpoint_every) of them), dts the dt of
+ * every step, work_dev 4*checkpoint_every state-sized device arrays: two sets of
+ * (checkpoint_every states after steps, checkpoint_every predictor states).  Each
+ * segment is recomputed (as gdfv_steps_dt) on a second stream while the adjoint steps
+ * of the segment after it (as gdfv_step_adjoint) run on the context's stream; returns
+ * after both finish.  last_ready != 0: the first set already holds the last
+ * segment's states and predictor states (kept by the forward pass, see
+ * gdfv_last_predictor_state), which are then not recomputed.  Same scope as
+ * gdfv_residual_vjp; no reference counterpart. */
+int gdfv_rollout_adjoint(int ctx, const double* const* ckpt_dev, int n_ckpt, const double* dts, int nsteps,
+                         int checkpoint_every, double* const* work_dev, int last_ready, double* lam_dev,
+                         double* g_inflow_dev);
+
+/* Predictor state U1 = U0 + dt*dU0 of the step gdfv_run took last, from the state U0
+ * before it (device arrays): what a forward pass keeps to differentiate its last
+ * steps without recomputing them.  Valid directly after the step.  No reference
+ * counterpart. */
+int gdfv_last_predictor_state(int ctx, const double* U0_dev, double* U1_out_dev);
 
 /* Device pointer of the current conserved state ([nq][total], borrowed, valid
  * until the next gdfv_run), and of the context's CUDA stream. */

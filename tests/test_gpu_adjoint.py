@@ -186,3 +186,51 @@ def test_step_chain_and_fused_step_adjoint():
     torch.cuda.synchronize()
     assert torch.allclose(lam, want, rtol=1e-13, atol=1e-13 * float(want.abs().max()))
     assert np.allclose(gin.cpu().numpy(), want_in.numpy(), rtol=1e-12, atol=1e-12 * float(want_in.abs().max()))
+
+
+def test_pipelined_rollout_adjoint_matches_sequential():
+    """gdfv_rollout_adjoint (segment recomputation on a second stream overlapping the
+    adjoint of the next segment) gives the lambda and inflow cotangents of the
+    sequential gdfv_steps_dt + gdfv_step_adjoint composition (to the rounding of the
+    FP64 atomic accumulation, whose order varies run to run)."""
+    from gdfv._lib import check, ffi
+    from gdfv.autograd import _p, step_adjoint, steps_dt
+    case = cases.c2_inflow_box(n=(40, 24, 20), noise_all=True)
+    _, sim = cases.build_pair(case)
+    U0 = torch.from_numpy(sim.get_conserved(0)).cuda()
+    K, nsteps = 4, 11
+    rng = np.random.default_rng(21)
+    dts = list(2.0e-7 * (1.0 + 0.2 * rng.random(nsteps)))
+    ckpts, states = [U0.clone()], [U0.clone()]
+    outs = [torch.empty_like(U0) for _ in range(nsteps)]
+    preds = [torch.empty_like(U0) for _ in range(nsteps)]
+    steps_dt(sim, U0, dts, outs, preds)
+    for s in range(1, (nsteps + K - 1) // K):
+        ckpts.append(outs[s * K - 1].clone())
+    lam0 = torch.from_numpy(rng.standard_normal(tuple(U0.shape))).cuda()
+    # sequential reference
+    lam = lam0.clone()
+    gin = torch.zeros((sim.n_inflow, 6), dtype=torch.float64, device=lam.device)
+    for n in reversed(range(nsteps)):
+        step_adjoint(sim, U0 if n == 0 else outs[n - 1], preds[n], dts[n], lam, gin)
+    torch.cuda.synchronize()
+    # pipelined
+    for last_ready in (0, 1):
+        lam2 = lam0.clone()
+        gin2 = torch.zeros_like(gin)
+        work = [torch.empty_like(U0) for _ in range(4 * K)]
+        if last_ready:   # the last segment (steps 8..10) handed over as a forward pass keeps it
+            s_last = (len(ckpts) - 1) * K
+            for m in range(nsteps - s_last):
+                work[K + m].copy_(preds[s_last + m])
+                if s_last + m < nsteps - 1:
+                    work[m].copy_(outs[s_last + m])
+        pc = ffi.new("double*[]", [_p(t) for t in ckpts])
+        pw = ffi.new("double*[]", [_p(t) for t in work])
+        pd = ffi.new("double[]", dts)
+        torch.cuda.synchronize()
+        check(sim.ctx, sim.L.gdfv_rollout_adjoint(sim.ctx, pc, len(ckpts), pd, nsteps, K, pw, last_ready, _p(lam2),
+                                                  _p(gin2)))
+        torch.cuda.synchronize()
+        assert torch.allclose(lam, lam2, rtol=1e-12, atol=1e-12 * float(lam.abs().max())), last_ready
+        assert torch.allclose(gin, gin2, rtol=1e-12, atol=0.0), last_ready
