@@ -346,8 +346,28 @@ __device__ __forceinline__ void recon_cell(const R* w, const R* wf, const NumPar
                                            const R* qp1, R* qm, R* qp) {
     if constexpr (sizeof(R) == 4 && OPT == 1) {
         const R e = wf[WF_EPS], P1 = wf[WF_P1], P2 = wf[WF_P2], R1 = wf[WF_R1], R2 = wf[WF_R2];
+        // scalars in pairs with packed float2 arithmetic (one instruction per pair),
+        // the same operations as the scalar form below
+        const float2 e2 = make_float2(e, e), m1 = make_float2(-1.0f, -1.0f);
+        const float2 P1v = make_float2(P1, P1), P2v = make_float2(P2, P2);
+        const float2 nR1v = make_float2(-R1, -R1), nR2v = make_float2(-R2, -R2);
 #pragma unroll
-        for (int s = 0; s < NRS; ++s) {
+        for (int s = 0; s + 1 < NRS; s += 2) {
+            const float2 L = make_float2(qm1[s], qm1[s + 1]), C = make_float2(q0[s], q0[s + 1]);
+            const float2 Rr = make_float2(qp1[s], qp1[s + 1]);
+            const float2 a = __ffma2_rn(L, m1, C);       // q0 - qm1
+            const float2 b = __ffma2_rn(C, m1, Rr);      // qp1 - q0
+            const float2 ab = __fmul2_rn(a, b);
+            const float2 num = __fadd2_rn(make_float2(ab.x + fabsf(ab.x), ab.y + fabsf(ab.y)), e2);
+            const float2 den = __fadd2_rn(__ffma2_rn(b, b, __fmul2_rn(a, a)), e2);
+            const float2 sl = __fmul2_rn(num, make_float2(1.0f / den.x, 1.0f / den.y));
+            const float2 vp = __ffma2_rn(sl, __ffma2_rn(P1v, b, __fmul2_rn(P2v, a)), C);
+            const float2 vm = __ffma2_rn(sl, __ffma2_rn(nR1v, b, __fmul2_rn(nR2v, a)), C);
+            qp[s] = vp.x; qp[s + 1] = vp.y;
+            qm[s] = vm.x; qm[s + 1] = vm.y;
+        }
+#pragma unroll
+        for (int s = NRS & ~1; s < NRS; ++s) {
             if (MHD && s == 8 && !P.divergence_cleaning) { qm[s] = q0[s]; qp[s] = q0[s]; continue; }
             const R a = q0[s] - qm1[s];
             const R b = qp1[s] - q0[s];
