@@ -409,35 +409,36 @@ __device__ __forceinline__ void recon_cell(const R* w, const R* wf, const NumPar
 __device__ __forceinline__ void ausmdv_f(float g, float gm1, bool efix, float rL, float uL, float vL, float wL,
                                          float eL, float aL, float rR, float uR, float vR, float wR, float eR, float aR,
                                          float* F) {
-    const float pL = rL * (gm1 * eL), pR = rR * (gm1 * eR);
-    const float keL = 0.5f * (uL * uL + vL * vL + wL * wL);
-    const float keR = 0.5f * (uR * uR + vR * vR + wR * wR);
-    const float HL = g * eL + keL, HR = g * eR + keR;
-    const float isum = 1.0f / (eL + eR);
-    const float alphaL = 2.0f * eL * isum, alphaR = 2.0f * eR * isum;
+    // left/right pairs in packed float2 arithmetic where both sides do the same
+    const float2 r = make_float2(rL, rR), u = make_float2(uL, uR), v = make_float2(vL, vR);
+    const float2 w = make_float2(wL, wR), e = make_float2(eL, eR);
+    const float2 p = __fmul2_rn(r, __fmul2_rn(make_float2(gm1, gm1), e));
+    const float2 ke = __fmul2_rn(make_float2(0.5f, 0.5f), __ffma2_rn(w, w, __ffma2_rn(v, v, __fmul2_rn(u, u))));
+    const float2 H = __ffma2_rn(make_float2(g, g), e, ke);
+    const float two_isum = 2.0f / (eL + eR);
+    const float2 alpha = __fmul2_rn(e, make_float2(two_isum, two_isum));
     const float am = fmaxf(aL, aR), iam = 1.0f / am;
-    const float ML = uL * iam, MR = uR * iam;
-    const float duL = 0.5f * (uL + fabsf(uL)), duR = 0.5f * (uR - fabsf(uR));
-    float pLplus, uLplus, pRminus, uRminus;
-    if (fabsf(ML) <= 1.0f) {
-        pLplus = pL * (ML + 1.0f) * (ML + 1.0f) * (2.0f - ML) * 0.25f;
-        uLplus = alphaL * ((uL + am) * (uL + am) * (0.25f * iam) - duL) + duL;
-    } else {
-        pLplus = uL > 0.0f ? pL : 0.0f;
-        uLplus = duL;
-    }
-    if (fabsf(MR) <= 1.0f) {
-        pRminus = pR * (MR - 1.0f) * (MR - 1.0f) * (2.0f + MR) * 0.25f;
-        uRminus = alphaR * (-(uR - am) * (uR - am) * (0.25f * iam) - duR) + duR;
-    } else {
-        pRminus = uR < 0.0f ? pR : 0.0f;
-        uRminus = duR;
-    }
-    const float ru_half = uLplus * rL + uRminus * rR;
+    const float2 M = __fmul2_rn(u, make_float2(iam, iam));
+    const float2 du = __fmul2_rn(make_float2(0.5f, 0.5f), make_float2(uL + fabsf(uL), uR - fabsf(uR)));
+    // subsonic splits: p (M +- 1)^2 (2 -+ M)/4 and alpha (Q - du) + du with
+    // Q = +-(u +- am)^2 / (4 am)
+    const float2 Mo = __fadd2_rn(M, make_float2(1.0f, -1.0f));
+    const float2 Mt = __ffma2_rn(M, make_float2(-1.0f, 1.0f), make_float2(2.0f, 2.0f));
+    const float2 psub = __fmul2_rn(__fmul2_rn(__fmul2_rn(p, make_float2(0.25f, 0.25f)), __fmul2_rn(Mo, Mo)), Mt);
+    const float2 ua = __fadd2_rn(u, make_float2(am, -am));
+    const float2 Q = __fmul2_rn(__fmul2_rn(ua, ua), make_float2(0.25f * iam, -0.25f * iam));
+    const float2 usub = __ffma2_rn(alpha, __ffma2_rn(du, make_float2(-1.0f, -1.0f), Q), du);
+    const bool subL = fabsf(M.x) <= 1.0f, subR = fabsf(M.y) <= 1.0f;
+    const float pLplus = subL ? psub.x : (uL > 0.0f ? p.x : 0.0f);
+    const float pRminus = subR ? psub.y : (uR < 0.0f ? p.y : 0.0f);
+    const float2 us = make_float2(subL ? usub.x : du.x, subR ? usub.y : du.y);
+    const float2 ru = __fmul2_rn(us, r);           // (uLplus rL, uRminus rR)
+    const float ru_half = ru.x + ru.y;
     const float p_half = pLplus + pRminus;
-    const float dp = 10.0f * fabsf(pL - pR) / fminf(pL, pR);
+    const float dp = 10.0f * fabsf(p.x - p.y) / fminf(p.x, p.y);
     const float sw = 0.5f * fminf(1.0f, dp);
-    const float ru2_AUSMV = uLplus * rL * uL + uRminus * rR * uR;
+    const float2 ruu = __fmul2_rn(ru, u);
+    const float ru2_AUSMV = ruu.x + ruu.y;
     const float ru2_AUSMD = 0.5f * (ru_half * (uL + uR) - fabsf(ru_half) * (uR - uL));
     const float ru2_half = (0.5f + sw) * ru2_AUSMV + (0.5f - sw) * ru2_AUSMD;
     const bool up = ru_half >= 0.0f;
@@ -445,20 +446,23 @@ __device__ __forceinline__ void ausmdv_f(float g, float gm1, bool efix, float rL
     F[1] = ru2_half + p_half;
     F[2] = ru_half * (up ? vL : vR);
     F[3] = ru_half * (up ? wL : wR);
-    F[4] = ru_half * (up ? HL : HR);
+    F[4] = ru_half * (up ? H.x : H.y);
     if (efix) {
         const float C_EFIX = 0.125f;
-        const bool caseA = ((uL - aL) < 0.0f) && ((uR - aR) > 0.0f);
-        const bool caseB = ((uL + aL) < 0.0f) && ((uR + aR) > 0.0f);
+        const float2 a = make_float2(aL, aR);
+        const float2 uma = __ffma2_rn(a, make_float2(-1.0f, -1.0f), u), upa = __fadd2_rn(u, a);
+        const bool caseA = (uma.x < 0.0f) && (uma.y > 0.0f);
+        const bool caseB = (upa.x < 0.0f) && (upa.y > 0.0f);
         float d_ua = 0.0f;
-        if (caseA && !caseB) d_ua = C_EFIX * ((uR - aR) - (uL - aL));
-        if (caseB && !caseA) d_ua = C_EFIX * ((uR + aR) - (uL + aL));
+        if (caseA && !caseB) d_ua = C_EFIX * (uma.y - uma.x);
+        if (caseB && !caseA) d_ua = C_EFIX * (upa.y - upa.x);
         if (d_ua != 0.0f) {
+            const float2 rv = __fmul2_rn(r, v), rw = __fmul2_rn(r, w), rH = __fmul2_rn(r, H), rU = __fmul2_rn(r, u);
             F[0] -= d_ua * (rR - rL);
-            F[1] -= d_ua * (rR * uR - rL * uL);
-            F[2] -= d_ua * (rR * vR - rL * vL);
-            F[3] -= d_ua * (rR * wR - rL * wL);
-            F[4] -= d_ua * (rR * HR - rL * HL);
+            F[1] -= d_ua * (rU.y - rU.x);
+            F[2] -= d_ua * (rv.y - rv.x);
+            F[3] -= d_ua * (rw.y - rw.x);
+            F[4] -= d_ua * (rH.y - rH.x);
         }
     }
 }
