@@ -633,8 +633,9 @@ namespace {
 
 bool vjp_supported(int ctx, const AdjView& v) {
     if (!v.prepared) { adjoint_set_error(ctx, "call gdfv_prepare first"); return false; }
-    if (v.mhd || v.flux != FLUX_AUSMDV || v.dims != 3) {
-        adjoint_set_error(ctx, "the adjoint supports the 3D Euler path with flux_calculator=ausmdv");
+    if (v.mhd || v.flux != FLUX_AUSMDV || v.dims != 3 || v.P.lmr_epsilon) {
+        adjoint_set_error(ctx, "the adjoint supports the 3D Euler path with flux_calculator=ausmdv "
+                               "and van_albada_variant=e4");
         return false;
     }
     return true;

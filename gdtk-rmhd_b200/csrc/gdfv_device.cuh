@@ -35,7 +35,7 @@ struct NumParams {
     int apply_limiter, extrema_clipping, apply_entropy_fix, glm_reference_indexing;
     int mhd, divergence_cleaning, dims, stringent_cfl;
     int nq;
-    int pad_;
+    int lmr_epsilon;    // van Albada epsilon scaled per face (lmr/onedinterp.d:147-151)
 };
 
 // Fixed ghost state of a supersonic-inflow face (FlowStateCopy, flow_state_copy.d:92-107)

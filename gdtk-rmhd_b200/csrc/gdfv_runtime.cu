@@ -208,6 +208,7 @@ struct Config {
     int tile_kchunk = 0;  // 0: chosen per block
     int persistent = 0;   // 1: stage kernels as a resident grid taking tiles from a queue
     int autotune = 0;     // time tile shapes and the launch form on the first run, keep the fastest
+    int lmr_epsilon = 0;  // van_albada_variant = lmr
     double cfl_value = 0.5, dt_init = 1.0e-3, dt_max = 1.0e-3;
     double eps_van_albada = 1.0e-12, R = 287.1, gamma = 1.4, divB_damping_length = 1.0;
     double max_velocity = 30000.0, max_temp = 50000.0, min_temp = 0.0;
@@ -482,7 +483,7 @@ int do_prepare(Context* c) {
     P.apply_limiter = g.apply_limiter; P.extrema_clipping = g.extrema_clipping;
     P.apply_entropy_fix = g.apply_entropy_fix; P.glm_reference_indexing = g.glm_reference_indexing;
     P.mhd = g.mhd; P.divergence_cleaning = g.divergence_cleaning; P.dims = g.dims;
-    P.stringent_cfl = g.stringent_cfl; P.nq = c->nq;
+    P.stringent_cfl = g.stringent_cfl; P.nq = c->nq; P.lmr_epsilon = g.lmr_epsilon;
     StepParams& sp = c->sp;
     sp.cfl_count = g.cfl_count; sp.n_stages = 2; sp.fixed_time_step = g.fixed_time_step;
     sp.mhd_cleaning = g.mhd && g.divergence_cleaning;
@@ -690,6 +691,10 @@ int gdfv_config_set_str(int ctx, const char* key, const char* value) {
         if (v == "fp64" || v == "double") c->cfg.precision = 0;
         else if (v == "fp32" || v == "float") c->cfg.precision = 1;
         else return fail(c, GDFV_ERR_ARG, "flux_precision is fp64 or fp32");
+    } else if (k == "van_albada_variant") {
+        if (v == "e4") c->cfg.lmr_epsilon = 0;
+        else if (v == "lmr") c->cfg.lmr_epsilon = 1;
+        else return fail(c, GDFV_ERR_ARG, "van_albada_variant is e4 or lmr");
     } else {
         return fail(c, GDFV_ERR_ARG, "unknown string option: " + k);
     }

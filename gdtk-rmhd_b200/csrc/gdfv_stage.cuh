@@ -387,10 +387,24 @@ __device__ __forceinline__ void recon_cell(const R* w, const R* wf, const NumPar
             if (MHD && s == 8 && !P.divergence_cleaning) { qm[s] = q0[s]; qp[s] = q0[s]; continue; }
             R dm = (q0[s] - qm1[s]) * t;
             R dp = (qp1[s] - q0[s]) * t;
-            R sl = R(1.0);
-            if (lim) sl = (dm * dp + rabs(dm * dp) + eps) / (dm * dm + dp * dp + eps);
+            R sl = R(1.0), slm = R(1.0);
+            if (lim) {
+                if (P.lmr_epsilon) {
+                    // lmr/onedinterp.d:147-151: each face's epsilon is scaled by the larger of
+                    // its two states, so the plus face (q0, qp1) and the minus face (qm1, q0)
+                    // of the cell get separate limiter values
+                    const R tiny = R(1e-12);
+                    const R ep = rmax(rmax(tiny, rabs(q0[s])), rmax(tiny, rabs(qp1[s]))) * eps * t;
+                    const R em = rmax(rmax(tiny, rabs(qm1[s])), rmax(tiny, rabs(q0[s]))) * eps * t;
+                    sl = (dm * dp + rabs(dm * dp) + ep) / (dm * dm + dp * dp + ep);
+                    slm = (dm * dp + rabs(dm * dp) + em) / (dm * dm + dp * dp + em);
+                } else {
+                    sl = (dm * dp + rabs(dm * dp) + eps) / (dm * dm + dp * dp + eps);
+                    slm = sl;
+                }
+            }
             R vp = q0[s] + sl * aL0 * (dp * w3 + dm * len);
-            R vm = q0[s] - sl * aR0 * (dp * len + dm * w3);
+            R vm = q0[s] - slm * aR0 * (dp * len + dm * w3);
             if (clip) {
                 vp = clip_fast(vp, q0[s], qp1[s]);
                 vm = clip_fast(vm, qm1[s], q0[s]);

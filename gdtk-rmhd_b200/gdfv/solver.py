@@ -22,7 +22,8 @@ FACE_INDEX = {"west": 0, "iminus": 0, "east": 1, "iplus": 1, "south": 2, "jminus
               "north": 3, "jplus": 3, "bottom": 4, "kminus": 4, "top": 5, "kplus": 5}
 FACE_NAMES = ["west", "east", "south", "north", "bottom", "top"]
 
-_STR_KEYS = ("flux_calculator", "gasdynamic_update_scheme", "thermo_interpolator", "flux_precision")
+_STR_KEYS = ("flux_calculator", "gasdynamic_update_scheme", "thermo_interpolator", "flux_precision",
+             "van_albada_variant")
 _INT_KEYS = ("interpolation_order", "dimensions", "MHD", "divergence_cleaning", "apply_limiter",
              "extrema_clipping", "apply_entropy_fix", "interpolate_in_local_frame", "stringent_cfl",
              "cfl_count", "max_attempts_for_step", "max_invalid_cells", "fixed_time_step",
@@ -41,6 +42,7 @@ class Config:
         self.gasdynamic_update_scheme = "predictor_corrector"
         self.thermo_interpolator = "rhou"
         self.flux_precision = "fp64"
+        self.van_albada_variant = "e4"   # "lmr": epsilon scaled per face as Eilmer 5 (lmr) does
         self.interpolation_order = 2
         self.dimensions = 3
         self.MHD = False

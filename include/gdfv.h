@@ -46,7 +46,9 @@ int gdfv_context_free(int ctx);
  * (e4/globalconfig.d:1858-2004 readers, :186-206 and :320-345 name->enum maps,
  * '-' accepted for '_').  Strings: flux_calculator (ausmdv | hllc | hlle),
  * gasdynamic_update_scheme (predictor_corrector | pc), thermo_interpolator (rhou),
- * flux_precision (fp64 | fp32).  Integers: interpolation_order (2), dimensions (2|3),
+ * flux_precision (fp64 | fp32), van_albada_variant (e4 | lmr: the limiter epsilon
+ * scaled per face by the larger state beside it and the face's length factor, as
+ * lmr/onedinterp.d:147-151 does; no e4 counterpart).  Integers: interpolation_order (2), dimensions (2|3),
  * MHD, divergence_cleaning, apply_limiter, extrema_clipping, apply_entropy_fix,
  * interpolate_in_local_frame (1), stringent_cfl, cfl_count, max_attempts_for_step,
  * max_invalid_cells, fixed_time_step, n_ghost_cell_layers (2), glm_reference_indexing,

@@ -532,6 +532,7 @@ int orc_set_int(int h, const char* key, int v) {
     else if (k == "max_attempts_for_step") c.max_attempts = v;
     else if (k == "max_invalid_cells") c.max_invalid_cells = v;
     else if (k == "chicken_compat") c.chicken_compat = v;
+    else if (k == "lmr_epsilon") c.lmr_epsilon = v;
     else { s->last_error = "unknown int key " + k; return -1; }
     return 0;
 }

@@ -64,6 +64,7 @@ struct Config {
     int max_attempts = 3;           // :951
     int max_invalid_cells = 0;      // :1018
     int chicken_compat = 0;         // unit lengths in the limiter and sound speed recomputed (src/chicken)
+    int lmr_epsilon = 0;            // van Albada epsilon scaled per face as lmr/onedinterp.d:147-151 does
     double eps_van_albada = 1.0e-12;
     double R = 287.1;
     double gamma = 1.4;
@@ -160,7 +161,15 @@ struct L2R2 {
         T delRplus = (qR1 - qR0) * two_over_lenR1_plus_lenR0;
         T sL = 1.0, sR = 1.0;
         if (cfg->apply_limiter) {
-            const double eps = cfg->eps_van_albada;
+            T eps = cfg->eps_van_albada;
+            if (cfg->lmr_epsilon) {
+                // lmr/onedinterp.d:147-151: epsilon dimensionalised by the larger of the
+                // two states beside the face and the face's length factor
+                T qqL = fmax_(T(1e-12), fabs_(qL0));
+                T qqR = fmax_(T(1e-12), fabs_(qR0));
+                T qq = fmax_(qqL, qqR);
+                eps = qq * cfg->eps_van_albada * two_over_lenR0_plus_lenL0;
+            }
             sL = (delLminus * del + fabs_(delLminus * del) + eps) / (delLminus * delLminus + del * del + eps);
             sR = (del * delRplus + fabs_(del * delRplus) + eps) / (del * del + delRplus * delRplus + eps);
         }

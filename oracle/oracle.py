@@ -62,7 +62,7 @@ class OracleSim:
 
     INT_KEYS = {"dimensions", "MHD", "divergence_cleaning", "apply_limiter", "extrema_clipping",
                 "apply_entropy_fix", "glm_reference_indexing", "stringent_cfl", "cfl_count",
-                "max_attempts_for_step", "max_invalid_cells", "chicken_compat"}
+                "max_attempts_for_step", "max_invalid_cells", "chicken_compat", "lmr_epsilon"}
 
     def __init__(self, **cfg):
         self.L = lib()
@@ -77,6 +77,10 @@ class OracleSim:
             rc = self.L.orc_set_int(self.h, b"flux_calculator", FLUX[value])
         elif key == "gasdynamic_update_scheme":
             rc = self.L.orc_set_int(self.h, b"update_scheme", SCHEME[value.replace("-", "_")])
+        elif key == "van_albada_variant":   # "e4" (default) or "lmr"
+            if value not in ("e4", "lmr"):
+                raise KeyError(value)
+            rc = self.L.orc_set_int(self.h, b"lmr_epsilon", int(value == "lmr"))
         elif key in self.INT_KEYS:
             rc = self.L.orc_set_int(self.h, key.encode(), int(value))
         else:

@@ -195,3 +195,29 @@ def test_failed_step_retry_and_abort_match_oracle(cfl, extra):
         # oracle statuses: -3 too many bad cells, -2 failed after max attempts
         assert code == (GDFV_ERR_BAD_CELLS if rc == -3 else GDFV_ERR_STEP_FAILED), (rc, code)
         print(f"cfl {cfl}: status rc={rc} code={code}")
+
+
+@pytest.mark.parametrize("case_name", ["inflow_partial", "shock_box"])
+def test_lmr_van_albada_variant_fp64(case_name):
+    """van_albada_variant=lmr (lmr/onedinterp.d:147-151: the limiter epsilon scaled per
+    face by the larger state beside it) against the oracle's face-wise form."""
+    case = cases.c2_inflow_box(n=(45, 19, 37)) if case_name == "inflow_partial" else cases.c1_shock_box(n=24)
+    case.config.update(van_albada_variant="lmr", epsilon_van_albada=1e-3)
+    orc, sim = run_both(case, 10)
+    assert compare_fp64(case, orc, sim) <= TOL_FP64
+    # the option changes the result (epsilon 1e-3 scaled by the state is not negligible)
+    e4 = cases.c1_shock_box(n=24) if case_name == "shock_box" else cases.c2_inflow_box(n=(45, 19, 37))
+    e4.config.update(epsilon_van_albada=1e-3)
+    _, sim_e4 = run_both(e4, 10)
+    assert not np.array_equal(sim_e4.get_conserved(0), sim.get_conserved(0))
+
+
+def test_lmr_van_albada_variant_fp32():
+    case = cases.c2_inflow_box(n=(48, 40, 36))
+    case.config.update(van_albada_variant="lmr", epsilon_van_albada=1e-3)
+    orc, sim = cases.build_pair(case, flux_precision="fp32")
+    assert orc.run(50) == 0
+    assert sim.run(max_step=50) == 50
+    Uo, Ug = orc.get_U(0), sim.get_conserved(0)
+    errs = [cases.rel_l2(Ug[0], Uo[0]), cases.rel_l2(Ug[1:4].ravel(), Uo[1:4].ravel()), cases.rel_l2(Ug[4], Uo[4])]
+    assert max(errs) <= TOL_FP32_L2, errs
