@@ -30,6 +30,7 @@ namespace gdfv {
 namespace {
 
 constexpr int NP = 6;  // rho, v0, v1, v2, u, a
+constexpr int SRC_DONE = -1;  // a stencil source whose cotangent has been added already
 
 __device__ __forceinline__ double sgn(double x) { return x < 0.0 ? -1.0 : 1.0; }
 
@@ -493,7 +494,7 @@ template <int D>
 __device__ __forceinline__ void face_thread(const AdjArgs& a, long long f) {
     const long long* off = a.face_off + D * (a.nblocks + 1);
     const bool act = f < off[a.nblocks];
-    int kind[4] = {SRC_INFLOW + 1, SRC_INFLOW + 1, SRC_INFLOW + 1, SRC_INFLOW + 1};
+    int kind[4] = {SRC_DONE, SRC_DONE, SRC_DONE, SRC_DONE};
     int inflow = -1;
     double gc[4][NP];
     for (int m = 0; m < 4; ++m)
@@ -522,7 +523,7 @@ __device__ __forceinline__ void face_thread(const AdjArgs& a, long long f) {
                 if (recv) gc[2][q] += v;
                 if (sent) gc[m][q] = 0.0;
             }
-            if (sent) kind[m] = SRC_INFLOW + 1;   // nothing left to scatter for this source
+            if (sent) kind[m] = SRC_DONE;   // nothing left to scatter for this source
         }
     }
     // Inflow ghost states are shared by every face along an inflow boundary: sum the
@@ -540,7 +541,7 @@ __device__ __forceinline__ void face_thread(const AdjArgs& a, long long f) {
                 key = inflow;
 #pragma unroll
                 for (int q = 0; q < NP; ++q) vin[q] += gc[m][q];
-                kind[m] = SRC_INFLOW + 1;
+                kind[m] = SRC_DONE;
             }
         }
         if (__ballot_sync(full, key >= 0)) {
@@ -564,7 +565,7 @@ __device__ __forceinline__ void face_thread(const AdjArgs& a, long long f) {
     const int b = face_coords<D>(a, f, i, j, k);
     const BlockDesc& B = a.blocks[b];
     for (int m = 0; m < 4; ++m)
-        if (kind[m] <= SRC_INFLOW) adj_scatter(a, stencil_src<D>(a, B, i, j, k, m), gc[m]);
+        if (kind[m] >= 0) adj_scatter(a, stencil_src<D>(a, B, i, j, k, m), gc[m]);
 }
 
 // All faces of the three directions in one launch: CTAs [0, nb0) take the i faces,
@@ -638,6 +639,13 @@ bool vjp_supported(int ctx, const AdjView& v) {
                                "and van_albada_variant=e4");
         return false;
     }
+    for (const BlockDesc& B : v.h_blocks)
+        for (int f = 0; f < 6; ++f)
+            if (B.bc_type[f] == BC_FIXED_P || B.bc_type[f] == BC_FIXED_PT || B.bc_type[f] == BC_SIMPLE_FLUX) {
+                adjoint_set_error(ctx, "the adjoint supports slip-wall, extrapolate, supersonic-inflow and "
+                                       "exchange boundaries");
+                return false;
+            }
     return true;
 }
 

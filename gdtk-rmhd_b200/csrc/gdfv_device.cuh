@@ -15,7 +15,8 @@ namespace gdfv {
 // Conserved-quantity slots, e4/conservedquantities.d:148-197 (3D or MHD ordering)
 enum : int { MASS = 0, XMOM = 1, YMOM = 2, ZMOM = 3, TOTENERGY = 4, XB = 5, YB = 6, ZB = 7, PSI = 8, DIVB = 9 };
 enum : int { FLUX_AUSMDV = 0, FLUX_HLLC = 1, FLUX_HLLE = 2 };
-enum : int { BC_SLIP_WALL = 0, BC_EXTRAPOLATE = 1, BC_INFLOW = 2, BC_EXCHANGE = 3 };
+enum : int { BC_SLIP_WALL = 0, BC_EXTRAPOLATE = 1, BC_INFLOW = 2, BC_EXCHANGE = 3, BC_FIXED_P = 4, BC_FIXED_PT = 5,
+             BC_SIMPLE_FLUX = 6 };
 // step status words
 enum : int { ST_OK = 0, ST_DECODE_FAILED = 1, ST_TOO_MANY_BAD_CELLS = 2 };
 

@@ -409,6 +409,8 @@ int do_prepare(Context* c) {
     const int nfaces = g.dims == 3 ? 6 : 4;
     long long off = 0;
     std::vector<InflowState> inflows;
+    struct FixedState { int block, face; InflowState state; };
+    std::vector<FixedState> fixed;
     c->h_blocks.clear();
     std::vector<TileDesc> tiles;
     const double Cv = g.R / (g.gamma - 1.0);
@@ -453,6 +455,18 @@ int do_prepare(Context* c) {
             }
             if (bc.type == BC_EXTRAPOLATE && (bc.x_order < 0 || bc.x_order > 1))
                 return fail(c, GDFV_ERR_ARG, "x_order must be 0 or 1");
+            if (bc.type == BC_SIMPLE_FLUX && g.mhd)
+                return fail(c, GDFV_ERR_ARG, "outflow_simple_flux is not defined for MHD (boundary_flux_effect.d:519)");
+            if (bc.type == BC_FIXED_P || bc.type == BC_FIXED_PT) {
+                // the outside state of fixed_p.d / fixed_pt.d: p (and rho = p/(T R), u = Cv T)
+                InflowState s{};
+                s.p = bc.inflow[0];
+                if (bc.type == BC_FIXED_PT) {
+                    s.rho = bc.inflow[0] / (bc.inflow[1] * g.R);
+                    s.u = Cv * bc.inflow[1];
+                }
+                fixed.push_back({(int)b, f, s});
+            }
             if (bc.type == BC_INFLOW) {
                 // FlowState:new{p=, T=, ...}: update_thermo_from_pT + update_sound_speed
                 InflowState s{};
@@ -471,10 +485,15 @@ int do_prepare(Context* c) {
         c->h_blocks.push_back(B);
         off += (long long)hb.n[0] * hb.n[1] * hb.n[2];
     }
+    // outside states of the fixed-p boundaries after the supersonic-inflow states
+    c->n_inflow = (int)inflows.size();
+    for (const FixedState& fx : fixed) {
+        c->h_blocks[fx.block].bc_inflow[fx.face] = (int)inflows.size();
+        inflows.push_back(fx.state);
+    }
     c->total = off;
     build_tiles(c, g.tile_kchunk, tiles);
     c->n_tiles = (int)tiles.size();
-    c->n_inflow = (int)inflows.size();
     NumParams& P = c->P;
     P.gas.R = g.R; P.gas.gamma = g.gamma; P.gas.Cv = Cv; P.gas.Cvinv = 1.0 / Cv;
     P.eps_van_albada = g.eps_van_albada;
@@ -798,6 +817,9 @@ int gdfv_block_set_bc(int ctx, int blk, int face, const char* bc_type, int x_ord
     else if (t == "outflow_simple_extrapolate" || t == "extrapolate") bc.type = BC_EXTRAPOLATE;
     else if (t == "inflow_supersonic") bc.type = BC_INFLOW;
     else if (t == "exchange_over_full_face" || t == "exchange" || t == "full_face_copy") bc.type = BC_EXCHANGE;
+    else if (t == "outflow_fixed_p") bc.type = BC_FIXED_P;
+    else if (t == "outflow_fixed_p_and_t") bc.type = BC_FIXED_PT;
+    else if (t == "outflow_simple_flux" || t == "outflow_simple") bc.type = BC_SIMPLE_FLUX;
     else return fail(c, GDFV_ERR_ARG, "unsupported boundary condition: " + t);
     bc.x_order = x_order;
     bc.other = other_blk;
@@ -805,6 +827,12 @@ int gdfv_block_set_bc(int ctx, int blk, int face, const char* bc_type, int x_ord
     if (bc.type == BC_INFLOW) {
         if (!inflow) return fail(c, GDFV_ERR_ARG, "inflow_supersonic needs a flow state");
         for (int q = 0; q < 9; ++q) bc.inflow[q] = inflow[q];
+    }
+    if (bc.type == BC_FIXED_P || bc.type == BC_FIXED_PT) {   // inflow = {p_outside, T_outside}
+        if (!inflow || !(inflow[0] > 0.0) || (bc.type == BC_FIXED_PT && !(inflow[1] > 0.0)))
+            return fail(c, GDFV_ERR_ARG, "outflow_fixed_p needs p_outside > 0 (and T_outside > 0 with _and_t)");
+        bc.inflow[0] = inflow[0];
+        bc.inflow[1] = bc.type == BC_FIXED_PT ? inflow[1] : 0.0;
     }
     c->blocks[blk].bc[face] = bc;
     return GDFV_OK;

@@ -86,7 +86,8 @@ __device__ __forceinline__ long long cell_index(const BlockDesc& B, int i, int j
 }
 
 // Where the state of block cell (i,j,k) comes from.
-enum : int { SRC_CELL = 0, SRC_MIRROR = 1, SRC_EXTRAP1_G0 = 2, SRC_EXTRAP1_G1 = 3, SRC_INFLOW = 4 };
+enum : int { SRC_CELL = 0, SRC_MIRROR = 1, SRC_EXTRAP1_G0 = 2, SRC_EXTRAP1_G1 = 3, SRC_INFLOW = 4, SRC_FIXEDP = 5,
+             SRC_FIXEDPT = 6 };
 struct CellSrc {
     const BlockDesc* blk;  // block holding the source cell(s)
     long long c0, c1;      // source cell (and the depth-1 cell for xOrder 1)
@@ -118,6 +119,13 @@ __device__ __forceinline__ CellSrc resolve(const StageArgs& A, const BlockDesc& 
     if (type == BC_SLIP_WALL) {
         s.kind = SRC_MIRROR;            // internal_copy_then_reflect.d:111-150
         s.c0 = at_depth(depth);
+    } else if (type == BC_FIXED_P || type == BC_FIXED_PT) {
+        // fixed_p.d:98-119 / fixed_pt.d:105-128: interior cell n with the outside p (T)
+        s.kind = type == BC_FIXED_P ? SRC_FIXEDP : SRC_FIXEDPT;
+        s.c0 = at_depth(depth);
+        s.inflow = B.bc_inflow[face];
+    } else if (type == BC_SIMPLE_FLUX) {
+        s.c0 = at_depth(0);             // its ghosts: ExtrapolateCopy, xOrder 0 (bc.lua:1548)
     } else if (type == BC_EXTRAPOLATE) {
         if (B.bc_xorder[face] == 0) {   // extrapolate_copy.d:124-147
             s.c0 = at_depth(0);
@@ -233,6 +241,22 @@ __device__ __noinline__ Prim<double> extrap1_ghost(const double* Uin, const doub
     return out;
 }
 
+// Ghost of OutFlowBC_FixedP / _FixedPT from the decoded interior cell e (rare path, out
+// of line): update_thermo_from_pT (ideal_gas.d:89-97) with the outside p (and T),
+// rho = p/(T R), u = Cv T; velocity and sound speed stay the interior cell's.
+static __device__ __noinline__ Prim<double> fixed_ghost(Prim<double> e, bool p_only, double p, double rho_pt, double u_pt,
+                                                 double Cvinv, double Cv, double Rg) {
+    if (p_only) {
+        const double T = e.u * Cvinv;
+        e.rho = p / (T * Rg);
+        e.u = Cv * T;
+    } else {
+        e.rho = rho_pt;
+        e.u = u_pt;
+    }
+    return e;
+}
+
 template <int STAGE, bool FAST, bool MHD, int NQ>
 __device__ __forceinline__ void finish_cell(const StageArgs& A, const double* Uin, const CellSrc& s,
                                             const double* U0, int i, int j, double dt, double damp,
@@ -261,10 +285,15 @@ __device__ __forceinline__ void finish_cell(const StageArgs& A, const double* Ui
                 out.B[1] = -cc * (3 * (x + 0.) * (y + 0.0));
             }
         }
-    } else if (s.kind == SRC_EXTRAP1_G0 || s.kind == SRC_EXTRAP1_G1) {
-        out = extrap1_ghost<STAGE, FAST, MHD, NQ>(Uin, A.dU0, A.total, s.blk->offset + s.c1, dt, damp,
-                                                  A.P.divergence_cleaning, A.P.gas.Cvinv, A.P.gas.gamma * A.P.gas.R,
-                                                  out, s.kind == SRC_EXTRAP1_G0);
+    } else if (s.kind > SRC_MIRROR) {   // the rare kinds, out of line (SRC_INFLOW returned above)
+        if (s.kind >= SRC_FIXEDP) {
+            const InflowState& o = A.inflow[s.inflow];
+            out = fixed_ghost(out, s.kind == SRC_FIXEDP, o.p, o.rho, o.u, A.P.gas.Cvinv, A.P.gas.Cv, A.P.gas.R);
+        } else {
+            out = extrap1_ghost<STAGE, FAST, MHD, NQ>(Uin, A.dU0, A.total, s.blk->offset + s.c1, dt, damp,
+                                                      A.P.divergence_cleaning, A.P.gas.Cvinv, A.P.gas.gamma * A.P.gas.R,
+                                                      out, s.kind == SRC_EXTRAP1_G0);
+        }
     }
 }
 
@@ -478,6 +507,36 @@ __device__ __forceinline__ void ausmdv_f(float g, float gm1, bool efix, float rL
             F[3] -= d_ua * (rw.y - rw.x);
             F[4] -= d_ua * (rH.y - rH.x);
         }
+    }
+}
+
+// boundary_flux_effect.d:504-645 BFE_SimpleOutflowFlux on a fixed Cartesian grid: the
+// boundary face (normal +axis D) takes the flux of the interior cell's state (prim
+// array pl, entry il) when the mass flux leaves the domain (outsign * m > 0), else the
+// face is closed (pressure only).  Fg in the global frame.
+template <class R, int D>
+__device__ __forceinline__ void simple_outflow_flux(const NumParams& P, const R* pl, int il, int stride, int outsign,
+                                                    R* Fg) {
+    const R rho = pl[il], u = pl[4 * stride + il];
+    const R v[3] = {pl[stride + il], pl[2 * stride + il], pl[3 * stride + il]};
+    const R p = rho * R(P.gas.R) * (u * R(P.gas.Cvinv));
+    const R nv[3] = {R(D == 0 ? 1.0 : 0.0), R(D == 1 ? 1.0 : 0.0), R(D == 2 ? 1.0 : 0.0)};
+    const R vn = v[0] * nv[0] + v[1] * nv[1] + v[2] * nv[2];
+    const R m = rho * vn;
+    const bool threeD = P.dims == 3;
+    if (R(outsign) * m > R(0.0)) {
+        Fg[MASS] = m;
+        Fg[XMOM] = p * nv[0] + v[0] * m;
+        Fg[YMOM] = p * nv[1] + v[1] * m;
+        Fg[ZMOM] = threeD ? p * nv[2] + v[2] * m : R(0.0);
+        const R utot = u + R(0.5) * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        Fg[TOTENERGY] = m * utot + p * vn;
+    } else {
+        Fg[MASS] = R(0.0);
+        Fg[XMOM] = nv[0] * p;
+        Fg[YMOM] = nv[1] * p;
+        Fg[ZMOM] = threeD ? nv[2] * p : R(0.0);
+        Fg[TOTENERGY] = p * R(0.0);
     }
 }
 
@@ -713,6 +772,14 @@ __global__ void __launch_bounds__(32 * (TJ + 1), MHD ? 1 : (sizeof(R) == 4 ? GDF
         const bool active = owner && ti < ni_t && tj < nj_t;
         const int pidx = (ti + 2) + PW * (tj + 2);     // own cell in a padded plane
         const bool has_k = (P.dims == 3);
+        // faces of this tile on a simple-outflow-flux boundary: bit 2*axis + (plus side)
+        int sfx = 0;
+        if (t.i0 == 0 && B.bc_type[0] == BC_SIMPLE_FLUX) sfx |= 1;
+        if (t.i0 + ni_t == B.n[0] && B.bc_type[1] == BC_SIMPLE_FLUX) sfx |= 2;
+        if (t.j0 == 0 && B.bc_type[2] == BC_SIMPLE_FLUX) sfx |= 4;
+        if (t.j0 + nj_t == B.n[1] && B.bc_type[3] == BC_SIMPLE_FLUX) sfx |= 8;
+        if (has_k && t.k0 == 0 && B.bc_type[4] == BC_SIMPLE_FLUX) sfx |= 16;
+        if (has_k && t.k1 == B.n[2] && B.bc_type[5] == BC_SIMPLE_FLUX) sfx |= 32;
         if (tid < 3 * W_N) w[tid / W_N][tid % W_N] = (R)B.w[tid / W_N][tid % W_N];
         if (tid < 3) {
             const double* bw = B.w[tid];
@@ -901,6 +968,36 @@ __global__ void __launch_bounds__(32 * (TJ + 1), MHD ? 1 : (sizeof(R) == 4 ? GDF
                 }
             }
             __syncthreads();
+
+            // ---------------- boundary faces with OutFlowBC_SimpleFlux (only tiles that have
+            // them): their flux is the interior cell's (boundary_flux_effect.d:504-645)
+            if (sfx) {
+                if (active && has_k) {
+                    if ((sfx & 16) && k == 0) simple_outflow_flux<R, 2>(P, cur, pidx, PLANE, -1, fB);
+                    if ((sfx & 32) && k + 1 == B.n[2]) simple_outflow_flux<R, 2>(P, cur, pidx, PLANE, 1, fT);
+                }
+                for (int e = tid; e < 2 * nj_t + 2 * ni_t; e += NT) {
+                    R F[NQ];
+                    if (e < 2 * nj_t) {             // i faces 0 (west) and ni_t (east) of row e / 2
+                        const int row = e >> 1, east = e & 1;
+                        if (!(sfx & (east ? 2 : 1))) continue;
+                        const int fi = east ? ni_t : 0;
+                        const int p = (fi + 2) + PW * (row + 2);
+                        simple_outflow_flux<R, 0>(P, cur, east ? p - 1 : p, PLANE, east ? 1 : -1, F);
+#pragma unroll
+                        for (int q = 0; q < NQ; ++q) FI[q * NFI + row * (TI + 1) + fi] = F[q];
+                    } else {                        // j faces 0 (south) and nj_t (north) of a column
+                        const int col = (e - 2 * nj_t) >> 1, north = (e - 2 * nj_t) & 1;
+                        if (!(sfx & (north ? 8 : 4))) continue;
+                        const int fj = north ? nj_t : 0;
+                        const int p = (col + 2) + PW * (fj + 2);
+                        simple_outflow_flux<R, 1>(P, cur, north ? p - PW : p, PLANE, north ? 1 : -1, F);
+#pragma unroll
+                        for (int q = 0; q < NQ; ++q) FJ[q * NFJ + fj * TI + col] = F[q];
+                    }
+                }
+                __syncthreads();
+            }
 
             // ---------------- phase D: residual (e4/fvcell.d:824-856, faces W, E, S, N, B, T) and update
             if (active) {

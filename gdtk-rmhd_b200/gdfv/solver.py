@@ -114,6 +114,33 @@ class OutFlowBC_SimpleExtrapolate:
         self.xOrder = int(xOrder)
 
 
+class OutFlowBC_SimpleFlux:
+    """bc.lua:1532-1556: ghost cells by ExtrapolateCopy (xOrder 0) and the boundary
+    face's flux from the interior cell (boundary_flux_effect.d:504-645)."""
+    name = "outflow_simple_flux"
+
+
+class OutFlowBC_FixedP:
+    """bc.lua:1558-1578: ghost cells copy the interior cells with the pressure fixed
+    at p_outside (fixed_p.d)."""
+    name = "outflow_fixed_p"
+
+    def __init__(self, p_outside, xOrder=0):
+        self.p_outside = float(p_outside)
+        self.xOrder = int(xOrder)
+
+
+class OutFlowBC_FixedPT:
+    """bc.lua:1580-1600: ghost cells copy the interior cells' velocity with pressure
+    and temperature fixed at p_outside, T_outside (fixed_pt.d)."""
+    name = "outflow_fixed_p_and_t"
+
+    def __init__(self, p_outside, T_outside, xOrder=0):
+        self.p_outside = float(p_outside)
+        self.T_outside = float(T_outside)
+        self.xOrder = int(xOrder)
+
+
 class InFlowBC_Supersonic:
     name = "inflow_supersonic"
 
@@ -186,6 +213,13 @@ class Simulation:
             self._bcs[blk][f] = arr  # keep alive
             inflow = ffi.cast("double*", arr.ctypes.data)
             self.n_inflow += 1
+        elif isinstance(bc, (OutFlowBC_FixedP, OutFlowBC_FixedPT)):
+            arr = np.zeros(9)
+            arr[0] = bc.p_outside
+            arr[1] = getattr(bc, "T_outside", 0.0)
+            self._bcs[blk][f] = arr
+            inflow = ffi.cast("double*", arr.ctypes.data)
+            x_order = bc.xOrder
         check(self.ctx, self.L.gdfv_block_set_bc(self.ctx, blk, f, bc.name.encode(), x_order, other,
                                                   other_face, inflow))
 

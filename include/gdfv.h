@@ -80,6 +80,11 @@ int gdfv_block_new(int ctx, int nic, int njc, int nkc, double dx, double dy, dou
  *                                B.x, B.y, B.z, psi} as FlowState:new{p=,T=,...} (:1251-1280)
  *   "exchange_over_full_face"    ExchangeBC_FullFace with orientation 0 onto the opposite
  *                                face other_face of block other_blk (:1603)
+ *   "outflow_simple_flux"        OutFlowBC_SimpleFlux (:1532-1556): ghosts copy the boundary
+ *                                cell, the boundary face's flux is the interior cell's
+ *                                (boundary_flux_effect.d:504-645); not with MHD
+ *   "outflow_fixed_p"            OutFlowBC_FixedP (:1558-1578), inflow = {p_outside}
+ *   "outflow_fixed_p_and_t"      OutFlowBC_FixedPT (:1580-1600), inflow = {p_outside, T_outside}
  * Ghost cells are never stored: the kernels synthesise them (ghost_cell_effect/*.d). */
 int gdfv_block_set_bc(int ctx, int blk, int face, const char* bc_type, int x_order,
                       int other_blk, int other_face, const double* inflow);

@@ -129,8 +129,23 @@ static void fill_ghosts(const Sim& sim, std::vector<std::vector<FlowState<T>>>& 
                             F[depth_index(b, face, -1 - n, p, q)] = s;
                         }
                         break;
+                    case BC_FIXED_P:
+                    case BC_FIXED_PT:
+                        // fixed_p.d:98-119, fixed_pt.d:105-128: ghost n is interior cell n with p
+                        // (and T) replaced and rho, u from update_thermo_from_pT; the velocity and
+                        // the sound speed stay those of the interior cell (the ExtrapolateCopy that
+                        // runs before is overwritten)
+                        for (int n = 0; n < 2; ++n) {
+                            FlowState<T> s = F[depth_index(b, face, n, p, q)];
+                            s.p = T(bc.p_out);
+                            if (bc.type == BC_FIXED_PT) s.Tg = T(bc.T_out);
+                            update_thermo_from_pT(g, s);
+                            F[depth_index(b, face, -1 - n, p, q)] = s;
+                        }
+                        break;
+                    case BC_SIMPLE_FLUX:   // OutFlowBC_SimpleFlux ghosts: ExtrapolateCopy, xOrder 0 (bc.lua:1548)
                     case BC_EXTRAPOLATE:
-                        if (bc.x_order == 0) {
+                        if (bc.type == BC_SIMPLE_FLUX || bc.x_order == 0) {
                             FlowState<T> s = F[depth_index(b, face, 0, p, q)];
                             F[depth_index(b, face, -1, p, q)] = s;
                             F[depth_index(b, face, -2, p, q)] = s;
@@ -170,6 +185,31 @@ static inline double cell_volume(const Block& b, int dims) {
     return dims == 2 ? b.dx * b.dy : b.dx * b.dy * b.dz;
 }
 
+// boundary_flux_effect.d:504-645 BFE_SimpleOutflowFlux.compute_outflow_flux on a fixed
+// Cartesian grid: the boundary face (normal +axis d) takes the flux of the interior
+// cell's state when it leaves the domain (outsign * mass flux > 0), else it is closed.
+template <class T>
+static void simple_outflow_flux(const Config& cfg, const FlowState<T>& fs, int d, int outsign, T* F) {
+    const double nv[3] = {d == 0 ? 1.0 : 0.0, d == 1 ? 1.0 : 0.0, d == 2 ? 1.0 : 0.0};
+    T vn = fs.vel[0] * nv[0] + fs.vel[1] * nv[1] + fs.vel[2] * nv[2];
+    T mass_flux = fs.rho * vn;
+    const bool threeD = cfg.dimensions == 3;
+    if (outsign * re(mass_flux) > 0.0) {
+        F[MASS] = mass_flux;
+        F[XMOM] = fs.p * nv[0] + fs.vel[0] * mass_flux;
+        F[YMOM] = fs.p * nv[1] + fs.vel[1] * mass_flux;
+        F[ZMOM] = threeD ? T(fs.p * nv[2] + fs.vel[2] * mass_flux) : T(0.0);
+        T utot = fs.u + 0.5 * (fs.vel[0] * fs.vel[0] + fs.vel[1] * fs.vel[1] + fs.vel[2] * fs.vel[2]);
+        F[TOTENERGY] = mass_flux * utot + fs.p * vn;
+    } else {
+        F[MASS] = 0.0;
+        F[XMOM] = nv[0] * fs.p;
+        F[YMOM] = nv[1] * fs.p;
+        F[ZMOM] = threeD ? T(nv[2] * fs.p) : T(0.0);
+        F[TOTENERGY] = fs.p * 0.0;
+    }
+}
+
 // Flux on every face, then dUdt for every interior cell.  fs holds the
 // decoded interior states; ghosts are filled here.
 template <class T>
@@ -207,6 +247,11 @@ static void eval_dUdt(const Sim& sim, std::vector<std::vector<FlowState<T>>>& fs
                 FlowState<T> Lft, Rght;
                 interp_l2r2(cfg, g, d, cL1, cL0, cR0, cR1, lenL1, lenL0, lenR0, lenR1, Lft, Rght);
                 interface_flux(cfg, g, sim.c_h, d, Lft, Rght, &flux[d][(size_t)f * nq]);
+                const int idx = d == 0 ? i : (d == 1 ? j : k);
+                if (idx == 0 && b.bc[2 * d].type == BC_SIMPLE_FLUX)
+                    simple_outflow_flux(cfg, cR0, d, -1, &flux[d][(size_t)f * nq]);
+                else if (idx == n[d] && b.bc[2 * d + 1].type == BC_SIMPLE_FLUX)
+                    simple_outflow_flux(cfg, cL0, d, 1, &flux[d][(size_t)f * nq]);
             }
         }
         double area[3] = {face_area(b, 0, cfg.dimensions), face_area(b, 1, cfg.dimensions),
@@ -586,6 +631,10 @@ int orc_set_bc(int h, int blk, int face, int type, int x_order, int other_blk, i
     if (!s || blk < 0 || blk >= (int)s->blocks.size() || face < 0 || face > 5) return -1;
     BoundaryCondition& bc = s->blocks[blk].bc[face];
     bc.type = type; bc.x_order = x_order; bc.other_block = other_blk; bc.other_face = other_face;
+    if ((type == BC_FIXED_P || type == BC_FIXED_PT) && inflow_pT) {
+        bc.p_out = inflow_pT[0];
+        bc.T_out = inflow_pT[1];
+    }
     if (type == BC_INFLOW && inflow_pT) {
         Gas g = s->gas();
         FlowState<double> fs;

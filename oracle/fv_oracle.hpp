@@ -43,7 +43,8 @@ inline cplx exp_(const cplx& x) { return std::exp(x); }
 // ---------------------------------------------------------------- options
 enum FluxCalc { FLUX_AUSMDV = 0, FLUX_HLLC = 1, FLUX_HLLE = 2 };
 enum Scheme { SCHEME_EULER = 0, SCHEME_PC = 1, SCHEME_TVD_RK3 = 2 };
-enum BcType { BC_SLIP_WALL = 0, BC_EXTRAPOLATE = 1, BC_INFLOW = 2, BC_EXCHANGE = 3 };
+enum BcType { BC_SLIP_WALL = 0, BC_EXTRAPOLATE = 1, BC_INFLOW = 2, BC_EXCHANGE = 3, BC_FIXED_P = 4, BC_FIXED_PT = 5,
+              BC_SIMPLE_FLUX = 6 };
 enum FaceId { WEST = 0, EAST = 1, SOUTH = 2, NORTH = 3, BOTTOM = 4, TOP = 5 };  // geom nomenclature.d:12-19
 
 // Conserved-quantity indices, e4/conservedquantities.d:148-197 (standard ordering, 3D or MHD)
@@ -565,6 +566,7 @@ struct BoundaryCondition {
     int other_block = -1;            // FullFaceCopy partner, orientation 0
     int other_face = -1;
     FlowState<double> inflow;        // FlowStateCopy state
+    double p_out = 0.0, T_out = 0.0; // GhostCellFixedP / GhostCellFixedPT (fixed_p.d, fixed_pt.d)
 };
 
 struct Block {

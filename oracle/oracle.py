@@ -16,7 +16,7 @@ _LIB = None
 
 FLUX = {"ausmdv": 0, "hllc": 1, "hlle": 2}
 SCHEME = {"euler": 0, "pc": 1, "predictor_corrector": 1, "tvd_rk3": 2}
-BC = {"wall_with_slip": 0, "extrapolate": 1, "inflow_supersonic": 2, "exchange": 3}
+BC = {"wall_with_slip": 0, "extrapolate": 1, "inflow_supersonic": 2, "exchange": 3, "fixed_p": 4, "fixed_pt": 5, "simple_flux": 6}
 FACES = {"west": 0, "east": 1, "south": 2, "north": 3, "bottom": 4, "top": 5}
 
 
@@ -102,7 +102,7 @@ class OracleSim:
         arr = np.zeros(9)
         if inflow is not None:
             arr[0] = inflow["p"]
-            arr[1] = inflow["T"]
+            arr[1] = inflow.get("T", 0.0)
             arr[2:5] = inflow.get("vel", (0.0, 0.0, 0.0))
             arr[5:8] = inflow.get("B", (0.0, 0.0, 0.0))
             arr[8] = inflow.get("psi", 0.0)

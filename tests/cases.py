@@ -214,7 +214,8 @@ def orszag_tang(n=(512, 512, 4), seed=99, precision="fp64", cleaning=True):
 
 # ---------------------------------------------------------------- builders
 _ORACLE_BC = {"wall_with_slip": "wall_with_slip", "outflow_simple_extrapolate": "extrapolate",
-              "inflow_supersonic": "inflow_supersonic", "exchange_over_full_face": "exchange"}
+              "inflow_supersonic": "inflow_supersonic", "exchange_over_full_face": "exchange",
+              "outflow_fixed_p": "fixed_p", "outflow_fixed_p_and_t": "fixed_pt", "outflow_simple_flux": "simple_flux"}
 
 
 def build_oracle(case):
@@ -227,9 +228,11 @@ def build_oracle(case):
         s.add_block(*b["n"], *b["d"], *b["origin"])
     for bi, b in enumerate(case.blocks):
         for face, (kind, kw) in b["bcs"].items():
+            inflow = kw.get("inflow")
+            if kind in ("outflow_fixed_p", "outflow_fixed_p_and_t"):
+                inflow = dict(p=kw["p_outside"], T=kw.get("T_outside", 0.0))
             s.set_bc(bi, face, _ORACLE_BC[kind], x_order=kw.get("x_order", 0),
-                     other_block=kw.get("other", -1), other_face=kw.get("other_face", -1),
-                     inflow=kw.get("inflow"))
+                     other_block=kw.get("other", -1), other_face=kw.get("other_face", -1), inflow=inflow)
         s.set_flow_rhoT(bi, b["rho"], b["vel"], b["T"], B=b["B"])
     s.init()
     return s
@@ -247,6 +250,12 @@ def build_gpu(case, **extra_config):
                 bc = gdfv.WallBC_WithSlip()
             elif kind == "outflow_simple_extrapolate":
                 bc = gdfv.OutFlowBC_SimpleExtrapolate(xOrder=kw.get("x_order", 0))
+            elif kind == "outflow_simple_flux":
+                bc = gdfv.OutFlowBC_SimpleFlux()
+            elif kind == "outflow_fixed_p":
+                bc = gdfv.OutFlowBC_FixedP(kw["p_outside"])
+            elif kind == "outflow_fixed_p_and_t":
+                bc = gdfv.OutFlowBC_FixedPT(kw["p_outside"], kw["T_outside"])
             elif kind == "inflow_supersonic":
                 inf = kw["inflow"]
                 bc = gdfv.InFlowBC_Supersonic(gdfv.FlowState(p=inf["p"], T=inf["T"], velx=inf["vel"][0],

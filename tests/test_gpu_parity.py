@@ -221,3 +221,42 @@ def test_lmr_van_albada_variant_fp32():
     Uo, Ug = orc.get_U(0), sim.get_conserved(0)
     errs = [cases.rel_l2(Ug[0], Uo[0]), cases.rel_l2(Ug[1:4].ravel(), Uo[1:4].ravel()), cases.rel_l2(Ug[4], Uo[4])]
     assert max(errs) <= TOL_FP32_L2, errs
+
+
+def _with_bcs(case, repl):
+    for b in case.blocks:
+        for face, spec in repl.items():
+            b["bcs"][face] = spec
+    return case
+
+
+OUTFLOW_BCS = {
+    "simple_flux": {"east": ("outflow_simple_flux", {}), "north": ("outflow_simple_flux", {})},
+    "fixed_p": {"east": ("outflow_fixed_p", dict(p_outside=5.0e4)), "top": ("outflow_fixed_p", dict(p_outside=8.0e4))},
+    "fixed_pt": {"west": ("outflow_fixed_p_and_t", dict(p_outside=1.2e5, T_outside=350.0)),
+                 "south": ("outflow_fixed_p_and_t", dict(p_outside=9.0e4, T_outside=280.0))},
+}
+
+
+@pytest.mark.parametrize("bc", sorted(OUTFLOW_BCS))
+def test_outflow_boundaries_fp64(bc):
+    """OutFlowBC_SimpleFlux (boundary face flux from the interior cell, both outflow
+    and closed faces), OutFlowBC_FixedP and OutFlowBC_FixedPT (ghost cells with the
+    outside p, T) against the oracle on the shock box (subsonic, both flow directions)
+    and on the supersonic inflow box with partial tiles."""
+    case = _with_bcs(cases.c1_shock_box(n=24), OUTFLOW_BCS[bc])
+    orc, sim = run_both(case, 10)
+    assert compare_fp64(case, orc, sim) <= TOL_FP64
+    case = _with_bcs(cases.c2_inflow_box(n=(45, 19, 37)), {"east": OUTFLOW_BCS[bc].get("east", ("outflow_simple_flux", {}))})
+    orc, sim = run_both(case, 8)
+    assert compare_fp64(case, orc, sim) <= TOL_FP64
+
+
+def test_outflow_boundaries_fp32():
+    case = _with_bcs(cases.c1_shock_box(n=24), {**OUTFLOW_BCS["simple_flux"], **OUTFLOW_BCS["fixed_pt"]})
+    orc, sim = cases.build_pair(case, flux_precision="fp32")
+    assert orc.run(20) == 0
+    assert sim.run(max_step=20) == 20
+    Uo, Ug = orc.get_U(0), sim.get_conserved(0)
+    errs = [cases.rel_l2(Ug[0], Uo[0]), cases.rel_l2(Ug[1:4].ravel(), Uo[1:4].ravel()), cases.rel_l2(Ug[4], Uo[4])]
+    assert max(errs) <= TOL_FP32_L2, errs
