@@ -246,6 +246,7 @@ struct Context {
     bool tuned = false;
     double tune_ms = 0.0;              // stage-1 + stage-2 time of the tuned configuration
     double* adj_scratch = nullptr;     // adjoint work arrays, allocated on first use
+    double* jvp_scratch = nullptr;     // Frechet JVP work arrays (U + sigma v, R0, R1, partial sums)
     int adj_ready = 0;
     long long adj_scratch_n = 0;
     cudaStream_t aux_stream[2] = {nullptr, nullptr};  // lowest / highest priority streams of the rollout adjoint
@@ -256,7 +257,7 @@ struct Context {
     ~Context() {
         if (graph) cudaGraphExecDestroy(graph);
         for (void* p : {(void*)U[0], (void*)U[1], (void*)dU0, (void*)d_blocks, (void*)d_tiles, (void*)d_inflow,
-                        (void*)d_ctl, (void*)d_maxsig, (void*)d_lastsig, (void*)d_bad, (void*)adj_scratch,
+                        (void*)d_ctl, (void*)d_maxsig, (void*)d_lastsig, (void*)d_bad, (void*)adj_scratch, (void*)jvp_scratch,
                         (void*)step_ctl, (void*)step_maxsig, (void*)step_lastsig})
             if (p) cudaFree(p);
         if (h_ctl) cudaFreeHost(h_ctl);
@@ -656,6 +657,36 @@ __global__ void step_dt_begin_kernel(Control* c, unsigned long long* maxsig, int
         c->attempt = 0; c->retrying = 0; c->steps_done = 0;
         c->tile_next = 0; c->tile_done = 0;
     }
+}
+
+// Frechet JVP helpers (e4/steadystate_core.d:1878-1970, :3040-3078).
+constexpr int kJvpSumBlocks = 592;   // 4 x 148 SMs
+// Per-CTA partial sums of eps*|U| + eps and v*v (added on the host in CTA order).
+__global__ void jvp_sums_kernel(const double* U, const double* v, long long n, double eps, double* partial) {
+    __shared__ double s1[256], s2[256];
+    double a = 0.0, b = 0.0;
+    for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < n; x += (long long)gridDim.x * blockDim.x) {
+        a += eps * fabs(U[x]) + eps;
+        b += v[x] * v[x];
+    }
+    s1[threadIdx.x] = a;
+    s2[threadIdx.x] = b;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) { s1[threadIdx.x] += s1[threadIdx.x + o]; s2[threadIdx.x] += s2[threadIdx.x + o]; }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) { partial[2 * blockIdx.x] = s1[0]; partial[2 * blockIdx.x + 1] = s2[0]; }
+}
+
+__global__ void jvp_axpy_kernel(const double* U, const double* v, double sigma, long long n, double* Up) {
+    long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (x < n) Up[x] = U[x] + sigma * v[x];
+}
+
+__global__ void jvp_diff_kernel(const double* R1, const double* R0, double sigma, long long n, double* Jv) {
+    long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (x < n) Jv[x] = (R1[x] - R0[x]) / sigma;
 }
 
 // Sets the dt of the next step of a gdfv_steps_dt chain; failure counts carry over.
@@ -1212,6 +1243,53 @@ int gdfv_residual(int ctx, const double* U_dev, double* R_dev) {
     A.U_in = U_dev;
     A.R_out = R_dev;
     CK(launch_stage(c, 0, A));
+    CK(cudaStreamSynchronize(c->stream));
+    return GDFV_OK;
+}
+
+int gdfv_residual_jvp(int ctx, const double* U_dev, const double* v_dev, const double* R0_dev, double sigma,
+                      double* Jv_dev, double* sigma_used) {
+    Context* c = get_ctx(ctx);
+    int st = check_ready(c, -1);
+    if (st) return st;
+    if (!U_dev || !v_dev || !Jv_dev) return fail(c, GDFV_ERR_ARG, "null pointer");
+    const long long n = (long long)c->nq * c->total;
+    if (!c->jvp_scratch) CK(cudaMalloc(&c->jvp_scratch, sizeof(double) * (3 * n + 2 * kJvpSumBlocks)));
+    double* Up = c->jvp_scratch;
+    double* R0 = Up + n;
+    double* R1 = R0 + n;
+    double* partial = R1 + n;
+    const unsigned nb = (unsigned)((n + 255) / 256);
+    if (!(sigma > 0.0)) {
+        // Knoll-McHugh perturbation (e4/steadystate_core.d:3040-3078):
+        // sigma = sum(eps |U| + eps) / (N max(||v||, sqrt(eps))), eps = 1e-7
+        const double eps = 1.0e-07;
+        jvp_sums_kernel<<<kJvpSumBlocks, 256, 0, c->stream>>>(U_dev, v_dev, n, eps, partial);
+        CK(cudaGetLastError());
+        std::vector<double> h(2 * kJvpSumBlocks);
+        CK(cudaMemcpyAsync(h.data(), partial, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        double sum = 0.0, v2 = 0.0;
+        for (int b = 0; b < kJvpSumBlocks; ++b) { sum += h[2 * b]; v2 += h[2 * b + 1]; }
+        double vnorm = std::sqrt(v2);
+        if (vnorm < std::sqrt(eps)) vnorm = std::sqrt(eps);
+        sigma = sum / ((double)n * vnorm);
+    }
+    if (sigma_used) *sigma_used = sigma;
+    StageArgs A = stage_args(c);
+    if (!R0_dev) {
+        A.U_in = U_dev;
+        A.R_out = R0;
+        CK(launch_stage(c, 0, A));
+        R0_dev = R0;
+    }
+    jvp_axpy_kernel<<<nb, 256, 0, c->stream>>>(U_dev, v_dev, sigma, n, Up);
+    CK(cudaGetLastError());
+    A.U_in = Up;
+    A.R_out = R1;
+    CK(launch_stage(c, 0, A));
+    jvp_diff_kernel<<<nb, 256, 0, c->stream>>>(R1, R0_dev, sigma, n, Jv_dev);
+    CK(cudaGetLastError());
     CK(cudaStreamSynchronize(c->stream));
     return GDFV_OK;
 }

@@ -1,6 +1,8 @@
 """torch.autograd wrappers over the hand-written adjoint kernels.
 
 * `residual(sim, U)`: R(U) with backward = gdfv_residual_vjp.
+* `jvp(sim, U, v)`: J v by the real Frechet derivative (gdfv_residual_jvp), the
+  Jacobian-vector product of a Newton-Krylov solver.
 * `rollout(sim, U0, theta, nsteps, checkpoint_every)`: nsteps predictor-corrector
   steps of the GPU solver from U0, differentiable in U0 and in the supersonic-
   inflow state theta = (p, T, vel.x).  The forward records each step's dt and
@@ -35,6 +37,20 @@ def vjp(sim, U, W):
     torch.cuda.current_stream().synchronize()
     check(sim.ctx, sim.L.gdfv_residual_vjp(sim.ctx, _p(U), _p(W), _p(G), ffi.cast("double*", gin.data_ptr())))
     return G, gin
+
+
+def jvp(sim, U, v, R0=None, sigma=0.0):
+    """Jv by the real Frechet derivative as evalJacobianVecProd computes it
+    (gdfv_residual_jvp); sigma <= 0 takes the Knoll-McHugh perturbation.
+    Returns (Jv, sigma used)."""
+    U = U.contiguous()
+    v = v.contiguous()
+    Jv = torch.empty_like(U)
+    used = ffi.new("double*")
+    torch.cuda.current_stream().synchronize()
+    check(sim.ctx, sim.L.gdfv_residual_jvp(sim.ctx, _p(U), _p(v), _p(R0.contiguous()) if R0 is not None else ffi.NULL,
+                                           float(sigma), _p(Jv), used))
+    return Jv, used[0]
 
 
 def residual_eval(sim, U):

@@ -124,6 +124,15 @@ int gdfv_set_time(int ctx, double time, int step, double dt_global);
  * on the state U.  Uses the context's current c_h. */
 int gdfv_residual(int ctx, const double* U_dev, double* R_dev);
 
+/* Jacobian-vector product of the residual as evalJacobianVecProd does it with the real
+ * Frechet derivative (e4/steadystate_core.d:1878-1970): Jv = (R(U + sigma v) - R0)/sigma,
+ * device arrays [nq][total].  R0_dev may be NULL (R(U) is then evaluated) or R(U) from
+ * the caller (a Newton-Krylov loop holds it).  sigma <= 0 takes the Knoll-McHugh
+ * perturbation (:3040-3078) sum(eps|U| + eps)/(N max(||v||, sqrt(eps))), eps = 1e-7,
+ * returned in sigma_used (may be NULL). */
+int gdfv_residual_jvp(int ctx, const double* U_dev, const double* v_dev, const double* R0_dev, double sigma,
+                      double* Jv_dev, double* sigma_used);
+
 /* Vector-Jacobian product of the residual: G = (dR/dU)^T W at the state U, device
  * arrays [nq][total] over all blocks (the adjoint of gdfv_residual, hand-written:
  * reverse of decode_conserved, interp_l2r2 and ausmdv, with the branches of the

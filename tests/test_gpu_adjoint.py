@@ -234,3 +234,27 @@ def test_pipelined_rollout_adjoint_matches_sequential():
         torch.cuda.synchronize()
         assert torch.allclose(lam, lam2, rtol=1e-12, atol=1e-12 * float(lam.abs().max())), last_ready
         assert torch.allclose(gin, gin2, rtol=1e-12, atol=0.0), last_ready
+
+
+@pytest.mark.parametrize("case_name", ["inflow", "multiblock"])
+def test_frechet_jvp_matches_oracle(case_name):
+    """gdfv_residual_jvp against the oracle's restatement of evalJacobianVecProd
+    (e4/steadystate_core.d:1878-1970): bit for bit with a given sigma and with the
+    GPU's Knoll-McHugh sigma (whose device reduction may round differently from the
+    oracle's sequential sum: checked to 1e-13), with and without a supplied R(U)."""
+    from gdfv.autograd import jvp, residual_eval
+    case = (cases.c2_inflow_box(n=(24, 16, 12)) if case_name == "inflow"
+            else cases.multiblock_lattice(nb=(2, 1, 2), sizes=(16, 24), seed=3))
+    orc, sim, U = _state_after(case, 4)
+    rng = np.random.default_rng(8)
+    v = rng.standard_normal(U.shape) * np.abs(U).max(axis=1, keepdims=True)
+    Ut, vt = torch.from_numpy(U).cuda(), torch.from_numpy(v).cuda()
+    Uo, vo = _gpu_to_oracle_layout(case, U), _gpu_to_oracle_layout(case, v)
+    Jv_o, sig_o = orc.jvp_real(Uo, vo)
+    Jv_g, sig_g = jvp(sim, Ut, vt)
+    assert abs(sig_g - sig_o) <= 1e-13 * sig_o
+    Jv_o2, _ = orc.jvp_real(Uo, vo, sigma=sig_g)
+    assert np.array_equal(_gpu_to_oracle_layout(case, Jv_g.cpu().numpy()), Jv_o2)
+    R0 = residual_eval(sim, Ut)
+    Jv_g2, _ = jvp(sim, Ut, vt, R0=R0, sigma=sig_g)
+    assert torch.equal(Jv_g, Jv_g2)
