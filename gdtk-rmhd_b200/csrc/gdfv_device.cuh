@@ -37,6 +37,7 @@ struct NumParams {
     int mhd, divergence_cleaning, dims, stringent_cfl;
     int nq;
     int lmr_epsilon;    // van Albada epsilon scaled per face (lmr/onedinterp.d:147-151)
+    int outflow_bcs;    // some face has OutFlowBC_FixedP, _FixedPT or _SimpleFlux
 };
 
 // Fixed ghost state of a supersonic-inflow face (FlowStateCopy, flow_state_copy.d:92-107)

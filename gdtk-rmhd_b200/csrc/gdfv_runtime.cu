@@ -412,6 +412,7 @@ int do_prepare(Context* c) {
     std::vector<InflowState> inflows;
     struct FixedState { int block, face; InflowState state; };
     std::vector<FixedState> fixed;
+    int outflow_bcs = 0;
     c->h_blocks.clear();
     std::vector<TileDesc> tiles;
     const double Cv = g.R / (g.gamma - 1.0);
@@ -458,6 +459,7 @@ int do_prepare(Context* c) {
                 return fail(c, GDFV_ERR_ARG, "x_order must be 0 or 1");
             if (bc.type == BC_SIMPLE_FLUX && g.mhd)
                 return fail(c, GDFV_ERR_ARG, "outflow_simple_flux is not defined for MHD (boundary_flux_effect.d:519)");
+            if (bc.type == BC_FIXED_P || bc.type == BC_FIXED_PT || bc.type == BC_SIMPLE_FLUX) outflow_bcs = 1;
             if (bc.type == BC_FIXED_P || bc.type == BC_FIXED_PT) {
                 // the outside state of fixed_p.d / fixed_pt.d: p (and rho = p/(T R), u = Cv T)
                 InflowState s{};
@@ -504,6 +506,7 @@ int do_prepare(Context* c) {
     P.apply_entropy_fix = g.apply_entropy_fix; P.glm_reference_indexing = g.glm_reference_indexing;
     P.mhd = g.mhd; P.divergence_cleaning = g.divergence_cleaning; P.dims = g.dims;
     P.stringent_cfl = g.stringent_cfl; P.nq = c->nq; P.lmr_epsilon = g.lmr_epsilon;
+    P.outflow_bcs = outflow_bcs;
     StepParams& sp = c->sp;
     sp.cfl_count = g.cfl_count; sp.n_stages = 2; sp.fixed_time_step = g.fixed_time_step;
     sp.mhd_cleaning = g.mhd && g.divergence_cleaning;

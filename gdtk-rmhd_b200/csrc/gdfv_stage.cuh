@@ -96,6 +96,9 @@ struct CellSrc {
 
 // At most one index may lie outside the block; the boundary condition of that
 // face supplies the ghost (e4/bc/ghost_cell_effect/*.d).
+// OUTF false: no face of the launch has an OutFlowBC_FixedP, _FixedPT or _SimpleFlux
+// boundary (those branches are left out).
+template <bool OUTF = true>
 __device__ __forceinline__ CellSrc resolve(const StageArgs& A, const BlockDesc& B, int i, int j, int k) {
     CellSrc s;
     s.blk = &B; s.c1 = -1; s.kind = SRC_CELL; s.axis = 0; s.inflow = 0;
@@ -119,12 +122,12 @@ __device__ __forceinline__ CellSrc resolve(const StageArgs& A, const BlockDesc& 
     if (type == BC_SLIP_WALL) {
         s.kind = SRC_MIRROR;            // internal_copy_then_reflect.d:111-150
         s.c0 = at_depth(depth);
-    } else if (type == BC_FIXED_P || type == BC_FIXED_PT) {
+    } else if (OUTF && (type == BC_FIXED_P || type == BC_FIXED_PT)) {
         // fixed_p.d:98-119 / fixed_pt.d:105-128: interior cell n with the outside p (T)
         s.kind = type == BC_FIXED_P ? SRC_FIXEDP : SRC_FIXEDPT;
         s.c0 = at_depth(depth);
         s.inflow = B.bc_inflow[face];
-    } else if (type == BC_SIMPLE_FLUX) {
+    } else if (OUTF && type == BC_SIMPLE_FLUX) {
         s.c0 = at_depth(0);             // its ghosts: ExtrapolateCopy, xOrder 0 (bc.lua:1548)
     } else if (type == BC_EXTRAPOLATE) {
         if (B.bc_xorder[face] == 0) {   // extrapolate_copy.d:124-147
@@ -257,7 +260,7 @@ static __device__ __noinline__ Prim<double> fixed_ghost(Prim<double> e, bool p_o
     return e;
 }
 
-template <int STAGE, bool FAST, bool MHD, int NQ>
+template <int STAGE, bool FAST, bool MHD, int NQ, bool OUTF>
 __device__ __forceinline__ void finish_cell(const StageArgs& A, const double* Uin, const CellSrc& s,
                                             const double* U0, int i, int j, double dt, double damp,
                                             Prim<double>& out) {
@@ -286,7 +289,7 @@ __device__ __forceinline__ void finish_cell(const StageArgs& A, const double* Ui
             }
         }
     } else if (s.kind > SRC_MIRROR) {   // the rare kinds, out of line (SRC_INFLOW returned above)
-        if (s.kind >= SRC_FIXEDP) {
+        if (OUTF && s.kind >= SRC_FIXEDP) {
             const InflowState& o = A.inflow[s.inflow];
             out = fixed_ghost(out, s.kind == SRC_FIXEDP, o.p, o.rho, o.u, A.P.gas.Cvinv, A.P.gas.Cv, A.P.gas.R);
         } else {
@@ -418,7 +421,7 @@ __device__ __forceinline__ void recon_cell(const R* w, const R* wf, const NumPar
             R dp = (qp1[s] - q0[s]) * t;
             R sl = R(1.0), slm = R(1.0);
             if (lim) {
-                if (P.lmr_epsilon) {
+                if (OPT == 0 && P.lmr_epsilon) {
                     // lmr/onedinterp.d:147-151: each face's epsilon is scaled by the larger of
                     // its two states, so the plus face (q0, qp1) and the minus face (qm1, q0)
                     // of the cell get separate limiter values
@@ -678,7 +681,7 @@ __device__ __forceinline__ double signal_fast(const NumParams& P, const double* 
 
 // Load the state of up to two cells per thread (on[m] says which): resolve, issue
 // every global load, then decode (keeps the loads in flight together).
-template <int STAGE, bool FAST, bool MHD, int NQ>
+template <int STAGE, bool FAST, bool MHD, int NQ, bool OUTF>
 __device__ __forceinline__ void load_two(const StageArgs& A, const double* Uin, const BlockDesc& B, double dt,
                                          double damp, bool on0, bool on1, const int* ci, const int* cj, const int* ck,
                                          Prim<double>* out) {
@@ -688,13 +691,13 @@ __device__ __forceinline__ void load_two(const StageArgs& A, const double* Uin, 
 #pragma unroll
     for (int m = 0; m < 2; ++m) {
         if (on[m]) {
-            s[m] = resolve(A, B, ci[m], cj[m], ck[m]);
+            s[m] = resolve<OUTF>(A, B, ci[m], cj[m], ck[m]);
             if (s[m].kind != SRC_INFLOW) fetch_U<STAGE, NQ>(A, Uin, *s[m].blk, s[m].c0, dt, damp, U0[m]);
         }
     }
 #pragma unroll
     for (int m = 0; m < 2; ++m) {
-        if (on[m]) finish_cell<STAGE, FAST, MHD, NQ>(A, Uin, s[m], U0[m], ci[m], cj[m], dt, damp, out[m]);
+        if (on[m]) finish_cell<STAGE, FAST, MHD, NQ, OUTF>(A, Uin, s[m], U0[m], ci[m], cj[m], dt, damp, out[m]);
     }
 }
 
@@ -772,14 +775,17 @@ __global__ void __launch_bounds__(32 * (TJ + 1), MHD ? 1 : (sizeof(R) == 4 ? GDF
         const bool active = owner && ti < ni_t && tj < nj_t;
         const int pidx = (ti + 2) + PW * (tj + 2);     // own cell in a padded plane
         const bool has_k = (P.dims == 3);
-        // faces of this tile on a simple-outflow-flux boundary: bit 2*axis + (plus side)
+        // faces of this tile on a simple-outflow-flux boundary: bit 2*axis + (plus side);
+        // the specialised path (OPT 1) runs only where there are none
         int sfx = 0;
-        if (t.i0 == 0 && B.bc_type[0] == BC_SIMPLE_FLUX) sfx |= 1;
-        if (t.i0 + ni_t == B.n[0] && B.bc_type[1] == BC_SIMPLE_FLUX) sfx |= 2;
-        if (t.j0 == 0 && B.bc_type[2] == BC_SIMPLE_FLUX) sfx |= 4;
-        if (t.j0 + nj_t == B.n[1] && B.bc_type[3] == BC_SIMPLE_FLUX) sfx |= 8;
-        if (has_k && t.k0 == 0 && B.bc_type[4] == BC_SIMPLE_FLUX) sfx |= 16;
-        if (has_k && t.k1 == B.n[2] && B.bc_type[5] == BC_SIMPLE_FLUX) sfx |= 32;
+        if (OPT == 0) {
+            if (t.i0 == 0 && B.bc_type[0] == BC_SIMPLE_FLUX) sfx |= 1;
+            if (t.i0 + ni_t == B.n[0] && B.bc_type[1] == BC_SIMPLE_FLUX) sfx |= 2;
+            if (t.j0 == 0 && B.bc_type[2] == BC_SIMPLE_FLUX) sfx |= 4;
+            if (t.j0 + nj_t == B.n[1] && B.bc_type[3] == BC_SIMPLE_FLUX) sfx |= 8;
+            if (has_k && t.k0 == 0 && B.bc_type[4] == BC_SIMPLE_FLUX) sfx |= 16;
+            if (has_k && t.k1 == B.n[2] && B.bc_type[5] == BC_SIMPLE_FLUX) sfx |= 32;
+        }
         if (tid < 3 * W_N) w[tid / W_N][tid % W_N] = (R)B.w[tid / W_N][tid % W_N];
         if (tid < 3) {
             const double* bw = B.w[tid];
@@ -808,11 +814,11 @@ __global__ void __launch_bounds__(32 * (TJ + 1), MHD ? 1 : (sizeof(R) == 4 ? GDF
             if (active) {
                 Prim<double> pr[2];
                 int ck[2] = {t.k0 - 2, t.k0 - 1};
-                load_two<STAGE, FAST, MHD, NQ>(A, Uin, B, dt, damp, true, true, ci, cj, ck, pr);
+                load_two<STAGE, FAST, MHD, NQ, OPT == 0>(A, Uin, B, dt, damp, true, true, ci, cj, ck, pr);
                 put_prim<R, NPV>(slot(t.k0 - 2), PLANE, pidx, pr[0]);
                 put_prim<R, NPV>(slot(t.k0 - 1), PLANE, pidx, pr[1]);
                 int ck2[2] = {t.k0, 0};
-                load_two<STAGE, FAST, MHD, NQ>(A, Uin, B, dt, damp, true, false, ci, cj, ck2, pr);
+                load_two<STAGE, FAST, MHD, NQ, OPT == 0>(A, Uin, B, dt, damp, true, false, ci, cj, ck2, pr);
                 put_prim<R, NPV>(slot(t.k0), PLANE, pidx, pr[0]);
                 // q+ of plane k0-1 (left state of face k0-1/2); own column only
                 R qm1[NRS], q0[NRS], qp1[NRS], qm[NRS];
@@ -822,7 +828,7 @@ __global__ void __launch_bounds__(32 * (TJ + 1), MHD ? 1 : (sizeof(R) == 4 ? GDF
                 recon_cell<R, NRS, MHD, OPT>(w[2], wf[2], P, qm1, q0, qp1, qm, kq_prev_p);
                 // plane k0+1 replaces k0-2 in the ring
                 int ck3[2] = {t.k0 + 1, 0};
-                load_two<STAGE, FAST, MHD, NQ>(A, Uin, B, dt, damp, true, false, ci, cj, ck3, pr);
+                load_two<STAGE, FAST, MHD, NQ, OPT == 0>(A, Uin, B, dt, damp, true, false, ci, cj, ck3, pr);
                 put_prim<R, NPV>(slot(t.k0 + 1), PLANE, pidx, pr[0]);
                 R qkm[NRS], qkp[NRS];
                 gather<R, NRS, 2>(slot(t.k0 - 1), PLANE, pidx, qm1);
@@ -838,7 +844,7 @@ __global__ void __launch_bounds__(32 * (TJ + 1), MHD ? 1 : (sizeof(R) == 4 ? GDF
             if (active) {
                 int ci[2] = {t.i0 + ti, 0}, cj[2] = {t.j0 + tj, 0}, ck[2] = {t.k0, 0};
                 Prim<double> pr[2];
-                load_two<STAGE, FAST, MHD, NQ>(A, Uin, B, dt, damp, true, false, ci, cj, ck, pr);
+                load_two<STAGE, FAST, MHD, NQ, OPT == 0>(A, Uin, B, dt, damp, true, false, ci, cj, ck, pr);
                 put_prim<R, NPV>(slot(t.k0), PLANE, pidx, pr[0]);
             }
         }
@@ -885,13 +891,13 @@ __global__ void __launch_bounds__(32 * (TJ + 1), MHD ? 1 : (sizeof(R) == 4 ? GDF
                 // together cost more registers (spills, occupancy) than their overlap gains
                 if (lead) {
                     Prim<double> pr[2];
-                    load_two<STAGE, FAST, MHD, NQ>(A, Uin, B, dt, damp, true, false, ci, cj, ck, pr);
+                    load_two<STAGE, FAST, MHD, NQ, OPT == 0>(A, Uin, B, dt, damp, true, false, ci, cj, ck, pr);
                     put_prim<R, NPV>(slot(k + 2), PLANE, pidx, pr[0]);
                 }
                 if (h_on) {
                     Prim<double> pr[2];
                     int ci2[2] = {h_ci, 0}, cj2[2] = {h_cj, 0}, ck2[2] = {k, 0};
-                    load_two<STAGE, FAST, MHD, NQ>(A, Uin, B, dt, damp, true, false, ci2, cj2, ck2, pr);
+                    load_two<STAGE, FAST, MHD, NQ, OPT == 0>(A, Uin, B, dt, damp, true, false, ci2, cj2, ck2, pr);
                     put_prim<R, NPV>(cur, PLANE, h_dst, pr[0]);
                 }
             }
@@ -971,7 +977,7 @@ __global__ void __launch_bounds__(32 * (TJ + 1), MHD ? 1 : (sizeof(R) == 4 ? GDF
 
             // ---------------- boundary faces with OutFlowBC_SimpleFlux (only tiles that have
             // them): their flux is the interior cell's (boundary_flux_effect.d:504-645)
-            if (sfx) {
+            if (OPT == 0 && sfx) {
                 if (active && has_k) {
                     if ((sfx & 16) && k == 0) simple_outflow_flux<R, 2>(P, cur, pidx, PLANE, -1, fB);
                     if ((sfx & 32) && k + 1 == B.n[2]) simple_outflow_flux<R, 2>(P, cur, pidx, PLANE, 1, fT);

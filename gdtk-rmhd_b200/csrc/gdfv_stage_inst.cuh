@@ -21,9 +21,10 @@ int& resident() {
 template <int STAGE, bool MHD, int FLUX>
 cudaError_t launch_one(const StageArgs& A, cudaStream_t s) {
     using G = Geo<Real, MHD, TJ>;
-    // defaults (limiter and extrema clipping on, e4 epsilon) take the specialised
-    // path, which also has the persistent form
-    if (A.P.apply_limiter && A.P.extrema_clipping && !A.P.lmr_epsilon) {
+    // defaults (limiter and extrema clipping on, e4 epsilon, none of the outflow
+    // boundaries with their own ghost or flux rule) take the specialised path, which
+    // also has the persistent form
+    if (A.P.apply_limiter && A.P.extrema_clipping && !A.P.lmr_epsilon && !A.P.outflow_bcs) {
         const int cap = resident<STAGE, MHD, FLUX>();
         if (A.persistent && cap > 0)
             stage_kernel<STAGE, Real, MHD, FLUX, TJ, 1, 1><<<cap < A.n_tiles ? cap : A.n_tiles, G::NT, G::bytes, s>>>(A);
