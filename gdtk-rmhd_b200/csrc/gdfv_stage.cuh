@@ -701,6 +701,22 @@ __device__ __forceinline__ void load_two(const StageArgs& A, const double* Uin, 
     }
 }
 
+// Load and decode one cell of the own block at global index g (interior cell: no
+// boundary rule applies).
+template <int STAGE, bool FAST, bool MHD, int NQ>
+__device__ __forceinline__ void load_direct(const StageArgs& A, const double* Uin, long long g, double dt, double damp,
+                                            Prim<double>& out) {
+    double U[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) U[q] = __ldg(Uin + (long long)q * A.total + g);
+    if (STAGE == 2) {
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) U[q] = d_add(U[q], d_mul(dt, __ldg(A.dU0 + (long long)q * A.total + g)));
+        if (NQ == 10 && A.P.divergence_cleaning) U[PSI] = d_mul(U[PSI], damp);
+    }
+    decode_prim<FAST, MHD>(A.P, U, out);
+}
+
 // Resident CTAs per SM the Euler kernels of each flux precision are compiled for
 // (register budget; three float-flux CTAs also fill the shared memory).
 #ifndef GDFV_MINB_FP32
@@ -877,12 +893,24 @@ __global__ void __launch_bounds__(32 * (TJ + 1), MHD ? 1 : (sizeof(R) == 4 ? GDF
             h_cj = t.j0 + hj;
             h_dst = (hi + 2) + PW * (hj + 2);
         }
+        // cell indices within the block (32-bit: the host limits a block to 2^31 - 1
+        // cells) in plane k of the own cell and of the halo cell when that lies inside
+        // the block (no boundary rule), advanced by one plane per step
+        const int pstride = B.n[0] * B.n[1];
+        int c_own = (t.i0 + ti) + B.n[0] * ((t.j0 + tj) + B.n[1] * t.k0);
+        const bool h_in = h_on && h_ci >= 0 && h_ci < B.n[0] && h_cj >= 0 && h_cj < B.n[1];
+        int c_halo = (h_in ? h_ci : 0) + B.n[0] * ((h_in ? h_cj : 0) + B.n[1] * t.k0);
+        // ring slots of planes k, k+1, k+2
+        int r0 = t.k0 % 3;
         const int f0 = owner ? G::EXTRA + tid : tid - NCOL;   // flat-list start and stride
         const int fstride = owner ? NCOL : 32;
         const int fend = owner ? 0x7fffffff : G::EXTRA;
 
         for (int k = t.k0; k < t.k1; ++k) {
-            R* cur = slot(k);
+            const int r1 = r0 == 2 ? 0 : r0 + 1, r2 = r1 == 2 ? 0 : r1 + 1;
+            R* cur = ring + r0 * (NPV * PLANE);
+            R* nx1 = ring + r1 * (NPV * PLANE);
+            R* nx2 = ring + r2 * (NPV * PLANE);
             // ---------------- phase A: leading plane k+2 (owners) and the halo of plane k
             {
                 const bool lead = active && has_k;
@@ -891,10 +919,17 @@ __global__ void __launch_bounds__(32 * (TJ + 1), MHD ? 1 : (sizeof(R) == 4 ? GDF
                 // together cost more registers (spills, occupancy) than their overlap gains
                 if (lead) {
                     Prim<double> pr[2];
-                    load_two<STAGE, FAST, MHD, NQ, OPT == 0>(A, Uin, B, dt, damp, true, false, ci, cj, ck, pr);
-                    put_prim<R, NPV>(slot(k + 2), PLANE, pidx, pr[0]);
+                    if (k + 2 < B.n[2])
+                        load_direct<STAGE, FAST, MHD, NQ>(A, Uin, B.offset + (c_own + 2 * pstride), dt, damp, pr[0]);
+                    else
+                        load_two<STAGE, FAST, MHD, NQ, OPT == 0>(A, Uin, B, dt, damp, true, false, ci, cj, ck, pr);
+                    put_prim<R, NPV>(nx2, PLANE, pidx, pr[0]);
                 }
-                if (h_on) {
+                if (h_in) {
+                    Prim<double> pr;
+                    load_direct<STAGE, FAST, MHD, NQ>(A, Uin, B.offset + c_halo, dt, damp, pr);
+                    put_prim<R, NPV>(cur, PLANE, h_dst, pr);
+                } else if (h_on) {
                     Prim<double> pr[2];
                     int ci2[2] = {h_ci, 0}, cj2[2] = {h_cj, 0}, ck2[2] = {k, 0};
                     load_two<STAGE, FAST, MHD, NQ, OPT == 0>(A, Uin, B, dt, damp, true, false, ci2, cj2, ck2, pr);
@@ -908,8 +943,8 @@ __global__ void __launch_bounds__(32 * (TJ + 1), MHD ? 1 : (sizeof(R) == 4 ? GDF
             if (active && has_k) {
                 R qm1[NRS], q0[NRS], qp1[NRS];
                 gather<R, NRS, 2>(cur, PLANE, pidx, qm1);
-                gather<R, NRS, 2>(slot(k + 1), PLANE, pidx, q0);
-                gather<R, NRS, 2>(slot(k + 2), PLANE, pidx, qp1);
+                gather<R, NRS, 2>(nx1, PLANE, pidx, q0);
+                gather<R, NRS, 2>(nx2, PLANE, pidx, qp1);
                 recon_cell<R, NRS, MHD, OPT>(w[2], wf[2], P, qm1, q0, qp1, kq_m, kq_p);
             }
             for (int f = f0; f < NRI + NRJ && f < fend; f += fstride) {
@@ -944,7 +979,7 @@ __global__ void __launch_bounds__(32 * (TJ + 1), MHD ? 1 : (sizeof(R) == 4 ? GDF
 #pragma unroll
             for (int q = 0; q < NQ; ++q) fT[q] = R(0);
             if (active && has_k) {
-                face_flux<R, MHD, FLUX, 2, NPV>(P, c_hR, kq_prev_p, kq_m, cur, pidx, slot(k + 1), pidx, PLANE, fT);
+                face_flux<R, MHD, FLUX, 2, NPV>(P, c_hR, kq_prev_p, kq_m, cur, pidx, nx1, pidx, PLANE, fT);
 #pragma unroll
                 for (int s = 0; s < NRS; ++s) kq_prev_p[s] = kq_p[s];
             }
@@ -1007,8 +1042,7 @@ __global__ void __launch_bounds__(32 * (TJ + 1), MHD ? 1 : (sizeof(R) == 4 ? GDF
 
             // ---------------- phase D: residual (e4/fvcell.d:824-856, faces W, E, S, N, B, T) and update
             if (active) {
-                const long long cell = cell_index(B, t.i0 + ti, t.j0 + tj, k);
-                const long long g = B.offset + cell;
+                const long long g = B.offset + c_own;
                 double dU[NQ];
                 if (FAST) {
                     // float path: differences of opposite faces in float (same-signed,
@@ -1081,13 +1115,16 @@ __global__ void __launch_bounds__(32 * (TJ + 1), MHD ? 1 : (sizeof(R) == 4 ? GDF
                         if (STAGE == 2) {
                             double sig = (FAST && !MHD) ? signal_fast(P, inv_len, s) : signal_frequency(P, B, s);
                             sig_max = fmax(sig_max, sig);
-                            if (cell == (long long)B.n[0] * B.n[1] * B.n[2] - 1) A.last_signal[blk] = sig;
+                            if (c_own == pstride * B.n[2] - 1) A.last_signal[blk] = sig;
                         }
                     }
                 }
             }
 #pragma unroll
             for (int q = 0; q < NQ; ++q) fB[q] = fT[q];
+            c_own += pstride;
+            c_halo += pstride;
+            r0 = r1;
         }
 
         if (STAGE == 2) {
