@@ -324,7 +324,7 @@ struct Src {
 __device__ Src adj_resolve(const AdjArgs& a, const BlockDesc& B, int i, int j, int k) {
     StageArgs A{};
     A.blocks = a.blocks;
-    CellSrc s = resolve(A, B, i, j, k);
+    CellSrc s = resolve<false>(A, B, i, j, k);   // no outflow boundaries with their own rule here
     return Src{s.blk, s.c0, s.c1, s.kind, s.axis, s.inflow};
 }
 
@@ -384,17 +384,27 @@ __device__ __forceinline__ int face_coords(const AdjArgs& a, long long f, int& i
     int b = 0;
     while (off[b + 1] <= f) ++b;
     const BlockDesc& B = a.blocks[b];
-    const long long lf = f - off[b];
-    const int nf0 = B.n[0] + (D == 0), nf1 = B.n[1] + (D == 1);
-    i = (int)(lf % nf0);
-    j = (int)((lf / nf0) % nf1);
-    k = (int)(lf / ((long long)nf0 * nf1));
+    // 32-bit: the host limits a block's faces of one direction to 2^31 - 1
+    const unsigned lf = (unsigned)(f - off[b]);
+    const unsigned nf0 = B.n[0] + (D == 0), nf1 = B.n[1] + (D == 1);
+    const unsigned r = lf / nf0;
+    i = (int)(lf - r * nf0);
+    k = (int)(r / nf1);
+    j = (int)(r - (unsigned)k * nf1);
     return b;
 }
 
-// Source of stencil cell m (index -2, -1, 0, +1 along D from the face).
+// Source of stencil cell m (index -2, -1, 0, +1 along D from the face).  A face
+// whose four stencil cells lie inside its block (the other two indices always do)
+// takes them directly; the boundary rules apply to the others.
 template <int D>
 __device__ __forceinline__ Src stencil_src(const AdjArgs& a, const BlockDesc& B, int i, int j, int k, int m) {
+    const int idxD = D == 0 ? i : (D == 1 ? j : k);
+    if (idxD >= 2 && idxD + 1 < B.n[D]) {
+        const int sD = D == 0 ? 1 : (D == 1 ? B.n[0] : B.n[0] * B.n[1]);
+        const int c = i + B.n[0] * (j + B.n[1] * k) + (m - 2) * sD;
+        return Src{&B, (long long)c, -1, SRC_CELL, D, 0};
+    }
     return adj_resolve(a, B, i - (D == 0 ? 2 - m : 0), j - (D == 1 ? 2 - m : 0), k - (D == 2 ? 2 - m : 0));
 }
 
@@ -404,10 +414,8 @@ __device__ __forceinline__ Src stencil_src(const AdjArgs& a, const BlockDesc& B,
 // themselves are resolved again when the cotangents are scattered.
 // rowid identifies the line of faces (block and the two other indices).
 template <int D>
-__device__ __forceinline__ void face_vjp(const AdjArgs& a, long long f, int* kind, int& inflow, double (*gc)[NP],
-                                         long long& rowid) {
-    int i, j, k;
-    const int b = face_coords<D>(a, f, i, j, k);
+__device__ __forceinline__ void face_vjp(const AdjArgs& a, int b, int i, int j, int k, int* kind, int& inflow,
+                                         double (*gc)[NP], long long& rowid) {
     const BlockDesc& B = a.blocks[b];
     rowid = (long long)b * 0x100000000ll + (D == 0 ? (long long)j + (long long)B.n[1] * k : (long long)i);
     double c[4][NP];
@@ -500,7 +508,11 @@ __device__ __forceinline__ void face_thread(const AdjArgs& a, long long f) {
     for (int m = 0; m < 4; ++m)
         for (int q = 0; q < NP; ++q) gc[m][q] = 0.0;
     long long rowid = -1 - (long long)threadIdx.x;   // distinct for inactive lanes
-    if (act) face_vjp<D>(a, f, kind, inflow, gc, rowid);
+    int b = 0, i = 0, j = 0, k = 0;
+    if (act) {
+        b = face_coords<D>(a, f, i, j, k);
+        face_vjp<D>(a, b, i, j, k, kind, inflow, gc, rowid);
+    }
     if (D == 0) {
         const unsigned full = 0xffffffffu;
         const int lane = threadIdx.x & 31;
@@ -561,8 +573,6 @@ __device__ __forceinline__ void face_thread(const AdjArgs& a, long long f) {
         }
     }
     if (!act) return;
-    int i, j, k;
-    const int b = face_coords<D>(a, f, i, j, k);
     const BlockDesc& B = a.blocks[b];
     for (int m = 0; m < 4; ++m)
         if (kind[m] >= 0) adj_scatter(a, stencil_src<D>(a, B, i, j, k, m), gc[m]);

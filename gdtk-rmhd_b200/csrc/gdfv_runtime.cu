@@ -421,9 +421,10 @@ int do_prepare(Context* c) {
         if (g.dims == 2 && hb.n[2] != 1) return fail(c, GDFV_ERR_ARG, "2D blocks have nkc = 1");
         for (int d = 0; d < (g.dims == 3 ? 3 : 2); ++d)
             if (hb.n[d] < 2) return fail(c, GDFV_ERR_ARG, "blocks need at least 2 cells per active direction");
-        // the stage kernels index cells within a block in 32-bit arithmetic
-        if ((long long)hb.n[0] * hb.n[1] * hb.n[2] > 2147483647LL)
-            return fail(c, GDFV_ERR_ARG, "a block has more than 2^31 - 1 cells (split it into several blocks)");
+        // the kernels index cells (and the adjoint faces of one direction) within a
+        // block in 32-bit arithmetic
+        if ((long long)(hb.n[0] + 1) * (hb.n[1] + 1) * (hb.n[2] + 1) > 2147483647LL)
+            return fail(c, GDFV_ERR_ARG, "a block has more than 2^31 - 1 cells or faces (split it into several blocks)");
         hb.offset = off;
         BlockDesc B{};
         for (int d = 0; d < 3; ++d) { B.n[d] = hb.n[d]; B.len[d] = hb.len[d]; fill_weights(hb.len[d], B.w[d]); }
