@@ -258,9 +258,16 @@ class Simulation:
         rho = fs.p / (fs.T * self.gas.R)
         self.set_flow_rhoT(blk, rho, fs.vel, fs.T, B=fs.B, psi=fs.psi)
 
-    def get_conserved(self, blk):
+    def get_conserved(self, blk, out=None):
+        """Conserved state of block blk as (nq, ncells) float64.  `out` (C-contiguous
+        float64 of that shape, e.g. a view of pinned host memory) is filled in place
+        and returned; without it a new array is allocated."""
         self.prepare()
-        out = np.zeros((self.nq, self.ncells(blk)))
+        shape = (self.nq, self.ncells(blk))
+        if out is None:
+            out = np.empty(shape)
+        elif out.shape != shape or out.dtype != np.float64 or not out.flags["C_CONTIGUOUS"]:
+            raise ValueError(f"out must be a C-contiguous float64 array of shape {shape}")
         check(self.ctx, self.L.gdfv_block_get_conserved(self.ctx, blk, ffi.cast("double*", out.ctypes.data)))
         return out
 

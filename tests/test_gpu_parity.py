@@ -260,3 +260,18 @@ def test_outflow_boundaries_fp32():
     Uo, Ug = orc.get_U(0), sim.get_conserved(0)
     errs = [cases.rel_l2(Ug[0], Uo[0]), cases.rel_l2(Ug[1:4].ravel(), Uo[1:4].ravel()), cases.rel_l2(Ug[4], Uo[4])]
     assert max(errs) <= TOL_FP32_L2, errs
+
+
+def test_get_conserved_into_caller_buffer():
+    """get_conserved(out=...) fills a caller-owned (pinned) array with the same state
+    as the allocating form and rejects a buffer of the wrong shape."""
+    import torch
+    case = cases.c2_inflow_box(n=(40, 24, 20))
+    sim = cases.build_gpu(case)
+    assert sim.run(max_step=3) == 3
+    ref = sim.get_conserved(0)
+    buf = torch.empty(ref.shape, dtype=torch.float64).pin_memory().numpy()
+    got = sim.get_conserved(0, out=buf)
+    assert got is buf and np.array_equal(buf, ref)
+    with pytest.raises(ValueError):
+        sim.get_conserved(0, out=np.empty((ref.shape[0], ref.shape[1] - 1)))
