@@ -320,8 +320,11 @@ def main():
     ap.add_argument("--accuracy-steps", type=int, default=1000,
                     help="steps after which the FP32 form is compared with FP64 (0: at the timed steps)")
     ap.add_argument("--no-extra", action="store_true", help="skip the multi-block, MHD and adjoint legs")
-    ap.add_argument("--profile-case", action="store_true",
-                    help="small case for ncu captures: 128^3, warmup steps then exit")
+    ap.add_argument("--profile-case", nargs="?", const="stage", default=None,
+                    choices=["stage", "mhd", "adjoint"],
+                    help="small case for ncu captures, then exit: stage = the 128^3 inflow box "
+                         "(FP32 then FP64 form, warmup steps); mhd = Orszag-Tang 512x512x4 (both forms, "
+                         "warmup steps); adjoint = 128x128x64 FP64 rollout of 10 steps and its backward")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -349,10 +352,23 @@ def main():
         sim.set_stream(stream.cuda_stream)
         return case, sim
 
-    if args.profile_case:
+    if args.profile_case == "stage":
         for prec in ("fp32", "fp64"):
             _, sim = make(prec)
             sim.run(max_step=max(3, args.warmup))
+        torch.cuda.synchronize()
+        return 0
+    if args.profile_case == "mhd":
+        for prec in ("fp32", "fp64"):
+            sim = cases.build_gpu(cases.orszag_tang(n=(512, 512, 4), precision=prec), fixed_time_step=True,
+                                  dt_init=8.0e-5, dt_max=8.0e-5)
+            sim.set_stream(stream.cuda_stream)
+            sim.run(max_step=max(3, args.warmup))
+            sim.close()
+        torch.cuda.synchronize()
+        return 0
+    if args.profile_case == "adjoint":
+        adjoint_over_forward(nsteps=10, checkpoint_every=10)
         torch.cuda.synchronize()
         return 0
 

@@ -104,3 +104,52 @@ def test_max_over_ranks_gloo_world2():
         p.join(timeout=120)
         assert p.exitcode == 0
     assert res == {0: 11.0, 1: 11.0}
+
+
+def _ctx_with_block(L, n, dims=3, flux=b"ausmdv"):
+    h = L.gdfv_context_new()
+    assert L.gdfv_config_set_int(h, b"dimensions", dims) == GDFV_OK
+    assert L.gdfv_config_set_str(h, b"flux_calculator", flux) == GDFV_OK
+    b = L.gdfv_block_new(h, n[0], n[1], n[2], 1e-3, 1e-3, 1e-3, 0, 0, 0)
+    return h, b
+
+
+def test_prepare_rejects_invalid_layouts_before_touching_the_device():
+    """Layout errors come back from gdfv_prepare as status codes with a message, like
+    the reference's C wrappers (src/gas/gas_cwrap.d:423-446), and before any device
+    allocation (this test runs without a GPU)."""
+    from gdfv._lib import GDFV_ERR_STATE
+    L = gdfv.lib()
+    h = L.gdfv_context_new()
+    assert L.gdfv_prepare(h) == GDFV_ERR_STATE          # no blocks
+    assert "no blocks" in last_error(h)
+    assert L.gdfv_block_new(h, 1 << 12, 1 << 12, 1 << 11, 1e-3, 1e-3, 1e-3, 0, 0, 0) == GDFV_ERR_ARG
+    L.gdfv_context_free(h)
+    # the kernels index a block's cells and faces in 32-bit arithmetic
+    h, b = _ctx_with_block(L, (1300, 1300, 1300))
+    assert b == 0
+    assert L.gdfv_prepare(h) == GDFV_ERR_ARG
+    assert "2^31" in last_error(h)
+    L.gdfv_context_free(h)
+    h, _ = _ctx_with_block(L, (16, 1, 16))                # one cell thick in an active direction
+    assert L.gdfv_prepare(h) == GDFV_ERR_ARG
+    L.gdfv_context_free(h)
+    h, _ = _ctx_with_block(L, (16, 16, 2), dims=2)        # 2D blocks have nkc = 1
+    assert L.gdfv_prepare(h) == GDFV_ERR_ARG
+    L.gdfv_context_free(h)
+    h, _ = _ctx_with_block(L, (16, 16, 16), flux=b"hlle")  # hlle is the MHD flux
+    assert L.gdfv_prepare(h) == GDFV_ERR_ARG
+    assert "MHD" in last_error(h)
+    L.gdfv_context_free(h)
+    # exchange across faces of different sizes, and onto the same face
+    h, b0 = _ctx_with_block(L, (16, 16, 16))
+    b1 = L.gdfv_block_new(h, 16, 8, 16, 1e-3, 1e-3, 1e-3, 0.016, 0, 0)
+    assert L.gdfv_block_set_bc(h, b0, 1, b"exchange_over_full_face", 0, b1, 0, ffi.NULL) == GDFV_OK
+    assert L.gdfv_block_set_bc(h, b1, 0, b"exchange_over_full_face", 0, b0, 1, ffi.NULL) == GDFV_OK
+    assert L.gdfv_prepare(h) == GDFV_ERR_ARG
+    assert "differ in size" in last_error(h)
+    L.gdfv_context_free(h)
+    h, b0 = _ctx_with_block(L, (16, 16, 16))
+    assert L.gdfv_block_set_bc(h, b0, 1, b"exchange_over_full_face", 0, b0, 1, ffi.NULL) == GDFV_OK
+    assert L.gdfv_prepare(h) == GDFV_ERR_ARG
+    L.gdfv_context_free(h)
