@@ -247,6 +247,7 @@ struct Context {
     double tune_ms = 0.0;              // stage-1 + stage-2 time of the tuned configuration
     double* adj_scratch = nullptr;     // adjoint work arrays, allocated on first use
     double* jvp_scratch = nullptr;     // Frechet JVP work arrays (U + sigma v, R0, R1, partial sums)
+    double* norm_scratch = nullptr;    // per-CTA partials and result of gdfv_residual_norms
     int adj_ready = 0;
     long long adj_scratch_n = 0;
     cudaStream_t aux_stream[2] = {nullptr, nullptr};  // lowest / highest priority streams of the rollout adjoint
@@ -258,6 +259,7 @@ struct Context {
         if (graph) cudaGraphExecDestroy(graph);
         for (void* p : {(void*)U[0], (void*)U[1], (void*)dU0, (void*)d_blocks, (void*)d_tiles, (void*)d_inflow,
                         (void*)d_ctl, (void*)d_maxsig, (void*)d_lastsig, (void*)d_bad, (void*)adj_scratch, (void*)jvp_scratch,
+                        (void*)norm_scratch,
                         (void*)step_ctl, (void*)step_maxsig, (void*)step_lastsig})
             if (p) cudaFree(p);
         if (h_ctl) cudaFreeHost(h_ctl);
@@ -651,6 +653,61 @@ void adjoint_set_error(int ctx, const std::string& msg) {
 __global__ void predictor_state_kernel(const double* U0, const double* dU0, double dt, long long n, double* U1) {
     long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (x < n) U1[x] = __dadd_rn(U0[x], __dmul_rn(dt, dU0[x]));
+}
+
+// Residual norms of dU/dt (e4/fluidblock.d:861-909): per CTA, the maximum of |dU/dt[q]|
+// for every q and the sum of squares of the quantities compute_L2_residual takes
+// (mass, x and y momentum, z momentum in 3D, total energy, with MHD xB and yB).
+// Grid-stride over cells, warp shuffles, then the warps in order: partial[cta][nq + 1].
+constexpr int kNormThreads = 256;
+__global__ void __launch_bounds__(kNormThreads) residual_norms_kernel(const double* dU, long long total, int nq,
+                                                                       int threeD, int mhd, double* partial) {
+    double mx[10], l2 = 0.0;
+#pragma unroll
+    for (int q = 0; q < 10; ++q) mx[q] = 0.0;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < total; x += stride) {
+#pragma unroll
+        for (int q = 0; q < 10; ++q) {
+            if (q >= nq) break;
+            const double v = __ldg(dU + (long long)q * total + x);
+            mx[q] = fmax(mx[q], fabs(v));
+            const bool in_l2 = q == MASS || q == XMOM || q == YMOM || (q == ZMOM && threeD) || q == TOTENERGY ||
+                               (mhd && (q == XB || q == YB));
+            if (in_l2) l2 += v * v;
+        }
+    }
+    __shared__ double s_part[kNormThreads / 32][11];
+    for (int o = 16; o > 0; o >>= 1) {
+        l2 += __shfl_xor_sync(0xffffffffu, l2, o);
+#pragma unroll
+        for (int q = 0; q < 10; ++q) mx[q] = fmax(mx[q], __shfl_xor_sync(0xffffffffu, mx[q], o));
+    }
+    const int wv = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+        for (int q = 0; q < 10; ++q) s_part[wv][q] = mx[q];
+        s_part[wv][10] = l2;
+    }
+    __syncthreads();
+    if (threadIdx.x <= nq) {
+        const int q = threadIdx.x == nq ? 10 : threadIdx.x;
+        double r = s_part[0][q];
+        for (int w = 1; w < kNormThreads / 32; ++w) r = q == 10 ? r + s_part[w][q] : fmax(r, s_part[w][q]);
+        partial[(long long)blockIdx.x * (nq + 1) + threadIdx.x] = r;
+    }
+}
+
+// The CTAs' partials in CTA order: out[q] = max for q < nq, out[nq] = sqrt(sum) (e4/simcore.d:1212).
+__global__ void residual_norms_final_kernel(const double* partial, int ncta, int nq, double* out) {
+    const int q = threadIdx.x;
+    if (q > nq) return;
+    double r = partial[q];
+    for (int b = 1; b < ncta; ++b) {
+        const double v = partial[(long long)b * (nq + 1) + q];
+        r = q == nq ? r + v : fmax(r, v);
+    }
+    out[q] = q == nq ? sqrt(r) : r;
 }
 
 // Resets the control record of a single fixed-dt step.
@@ -1362,6 +1419,35 @@ int gdfv_last_predictor_state(int ctx, const double* U0_dev, double* U1_out_dev)
     predictor_state_kernel<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(U0_dev, c->dU0, c->h_ctl->dt_global, n,
                                                                                U1_out_dev);
     CK(cudaGetLastError());
+    return GDFV_OK;
+}
+
+int gdfv_residual_norms(int ctx, double* Linf, double* L2) {
+    Context* c = get_ctx(ctx);
+    int st = check_ready(c, -1);
+    if (st) return st;
+    if (!L2) return fail(c, GDFV_ERR_ARG, "null pointer");
+    if (read_ctl(c)) return GDFV_ERR_CUDA;
+    if (c->h_ctl->step < 1) return fail(c, GDFV_ERR_STATE, "no step taken yet");
+    int n_sm = 0;
+    CK(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, c->device));
+    const long long want = (c->total + kNormThreads - 1) / kNormThreads;
+    const int ncta = (int)std::max(1LL, std::min<long long>(want, 8LL * n_sm));
+    const int nq = c->nq;
+    if (!c->norm_scratch) CK(cudaMalloc(&c->norm_scratch, sizeof(double) * ((size_t)8 * n_sm * 11 + 16)));
+    double* out = c->norm_scratch;
+    double* partial = c->norm_scratch + 16;
+    residual_norms_kernel<<<ncta, kNormThreads, 0, c->stream>>>(c->dU0, c->total, nq, c->cfg.dims == 3, c->cfg.mhd,
+                                                                 partial);
+    CK(cudaGetLastError());
+    residual_norms_final_kernel<<<1, 32, 0, c->stream>>>(partial, ncta, nq, out);
+    CK(cudaGetLastError());
+    double h[11];
+    CK(cudaMemcpyAsync(h, out, sizeof(double) * (nq + 1), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (Linf)
+        for (int q = 0; q < nq; ++q) Linf[q] = h[q];
+    *L2 = h[nq];
     return GDFV_OK;
 }
 

@@ -315,6 +315,15 @@ class Simulation:
     def set_stream(self, stream_handle):
         check(self.ctx, self.L.gdfv_set_stream(self.ctx, ffi.cast("void*", stream_handle)))
 
+    def residual_norms(self):
+        """(Linf[nq], L2) of dU/dt of the last step's predictor stage, the figures the
+        reference writes with report_residuals (e4/simcore.d:1193-1212)."""
+        self.prepare()
+        linf = ffi.new("double[]", self.nq)
+        l2 = ffi.new("double*")
+        check(self.ctx, self.L.gdfv_residual_norms(self.ctx, linf, l2))
+        return np.array([linf[q] for q in range(self.nq)]), float(l2[0])
+
     def time_stages(self, reps=10):
         ms = ffi.new("double[2]")
         check(self.ctx, self.L.gdfv_time_stages(self.ctx, int(reps), ms))

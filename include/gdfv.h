@@ -191,6 +191,19 @@ int gdfv_rollout_adjoint(int ctx, const double* const* ckpt_dev, int n_ckpt, con
  * counterpart. */
 int gdfv_last_predictor_state(int ctx, const double* U0_dev, double* U1_out_dev);
 
+/* Residual norms of the step gdfv_run took last, as Eilmer reports them with
+ * report_residuals (e4/simcore.d:1193-1195, :1212): Linf[q] = max over all cells of
+ * |dU/dt[q]| of the step's predictor stage, q < nq
+ * (FluidBlock.compute_Linf_residuals, e4/fluidblock.d:861-876, max over blocks
+ * e4/simcore.d:1683-1695); L2 = sqrt of the sum over all cells of the squares of
+ * mass, x and y momentum, z momentum (3D), total energy and, with MHD, xB and yB
+ * (FluidBlock.compute_L2_residual, e4/fluidblock.d:879-909, summed over blocks
+ * e4/simcore.d:1697-1706).  Linf may be NULL.  Reduced on the device (warp shuffles,
+ * then the per-CTA partials in a fixed order); waits for the context's stream.
+ * gdfv_step_dt, gdfv_steps_dt and gdfv_time_stages overwrite the predictor
+ * derivative these norms are taken of. */
+int gdfv_residual_norms(int ctx, double* Linf, double* L2);
+
 /* Device pointer of the current conserved state ([nq][total], borrowed, valid
  * until the next gdfv_run), and of the context's CUDA stream. */
 int gdfv_state_device_ptr(int ctx, double** U_dev);
