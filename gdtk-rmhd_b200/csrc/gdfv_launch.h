@@ -14,8 +14,16 @@ namespace gdfv {
 #ifndef GDFV_TJ_FP32
 #define GDFV_TJ_FP32 8
 #endif
+// rows of the float-flux MHD kernels (their ten variables need more shared memory per row)
+#ifndef GDFV_TJ_FP32_MHD
+#define GDFV_TJ_FP32_MHD 6
+#endif
 constexpr int TJ_FP64 = GDFV_TJ_FP64;
 constexpr int TJ_FP32 = GDFV_TJ_FP32;
+constexpr int TJ_FP32_MHD = GDFV_TJ_FP32_MHD;
+
+// Rows per column tile of the kernels a run launches.
+inline int tile_rows(int precision, bool mhd) { return precision == 0 ? TJ_FP64 : (mhd ? TJ_FP32_MHD : TJ_FP32); }
 
 // Launch one stage (0 = residual only, 1 = predictor, 2 = corrector) over A.n_tiles tiles.
 cudaError_t launch_stage_fp64(int stage, int flux, bool mhd, const StageArgs& A, cudaStream_t s);

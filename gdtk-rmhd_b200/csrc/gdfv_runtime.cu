@@ -382,7 +382,7 @@ void fill_weights(double len, double* w) {
 // starts the long tiles of uneven blocks first.
 void build_tiles(Context* c, int kchunk, std::vector<TileDesc>& tiles) {
     tiles.clear();
-    const int TJ = c->cfg.precision == 0 ? TJ_FP64 : TJ_FP32;
+    const int TJ = tile_rows(c->cfg.precision, c->cfg.mhd);
     for (size_t b = 0; b < c->blocks.size(); ++b) {
         const HostBlock& hb = c->blocks[b];
         int kc = kchunk > 0 ? kchunk : std::min(hb.n[2], 32);

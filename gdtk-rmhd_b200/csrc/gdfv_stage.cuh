@@ -725,11 +725,16 @@ __device__ __forceinline__ void load_direct(const StageArgs& A, const double* Ui
 #ifndef GDFV_MINB_FP64
 #define GDFV_MINB_FP64 2
 #endif
+// MHD kernels: FP64 ones are held to one CTA per SM by their shared memory
+#ifndef GDFV_MINB_MHD_FP32
+#define GDFV_MINB_MHD_FP32 2
+#endif
 
 // PERS = 1: persistent grid over the tile queue; 0: one CTA per tile (no
 // state carried between tiles, so the compiler keeps fewer values live).
 template <int STAGE, class R, bool MHD, int FLUX, int TJ, int OPT, int PERS>
-__global__ void __launch_bounds__(32 * (TJ + 1), MHD ? 1 : (sizeof(R) == 4 ? GDFV_MINB_FP32 : GDFV_MINB_FP64))
+__global__ void __launch_bounds__(32 * (TJ + 1), MHD ? (sizeof(R) == 4 ? GDFV_MINB_MHD_FP32 : 1)
+                                                       : (sizeof(R) == 4 ? GDFV_MINB_FP32 : GDFV_MINB_FP64))
     stage_kernel(StageArgs A) {
     using G = Geo<R, MHD, TJ>;
     constexpr int TI = G::TI, NT = G::NT, NCOL = G::NCOL, PW = G::PW, PLANE = G::PLANE;

@@ -1,6 +1,6 @@
 // gdfv_stage_inst.cuh -- launch and configuration of the stage-kernel
 // instantiations of one flux precision.  Included once by each precision's
-// translation unit, which defines GDFV_REAL, GDFV_TJ, GDFV_LAUNCH and
+// translation unit, which defines GDFV_REAL, GDFV_TJ (Euler rows), GDFV_TJ_MHD, GDFV_LAUNCH and
 // GDFV_CONFIGURE first.
 #include "gdfv_launch.h"
 
@@ -8,7 +8,8 @@ namespace gdfv {
 
 namespace {
 using Real = GDFV_REAL;
-constexpr int TJ = GDFV_TJ;
+constexpr int TJ_E = GDFV_TJ;       // Euler kernels
+constexpr int TJ_M = GDFV_TJ_MHD;   // MHD kernels
 
 // Resident CTAs on the device (CTAs per SM x SMs) of the persistent
 // instantiation: the grid of the persistent launch.
@@ -20,6 +21,7 @@ int& resident() {
 
 template <int STAGE, bool MHD, int FLUX>
 cudaError_t launch_one(const StageArgs& A, cudaStream_t s) {
+    constexpr int TJ = MHD ? TJ_M : TJ_E;
     using G = Geo<Real, MHD, TJ>;
     // defaults (limiter and extrema clipping on, e4 epsilon, none of the outflow
     // boundaries with their own ghost or flux rule) take the specialised path, which
@@ -43,6 +45,7 @@ cudaError_t set_smem(K k, size_t bytes) {
 
 template <int STAGE, bool MHD, int FLUX>
 cudaError_t configure_one(int n_sm) {
+    constexpr int TJ = MHD ? TJ_M : TJ_E;
     using G = Geo<Real, MHD, TJ>;
     cudaError_t e = set_smem(stage_kernel<STAGE, Real, MHD, FLUX, TJ, 0, 0>, G::bytes);
     if (e == cudaSuccess) e = set_smem(stage_kernel<STAGE, Real, MHD, FLUX, TJ, 1, 0>, G::bytes);
