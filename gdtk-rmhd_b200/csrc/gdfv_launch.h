@@ -9,7 +9,7 @@ namespace gdfv {
 
 // Rows of cells per column tile (the tile is 32 x TJ columns) of each flux precision.
 #ifndef GDFV_TJ_FP64
-#define GDFV_TJ_FP64 4
+#define GDFV_TJ_FP64 6
 #endif
 #ifndef GDFV_TJ_FP32
 #define GDFV_TJ_FP32 8
