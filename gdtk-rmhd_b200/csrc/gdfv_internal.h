@@ -11,7 +11,7 @@ namespace gdfv {
 struct NoallocView {
     int prepared, precision, flux, mhd, nblocks, max_invalid_cells;
     long long total;
-    int nq, n_tiles;
+    int nq, n_tiles, n_tiles2;   // n_tiles2 > 0: the corrector's table follows the first
     const BlockDesc* d_blocks;
     const TileDesc* d_tiles;
     const InflowState* d_inflow;

@@ -121,6 +121,7 @@ extern "C" int gdfv_step_noalloc(int ctx, const double* U_in_dev, double* U_out_
     A.total = v.total;
     A.P = v.P;
     A.n_tiles = v.n_tiles;
+    A.n_tiles2 = v.n_tiles2;
     A.max_invalid_cells = v.max_invalid_cells;
     A.persistent = v.persistent;
 

@@ -48,7 +48,7 @@ struct StageArgs {
     int n_tiles;
     int max_invalid_cells;
     int persistent;           // grid of resident CTAs striding over the tiles
-    int pad_;
+    int n_tiles2;             // > 0: the corrector's own tile table follows the first (other rows)
 };
 
 // Compile-time geometry of the tile and of the shared-memory layout.

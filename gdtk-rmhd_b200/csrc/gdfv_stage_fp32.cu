@@ -4,6 +4,7 @@
 #include "gdfv_launch.h"
 #define GDFV_REAL float
 #define GDFV_TJ TJ_FP32
+#define GDFV_TJ_CORR TJ_FP32_CORR
 #define GDFV_TJ_MHD TJ_FP32_MHD
 #define GDFV_LAUNCH launch_stage_fp32
 #define GDFV_CONFIGURE configure_stage_fp32

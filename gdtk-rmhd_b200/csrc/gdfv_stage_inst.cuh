@@ -1,6 +1,7 @@
 // gdfv_stage_inst.cuh -- launch and configuration of the stage-kernel
 // instantiations of one flux precision.  Included once by each precision's
-// translation unit, which defines GDFV_REAL, GDFV_TJ (Euler rows), GDFV_TJ_MHD, GDFV_LAUNCH and
+// translation unit, which defines GDFV_REAL, GDFV_TJ (Euler rows), GDFV_TJ_CORR (Euler
+// corrector rows), GDFV_TJ_MHD, GDFV_LAUNCH and
 // GDFV_CONFIGURE first.
 #include "gdfv_launch.h"
 
@@ -8,26 +9,32 @@ namespace gdfv {
 
 namespace {
 using Real = GDFV_REAL;
-constexpr int TJ_E = GDFV_TJ;       // Euler kernels
-constexpr int TJ_M = GDFV_TJ_MHD;   // MHD kernels
+constexpr int TJ_E = GDFV_TJ;        // Euler kernels
+constexpr int TJ_E2 = GDFV_TJ_CORR;  // Euler corrector (stage 2)
+constexpr int TJ_M = GDFV_TJ_MHD;    // MHD kernels
+
+// Rows of the kernels of a stage: the Euler corrector has a second instantiation
+// with its own rows (TJ_E2), launched over the corrector's tile table when the
+// runtime built one (n_tiles2 > 0).
+template <bool MHD>
+constexpr int rows() { return MHD ? TJ_M : TJ_E; }
 
 // Resident CTAs on the device (CTAs per SM x SMs) of the persistent
 // instantiation: the grid of the persistent launch.
-template <int STAGE, bool MHD, int FLUX>
+template <int STAGE, bool MHD, int FLUX, int TJ>
 int& resident() {
     static int v = 0;
     return v;
 }
 
-template <int STAGE, bool MHD, int FLUX>
-cudaError_t launch_one(const StageArgs& A, cudaStream_t s) {
-    constexpr int TJ = MHD ? TJ_M : TJ_E;
+template <int STAGE, bool MHD, int FLUX, int TJ>
+cudaError_t launch_rows(const StageArgs& A, cudaStream_t s) {
     using G = Geo<Real, MHD, TJ>;
     // defaults (limiter and extrema clipping on, e4 epsilon, none of the outflow
     // boundaries with their own ghost or flux rule) take the specialised path, which
     // also has the persistent form
     if (A.P.apply_limiter && A.P.extrema_clipping && !A.P.lmr_epsilon && !A.P.outflow_bcs) {
-        const int cap = resident<STAGE, MHD, FLUX>();
+        const int cap = resident<STAGE, MHD, FLUX, TJ>();
         if (A.persistent && cap > 0)
             stage_kernel<STAGE, Real, MHD, FLUX, TJ, 1, 1><<<cap < A.n_tiles ? cap : A.n_tiles, G::NT, G::bytes, s>>>(A);
         else
@@ -38,14 +45,26 @@ cudaError_t launch_one(const StageArgs& A, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+template <int STAGE, bool MHD, int FLUX>
+cudaError_t launch_one(const StageArgs& A, cudaStream_t s) {
+    if constexpr (STAGE == 2 && !MHD && TJ_E2 != TJ_E) {
+        if (A.n_tiles2 > 0) {   // the corrector's own tile table follows the first
+            StageArgs A2 = A;
+            A2.tiles = A.tiles + A.n_tiles;
+            A2.n_tiles = A.n_tiles2;
+            return launch_rows<2, MHD, FLUX, TJ_E2>(A2, s);
+        }
+    }
+    return launch_rows<STAGE, MHD, FLUX, rows<MHD>()>(A, s);
+}
+
 template <class K>
 cudaError_t set_smem(K k, size_t bytes) {
     return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
-template <int STAGE, bool MHD, int FLUX>
-cudaError_t configure_one(int n_sm) {
-    constexpr int TJ = MHD ? TJ_M : TJ_E;
+template <int STAGE, bool MHD, int FLUX, int TJ>
+cudaError_t configure_rows(int n_sm) {
     using G = Geo<Real, MHD, TJ>;
     cudaError_t e = set_smem(stage_kernel<STAGE, Real, MHD, FLUX, TJ, 0, 0>, G::bytes);
     if (e == cudaSuccess) e = set_smem(stage_kernel<STAGE, Real, MHD, FLUX, TJ, 1, 0>, G::bytes);
@@ -55,8 +74,16 @@ cudaError_t configure_one(int n_sm) {
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, stage_kernel<STAGE, Real, MHD, FLUX, TJ, 1, 1>, G::NT,
                                                       G::bytes);
     if (e != cudaSuccess) return e;
-    resident<STAGE, MHD, FLUX>() = per_sm * n_sm;
+    resident<STAGE, MHD, FLUX, TJ>() = per_sm * n_sm;
     return cudaSuccess;
+}
+
+template <int STAGE, bool MHD, int FLUX>
+cudaError_t configure_one(int n_sm) {
+    cudaError_t e = configure_rows<STAGE, MHD, FLUX, rows<MHD>()>(n_sm);
+    if constexpr (STAGE == 2 && !MHD && TJ_E2 != TJ_E)
+        if (e == cudaSuccess) e = configure_rows<2, MHD, FLUX, TJ_E2>(n_sm);
+    return e;
 }
 
 template <int STAGE>

@@ -61,7 +61,9 @@ int gdfv_context_free(int ctx);
  * one CTA per tile),
  * autotune (1: the first gdfv_run times the tile k-chunks and both launch forms and
  * keeps the fastest).  gdfv_config_get_double also reads tile_kchunk, persistent,
- * autotune and autotune_stage_ms (stage 1 + stage 2 time of the tuned choice). */
+ * autotune and autotune_stage_ms (stage 1 + stage 2 time of the tuned choice), and after
+ * gdfv_prepare tile_rows and tile_rows_corrector (rows per column tile of the stages
+ * and of the corrector, which may take taller or shorter tiles of its own). */
 int gdfv_config_set_str(int ctx, const char* key, const char* value);
 int gdfv_config_set_int(int ctx, const char* key, long long value);
 int gdfv_config_set_double(int ctx, const char* key, double value);

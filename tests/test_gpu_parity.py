@@ -275,3 +275,29 @@ def test_get_conserved_into_caller_buffer():
     assert got is buf and np.array_equal(buf, ref)
     with pytest.raises(ValueError):
         sim.get_conserved(0, out=np.empty((ref.shape[0], ref.shape[1] - 1)))
+
+
+def test_corrector_tile_rows():
+    """The float Euler corrector runs over tiles of its own rows when they fill the
+    block better (here 56 rows: 8 tiles of 7); the results match the oracle as the
+    other float tests do, in the per-tile and the persistent launch form, and the two
+    forms agree to float rounding.  A block height of 16 keeps the shared rows."""
+    case = cases.c2_inflow_box(n=(40, 56, 24))
+    orc = cases.build_oracle(case)
+    assert orc.run(20) == 0
+    Uo = orc.get_U(0)
+    states = {}
+    for pers in (False, True):
+        sim = cases.build_gpu(case, flux_precision="fp32", persistent=pers)
+        assert sim.option("tile_rows") == 8 and sim.option("tile_rows_corrector") == 7
+        assert sim.run(max_step=20) == 20
+        Ug = sim.get_conserved(0)
+        errs = [cases.rel_l2(Ug[0], Uo[0]), cases.rel_l2(Ug[1:4].ravel(), Uo[1:4].ravel()), cases.rel_l2(Ug[4], Uo[4])]
+        assert max(errs) <= TOL_FP32_L2, (pers, errs)
+        states[pers] = Ug
+        sim.close()
+    for q in range(5):
+        assert cases.rel_l2(states[True][q], states[False][q]) <= 1e-6, q
+    sim = cases.build_gpu(cases.c2_inflow_box(n=(40, 16, 24)), flux_precision="fp32")
+    assert sim.option("tile_rows_corrector") == 8
+    sim.close()
