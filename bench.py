@@ -321,10 +321,12 @@ def main():
                     help="steps after which the FP32 form is compared with FP64 (0: at the timed steps)")
     ap.add_argument("--no-extra", action="store_true", help="skip the multi-block, MHD and adjoint legs")
     ap.add_argument("--profile-case", nargs="?", const="stage", default=None,
-                    choices=["stage", "mhd", "adjoint"],
+                    choices=["stage", "corrector", "mhd", "adjoint"],
                     help="small case for ncu captures, then exit: stage = the 128^3 inflow box "
-                         "(FP32 then FP64 form, warmup steps); mhd = Orszag-Tang 512x512x4 (both forms, "
-                         "warmup steps); adjoint = 128x128x64 FP64 rollout of 10 steps and its backward")
+                         "(FP32 then FP64 form, warmup steps); corrector = the inflow box at 128x112x128, "
+                         "FP32 form, whose rows take the 7-row corrector tiles the 256^3 run uses; mhd = "
+                         "Orszag-Tang 512x512x4 (both forms, warmup steps); adjoint = 128x128x64 FP64 "
+                         "rollout of 10 steps and its backward")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -356,6 +358,14 @@ def main():
         for prec in ("fp32", "fp64"):
             _, sim = make(prec)
             sim.run(max_step=max(3, args.warmup))
+        torch.cuda.synchronize()
+        return 0
+    if args.profile_case == "corrector":
+        case = cases.c2_inflow_box(n=(128, 112, 128), flux=args.flux, precision="fp32", seed=4321)
+        sim = cases.build_gpu(case)
+        sim.set_stream(stream.cuda_stream)
+        assert sim.option("tile_rows_corrector") == 7
+        sim.run(max_step=max(3, args.warmup))
         torch.cuda.synchronize()
         return 0
     if args.profile_case == "mhd":
@@ -407,7 +417,10 @@ def main():
     peak, peak_kind = measured_peaks()
     ach2 = BYTES_STAGE2 * cells / (st2 * 1e-3) / 1e9
     traffic = None
-    tf = os.path.join(ROOT, "profiles", "stage_kernel_fp32_128cube.md")
+    # ncu DRAM bytes per cell of the corrector the run launches (its own 7-row tiles or
+    # the shared 8-row ones), captured on a smaller case
+    tf = os.path.join(ROOT, "profiles", "stage_kernel_fp32_corrector7_128x112x128.md"
+                      if sim32.option("tile_rows_corrector") == 7 else "stage_kernel_fp32_128cube.md")
     if os.path.exists(tf):
         import re
         with open(tf) as f:
