@@ -317,6 +317,9 @@ def main():
     ap.add_argument("--size", type=int, default=256)
     ap.add_argument("--flux", default="ausmdv", choices=["ausmdv", "hllc"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--autotune", type=int, default=1, choices=[0, 1],
+                    help="1: the library's autotuner picks the tile k-chunk and launch form on the first "
+                         "(warm-up) run of each timed simulation")
     ap.add_argument("--accuracy-steps", type=int, default=1000,
                     help="steps after which the FP32 form is compared with FP64 (0: at the timed steps)")
     ap.add_argument("--no-extra", action="store_true", help="skip the multi-block, MHD and adjoint legs")
@@ -350,7 +353,7 @@ def main():
 
     def make(prec):
         case = cases.c2_inflow_box(n=shape, flux=args.flux, precision=prec, seed=4321)
-        sim = cases.build_gpu(case)
+        sim = cases.build_gpu(case, autotune=bool(args.autotune))
         sim.set_stream(stream.cuda_stream)
         return case, sim
 
@@ -480,6 +483,9 @@ def main():
         "clocks": results["fp32"]["clocks"],
         "clocks_fp64": results["fp64"]["clocks"],
     }
+    line["config"].update(autotune=bool(args.autotune), tile_kchunk=sim32.option("tile_kchunk"),
+                          persistent=bool(sim32.option("persistent")), tile_rows=sim32.option("tile_rows"),
+                          tile_rows_corrector=sim32.option("tile_rows_corrector"))
     line["accuracy"] = acc
     if not args.no_extra:
         for sim in list(sims.values()) + [(None, sim_e2e)]:
