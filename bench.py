@@ -324,12 +324,13 @@ def main():
                     help="steps after which the FP32 form is compared with FP64 (0: at the timed steps)")
     ap.add_argument("--no-extra", action="store_true", help="skip the multi-block, MHD and adjoint legs")
     ap.add_argument("--profile-case", nargs="?", const="stage", default=None,
-                    choices=["stage", "corrector", "mhd", "adjoint"],
+                    choices=["stage", "corrector", "mhd", "adjoint", "norms"],
                     help="small case for ncu captures, then exit: stage = the 128^3 inflow box "
                          "(FP32 then FP64 form, warmup steps); corrector = the inflow box at 128x112x128, "
                          "FP32 form, whose rows take the 7-row corrector tiles the 256^3 run uses; mhd = "
                          "Orszag-Tang 512x512x4 (both forms, warmup steps); adjoint = 128x128x64 FP64 "
-                         "rollout of 10 steps and its backward")
+                         "rollout of 10 steps and its backward; norms = the 256^3 box, FP32 form, warmup "
+                         "steps then the residual norms twice")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -347,7 +348,7 @@ def main():
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
-    n = 128 if args.profile_case else args.size
+    n = 128 if args.profile_case and args.profile_case != "norms" else args.size
     shape = (n, n, n)
     stream = torch.cuda.Stream()  # a capturable (non-default) stream shared with the library
 
@@ -369,6 +370,13 @@ def main():
         sim.set_stream(stream.cuda_stream)
         assert sim.option("tile_rows_corrector") == 7
         sim.run(max_step=max(3, args.warmup))
+        torch.cuda.synchronize()
+        return 0
+    if args.profile_case == "norms":
+        _, sim = make("fp32")
+        sim.run(max_step=max(3, args.warmup))
+        for _ in range(2):
+            sim.residual_norms()
         torch.cuda.synchronize()
         return 0
     if args.profile_case == "mhd":

@@ -692,56 +692,78 @@ __global__ void predictor_state_kernel(const double* U0, const double* dU0, doub
 // Residual norms of dU/dt (e4/fluidblock.d:861-909): per CTA, the maximum of |dU/dt[q]|
 // for every q and the sum of squares of the quantities compute_L2_residual takes
 // (mass, x and y momentum, z momentum in 3D, total energy, with MHD xB and yB).
-// Grid-stride over cells, warp shuffles, then the warps in order: partial[cta][nq + 1].
+// Grid-stride over cells, two cells per step (2 NQ loads in flight), warp shuffles,
+// then the warps in order: partial[cta][NQ + 1].
 constexpr int kNormThreads = 256;
-__global__ void __launch_bounds__(kNormThreads) residual_norms_kernel(const double* dU, long long total, int nq,
-                                                                       int threeD, int mhd, double* partial) {
-    double mx[10], l2 = 0.0;
+template <int NQ>
+__global__ void __launch_bounds__(kNormThreads) residual_norms_kernel(const double* __restrict__ dU, long long total,
+                                                                       int threeD, double* partial) {
+    double mx[NQ], l2 = 0.0;
 #pragma unroll
-    for (int q = 0; q < 10; ++q) mx[q] = 0.0;
+    for (int q = 0; q < NQ; ++q) mx[q] = 0.0;
+    auto in_l2 = [&](int q) {
+        return q == MASS || q == XMOM || q == YMOM || (q == ZMOM && threeD) || q == TOTENERGY || q == XB || q == YB;
+    };
     const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < total; x += stride) {
+    long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    for (; x + stride < total; x += 2 * stride) {
+        double a[NQ], b[NQ];
 #pragma unroll
-        for (int q = 0; q < 10; ++q) {
-            if (q >= nq) break;
-            const double v = __ldg(dU + (long long)q * total + x);
-            mx[q] = fmax(mx[q], fabs(v));
-            const bool in_l2 = q == MASS || q == XMOM || q == YMOM || (q == ZMOM && threeD) || q == TOTENERGY ||
-                               (mhd && (q == XB || q == YB));
-            if (in_l2) l2 += v * v;
+        for (int q = 0; q < NQ; ++q) {
+            a[q] = __ldg(dU + (long long)q * total + x);
+            b[q] = __ldg(dU + (long long)q * total + x + stride);
+        }
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+            mx[q] = fmax(mx[q], fmax(fabs(a[q]), fabs(b[q])));
+            if (in_l2(q)) l2 += a[q] * a[q] + b[q] * b[q];
         }
     }
-    __shared__ double s_part[kNormThreads / 32][11];
+    if (x < total) {
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+            const double v = __ldg(dU + (long long)q * total + x);
+            mx[q] = fmax(mx[q], fabs(v));
+            if (in_l2(q)) l2 += v * v;
+        }
+    }
+    __shared__ double s_part[kNormThreads / 32][NQ + 1];
     for (int o = 16; o > 0; o >>= 1) {
         l2 += __shfl_xor_sync(0xffffffffu, l2, o);
 #pragma unroll
-        for (int q = 0; q < 10; ++q) mx[q] = fmax(mx[q], __shfl_xor_sync(0xffffffffu, mx[q], o));
+        for (int q = 0; q < NQ; ++q) mx[q] = fmax(mx[q], __shfl_xor_sync(0xffffffffu, mx[q], o));
     }
     const int wv = threadIdx.x >> 5;
     if ((threadIdx.x & 31) == 0) {
 #pragma unroll
-        for (int q = 0; q < 10; ++q) s_part[wv][q] = mx[q];
-        s_part[wv][10] = l2;
+        for (int q = 0; q < NQ; ++q) s_part[wv][q] = mx[q];
+        s_part[wv][NQ] = l2;
     }
     __syncthreads();
-    if (threadIdx.x <= nq) {
-        const int q = threadIdx.x == nq ? 10 : threadIdx.x;
+    if (threadIdx.x <= NQ) {
+        const int q = threadIdx.x;
         double r = s_part[0][q];
-        for (int w = 1; w < kNormThreads / 32; ++w) r = q == 10 ? r + s_part[w][q] : fmax(r, s_part[w][q]);
-        partial[(long long)blockIdx.x * (nq + 1) + threadIdx.x] = r;
+        for (int w = 1; w < kNormThreads / 32; ++w) r = q == NQ ? r + s_part[w][q] : fmax(r, s_part[w][q]);
+        partial[(long long)blockIdx.x * (NQ + 1) + q] = r;
     }
 }
 
-// The CTAs' partials in CTA order: out[q] = max for q < nq, out[nq] = sqrt(sum) (e4/simcore.d:1212).
+// The CTAs' partials, one warp per quantity in a fixed order: out[q] = max for q < nq,
+// out[nq] = sqrt(sum) (e4/simcore.d:1212).  Launched with 32 (nq + 1) threads.
 __global__ void residual_norms_final_kernel(const double* partial, int ncta, int nq, double* out) {
-    const int q = threadIdx.x;
+    const int q = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (q > nq) return;
-    double r = partial[q];
-    for (int b = 1; b < ncta; ++b) {
+    const bool sum = q == nq;
+    double r = 0.0;   // maxima of magnitudes start at 0
+    for (int b = lane; b < ncta; b += 32) {
         const double v = partial[(long long)b * (nq + 1) + q];
-        r = q == nq ? r + v : fmax(r, v);
+        r = sum ? r + v : fmax(r, v);
     }
-    out[q] = q == nq ? sqrt(r) : r;
+    for (int o = 16; o > 0; o >>= 1) {
+        const double t = __shfl_xor_sync(0xffffffffu, r, o);
+        r = sum ? r + t : fmax(r, t);
+    }
+    if (lane == 0) out[q] = sum ? sqrt(r) : r;
 }
 
 // Resets the control record of a single fixed-dt step.
@@ -1469,18 +1491,23 @@ int gdfv_residual_norms(int ctx, double* Linf, double* L2) {
     if (!L2) return fail(c, GDFV_ERR_ARG, "null pointer");
     if (read_ctl(c)) return GDFV_ERR_CUDA;
     if (c->h_ctl->step < 1) return fail(c, GDFV_ERR_STATE, "no step taken yet");
-    int n_sm = 0;
+    int n_sm = 0, per_sm = 0;
     CK(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, c->device));
-    const long long want = (c->total + kNormThreads - 1) / kNormThreads;
-    const int ncta = (int)std::max(1LL, std::min<long long>(want, 8LL * n_sm));
     const int nq = c->nq;
+    // one wave of resident CTAs (at most 8 per SM: the partials' capacity)
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, nq == 10 ? residual_norms_kernel<10> : residual_norms_kernel<5>, kNormThreads, 0));
+    const long long want = (c->total + kNormThreads - 1) / kNormThreads;
+    const int ncta = (int)std::max(1LL, std::min<long long>(want, (long long)std::min(std::max(per_sm, 1), 8) * n_sm));
     if (!c->norm_scratch) CK(cudaMalloc(&c->norm_scratch, sizeof(double) * ((size_t)8 * n_sm * 11 + 16)));
     double* out = c->norm_scratch;
     double* partial = c->norm_scratch + 16;
-    residual_norms_kernel<<<ncta, kNormThreads, 0, c->stream>>>(c->dU0, c->total, nq, c->cfg.dims == 3, c->cfg.mhd,
-                                                                 partial);
+    if (nq == 10)
+        residual_norms_kernel<10><<<ncta, kNormThreads, 0, c->stream>>>(c->dU0, c->total, c->cfg.dims == 3, partial);
+    else
+        residual_norms_kernel<5><<<ncta, kNormThreads, 0, c->stream>>>(c->dU0, c->total, c->cfg.dims == 3, partial);
     CK(cudaGetLastError());
-    residual_norms_final_kernel<<<1, 32, 0, c->stream>>>(partial, ncta, nq, out);
+    residual_norms_final_kernel<<<1, 32 * (nq + 1), 0, c->stream>>>(partial, ncta, nq, out);
     CK(cudaGetLastError());
     double h[11];
     CK(cudaMemcpyAsync(h, out, sizeof(double) * (nq + 1), cudaMemcpyDeviceToHost, c->stream));
