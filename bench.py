@@ -135,7 +135,7 @@ def chicken_baseline(steps, warmup):
     return chicken_job.bench(exe, steps=steps, warmup=warmup)
 
 
-def adjoint_over_forward(nsteps=50, checkpoint_every=10, shape=(128, 128, 64)):
+def adjoint_over_forward(nsteps=50, checkpoint_every=10, shape=(128, 128, 64), autotune=False):
     """Adjoint configuration: 128x128x64 M=3 inflow box (FP64, ausmdv), J = pressure
     integral over the y-min wall after 50 steps, gradient w.r.t. U0 and the inflow
     state through the checkpointed rollout (every 10 steps).  Returns the ratio of
@@ -148,7 +148,7 @@ def adjoint_over_forward(nsteps=50, checkpoint_every=10, shape=(128, 128, 64)):
     from test_gpu_adjoint import wall_pressure
     case = cases.c2_inflow_box(n=shape)
     inf = cases.inflow_state_m3()
-    sim = cases.build_gpu(case)
+    sim = cases.build_gpu(case, autotune=autotune)
     stream = torch.cuda.Stream()
     sim.set_stream(stream.cuda_stream)
     U0 = torch.from_numpy(sim.get_conserved(0)).cuda()
