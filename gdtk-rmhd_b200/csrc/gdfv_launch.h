@@ -23,16 +23,23 @@ namespace gdfv {
 #ifndef GDFV_TJ_FP32_CORR
 #define GDFV_TJ_FP32_CORR 7
 #endif
+// rows of the FP64 MHD kernels (one CTA per SM: their shared memory allows no second)
+#ifndef GDFV_TJ_FP64_MHD
+#define GDFV_TJ_FP64_MHD 7
+#endif
 constexpr int TJ_FP64 = GDFV_TJ_FP64;
+constexpr int TJ_FP64_MHD = GDFV_TJ_FP64_MHD;
 constexpr int TJ_FP32_CORR = GDFV_TJ_FP32_CORR;
 constexpr int TJ_FP32 = GDFV_TJ_FP32;
 constexpr int TJ_FP32_MHD = GDFV_TJ_FP32_MHD;
 
 // Rows per column tile of the kernels a run launches.
-inline int tile_rows(int precision, bool mhd) { return precision == 0 ? TJ_FP64 : (mhd ? TJ_FP32_MHD : TJ_FP32); }
+inline int tile_rows(int precision, bool mhd) {
+    return precision == 0 ? (mhd ? TJ_FP64_MHD : TJ_FP64) : (mhd ? TJ_FP32_MHD : TJ_FP32);
+}
 // Rows per column tile of the corrector (stage 2) of a run.
 inline int tile_rows_corrector(int precision, bool mhd) {
-    return precision == 0 ? TJ_FP64 : (mhd ? TJ_FP32_MHD : TJ_FP32_CORR);
+    return precision == 0 ? (mhd ? TJ_FP64_MHD : TJ_FP64) : (mhd ? TJ_FP32_MHD : TJ_FP32_CORR);
 }
 
 // Launch one stage (0 = residual only, 1 = predictor, 2 = corrector) over A.n_tiles tiles.
