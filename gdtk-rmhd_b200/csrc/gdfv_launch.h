@@ -27,7 +27,12 @@ namespace gdfv {
 #ifndef GDFV_TJ_FP64_MHD
 #define GDFV_TJ_FP64_MHD 7
 #endif
+// rows of the FP64 Euler corrector (by default those of the FP64 kernels)
+#ifndef GDFV_TJ_FP64_CORR
+#define GDFV_TJ_FP64_CORR GDFV_TJ_FP64
+#endif
 constexpr int TJ_FP64 = GDFV_TJ_FP64;
+constexpr int TJ_FP64_CORR = GDFV_TJ_FP64_CORR;
 constexpr int TJ_FP64_MHD = GDFV_TJ_FP64_MHD;
 constexpr int TJ_FP32_CORR = GDFV_TJ_FP32_CORR;
 constexpr int TJ_FP32 = GDFV_TJ_FP32;
@@ -39,7 +44,7 @@ inline int tile_rows(int precision, bool mhd) {
 }
 // Rows per column tile of the corrector (stage 2) of a run.
 inline int tile_rows_corrector(int precision, bool mhd) {
-    return precision == 0 ? (mhd ? TJ_FP64_MHD : TJ_FP64) : (mhd ? TJ_FP32_MHD : TJ_FP32_CORR);
+    return precision == 0 ? (mhd ? TJ_FP64_MHD : TJ_FP64_CORR) : (mhd ? TJ_FP32_MHD : TJ_FP32_CORR);
 }
 
 // Launch one stage (0 = residual only, 1 = predictor, 2 = corrector) over A.n_tiles tiles.
