@@ -31,7 +31,12 @@ namespace gdfv {
 #ifndef GDFV_TJ_FP64_CORR
 #define GDFV_TJ_FP64_CORR GDFV_TJ_FP64
 #endif
+// rows of the float-flux MHD corrector (by default those of the float MHD kernels)
+#ifndef GDFV_TJ_FP32_MHD_CORR
+#define GDFV_TJ_FP32_MHD_CORR GDFV_TJ_FP32_MHD
+#endif
 constexpr int TJ_FP64 = GDFV_TJ_FP64;
+constexpr int TJ_FP32_MHD_CORR = GDFV_TJ_FP32_MHD_CORR;
 constexpr int TJ_FP64_CORR = GDFV_TJ_FP64_CORR;
 constexpr int TJ_FP64_MHD = GDFV_TJ_FP64_MHD;
 constexpr int TJ_FP32_CORR = GDFV_TJ_FP32_CORR;
@@ -44,7 +49,7 @@ inline int tile_rows(int precision, bool mhd) {
 }
 // Rows per column tile of the corrector (stage 2) of a run.
 inline int tile_rows_corrector(int precision, bool mhd) {
-    return precision == 0 ? (mhd ? TJ_FP64_MHD : TJ_FP64_CORR) : (mhd ? TJ_FP32_MHD : TJ_FP32_CORR);
+    return precision == 0 ? (mhd ? TJ_FP64_MHD : TJ_FP64_CORR) : (mhd ? TJ_FP32_MHD_CORR : TJ_FP32_CORR);
 }
 
 // Launch one stage (0 = residual only, 1 = predictor, 2 = corrector) over A.n_tiles tiles.

@@ -6,6 +6,7 @@
 #define GDFV_TJ TJ_FP32
 #define GDFV_TJ_CORR TJ_FP32_CORR
 #define GDFV_TJ_MHD TJ_FP32_MHD
+#define GDFV_TJ_MHD_CORR TJ_FP32_MHD_CORR
 #define GDFV_LAUNCH launch_stage_fp32
 #define GDFV_CONFIGURE configure_stage_fp32
 #include "gdfv_stage_inst.cuh"

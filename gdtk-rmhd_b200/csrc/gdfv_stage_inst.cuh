@@ -1,7 +1,7 @@
 // gdfv_stage_inst.cuh -- launch and configuration of the stage-kernel
 // instantiations of one flux precision.  Included once by each precision's
 // translation unit, which defines GDFV_REAL, GDFV_TJ (Euler rows), GDFV_TJ_CORR (Euler
-// corrector rows), GDFV_TJ_MHD, GDFV_LAUNCH and
+// corrector rows), GDFV_TJ_MHD, GDFV_TJ_MHD_CORR, GDFV_LAUNCH and
 // GDFV_CONFIGURE first.
 #include "gdfv_launch.h"
 
@@ -12,12 +12,15 @@ using Real = GDFV_REAL;
 constexpr int TJ_E = GDFV_TJ;        // Euler kernels
 constexpr int TJ_E2 = GDFV_TJ_CORR;  // Euler corrector (stage 2)
 constexpr int TJ_M = GDFV_TJ_MHD;    // MHD kernels
+constexpr int TJ_M2 = GDFV_TJ_MHD_CORR;  // MHD corrector (stage 2)
 
-// Rows of the kernels of a stage: the Euler corrector has a second instantiation
-// with its own rows (TJ_E2), launched over the corrector's tile table when the
+// Rows of the kernels of a stage: a corrector may have a second instantiation with
+// its own rows (TJ_E2, TJ_M2), launched over the corrector's tile table when the
 // runtime built one (n_tiles2 > 0).
 template <bool MHD>
 constexpr int rows() { return MHD ? TJ_M : TJ_E; }
+template <bool MHD>
+constexpr int rows_corrector() { return MHD ? TJ_M2 : TJ_E2; }
 
 // Resident CTAs on the device (CTAs per SM x SMs) of the persistent
 // instantiation: the grid of the persistent launch.
@@ -47,12 +50,12 @@ cudaError_t launch_rows(const StageArgs& A, cudaStream_t s) {
 
 template <int STAGE, bool MHD, int FLUX>
 cudaError_t launch_one(const StageArgs& A, cudaStream_t s) {
-    if constexpr (STAGE == 2 && !MHD && TJ_E2 != TJ_E) {
+    if constexpr (STAGE == 2 && rows_corrector<MHD>() != rows<MHD>()) {
         if (A.n_tiles2 > 0) {   // the corrector's own tile table follows the first
             StageArgs A2 = A;
             A2.tiles = A.tiles + A.n_tiles;
             A2.n_tiles = A.n_tiles2;
-            return launch_rows<2, MHD, FLUX, TJ_E2>(A2, s);
+            return launch_rows<2, MHD, FLUX, rows_corrector<MHD>()>(A2, s);
         }
     }
     return launch_rows<STAGE, MHD, FLUX, rows<MHD>()>(A, s);
@@ -81,8 +84,8 @@ cudaError_t configure_rows(int n_sm) {
 template <int STAGE, bool MHD, int FLUX>
 cudaError_t configure_one(int n_sm) {
     cudaError_t e = configure_rows<STAGE, MHD, FLUX, rows<MHD>()>(n_sm);
-    if constexpr (STAGE == 2 && !MHD && TJ_E2 != TJ_E)
-        if (e == cudaSuccess) e = configure_rows<2, MHD, FLUX, TJ_E2>(n_sm);
+    if constexpr (STAGE == 2 && rows_corrector<MHD>() != rows<MHD>())
+        if (e == cudaSuccess) e = configure_rows<2, MHD, FLUX, rows_corrector<MHD>()>(n_sm);
     return e;
 }
 
