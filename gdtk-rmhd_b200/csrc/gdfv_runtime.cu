@@ -1221,7 +1221,7 @@ int autotune(Context* c) {
     std::vector<int> kcs;
     if (c->cfg.dims == 2) kcs.push_back(1);
     else
-        for (int kc : {8, 16, 32, 64, 128})
+        for (int kc : {8, 12, 16, 24, 32, 64, 128})
             if (kc <= maxk || kcs.empty()) kcs.push_back(kc);
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
