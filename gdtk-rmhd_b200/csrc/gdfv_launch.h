@@ -16,7 +16,7 @@ namespace gdfv {
 #endif
 // rows of the float-flux MHD kernels (their ten variables need more shared memory per row)
 #ifndef GDFV_TJ_FP32_MHD
-#define GDFV_TJ_FP32_MHD 6
+#define GDFV_TJ_FP32_MHD 7
 #endif
 // rows of the float-flux Euler corrector: with 7 rows its CTAs of 256 threads get 80
 // registers (fewer spills) at the same 3 CTAs per SM
