@@ -306,3 +306,25 @@ def test_corrector_tile_rows(flux):
     sim = cases.build_gpu(cases.c2_inflow_box(n=(40, 16, 24)), flux_precision="fp32")
     assert sim.option("tile_rows_corrector") == 8
     sim.close()
+
+
+def test_calls_with_nothing_to_do():
+    """Empty requests leave the state alone: a run of zero steps takes none and changes no
+    cell (the reference's loop stops at max_step before stepping, e4/simcore.d:1055-1366);
+    the residual norms before any step report a state error instead of numbers, and
+    the same context then steps normally, matching the oracle."""
+    from gdfv._lib import GDFV_ERR_STATE, GdfvError
+    case = cases.c2_inflow_box(n=(40, 24, 20))
+    sim = cases.build_gpu(case)
+    U0 = sim.get_conserved(0).copy()
+    assert sim.run(max_step=0) == 0
+    assert np.array_equal(sim.get_conserved(0), U0)
+    assert sim.time()["step"] == 0
+    with pytest.raises(GdfvError) as err:
+        sim.residual_norms()
+    assert err.value.code == GDFV_ERR_STATE and "no step" in str(err.value)
+    orc = cases.build_oracle(case)
+    assert orc.run(3) == 0 and sim.run(max_step=3) == 3
+    errs = cases.cell_errors(sim.get_conserved(0), orc.get_U(0), False)
+    assert max(errs.values()) <= TOL_FP64, errs
+    sim.close()
