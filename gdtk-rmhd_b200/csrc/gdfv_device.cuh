@@ -99,6 +99,25 @@ template <> __device__ __forceinline__ float rmax<float>(float a, float b) { ret
 template <class R> __device__ __forceinline__ R rsqrt_(R x) { return sqrt(x); }
 template <> __device__ __forceinline__ float rsqrt_<float>(float x) { return sqrtf(x); }
 
+// Dipole field that an MHD slip-wall ghost at (x, y) with |x| < 0.4136 takes
+// (e4/bc/ghost_cell_effect/internal_copy_then_reflect.d:140-143).  The reference
+// writes D's `^^`; with an integer exponent that is std.math.pow(F, int), which
+// multiplies by repeated squaring: s^^2 = s*s, s^^3 = s*(s*s), s^^5 = s*((s*s)*(s*s)).
+// ^^0.5 is the square root.  Written as those products here and in the oracle, in
+// FP64 without contraction, both sides give the same bits.
+__device__ __forceinline__ void dipole_field(double x, double y, double& Bx, double& By) {
+    const double xs = x + 0., ys = y + 0.0;
+    const double x2 = d_mul(xs, xs), y2 = d_mul(ys, ys);
+    const double r = sqrt(d_add(x2, y2));
+    const double r2 = d_mul(r, r);
+    const double r5 = d_mul(r, d_mul(r2, r2));
+    const double h = 0.82 / 2;
+    const double h3 = d_mul(h, d_mul(h, h));
+    const double cc = d_mul(0.1, h3) / d_mul(2.0, r5);
+    Bx = -cc * __dsub_rn(d_mul(2.0, x2), y2);
+    By = -cc * d_mul(d_mul(3.0, xs), ys);
+}
+
 // src/nm/limiters.d:41-50
 template <class R>
 __device__ __forceinline__ R clip_to_limits(R q, R A, R B) {

@@ -19,9 +19,13 @@ struct NoallocView {
     double c_h;
     cudaStream_t stream;
     int persistent;
+    long long max_block_cells;   // cells of the largest block
 };
 bool noalloc_view(int ctx, NoallocView* v);
 void noalloc_set_error(int ctx, const std::string& msg);
+// Records the failing cell (global index g) for gdfv_last_bad_cell and returns its
+// description for an error message ("" when g names no cell).
+std::string noalloc_bad_cell_text(int ctx, long long g);
 
 // What the adjoint (gdfv_adjoint.cu) needs of a context (gdfv_runtime.cu).
 struct AdjView {

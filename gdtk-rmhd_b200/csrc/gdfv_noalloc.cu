@@ -20,7 +20,13 @@
 //     counters and signal maxima it needs before its kernels run;
 //   * the first call on a device resolves the array's device address
 //     (cudaGetSymbolAddress) and caches it, so make that first call before any
-//     stream capture begins on that device.
+//     stream capture begins on that device.  A cached address that no longer
+//     names device memory (the device was reset, cudaDeviceReset, and its
+//     context made anew) is looked up again;
+//   * MHD with divergence cleaning: c_h is the rule of a gdfv_run step
+//     (e4/simcore.d:1625-1648 update_ch_for_divergence_cleaning with
+//     e4/fluidblock.d:975-995) applied to the signal frequency of U_in, which a
+//     first kernel reduces per block into the scratch.
 #include <cuda_runtime.h>
 
 #include <climits>
@@ -65,6 +71,41 @@ __global__ void noalloc_begin_kernel(Control* c, unsigned long long* maxsig, int
     }
 }
 
+// Per-block maximum of the signal frequency of U (e4/fvcell.d:975-1059) into
+// maxsig[blockIdx.y] (bit patterns of positive doubles), as the initial scan of a
+// gdfv_run does.
+__global__ void noalloc_signal_kernel(const double* U, long long total, const BlockDesc* blocks, NumParams P,
+                                      unsigned long long* maxsig) {
+    const int blk = blockIdx.y;
+    const BlockDesc& B = blocks[blk];
+    const long long n = (long long)B.n[0] * B.n[1] * B.n[2];
+    double sig = 0.0;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+        double u[10];
+        for (int q = 0; q < P.nq; ++q) u[q] = U[q * total + B.offset + c];
+        Prim<double> s;
+        double p, T;
+        if (decode(P, u, s, p, T) == 0) sig = fmax(sig, signal_frequency(P, B, s));
+    }
+    for (int o = 16; o > 0; o >>= 1) sig = fmax(sig, __shfl_xor_sync(0xffffffffu, sig, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(&maxsig[blk], (unsigned long long)__double_as_longlong(sig));
+}
+
+// c_h from the signal maxima with the operations of the step controller's rule
+// (cfl_max = signal dt, c_h = min over blocks of cfl_max L_min / dt); then the
+// maxima are cleared for the corrector's reduction.
+__global__ void noalloc_ch_kernel(Control* c, const BlockDesc* blocks, unsigned long long* maxsig, int nblocks) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const double dt = c->dt_global;
+    for (int b = 0; b < nblocks; ++b) {
+        const double smax = __longlong_as_double((long long)maxsig[b]);
+        const double cfl_max = smax * dt;
+        const double ch = cfl_max * blocks[b].L_min / dt;
+        c->c_h = b == 0 ? ch : fmin(ch, c->c_h);
+        maxsig[b] = 0ull;
+    }
+}
+
 }  // namespace
 }  // namespace gdfv
 
@@ -93,6 +134,14 @@ extern "C" int gdfv_step_noalloc(int ctx, const double* U_in_dev, double* U_out_
     double* base = nullptr;
     {
         std::lock_guard<std::mutex> lk(g_mu);
+        if (g_addr[dev]) {
+            // a device reset ends the context the cached address belonged to
+            cudaPointerAttributes at{};
+            if (cudaPointerGetAttributes(&at, g_addr[dev]) != cudaSuccess || at.type != cudaMemoryTypeDevice) {
+                cudaGetLastError();
+                g_addr[dev] = nullptr;
+            }
+        }
         if (!g_addr[dev]) {
             // once per device, with that device current
             e = cudaGetSymbolAddress((void**)&g_addr[dev], g_step_scratch);
@@ -125,8 +174,18 @@ extern "C" int gdfv_step_noalloc(int ctx, const double* U_in_dev, double* U_out_
     A.max_invalid_cells = v.max_invalid_cells;
     A.persistent = v.persistent;
 
-    noalloc_begin_kernel<<<1, 256, 0, v.stream>>>(ctl, maxsig, v.nblocks, dt, v.c_h);
+    noalloc_begin_kernel<<<1, 256, 0, v.stream>>>(ctl, maxsig, v.nblocks, dt, 0.0);
     e = cudaGetLastError();
+    if (e == cudaSuccess && v.mhd && v.P.divergence_cleaning) {
+        const long long per = (v.max_block_cells + 255) / 256;
+        const dim3 grid((unsigned)(per < 256 ? per : 256), (unsigned)v.nblocks);
+        noalloc_signal_kernel<<<grid, 256, 0, v.stream>>>(U_in_dev, v.total, v.d_blocks, v.P, maxsig);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) {
+            noalloc_ch_kernel<<<1, 32, 0, v.stream>>>(ctl, v.d_blocks, maxsig, v.nblocks);
+            e = cudaGetLastError();
+        }
+    }
     for (int stage = 1; stage <= 2 && e == cudaSuccess; ++stage) {
         e = v.precision == 0 ? launch_stage_fp64(stage, v.flux, v.mhd, A, v.stream)
                              : launch_stage_fp32(stage, v.flux, v.mhd, A, v.stream);
@@ -140,11 +199,12 @@ extern "C" int gdfv_step_noalloc(int ctx, const double* U_in_dev, double* U_out_
     }
     if (n_bad_cells) *n_bad_cells = h.n_fail + h.n_invalid1 + h.n_invalid2;
     if (h.n_fail > 0) {
-        noalloc_set_error(ctx, "gdfv_step_noalloc: a cell failed to decode; U_out is not a valid step");
+        noalloc_set_error(ctx, "gdfv_step_noalloc: a cell failed to decode; U_out is not a valid step." +
+                                   noalloc_bad_cell_text(ctx, h.first_bad_cell));
         return GDFV_ERR_STEP_FAILED;
     }
     if (h.n_invalid1 > v.max_invalid_cells || h.n_invalid2 > v.max_invalid_cells) {
-        noalloc_set_error(ctx, "gdfv_step_noalloc: too many bad cells");
+        noalloc_set_error(ctx, "gdfv_step_noalloc: too many bad cells." + noalloc_bad_cell_text(ctx, h.first_bad_cell));
         return GDFV_ERR_BAD_CELLS;
     }
     return GDFV_OK;

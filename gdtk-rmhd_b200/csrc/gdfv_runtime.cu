@@ -252,6 +252,8 @@ struct Context {
     int adj_ready = 0;
     long long adj_scratch_n = 0;
     cudaStream_t aux_stream[2] = {nullptr, nullptr};  // lowest / highest priority streams of the rollout adjoint
+    long long last_bad_cell = -1;      // global index of the cell the last failure reported (-1: none)
+    std::vector<double> h_inflow;      // supersonic-inflow states as uploaded, 9 doubles each (p, T, vel, B, psi)
     Control* step_ctl = nullptr;       // control record of gdfv_step_dt
     unsigned long long* step_maxsig = nullptr;
     double* step_lastsig = nullptr;
@@ -290,6 +292,43 @@ int fail(Context* c, int code, const std::string& msg) {
 
 int cuda_fail(Context* c, cudaError_t e, const char* where) {
     return fail(c, GDFV_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+// Block, (i, j, k) and cell-centre position of the cell at global index g (the
+// cell id of the reference's SFluidBlock is i + nic (j + njc k)).
+bool locate_cell(const Context* c, long long g, int* blk, int* ijk, double* pos) {
+    if (g < 0 || g >= c->total) return false;
+    for (size_t b = 0; b < c->blocks.size(); ++b) {
+        const HostBlock& hb = c->blocks[b];
+        const long long n = (long long)hb.n[0] * hb.n[1] * hb.n[2];
+        if (g < hb.offset || g >= hb.offset + n) continue;
+        const long long id = g - hb.offset;
+        const int ii[3] = {(int)(id % hb.n[0]), (int)((id / hb.n[0]) % hb.n[1]), (int)(id / ((long long)hb.n[0] * hb.n[1]))};
+        if (blk) *blk = (int)b;
+        for (int d = 0; d < 3; ++d) {
+            if (ijk) ijk[d] = ii[d];
+            if (pos) pos[d] = hb.origin[d] + ((double)ii[d] + 0.5) * hb.len[d];
+        }
+        if (pos && c->cfg.dims == 2) pos[2] = 0.0;
+        return true;
+    }
+    return false;
+}
+
+// Records the failing cell of a failed step and describes it as the reference's
+// decode failure and invalid-cell report do (e4/fvcell.d:610-640: block id, cell id,
+// position; e4/fluidblock.d:607-675).
+std::string bad_cell_text(Context* c, long long g) {
+    int blk = 0, ijk[3] = {0, 0, 0};
+    double pos[3] = {0.0, 0.0, 0.0};
+    if (!locate_cell(c, g, &blk, ijk, pos)) { c->last_bad_cell = -1; return ""; }
+    c->last_bad_cell = g;
+    const HostBlock& hb = c->blocks[blk];
+    const long long id = ijk[0] + (long long)hb.n[0] * (ijk[1] + (long long)hb.n[1] * ijk[2]);
+    char buf[256];
+    std::snprintf(buf, sizeof buf, " First bad cell: blk-id= %d cell-id= %lld (i,j,k)= (%d,%d,%d) x= %.17g y= %.17g z= %.17g",
+                  blk, id, ijk[0], ijk[1], ijk[2], pos[0], pos[1], pos[2]);
+    return buf;
 }
 
 #define CK(call)                                                      \
@@ -450,6 +489,7 @@ int do_prepare(Context* c) {
     std::vector<FixedState> fixed;
     int outflow_bcs = 0;
     c->h_blocks.clear();
+    c->h_inflow.clear();
     std::vector<TileDesc> tiles;
     const double Cv = g.R / (g.gamma - 1.0);
     for (size_t b = 0; b < c->blocks.size(); ++b) {
@@ -523,6 +563,7 @@ int do_prepare(Context* c) {
                 s.psi = bc.inflow[8];
                 B.bc_inflow[f] = (int)inflows.size();
                 inflows.push_back(s);
+                c->h_inflow.insert(c->h_inflow.end(), bc.inflow, bc.inflow + 9);
             }
         }
         c->h_blocks.push_back(B);
@@ -645,6 +686,9 @@ bool noalloc_view(int ctx, NoallocView* v) {
     v->c_h = c->h_ctl ? c->h_ctl->c_h : 0.0;
     v->stream = c->stream;
     v->persistent = c->cfg.persistent;
+    v->max_block_cells = 0;
+    for (const HostBlock& hb : c->blocks)
+        v->max_block_cells = std::max(v->max_block_cells, (long long)hb.n[0] * hb.n[1] * hb.n[2]);
     return true;
 }
 
@@ -652,6 +696,11 @@ void noalloc_set_error(int ctx, const std::string& msg) {
     Context* c = get_ctx(ctx);
     if (c) c->err = msg;
     else g_err = msg;
+}
+
+std::string noalloc_bad_cell_text(int ctx, long long g) {
+    Context* c = get_ctx(ctx);
+    return c ? bad_cell_text(c, g) : std::string();
 }
 
 bool adjoint_view(int ctx, AdjView* v) {
@@ -1166,9 +1215,10 @@ int steps_dt_status(int ctx, cudaStream_t stream) {
     Control h{};
     CK(cudaMemcpyAsync(&h, c->step_ctl, sizeof(Control), cudaMemcpyDeviceToHost, stream));
     CK(cudaStreamSynchronize(stream));
-    if (h.n_fail > 0) return fail(c, GDFV_ERR_STEP_FAILED, "fixed-dt step: a cell failed to decode");
+    if (h.n_fail > 0)
+        return fail(c, GDFV_ERR_STEP_FAILED, "fixed-dt step: a cell failed to decode." + bad_cell_text(c, h.first_bad_cell));
     if (h.n_invalid1 > c->cfg.max_invalid_cells || h.n_invalid2 > c->cfg.max_invalid_cells)
-        return fail(c, GDFV_ERR_BAD_CELLS, "fixed-dt step: too many bad cells");
+        return fail(c, GDFV_ERR_BAD_CELLS, "fixed-dt step: too many bad cells." + bad_cell_text(c, h.first_bad_cell));
     return GDFV_OK;
 }
 
@@ -1318,9 +1368,42 @@ int gdfv_run(int ctx, int max_steps, double max_time, int* steps_taken) {
     }
     if (steps_taken) *steps_taken = c->h_ctl->step - start_step;
     if (c->h_ctl->status == ST_TOO_MANY_BAD_CELLS)
-        return fail(c, GDFV_ERR_BAD_CELLS, "Too many bad cells during explicit gasdynamic update.");
+        return fail(c, GDFV_ERR_BAD_CELLS, "Too many bad cells during explicit gasdynamic update." +
+                                               bad_cell_text(c, c->h_ctl->first_bad_cell));
     if (c->h_ctl->status == ST_DECODE_FAILED)
-        return fail(c, GDFV_ERR_STEP_FAILED, "Explicit update failed after max_attempts_for_step attempts.");
+        return fail(c, GDFV_ERR_STEP_FAILED, "Explicit update failed after max_attempts_for_step attempts." +
+                                                 bad_cell_text(c, c->h_ctl->first_bad_cell));
+    return GDFV_OK;
+}
+
+int gdfv_last_bad_cell(int ctx, int* blk, int* ijk, double* pos) {
+    Context* c = get_ctx(ctx);
+    int st = check_ready(c, -1);
+    if (st) return st;
+    if (c->last_bad_cell < 0) return fail(c, GDFV_ERR_STATE, "no failed step has reported a cell");
+    locate_cell(c, c->last_bad_cell, blk, ijk, pos);
+    return GDFV_OK;
+}
+
+int gdfv_set_inflow(int ctx, int index, const double* state) {
+    Context* c = get_ctx(ctx);
+    int st = check_ready(c, -1);
+    if (st) return st;
+    if (index < 0 || index >= c->n_inflow || !state) return fail(c, GDFV_ERR_ARG, "bad inflow index or state");
+    const Config& g = c->cfg;
+    const double p = state[0], T = state[1];
+    if (!(p > 0.0) || !(T > 0.0)) return fail(c, GDFV_ERR_ARG, "inflow needs p > 0 and T > 0");
+    // as gdfv_prepare builds it: FlowState:new{p=, T=} (update_thermo_from_pT, update_sound_speed)
+    InflowState s{};
+    s.p = p;
+    s.rho = p / (T * g.R);
+    s.u = (g.R / (g.gamma - 1.0)) * T;
+    s.a = std::sqrt(g.gamma * g.R * T);
+    for (int d = 0; d < 3; ++d) { s.vel[d] = state[2 + d]; s.B[d] = state[5 + d]; }
+    s.psi = state[8];
+    CK(cudaMemcpyAsync(c->d_inflow + index, &s, sizeof(InflowState), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    std::copy(state, state + 9, c->h_inflow.begin() + 9 * (size_t)index);
     return GDFV_OK;
 }
 
@@ -1451,9 +1534,10 @@ int gdfv_step_dt(int ctx, const double* U_in_dev, double* U_out_dev, double dt, 
     Control h{};
     CK(cudaMemcpyAsync(&h, c->step_ctl, sizeof(Control), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
-    if (h.n_fail > 0) return fail(c, GDFV_ERR_STEP_FAILED, "gdfv_step_dt: a cell failed to decode");
+    if (h.n_fail > 0)
+        return fail(c, GDFV_ERR_STEP_FAILED, "gdfv_step_dt: a cell failed to decode." + bad_cell_text(c, h.first_bad_cell));
     if (h.n_invalid1 > c->cfg.max_invalid_cells || h.n_invalid2 > c->cfg.max_invalid_cells)
-        return fail(c, GDFV_ERR_BAD_CELLS, "gdfv_step_dt: too many bad cells");
+        return fail(c, GDFV_ERR_BAD_CELLS, "gdfv_step_dt: too many bad cells." + bad_cell_text(c, h.first_bad_cell));
     return GDFV_OK;
 }
 

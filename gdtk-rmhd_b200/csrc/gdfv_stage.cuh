@@ -281,12 +281,7 @@ __device__ __forceinline__ void finish_cell(const StageArgs& A, const double* Ui
             const BlockDesc& B = *s.blk;
             double x = B.x0 + ((double)i + 0.5) * B.len[0];
             double y = B.y0 + ((double)j + 0.5) * B.len[1];
-            if (x > -0.4136 && x < 0.4136) {
-                double r = pow(pow(pow(x + 0., 2.0) + pow(y + 0.0, 2.0), 0.5), 5.0);
-                double cc = ((0.1) * pow(0.82 / 2, 3.0)) / (2 * r);
-                out.B[0] = -cc * (2 * pow(x + 0., 2.0) - pow(y + 0.0, 2.0));
-                out.B[1] = -cc * (3 * (x + 0.) * (y + 0.0));
-            }
+            if (x > -0.4136 && x < 0.4136) dipole_field(x, y, out.B[0], out.B[1]);
         }
     } else if (s.kind > SRC_MIRROR) {   // the rare kinds, out of line (SRC_INFLOW returned above)
         if (OUTF && s.kind >= SRC_FIXEDP) {
@@ -1116,7 +1111,11 @@ __global__ void __launch_bounds__(32 * (TJ + 1), MHD ? (sizeof(R) == 4 ? GDFV_MI
                         atomicMin(reinterpret_cast<unsigned long long*>(&A.ctl->first_bad_cell),
                                   (unsigned long long)g);
                     } else {
-                        if (!check_data(P, s, p, T)) atomicAdd(STAGE == 1 ? &A.ctl->n_invalid1 : &A.ctl->n_invalid2, 1);
+                        if (!check_data(P, s, p, T)) {
+                            atomicAdd(STAGE == 1 ? &A.ctl->n_invalid1 : &A.ctl->n_invalid2, 1);
+                            atomicMin(reinterpret_cast<unsigned long long*>(&A.ctl->first_bad_cell),
+                                      (unsigned long long)g);
+                        }
                         if (STAGE == 2) {
                             double sig = (FAST && !MHD) ? signal_fast(P, inv_len, s) : signal_frequency(P, B, s);
                             sig_max = fmax(sig_max, sig);

@@ -5,7 +5,9 @@
   Jacobian-vector product of a Newton-Krylov solver.
 * `rollout(sim, U0, theta, nsteps, checkpoint_every)`: nsteps predictor-corrector
   steps of the GPU solver from U0, differentiable in U0 and in the supersonic-
-  inflow state theta = (p, T, vel.x).  The forward records each step's dt and
+  inflow state theta = (p, T, vel.x), which the forward sets on every supersonic-
+  inflow face (the other components of each face's state stay as configured), so
+  that dJ/dtheta sums the cotangents of all those faces.  The forward records each step's dt and
   keeps a copy of the state every `checkpoint_every` steps; the backward
   (gdfv_rollout_adjoint) recomputes each segment from its checkpoint
   (bit-identical to the forward steps) on a second stream while it applies the
@@ -131,6 +133,12 @@ class Rollout(torch.autograd.Function):
         work = [torch.empty_like(U0) for _ in range(4 * K)]
         outs0, preds0 = work[:K], work[K:2 * K]
         s_last = ((nsteps + K - 1) // K - 1) * K
+        # theta is the state of every supersonic-inflow face for this rollout
+        p, T, vx = [float(x) for x in theta.detach().cpu()]
+        for i, st in enumerate(sim.inflow_states()):
+            s = st.copy()
+            s[0], s[1], s[2] = p, T, vx
+            sim.set_inflow(i, s)
         sim.set_time(0.0, 0, sim.config.dt_init)
         torch.cuda.current_stream().synchronize()
         state = _state_view(sim)
@@ -167,7 +175,9 @@ class Rollout(torch.autograd.Function):
         torch.cuda.synchronize()
         check(sim.ctx, sim.L.gdfv_rollout_adjoint(sim.ctx, pc, nseg, pd, len(dts), K, pw, 1, _p(lam), _p(gin)))
         ctx.work = None
-        gtheta = inflow_chain(sim, ctx.theta, gin[0].cpu()).to(ctx.theta.device)
+        gin = gin.cpu()
+        gtheta = sum(inflow_chain(sim, ctx.theta, gin[i]) for i in range(max(1, sim.n_inflow)))
+        gtheta = gtheta.to(ctx.theta.device)
         return lam, gtheta, None, None, None
 
 

@@ -169,7 +169,7 @@ class Simulation:
         self.blocks = []
         self._bcs = []
         self._prepared = False
-        self.n_inflow = 0   # supersonic-inflow faces, in the order the library numbers them
+        self._inflow = {}   # (block, face) -> state array of a supersonic-inflow face
 
     # ---------------------------------------------------------------- setup
     def _apply_config(self):
@@ -200,19 +200,48 @@ class Simulation:
             self.set_bc(b, face, bc)
         return b
 
+    def inflow_states(self):
+        """State arrays {p, T, vel.x, vel.y, vel.z, B.x, B.y, B.z, psi} of the
+        supersonic-inflow faces in the order the library numbers them (by block, then
+        face; faces beyond the active ones of a 2D run carry none)."""
+        nfaces = 6 if int(self.config.dimensions) == 3 else 4
+        return [self._inflow[k] for k in sorted(self._inflow) if k[1] < nfaces]
+
+    @property
+    def n_inflow(self):
+        return len(self.inflow_states())
+
+    def set_inflow(self, index, flowState):
+        """Replace the state of supersonic-inflow face `index` (inflow_states order)
+        after preparation; the next step uses it."""
+        self.prepare()
+        arr = np.ascontiguousarray(flowState.as_array() if hasattr(flowState, "as_array") else flowState,
+                                   dtype=np.float64)
+        check(self.ctx, self.L.gdfv_set_inflow(self.ctx, int(index), ffi.cast("double*", arr.ctypes.data)))
+        self.inflow_states()[index][:] = arr
+
+    def last_bad_cell(self):
+        """(block, (i, j, k), (x, y, z)) of the cell the last failed step reported."""
+        blk = ffi.new("int*")
+        ijk = ffi.new("int[3]")
+        pos = ffi.new("double[3]")
+        check(self.ctx, self.L.gdfv_last_bad_cell(self.ctx, blk, ijk, pos))
+        return blk[0], (ijk[0], ijk[1], ijk[2]), (pos[0], pos[1], pos[2])
+
     def set_bc(self, blk, face, bc):
         f = FACE_INDEX[face] if isinstance(face, str) else int(face)
         x_order, other, other_face = 0, -1, -1
         inflow = ffi.NULL
+        self._inflow.pop((blk, f), None)
         if isinstance(bc, OutFlowBC_SimpleExtrapolate):
             x_order = bc.xOrder
         elif isinstance(bc, ExchangeBC_FullFace):
             other, other_face = bc.otherBlock, bc.otherFace
         elif isinstance(bc, InFlowBC_Supersonic):
-            arr = bc.flowState.as_array()
+            arr = np.array(bc.flowState.as_array(), dtype=np.float64)
             self._bcs[blk][f] = arr  # keep alive
             inflow = ffi.cast("double*", arr.ctypes.data)
-            self.n_inflow += 1
+            self._inflow[(blk, f)] = arr
         elif isinstance(bc, (OutFlowBC_FixedP, OutFlowBC_FixedPT)):
             arr = np.zeros(9)
             arr[0] = bc.p_outside

@@ -115,6 +115,26 @@ long long gdfv_total_cells(int ctx);
  * retry with dt*0.2 and the bad-cell abort run on the device.
  * Returns 0, GDFV_ERR_BAD_CELLS or GDFV_ERR_STEP_FAILED. */
 int gdfv_run(int ctx, int max_steps, double max_time, int* steps_taken);
+/* Where the last failed step failed: block id, (i, j, k) within the block and the
+ * cell-centre position (x, y, z) of the failing cell with the lowest index among the
+ * cells that failed to decode or failed check_data in the step's last attempt.  The
+ * reference names that cell in its exceptions and reports: decode_conserved's "Bad
+ * cell" (e4/fvcell.d:610-640: blk-id, cell-id, x, y, z) and count_invalid_cells
+ * (e4/fluidblock.d:607-675); the error message of the failed call (gdfv_run,
+ * gdfv_step_dt, gdfv_steps_dt, gdfv_step_noalloc) carries the same, with the cell id
+ * i + nic (j + njc k).  Any pointer may be NULL.  GDFV_ERR_STATE when no failed step
+ * has reported a cell. */
+int gdfv_last_bad_cell(int ctx, int* blk, int* ijk, double* pos);
+
+/* Replace the state of supersonic-inflow face `index` (faces numbered in the order
+ * gdfv_block_set_bc defined them) after gdfv_prepare: state = {p, T, vel.x, vel.y,
+ * vel.z, B.x, B.y, B.z, psi} as for "inflow_supersonic".  The ghost state is the
+ * FlowState that InFlowBC_Supersonic carries into FlowStateCopy
+ * (e4/bc/ghost_cell_effect/flow_state_copy.d:92-107), built with FlowState:new{p=,T=};
+ * the reference fixes it at preparation and has no run-time counterpart.  The next
+ * step uses it (captured steps read it from device memory). */
+int gdfv_set_inflow(int ctx, int index, const double* state);
+
 /* out5 = {time, dt_global, c_h, cfl_max, dt_allow}; step = steps taken so far. */
 int gdfv_get_time(int ctx, double* out5, int* step);
 /* Set the simulation time, step counter and dt_global (e.g. after a restart). */
@@ -226,10 +246,12 @@ int gdfv_time_stages(int ctx, int reps, double* ms);
  * blocks must not exceed GDFV_NOALLOC_MAX_BLOCKS, else GDFV_ERR_ARG.  All calls share
  * that array, so calls whose kernels overlap on the GPU race; calls made one after
  * another on the context's stream are safe.  The first call on a device looks up the
- * array's address; make it before any stream capture starts on that device.  MHD runs
- * use the c_h of the context's last gdfv_run.  n_bad_cells (may be NULL) receives the
- * decode failures plus invalid cells; a decode failure returns GDFV_ERR_STEP_FAILED
- * (no retry is attempted). */
+ * array's address; make it before any stream capture starts on that device (after a
+ * device reset the address is looked up again).  MHD runs with divergence cleaning
+ * take c_h by the rule of a gdfv_run step from the signal frequency of U_in (reduced
+ * into the same scratch).  n_bad_cells (may be NULL) receives the decode failures plus
+ * invalid cells; a decode failure returns GDFV_ERR_STEP_FAILED (no retry is
+ * attempted); gdfv_last_bad_cell then locates the failing cell. */
 #define GDFV_NOALLOC_MAX_VALUES 4194304LL
 #define GDFV_NOALLOC_MAX_BLOCKS 1024
 int gdfv_step_noalloc(int ctx, const double* U_in_dev, double* U_out_dev, double dt, int* n_bad_cells);

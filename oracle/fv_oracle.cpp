@@ -120,10 +120,17 @@ static void fill_ghosts(const Sim& sim, std::vector<std::vector<FlowState<T>>>& 
                                 double x = b.x0 + (ijk[0] + 0.5) * b.dx;
                                 double y = b.y0 + (ijk[1] + 0.5) * b.dy;
                                 if (x > -0.4136 && x < 0.4136) {
-                                    double r = std::pow(std::pow(std::pow(x + 0., 2) + std::pow(y + 0.0, 2), 0.5), 5);
-                                    double c = ((0.1) * std::pow(0.82 / 2, 3)) / (2 * r);
-                                    s.B[0] = -c * (2 * std::pow(x + 0., 2) - std::pow(y + 0.0, 2));
-                                    s.B[1] = -c * (3 * (x + 0.) * (y + 0.0));
+                                    // D's `^^` with an integer exponent is std.math.pow(F, int):
+                                    // repeated squaring, s^^2 = s*s, s^^3 = s*(s*s),
+                                    // s^^5 = s*((s*s)*(s*s)); ^^0.5 is the square root
+                                    const double xs = x + 0., ys = y + 0.0;
+                                    const double x2 = xs * xs, y2 = ys * ys;
+                                    const double r = std::sqrt(x2 + y2);
+                                    const double r5 = r * ((r * r) * (r * r));
+                                    const double h = 0.82 / 2;
+                                    const double c = (0.1 * (h * (h * h))) / (2.0 * r5);
+                                    s.B[0] = -c * (2.0 * x2 - y2);
+                                    s.B[1] = -c * ((3.0 * xs) * ys);
                                 }
                             }
                             F[depth_index(b, face, -1 - n, p, q)] = s;

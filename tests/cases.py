@@ -212,6 +212,35 @@ def orszag_tang(n=(512, 512, 4), seed=99, precision="fp64", cleaning=True):
     return c
 
 
+def mhd_slip_dipole(n=(64, 48, 4), seed=31, precision="fp64"):
+    """Ideal MHD (hlle + GLM, gamma 5/3, R 1) in x in [-0.5, 0.5], y in [0.45, 1.2],
+    z in [0, 4/64]: slip walls on the y and z faces, periodic in x.  Every wall ghost
+    with |x| < 0.4136 takes the dipole field of internal_copy_then_reflect.d:140-143
+    (the y-min wall sits at r >= 0.45 from the dipole, so the field stays moderate).
+    Uniform rho 1, p 1 with 1% density noise, v = (0.2, 0.05 sin 2 pi x, 0),
+    B = (0.1, 0.05 cos 2 pi x, 0.02)."""
+    R = 1.0
+    c = Case("mhd_slip_dipole", dict(flux_calculator="hlle", MHD=1, divergence_cleaning=1, stringent_cfl=1,
+                                     flux_precision=precision, dt_init=2e-3, dt_max=5e-3), R, 5.0 / 3.0)
+    nic, njc, nkc = n
+    dx, dy = 1.0 / nic, 0.75 / njc
+    dz = dx
+    x0, y0 = -0.5, 0.45
+    rng = np.random.default_rng(seed)
+    x = x0 + (np.arange(nic) + 0.5) * dx
+    X = np.broadcast_to(x[None, None, :], (nkc, njc, nic))
+    rho = _noisy_rho(rng, 1.0, (nkc, njc, nic))
+    T = 1.0 / (rho * R)
+    vel = (np.full(X.shape, 0.2), 0.05 * np.sin(2 * np.pi * X), np.zeros(X.shape))
+    B = (np.full(X.shape, 0.1), 0.05 * np.cos(2 * np.pi * X), np.full(X.shape, 0.02))
+    bcs = {"west": ("exchange_over_full_face", dict(other=0, other_face="east")),
+           "east": ("exchange_over_full_face", dict(other=0, other_face="west")),
+           "south": ("wall_with_slip", {}), "north": ("wall_with_slip", {}),
+           "bottom": ("wall_with_slip", {}), "top": ("wall_with_slip", {})}
+    c.add_block(n, (dx, dy, dz), (x0, y0, 0.0), bcs, rho, vel, T, B=B)
+    return c
+
+
 # ---------------------------------------------------------------- builders
 _ORACLE_BC = {"wall_with_slip": "wall_with_slip", "outflow_simple_extrapolate": "extrapolate",
               "inflow_supersonic": "inflow_supersonic", "exchange_over_full_face": "exchange",

@@ -156,6 +156,66 @@ def test_rollout_gradients_smooth_configuration():
                       ((1e-6, 1e-4), (1e-7, 2e-5)))
 
 
+def test_rollout_theta_drives_every_inflow_face():
+    """The rollout's inflow state theta = (p, T, vel.x) is the state of every
+    supersonic-inflow face in the forward: at a theta other than the configured one,
+    on a lattice with two inflow faces, the rollout's final state equals (bit for bit)
+    a run of a simulation configured with theta, and dJ/dtheta -- the cotangents of
+    both faces summed -- matches central differences in p and T (limiter and clipping
+    off, so the differences converge quadratically)."""
+    from gdfv.autograd import rollout, step_dt
+    smooth = dict(apply_limiter=False, extrema_clipping=False)
+    inf = cases.inflow_state_m3()
+
+    def make(inflow):
+        c = cases.multiblock_lattice(nb=(1, 2, 1), sizes=(16,), seed=3)
+        c.config.update(smooth)
+        for b in c.blocks:
+            if b["bcs"]["west"][0] == "inflow_supersonic":
+                b["bcs"]["west"] = ("inflow_supersonic", dict(inflow=inflow))
+        return c
+
+    def state(s):
+        return np.concatenate([s.get_conserved(b) for b in range(2)], axis=1)
+
+    def load(s, U):
+        n = U.shape[1] // 2
+        for b in range(2):
+            s.set_conserved(b, U[:, b * n:(b + 1) * n])
+
+    inf2 = dict(inf, p=inf["p"] * 1.05, T=inf["T"] * 0.98)
+    _, sim = cases.build_pair(make(inf))
+    assert sim.n_inflow == 2
+    U0np = state(sim)
+    U0 = torch.from_numpy(U0np).cuda()
+    theta = torch.tensor([inf2["p"], inf2["T"], inf2["vel"][0]], dtype=torch.float64, requires_grad=True)
+    wts = torch.from_numpy(np.random.default_rng(5).standard_normal(U0np.shape)).cuda()
+    nsteps = 8
+    UN = rollout(sim, U0.clone(), theta, nsteps, 4)
+    (UN * wts).sum().backward()
+
+    sim2 = cases.build_gpu(make(inf2))
+    load(sim2, U0np)
+    dts = []
+    for _ in range(nsteps):
+        assert sim2.run(max_step=1) == 1
+        dts.append(sim2.time()["dt"])
+    assert np.array_equal(UN.detach().cpu().numpy(), state(sim2))
+
+    def J_of(inflow):
+        s = cases.build_gpu(make(inflow))
+        X = U0
+        for dt in dts:
+            X = step_dt(s, X, dt)
+        return float((X * wts).sum())
+
+    for comp, key in ((0, "p"), (1, "T")):
+        h = 1e-6 * inf2[key]
+        fd = (J_of(dict(inf2, **{key: inf2[key] + h})) - J_of(dict(inf2, **{key: inf2[key] - h}))) / (2 * h)
+        ad = float(theta.grad[comp])
+        assert abs(fd - ad) <= 1e-4 * abs(fd), (key, fd, ad)
+
+
 def test_step_chain_and_fused_step_adjoint():
     """gdfv_steps_dt equals repeated gdfv_step_dt bit for bit (states and predictor
     states), and gdfv_step_adjoint equals the predictor-corrector adjoint composed

@@ -34,8 +34,9 @@ def compare_fp64(case, orc, sim):
     return worst
 
 
-@pytest.mark.parametrize("nsteps", [1, 20])
+@pytest.mark.parametrize("nsteps", [1, 20, 100])
 def test_c1_shock_box_fp64(nsteps):
+    """The 32^3 shock box at 1, 20 and its configured 100 steps."""
     case = cases.c1_shock_box(n=32)
     orc, sim = run_both(case, nsteps)
     assert compare_fp64(case, orc, sim) <= TOL_FP64
@@ -137,6 +138,56 @@ def test_c3_lattice_uneven_blocks_fp64():
     assert compare_fp64(case, orc, sim) <= TOL_FP64
 
 
+def _lattice_full_sizes():
+    # the batched multi-block configuration at its full size range: 64 blocks on a 4x4x4
+    # lattice, per-axis sizes drawn by seed 2024 from {16,32,48,64,96,128} (14.6 M cells)
+    return dict(nb=(4, 4, 4), sizes=(16, 32, 48, 64, 96, 128), seed=2024)
+
+
+def test_c3_lattice_full_sizes_fp64():
+    """The 64-block lattice at its full size range, FP64, persistent launch: bit-level
+    parity with the oracle after 2 steps on every block."""
+    case = cases.multiblock_lattice(**_lattice_full_sizes())
+    orc, sim = run_both(case, 2, persistent=True)
+    assert compare_fp64(case, orc, sim) <= TOL_FP64
+
+
+def test_c3_lattice_full_sizes_fp32():
+    """The float-flux form on the same 64-block lattice, with the schedule the
+    library's autotuner picks (as the throughput measurement runs it), against the
+    FP64 oracle: relative L2 of rho, momentum (pooled) and energy <= 1e-6 after 3 steps."""
+    case = cases.multiblock_lattice(precision="fp32", **_lattice_full_sizes())
+    orc, sim = cases.build_pair(case, autotune=True)
+    assert orc.run(3) == 0
+    assert sim.run(max_step=3) == 3
+    Uo = np.concatenate([orc.get_U(b) for b in range(len(case.blocks))], axis=1)
+    Ug = np.concatenate([sim.get_conserved(b) for b in range(len(case.blocks))], axis=1)
+    errs = [cases.rel_l2(Ug[0], Uo[0]), cases.rel_l2(Ug[1:4].ravel(), Uo[1:4].ravel()), cases.rel_l2(Ug[4], Uo[4])]
+    assert max(errs) <= TOL_FP32_L2, errs
+
+
+def test_mhd_slip_wall_dipole_fp64():
+    """MHD with slip walls whose ghosts cross |x| < 0.4136, where the wall ghost takes
+    the dipole field of internal_copy_then_reflect.d:140-143: bit-level parity."""
+    case = cases.mhd_slip_dipole()
+    orc, sim = run_both(case, 20)
+    assert compare_fp64(case, orc, sim) <= TOL_FP64
+    # the dipole branch is live: the wall ghosts' field differs from the mirrored cell's
+    b = case.blocks[0]
+    assert b["origin"][0] < -0.4136 and b["origin"][0] + b["n"][0] * b["d"][0] > 0.4136
+
+
+def test_mhd_slip_wall_dipole_fp32():
+    case = cases.mhd_slip_dipole(precision="fp32")
+    orc, sim = cases.build_pair(case, fixed_time_step=True, dt_init=2e-3, dt_max=2e-3)
+    assert orc.run(20, fixed_dt=2e-3) == 0
+    assert sim.run(max_step=20) == 20
+    Uo, Ug = orc.get_U(0), sim.get_conserved(0)
+    errs = [cases.rel_l2(Ug[0], Uo[0]), cases.rel_l2(Ug[1:4].ravel(), Uo[1:4].ravel()), cases.rel_l2(Ug[4], Uo[4]),
+            cases.rel_l2(Ug[5:8].ravel(), Uo[5:8].ravel())]
+    assert max(errs) <= TOL_FP32_L2, errs
+
+
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 def test_schedule_does_not_change_results(precision):
     """Tile k-chunk, launch form and the autotuner's choice change who computes a
@@ -195,6 +246,40 @@ def test_failed_step_retry_and_abort_match_oracle(cfl, extra):
         # oracle statuses: -3 too many bad cells, -2 failed after max attempts
         assert code == (GDFV_ERR_BAD_CELLS if rc == -3 else GDFV_ERR_STEP_FAILED), (rc, code)
         print(f"cfl {cfl}: status rc={rc} code={code}")
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_failed_step_reports_the_bad_cell(precision):
+    """A failed step names its cell as the reference's invalid-cell report does
+    (e4/fluidblock.d:607-675: block id, cell id, position): one cell of block 1 of a
+    two-block lattice at rest moves at 1000 m/s against flowstate_limits_max_velocity
+    800, so check_data fails there after the predictor and the run stops with
+    GDFV_ERR_BAD_CELLS; gdfv_last_bad_cell and the message give that cell."""
+    from gdfv._lib import GDFV_ERR_BAD_CELLS, GDFV_ERR_STATE, GdfvError
+    case = cases.multiblock_lattice(nb=(2, 1, 1), sizes=(16,), seed=8, precision=precision)
+    case.blocks[0]["bcs"]["west"] = ("outflow_simple_extrapolate", dict(x_order=0))
+    for b in case.blocks:
+        b["vel"] = (0.0, 0.0, 0.0)
+    case.config.update(flowstate_limits_max_velocity=800.0)
+    sim = cases.build_gpu(case)
+    with pytest.raises(GdfvError) as nothing:
+        sim.last_bad_cell()
+    assert nothing.value.code == GDFV_ERR_STATE
+    i, j, k = 5, 7, 3
+    U = sim.get_conserved(1)
+    c = i + 16 * (j + 16 * k)
+    U[4, c] += 0.5 * U[0, c] * 1000.0 ** 2
+    U[1, c] = U[0, c] * 1000.0
+    sim.set_conserved(1, U)
+    with pytest.raises(GdfvError) as err:
+        sim.run(max_step=2)
+    assert err.value.code == GDFV_ERR_BAD_CELLS
+    blk, ijk, pos = sim.last_bad_cell()
+    assert (blk, ijk) == (1, (i, j, k))
+    b = case.blocks[1]
+    expect = [b["origin"][d] + (ijk[d] + 0.5) * b["d"][d] for d in range(3)]
+    assert np.allclose(pos, expect, rtol=0, atol=1e-15)
+    assert f"blk-id= 1 cell-id= {c} (i,j,k)= ({i},{j},{k})" in str(err.value)
 
 
 @pytest.mark.parametrize("case_name", ["inflow_partial", "shock_box"])
