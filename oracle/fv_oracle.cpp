@@ -164,6 +164,11 @@ static void fill_ghosts(const Sim& sim, std::vector<std::vector<FlowState<T>>>& 
                                                F[depth_index(b, face, -2, p, q)], edge, cfg.mhd);
                         }
                         break;
+                    case BC_USER_GHOST:   // user_defined_effects.d:243-308: the states the UDF returns
+                        for (int n = 0; n < 2; ++n)
+                            F[depth_index(b, face, -1 - n, p, q)] =
+                                promote<T>(bc.ghost[((size_t)n * nq_ + q) * np + p]);
+                        break;
                     case BC_INFLOW: {
                         FlowState<T> s = promote<T>(bc.inflow);
                         F[depth_index(b, face, -1, p, q)] = s;
@@ -288,7 +293,9 @@ static void eval_dUdt(const Sim& sim, std::vector<std::vector<FlowState<T>>>& fs
                     double a = outsign * area[d];
                     si -= flux[d][fidx[fc] * nq + q] * a;
                 }
-                R[(size_t)c * nq + q] = vol_inv * si + 0.0;
+                // dUdt = vol_inv * integral + Q (fvcell.d:824-856); Q: the user-defined source
+                // (add_udf_source_vector, fvcell.d:1263-1267), zero without one
+                R[(size_t)c * nq + q] = vol_inv * si + (b.Q.empty() ? 0.0 : b.Q[(size_t)c * nq + q]);
             }
         }
     }
@@ -651,6 +658,43 @@ int orc_set_bc(int h, int blk, int face, int type, int x_order, int other_blk, i
         if (!update_thermo_from_pT(g, fs) || !update_sound_speed(g, fs)) return -1;
         bc.inflow = fs;
     }
+    return 0;
+}
+
+// Ghost states of a face from the caller (UserDefinedGhostCell): pTv[(layer*nq_ + q)*np + p][5] =
+// p, T, vel.x, vel.y, vel.z; each becomes a FlowState by update_thermo_from_pT and
+// update_sound_speed (user_defined_effects.d:175-240).
+int orc_set_ghost_states(int h, int blk, int face, const double* pTv) {
+    Sim* s = get(h);
+    if (!s || blk < 0 || blk >= (int)s->blocks.size() || face < 0 || face > 5 || !pTv) return -1;
+    Block& b = s->blocks[blk];
+    int np, nq_;
+    face_extent(b, face, np, nq_);
+    Gas g = s->gas();
+    BoundaryCondition& bc = b.bc[face];
+    bc.type = BC_USER_GHOST;
+    bc.ghost.assign((size_t)2 * np * nq_, FlowState<double>());
+    for (size_t m = 0; m < bc.ghost.size(); ++m) {
+        FlowState<double>& fs = bc.ghost[m];
+        const double* v = pTv + 5 * m;
+        fs.p = v[0]; fs.Tg = v[1];
+        fs.vel[0] = v[2]; fs.vel[1] = v[3]; fs.vel[2] = v[4];
+        if (!update_thermo_from_pT(g, fs) || !update_sound_speed(g, fs)) { s->last_error = "bad ghost state"; return -1; }
+    }
+    return 0;
+}
+
+// Fixed source term of every cell of a block, SoA [nq][ncells] (the user-defined source
+// terms Qudf of a steady manufactured solution, added in time_derivatives).
+int orc_set_source(int h, int blk, const double* Q) {
+    Sim* s = get(h);
+    if (!s || blk < 0 || blk >= (int)s->blocks.size() || !Q) return -1;
+    Block& b = s->blocks[blk];
+    const int nq = s->nq();
+    const size_t N = b.ncells();
+    b.Q.assign(N * nq, 0.0);
+    for (size_t c = 0; c < N; ++c)
+        for (int q = 0; q < nq; ++q) b.Q[c * nq + q] = Q[q * N + c];
     return 0;
 }
 

@@ -44,7 +44,7 @@ inline cplx exp_(const cplx& x) { return std::exp(x); }
 enum FluxCalc { FLUX_AUSMDV = 0, FLUX_HLLC = 1, FLUX_HLLE = 2 };
 enum Scheme { SCHEME_EULER = 0, SCHEME_PC = 1, SCHEME_TVD_RK3 = 2 };
 enum BcType { BC_SLIP_WALL = 0, BC_EXTRAPOLATE = 1, BC_INFLOW = 2, BC_EXCHANGE = 3, BC_FIXED_P = 4, BC_FIXED_PT = 5,
-              BC_SIMPLE_FLUX = 6 };
+              BC_SIMPLE_FLUX = 6, BC_USER_GHOST = 7 };
 enum FaceId { WEST = 0, EAST = 1, SOUTH = 2, NORTH = 3, BOTTOM = 4, TOP = 5 };  // geom nomenclature.d:12-19
 
 // Conserved-quantity indices, e4/conservedquantities.d:148-197 (standard ordering, 3D or MHD)
@@ -567,6 +567,9 @@ struct BoundaryCondition {
     int other_face = -1;
     FlowState<double> inflow;        // FlowStateCopy state
     double p_out = 0.0, T_out = 0.0; // GhostCellFixedP / GhostCellFixedPT (fixed_p.d, fixed_pt.d)
+    // UserDefinedGhostCell (e4/bc/ghost_cell_effect/user_defined_effects.d:108-308): ghost
+    // states given by the caller, [layer][q][p] over the face (face_extent order)
+    std::vector<FlowState<double>> ghost;
 };
 
 struct Block {
@@ -586,6 +589,7 @@ struct Block {
     std::vector<FlowState<double>> fs;   // padded
     std::vector<double> U[4];            // interior, cell-major: U[l][c*n + q]
     std::vector<double> dUdt[4];
+    std::vector<double> Q;               // fixed source term per cell, cell-major (empty: none)
     double length(int d) const { return d == 0 ? dx : (d == 1 ? dy : dz); }
 };
 

@@ -49,6 +49,8 @@ def lib():
         L.orc_jvp_real.argtypes = [ctypes.c_int, dp, dp, ctypes.c_double, dp, dp]
         L.orc_face_flux.argtypes = [ctypes.c_int, ctypes.c_int, dp, ctypes.c_double, dp]
         L.orc_last_error.argtypes = [ctypes.c_int, ctypes.c_char_p, ctypes.c_int]
+        L.orc_set_ghost_states.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, dp]
+        L.orc_set_source.argtypes = [ctypes.c_int, ctypes.c_int, dp]
         _LIB = L
     return _LIB
 
@@ -95,7 +97,40 @@ class OracleSim:
     def add_block(self, nic, njc, nkc, dx, dy, dz, x0=0.0, y0=0.0, z0=0.0):
         b = self.L.orc_add_block(self.h, nic, njc, nkc, dx, dy, dz, x0, y0, z0)
         self.blocks.append((nic, njc, nkc))
+        self.geometry = getattr(self, "geometry", []) + [((dx, dy, dz), (x0, y0, z0))]
         return b
+
+    def ghost_positions(self, blk, face):
+        """Centres of the two ghost layers beyond a face, [layer][q][p] x (x, y, z), in
+        the face's (p, q) order: p along axis (d+1)%3, q along (d+2)%3 (d the face's axis)."""
+        f = FACES[face] if isinstance(face, str) else face
+        d, plus = f // 2, f % 2
+        n = self.blocks[blk]
+        (ln, org) = self.geometry[blk]
+        a1, a2 = (d + 1) % 3, (d + 2) % 3
+        out = np.zeros((2, n[a2], n[a1], 3))
+        for layer in range(2):
+            idx = n[d] + layer if plus else -1 - layer
+            for q in range(n[a2]):
+                for p in range(n[a1]):
+                    ijk = [0, 0, 0]
+                    ijk[d], ijk[a1], ijk[a2] = idx, p, q
+                    out[layer, q, p] = [org[c] + (ijk[c] + 0.5) * ln[c] for c in range(3)]
+        return out
+
+    def set_ghost_states(self, blk, face, pTv):
+        """Ghost states of a face given by the caller (as UserDefinedGhostCell supplies
+        them): pTv [2][q][p][5] = p, T, vel.x, vel.y, vel.z, positions as ghost_positions."""
+        f = FACES[face] if isinstance(face, str) else face
+        arr = np.ascontiguousarray(pTv, dtype=np.float64)
+        if self.L.orc_set_ghost_states(self.h, blk, f, _p(arr)) != 0:
+            raise ValueError("bad ghost states")
+
+    def set_source(self, blk, Q):
+        """Fixed per-cell source term [nq][ncells] added to dU/dt (user-defined source)."""
+        arr = np.ascontiguousarray(Q, dtype=np.float64)
+        if self.L.orc_set_source(self.h, blk, _p(arr)) != 0:
+            raise ValueError("bad source")
 
     def set_bc(self, blk, face, kind, x_order=0, other_block=-1, other_face=-1, inflow=None):
         """inflow: dict with p, T, vel=(3,), B=(3,), psi (FlowState:new{p=,T=,...})."""

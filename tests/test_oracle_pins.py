@@ -3,6 +3,11 @@
 * the reference's own integration-test answers (tests/golden/reference_job_answers.json):
   examples/eilmer/3D/sod-shock-tube/sg/sod-test.rb and
   examples/eilmer/2D/MHDShockTube/MHD-ShockTube-Test.rb;
+* the reference's 2D Euler method-of-manufactured-solutions smoke test
+  (examples/eilmer/2D/manufactured-solution/sg/smoke-tests/mms-euler-test.rb): steps
+  to t = 60 ms and the density error norms, which pin the Eilmer-4 branches that the
+  chicken golden switches off (entropy fix, face-frame velocity, the cell-centre sound
+  speed kept through the rhou update, predictor-corrector);
 * the reference's own compiled chicken solver: a golden run committed in
   tests/golden/chicken_lattice.npz (made by tests/golden/make_golden.py), and a
   live run when oracle/_ref/chkn-run has been built here.
@@ -135,3 +140,77 @@ def test_oracle_matches_chicken_live_periodic():
     flows, _, _ = cj.run(job, 1.0e-8, 15)
     s, index = _oracle_for_chicken_job(job, 1.0e-8, 15)
     _compare_with_chicken(s, index, flows, 1e-12)
+
+
+def mms_euler_oracle():
+    """examples/eilmer/2D/manufactured-solution/sg/smoke-tests with case-euler.txt
+    (mms.lua, case 1): 2D, 16 x 16 cells on the unit square as 2 x 2 blocks of 8 x 8
+    (FBArray nib = njb = 2, full-face exchange inside), ausmdv, interpolation order 2
+    with limiter and extrema clipping off, predictor-corrector, stringent CFL 0.5,
+    dt_init 1e-6, ideal gas R = 287, gamma = 1.4; initial state p = 1e5, T = p/R,
+    vel = (800, 800); west and south faces: ghost cells from the manufactured solution
+    (UserDefinedBC), north and east: OutFlowBC_SimpleExtrapolate xOrder 1; the
+    manufactured source terms in every cell.  Fields from tests/golden/mms_euler_16.npz
+    (tests/golden/make_mms.py)."""
+    from oracle import OracleSim
+    g = np.load(os.path.join(GOLDEN, "mms_euler_16.npz"))
+    R, gamma = float(g["R"]), float(g["gamma"])
+    s = OracleSim(R=R, gamma=gamma, flux_calculator="ausmdv", dimensions=2, apply_limiter=0, extrema_clipping=0,
+                  stringent_cfl=1, cfl_value=0.5, dt_init=1.0e-6)
+    n, h = 8, 1.0 / 16
+    for bj in range(2):
+        for bi in range(2):
+            s.add_block(n, n, 1, h, h, 1.0, 0.5 * bi, 0.5 * bj, 0.0)
+    idx = lambda bi, bj: bi + 2 * bj
+    for bj in range(2):
+        for bi in range(2):
+            b = idx(bi, bj)
+            if bi == 0:
+                s.set_ghost_states(b, "west", g["ghost_west"][:, None, bj * n:(bj + 1) * n, :])
+            else:
+                s.set_bc(b, "west", "exchange", other_block=idx(0, bj), other_face="east")
+            if bi == 1:
+                s.set_bc(b, "east", "extrapolate", x_order=1)
+            else:
+                s.set_bc(b, "east", "exchange", other_block=idx(1, bj), other_face="west")
+            if bj == 0:
+                s.set_ghost_states(b, "south", g["ghost_south"][:, bi * n:(bi + 1) * n, None, :])
+            else:
+                s.set_bc(b, "south", "exchange", other_block=idx(bi, 0), other_face="north")
+            if bj == 1:
+                s.set_bc(b, "north", "extrapolate", x_order=1)
+            else:
+                s.set_bc(b, "north", "exchange", other_block=idx(bi, 1), other_face="south")
+            p0 = 1.0e5
+            T0 = p0 / R
+            s.set_flow_rhoT(b, p0 / (T0 * R), (800.0, 800.0, 0.0), T0)
+            Q = g["Q"][:, bj * n:(bj + 1) * n, bi * n:(bi + 1) * n].reshape(5, n * n)
+            s.set_source(b, Q)
+    s.init()
+    return s, g
+
+
+def test_oracle_e4_mode_pinned_by_mms_euler():
+    """mms-euler-test.rb: 2620 +/- 3 steps to t = 60 ms, and the volume-weighted norms of
+    the density error against the manufactured solution (flowsolution.d:305-345:
+    L1 = sum V|e| / sum V, L2 = sqrt(sum V e^2 / sum V), Linf = max |e|) within a
+    relative 1e-3 of L1 = 5.992287970340e-04, L2 = 8.134693405237e-04,
+    Linf = 2.746228919538e-03 (mms-euler-test.rb:38, :47-62).  The oracle takes exactly
+    2620 steps and meets the three norms to about 1e-11 relative (the reference prints
+    13 significant digits); asserted at 1e-9 as well as at the reference's 1e-3."""
+    s, g = mms_euler_oracle()
+    assert s.run(100000, max_time=60.0e-3) == 0, s.last_error()
+    steps = s.time()["step"]
+    assert abs(steps - 2620) < 3, steps
+    assert steps == 2620
+    n = 8
+    err = np.zeros((16, 16))
+    for bj in range(2):
+        for bi in range(2):
+            rho = s.get_flow(bi + 2 * bj)["rho"].reshape(n, n)
+            err[bj * n:(bj + 1) * n, bi * n:(bi + 1) * n] = rho - g["rho_exact"][bj * n:(bj + 1) * n, bi * n:(bi + 1) * n]
+    norms = {"L1": np.mean(np.abs(err)), "L2": np.sqrt(np.mean(err ** 2)), "Linf": np.max(np.abs(err))}
+    refs = {"L1": 5.992287970340e-04, "L2": 8.134693405237e-04, "Linf": 2.746228919538e-03}
+    for k, ref in refs.items():
+        assert abs(norms[k] - ref) / ref < 1.0e-3, (k, norms[k], ref, steps)
+        assert abs(norms[k] - ref) / ref < 1.0e-9, (k, norms[k], ref)
