@@ -344,8 +344,31 @@ static double block_L_min(const Config& cfg, const Block& b) {
 }
 
 // e4/simcore_gasdynamic_step.d:60-160 with e4/fluidblock.d:998-1095
+// chicken's rule (src/chicken/simulate.cu:206-221 with block.cu:979-990 estimate_allowed_dt
+// and cell.cu:156-164 estimate_local_dt): dt_init until the first check; every cfl_count
+// steps after step 0, dt = min(1.5 dt, min over cells of cfl min(L/(|v.n| + a))) over the
+// cell lengths and unit face normals of each index direction.
+static void chicken_time_step_size(Sim& sim) {
+    const Config& cfg = sim.cfg;
+    if (!(sim.step > 0 && (sim.step % cfg.cfl_count) == 0)) return;
+    double smallest = std::numeric_limits<double>::max();
+    for (auto& b : sim.blocks)
+        for (int k = 0; k < b.nkc; ++k)
+            for (int j = 0; j < b.njc; ++j)
+                for (int i = 0; i < b.nic; ++i) {
+                    const FlowState<double>& fs = b.fs[b.pidx(i, j, k)];
+                    const double isig = b.dx / (std::fabs(fs.vel[0]) + fs.a);
+                    const double jsig = b.dy / (std::fabs(fs.vel[1]) + fs.a);
+                    const double ksig = b.dz / (std::fabs(fs.vel[2]) + fs.a);
+                    smallest = std::fmin(smallest, cfg.cfl * std::fmin(std::fmin(isig, jsig), ksig));
+                }
+    sim.dt_allow = smallest;
+    sim.dt_global = std::fmin(1.5 * sim.dt_global, smallest);
+}
+
 static void determine_time_step_size(Sim& sim) {
     const Config& cfg = sim.cfg;
+    if (cfg.chicken_compat) { chicken_time_step_size(sim); return; }
     bool do_dt_check_now = (sim.step % cfg.cfl_count) == 0;
     if (!do_dt_check_now) return;
     double cfl_allow = sim.n_stages() == 1 ? 0.9 : (sim.n_stages() == 2 ? 1.2 : 1.6);

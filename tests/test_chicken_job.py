@@ -130,3 +130,166 @@ def test_loaded_job_matches_oracle_and_writes_back(tmp_path):
         assert np.allclose(back[b]["velx"], U[1] / U[0], rtol=1e-14, atol=0)
     with open(os.path.join(d, "times.data")) as f:
         assert f.read().split()[-2] == "1"
+
+
+# ---------------------------------------------------------------- the reference's own job
+FFS = os.path.join(ROOT, "tests", "golden", "ffs_job")
+FACE_NAMES = {"iminus": "west", "iplus": "east", "jminus": "south", "jplus": "north", "kminus": "bottom",
+              "kplus": "top"}
+OPPOSITE = {"west": "east", "east": "west", "south": "north", "north": "south", "bottom": "top", "top": "bottom"}
+
+
+def oracle_from_job(jobdir, chicken_mode):
+    """The oracle set up from a chicken job directory as gdfv.chicken.load_job reads it:
+    active blocks with their grid's spacing and origin, face tags (missing tags are slip
+    walls), the tagged inflow states and the flow file's rho, T and velocity.
+    chicken_mode: chicken's own scheme (TVD-RK3, global-frame velocity, no clipping or
+    entropy fix, recomputed sound speed, chicken's dt rule); else the Eilmer-4 options
+    the GPU path computes with."""
+    from oracle import OracleSim
+    job = chicken.ChickenJob(jobdir)
+    cfg = job.cfg
+    opts = dict(flux_calculator="ausmdv", R=job.R, gamma=job.gamma, cfl_value=float(cfg["cfl_values"][0]),
+                dt_init=float(cfg.get("dt_init", 1e-6)), cfl_count=int(cfg.get("cfl_count", 10)))
+    if chicken_mode:
+        opts.update(gasdynamic_update_scheme="tvd_rk3", chicken_compat=1, apply_entropy_fix=0, extrema_clipping=0)
+    s = OracleSim(**opts)
+    blocks = job.active_blocks()
+    index = {b: n for n, b in enumerate(blocks)}
+    geom = {}
+    for b in blocks:
+        nic, njc, nkc = job.shape(b)
+        path = os.path.join(jobdir, "grid", f"grid-{b[0]:04d}-{b[1]:04d}-{b[2]:04d}.gz")
+        d, origin = chicken.uniform_geometry(chicken.read_grid(path, nic, njc, nkc), path)
+        geom[b] = (d, origin)
+        s.add_block(nic, njc, nkc, *d, *origin)
+    for b in blocks:
+        for face in chicken.FACES:
+            bc = job.blocks[b]["bcs"].get(face, {"tag": "wall_with_slip"})
+            name = FACE_NAMES[face]
+            if bc["tag"] == "exchange":
+                s.set_bc(index[b], name, "exchange", other_block=index[job.neighbour(b, face)],
+                         other_face=OPPOSITE[name])
+            elif bc["tag"] == "inflow":
+                fs = job.flow_states[bc["flow_state_index"]]
+                s.set_bc(index[b], name, "inflow_supersonic", inflow=dict(p=fs["p"], T=fs["T"], vel=fs["vel"]))
+            elif bc["tag"] == "outflow":
+                s.set_bc(index[b], name, "extrapolate")
+            else:
+                assert bc["tag"] == "wall_with_slip", bc
+                s.set_bc(index[b], name, "wall_with_slip")
+    for b in blocks:
+        nic, njc, nkc = job.shape(b)
+        fl = chicken.read_flow(os.path.join(jobdir, "flow", "t0000", f"flow-{b[0]:04d}-{b[1]:04d}-{b[2]:04d}.gz"),
+                               nic * njc * nkc, job.iovars)
+        shp = (nkc, njc, nic)
+        s.set_flow_rhoT(index[b], fl["rho"].reshape(shp), tuple(fl[v].reshape(shp) for v in ("velx", "vely", "velz")),
+                        fl["T"].reshape(shp))
+    s.init()
+    return s, job, index, geom
+
+
+def shock_position(p, x):
+    """examples/chicken/test_chicken.py:45-71: along the bottom row of block (0,0,0), the
+    first cell whose pressure exceeds the freestream by 1%, and the position where the
+    pressure, interpolated linearly from the cell before, reaches the normal-shock value
+    1047025 Pa; returns (position, one cell width)."""
+    p0 = p[0]
+    idx = int(np.argmax(p > p0 + 0.01 * p0))
+    assert idx != 0
+    xp, pp, xs, ps = x[idx - 1], p[idx - 1], x[idx], p[idx]
+    pn = 1047025.00
+    return (xs - xp) / (ps - pp) * (pn - pp) + xp, xs - xp
+
+
+FFS_SHOCK_X = 0.41369441539674984   # examples/chicken/test_chicken.py:70
+
+
+def test_ffs_job_shock_position_chicken_scheme():
+    """The reference's forward-facing-step job (prepared by its own chkn_prep.py, inactive
+    blocks below the step, slip walls by default) through the oracle in chicken's scheme
+    and dt rule to t = 1 ms: the shock stands where test_chicken.py asserts it, within
+    its tolerance of a tenth of a cell."""
+    s, job, index, geom = oracle_from_job(FFS, chicken_mode=True)
+    assert len(index) == 21 and len(job.blocks) == 25
+    assert s.run(job.cfg["max_step"], max_time=job.cfg["max_time"]) == 0
+    nic, njc, nkc = job.shape((0, 0, 0))
+    p = s.get_flow(index[(0, 0, 0)])["p"].reshape(nkc, njc, nic)[0, 0, :]
+    (dx, _, _), (x0, _, _) = geom[(0, 0, 0)]
+    x = x0 + (np.arange(nic) + 0.5) * dx
+    xn, cell = shock_position(p, x)
+    assert abs(xn - FFS_SHOCK_X) < 0.1 * cell, (xn, FFS_SHOCK_X, s.time())
+
+
+def test_ffs_job_oracle_matches_live_chicken(tmp_path):
+    """The same job run by the reference's compiled chicken (CPU build, when present here)
+    for 25 steps -- through two dt checks -- against the oracle in chicken's scheme:
+    every block, every field to 1e-12 of the field's scale (the grid files' vertices
+    differ from uniform spacing in the last bits)."""
+    import shutil
+    import subprocess
+    if not cj.available():
+        pytest.skip("oracle/_ref/chkn-run not built")
+    d = str(tmp_path / "ffs")
+    shutil.copytree(FFS, d)
+    import json
+    with open(os.path.join(d, "config.json")) as f:
+        cfg = json.load(f)
+    cfg["max_step"] = 25
+    with open(os.path.join(d, "config.json"), "w") as f:
+        json.dump(cfg, f)
+    # chicken's binary files (same values as the gzipped text): the flow is written back
+    # at full precision (the text format keeps 6 significant digits)
+    job = chicken.ChickenJob(d)
+    for b in job.blocks:
+        nic, njc, nkc = job.shape(b)
+        name = f"{b[0]:04d}-{b[1]:04d}-{b[2]:04d}"
+        verts = chicken.read_grid(os.path.join(d, "grid", f"grid-{name}.gz"), nic, njc, nkc)
+        hdr = np.array([3.0, 0.0, 0.0, nic + 1, njc + 1, nkc + 1])
+        with open(os.path.join(d, "grid", f"grid-{name}.bin"), "wb") as f:
+            f.write(hdr.tobytes() + np.ascontiguousarray(verts.reshape(-1, 3)).tobytes())
+        fl = chicken.read_flow(os.path.join(d, "flow", "t0000", f"flow-{name}.gz"), nic * njc * nkc, job.iovars)
+        np.concatenate([fl[v] for v in job.iovars]).tofile(os.path.join(d, "flow", "t0000", f"flow-{name}.bin"))
+    r = subprocess.run([cj.EXE, "--job=ffs", "--binary"], capture_output=True, text=True, cwd=str(tmp_path))
+    assert r.returncode == 0, r.stdout[-400:] + r.stderr[-400:]
+    tdirs = sorted(x for x in os.listdir(os.path.join(d, "flow")) if x.startswith("t"))
+    s, job, index, _ = oracle_from_job(FFS, chicken_mode=True)
+    assert s.run(25) == 0
+    for b, n in index.items():
+        nic, njc, nkc = job.shape(b)
+        fc = chicken.read_flow(os.path.join(d, "flow", tdirs[-1], f"flow-{b[0]:04d}-{b[1]:04d}-{b[2]:04d}.bin"),
+                               nic * njc * nkc, job.iovars)
+        fo = s.get_flow(n)
+        speed = np.max(np.hypot(fc["velx"], fc["vely"]))
+        for key, ck in (("rho", "rho"), ("vx", "velx"), ("vy", "vely"), ("p", "p"), ("T", "T")):
+            # velocity components against the speed (chicken's vertex-derived face normals
+            # leave ~1e-13 m/s in the components that are zero on the exact grid)
+            scale = speed if key in ("vx", "vy") else np.max(np.abs(fc[ck]))
+            assert np.max(np.abs(fo[key] - fc[ck])) <= 1e-12 * scale, (b, key)
+
+
+@pytest.mark.gpu
+def test_ffs_job_on_gpu_matches_oracle():
+    """The reference's forward-facing-step job dir loaded unchanged by gdfv.chicken (21
+    active blocks, 4 inactive; inflow, exchange, outflow and default slip-wall tags) and
+    run in FP64 on the GPU: per-cell agreement with the oracle set up from the same
+    directory (Eilmer-4 options) to 1e-12 after 40 steps; then on to t = 1 ms, where the
+    GPU path's shock (Eilmer's predictor-corrector, clipping and entropy fix) stands
+    within one cell of the position chicken's scheme gives."""
+    sim, job = chicken.load_job(FFS)
+    s, _, index, geom = oracle_from_job(FFS, chicken_mode=False)
+    assert set(index) == set(job.index)
+    for b, n in index.items():   # the same conserved start on both sides
+        sim.set_conserved(job.index[b], s.get_U(n))
+        assert s.set_U(n, s.get_U(n)) == 0
+    assert s.run(40) == 0
+    assert sim.run(max_step=40) == 40
+    for b, n in index.items():
+        errs = cases.cell_errors(sim.get_conserved(job.index[b]), s.get_U(n), False)
+        assert max(errs.values()) <= 1e-12, (b, errs)
+    sim.run(max_step=job.cfg["max_step"], max_time=job.cfg["max_time"])
+    nic, njc, nkc = job.shape((0, 0, 0))
+    p = sim.get_flow(job.index[(0, 0, 0)])["p"].reshape(nkc, njc, nic)[0, 0, :]
+    (dx, _, _), (x0, _, _) = geom[(0, 0, 0)]
+    xn, cell = shock_position(p, x0 + (np.arange(nic) + 0.5) * dx)
+    assert abs(xn - FFS_SHOCK_X) < cell, (xn, FFS_SHOCK_X)
