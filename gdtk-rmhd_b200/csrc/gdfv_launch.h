@@ -52,9 +52,20 @@ inline int tile_rows_corrector(int precision, bool mhd) {
     return precision == 0 ? (mhd ? TJ_FP64_MHD : TJ_FP64_CORR) : (mhd ? TJ_FP32_MHD_CORR : TJ_FP32_CORR);
 }
 
+// Options under which the float-flux Euler stages run the kernel on decoded float
+// primitives (gdfv_stage_f32.cuh) when the arguments carry primitive buffers: the
+// defaults (limiter and extrema clipping on, e4 epsilon), no outflow boundary with a
+// flux or ghost rule of its own, 3D.
+inline bool float_euler_path(const NumParams& P) {
+    return !P.mhd && P.apply_limiter && P.extrema_clipping && !P.lmr_epsilon && !P.outflow_bcs && P.dims == 3;
+}
+
 // Launch one stage (0 = residual only, 1 = predictor, 2 = corrector) over A.n_tiles tiles.
 cudaError_t launch_stage_fp64(int stage, int flux, bool mhd, const StageArgs& A, cudaStream_t s);
 cudaError_t launch_stage_fp32(int stage, int flux, bool mhd, const StageArgs& A, cudaStream_t s);
+// Float primitives (rho, vel, u, a; SoA [6][total]) of the state U, for the float
+// Euler path, enqueued on stream s.
+void prims_f32(const double* U, long long total, const NumParams& P, float* Pout, cudaStream_t s);
 // Raise the dynamic shared-memory limit of every instantiation (once per device).
 cudaError_t configure_stage_fp64();
 cudaError_t configure_stage_fp32();

@@ -252,6 +252,9 @@ struct Context {
     int adj_ready = 0;
     long long adj_scratch_n = 0;
     cudaStream_t aux_stream[2] = {nullptr, nullptr};  // lowest / highest priority streams of the rollout adjoint
+    float* prim[2] = {nullptr, nullptr};  // float primitives of U[0], U[1] (float Euler path)
+    float* prim1 = nullptr;            // float primitives of the predictor state
+    bool prims_valid = false;          // prim[parity] holds the primitives of the current state
     long long last_bad_cell = -1;      // global index of the cell the last failure reported (-1: none)
     std::vector<double> h_inflow;      // supersonic-inflow states as uploaded, 9 doubles each (p, T, vel, B, psi)
     Control* step_ctl = nullptr;       // control record of gdfv_step_dt
@@ -262,7 +265,7 @@ struct Context {
         if (graph) cudaGraphExecDestroy(graph);
         for (void* p : {(void*)U[0], (void*)U[1], (void*)dU0, (void*)d_blocks, (void*)d_tiles, (void*)d_inflow,
                         (void*)d_ctl, (void*)d_maxsig, (void*)d_lastsig, (void*)d_bad, (void*)adj_scratch, (void*)jvp_scratch,
-                        (void*)norm_scratch,
+                        (void*)norm_scratch, (void*)prim[0], (void*)prim[1], (void*)prim1,
                         (void*)step_ctl, (void*)step_maxsig, (void*)step_lastsig})
             if (p) cudaFree(p);
         if (h_ctl) cudaFreeHost(h_ctl);
@@ -365,13 +368,40 @@ StageArgs stage_args(Context* c) {
     return A;
 }
 
+// Arguments of the context's own stepping (gdfv_run, the autotuner, gdfv_time_stages):
+// with the float Euler path, the primitive buffers of the state buffers it steps
+// (state_parity: which of U[0], U[1] the control record's step parity 0 names).
+StageArgs stage_args_run(Context* c, int state_parity = 0) {
+    StageArgs A = stage_args(c);
+    if (c->prim[0]) {
+        A.prim[0] = c->prim[state_parity];
+        A.prim[1] = c->prim[state_parity ^ 1];
+        A.prim1 = c->prim1;
+    }
+    return A;
+}
+
+int read_ctl(Context* c);
+
+// Float primitives of the current state for the float Euler path, when the state was
+// set from outside a stage since they were last made.
+int ensure_prims(Context* c) {
+    if (!c->prim[0] || c->prims_valid) return GDFV_OK;
+    if (read_ctl(c)) return GDFV_ERR_CUDA;
+    const int parity = c->h_ctl->step & 1;
+    prims_f32(c->U[parity], c->total, c->P, c->prim[parity], c->stream);
+    CK(cudaGetLastError());
+    c->prims_valid = true;
+    return GDFV_OK;
+}
+
 cudaError_t launch_stage(Context* c, int stage, const StageArgs& A) {
     if (c->cfg.precision == 0) return launch_stage_fp64(stage, c->cfg.flux, c->cfg.mhd, A, c->stream);
     return launch_stage_fp32(stage, c->cfg.flux, c->cfg.mhd, A, c->stream);
 }
 
 cudaError_t enqueue_step(Context* c) {
-    StageArgs A = stage_args(c);
+    StageArgs A = stage_args_run(c);
     step_begin_kernel<<<1, 1, 0, c->stream>>>(c->d_ctl, c->d_blocks, c->d_maxsig, c->d_lastsig, c->sp);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -611,6 +641,13 @@ int do_prepare(Context* c) {
     CK(cudaMemset(c->U[0], 0, bytes));
     CK(cudaMemset(c->U[1], 0, bytes));
     CK(cudaMemset(c->dU0, 0, bytes));
+    if (g.precision == 1 && float_euler_path(c->P)) {
+        const size_t pbytes = sizeof(float) * 6 * (size_t)c->total;
+        CK(cudaMalloc(&c->prim[0], pbytes));
+        CK(cudaMalloc(&c->prim[1], pbytes));
+        CK(cudaMalloc(&c->prim1, pbytes));
+    }
+    c->prims_valid = false;
     CK(cudaMalloc(&c->d_blocks, sizeof(BlockDesc) * c->h_blocks.size()));
     CK(cudaMemcpy(c->d_blocks, c->h_blocks.data(), sizeof(BlockDesc) * c->h_blocks.size(), cudaMemcpyHostToDevice));
     CK(cudaMalloc(&c->d_tiles, sizeof(TileDesc) * tiles.size()));
@@ -986,8 +1023,8 @@ int gdfv_config_get_double(int ctx, const char* key, double* value) {
     else if (k == "autotune") *value = g.autotune;
     else if (k == "autotune_stage_ms") *value = c->tune_ms;
     else if (k == "tile_rows") *value = tile_rows(g.precision, g.mhd);
-    else if (k == "tile_rows_corrector")
-        *value = c->n_tiles2 > 0 ? tile_rows_corrector(g.precision, g.mhd) : tile_rows(g.precision, g.mhd);
+    else if (k == "tile_rows_corrector")   // the float Euler path runs both stages on the first table
+        *value = c->n_tiles2 > 0 && !c->prim[0] ? tile_rows_corrector(g.precision, g.mhd) : tile_rows(g.precision, g.mhd);
     else return fail(c, GDFV_ERR_ARG, "unknown real option: " + k);
     return GDFV_OK;
 }
@@ -1094,6 +1131,7 @@ int gdfv_block_set_flow_rhoT(int ctx, int blk, const double* prim) {
     if (e != cudaSuccess) return cuda_fail(c, e, "set_flow_rhoT");
     if (bad) return fail(c, GDFV_ERR_ARG, "initial state has T <= 0 or rho <= 0");
     c->signal_valid = false;
+    c->prims_valid = false;
     return GDFV_OK;
 }
 
@@ -1111,6 +1149,7 @@ int gdfv_block_set_conserved(int ctx, int blk, const double* U) {
                            c->stream));
     CK(cudaStreamSynchronize(c->stream));
     c->signal_valid = false;
+    c->prims_valid = false;
     return GDFV_OK;
 }
 
@@ -1287,7 +1326,7 @@ int autotune(Context* c) {
         int st = upload_tiles(c, tiles, n1, n2);
         if (st) { cudaEventDestroy(e0); cudaEventDestroy(e1); return st; }
         for (int pers = 1; pers >= 0 && e == cudaSuccess; --pers) {
-            StageArgs A = stage_args(c);
+            StageArgs A = stage_args_run(c, parity);
             A.Ubuf[0] = c->U[parity];
             A.Ubuf[1] = c->U[parity ^ 1];
             A.ctl = c->step_ctl;
@@ -1336,6 +1375,7 @@ int gdfv_run(int ctx, int max_steps, double max_time, int* steps_taken) {
     if (!c->signal_valid) {
         if ((st = scan_signal(c)) != GDFV_OK) return st;
     }
+    if ((st = ensure_prims(c)) != GDFV_OK) return st;
     if (c->cfg.autotune && !c->tuned) {
         if ((st = autotune(c)) != GDFV_OK) return st;
     }
@@ -1440,6 +1480,7 @@ int gdfv_set_time(int ctx, double time, int step, double dt_global) {
     c->h_ctl->retrying = 0;
     if (write_ctl(c)) return GDFV_ERR_CUDA;
     c->signal_valid = false;
+    c->prims_valid = false;
     return GDFV_OK;
 }
 
@@ -1609,6 +1650,7 @@ int gdfv_state_device_ptr(int ctx, double** U_dev) {
     if (!U_dev) return fail(c, GDFV_ERR_ARG, "null pointer");
     if (read_ctl(c)) return GDFV_ERR_CUDA;
     *U_dev = c->U[c->h_ctl->step & 1];
+    c->prims_valid = false;   // the caller may write the state through the pointer
     return GDFV_OK;
 }
 
@@ -1629,6 +1671,7 @@ int gdfv_time_stages(int ctx, int reps, double* ms) {
     if (st) return st;
     if (reps < 1 || !ms) return fail(c, GDFV_ERR_ARG, "bad argument");
     if (!c->signal_valid && (st = scan_signal(c)) != GDFV_OK) return st;
+    if ((st = ensure_prims(c)) != GDFV_OK) return st;
     if (read_ctl(c)) return GDFV_ERR_CUDA;
     Control saved = *c->h_ctl;
     // a step that cannot halt: the kernels run, the step counter does not move
@@ -1638,7 +1681,7 @@ int gdfv_time_stages(int ctx, int reps, double* ms) {
     c->h_ctl->n_fail = 0;
     c->h_ctl->n_invalid1 = 0;
     if (write_ctl(c)) return GDFV_ERR_CUDA;
-    StageArgs A = stage_args(c);
+    StageArgs A = stage_args_run(c);
     cudaEvent_t e0, e1, e2;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));

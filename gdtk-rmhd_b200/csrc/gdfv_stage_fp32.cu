@@ -9,4 +9,5 @@
 #define GDFV_TJ_MHD_CORR TJ_FP32_MHD_CORR
 #define GDFV_LAUNCH launch_stage_fp32
 #define GDFV_CONFIGURE configure_stage_fp32
+#define GDFV_FLOAT_EULER_PATH 1
 #include "gdfv_stage_inst.cuh"

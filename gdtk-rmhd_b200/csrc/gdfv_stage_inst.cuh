@@ -4,6 +4,9 @@
 // corrector rows), GDFV_TJ_MHD, GDFV_TJ_MHD_CORR, GDFV_LAUNCH and
 // GDFV_CONFIGURE first.
 #include "gdfv_launch.h"
+#if GDFV_FLOAT_EULER_PATH
+#include "gdfv_stage_f32.cuh"
+#endif
 
 namespace gdfv {
 
@@ -21,6 +24,11 @@ template <bool MHD>
 constexpr int rows() { return MHD ? TJ_M : TJ_E; }
 template <bool MHD>
 constexpr int rows_corrector() { return MHD ? TJ_M2 : TJ_E2; }
+
+template <class K>
+cudaError_t set_smem(K k, size_t bytes) {
+    return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
 
 // Resident CTAs on the device (CTAs per SM x SMs) of the persistent
 // instantiation: the grid of the persistent launch.
@@ -48,8 +56,47 @@ cudaError_t launch_rows(const StageArgs& A, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+#if GDFV_FLOAT_EULER_PATH
+// The float Euler kernel on decoded primitives (gdfv_stage_f32.cuh) over the first tile
+// table (rows TJ_E in both stages).
+template <int STAGE, int FLUX, int PERS>
+int& resident_f32() {
+    static int v = 0;
+    return v;
+}
+
+template <int STAGE, int FLUX>
+cudaError_t launch_f32(const StageArgs& A, cudaStream_t s) {
+    using G = GeoF<TJ_E>;
+    const int cap = resident_f32<STAGE, FLUX, 1>();
+    if (A.persistent && cap > 0)
+        stage_f32_kernel<STAGE, FLUX, TJ_E, 1><<<cap < A.n_tiles ? cap : A.n_tiles, G::NT, G::bytes, s>>>(A);
+    else
+        stage_f32_kernel<STAGE, FLUX, TJ_E, 0><<<A.n_tiles, G::NT, G::bytes, s>>>(A);
+    return cudaGetLastError();
+}
+
+template <int STAGE, int FLUX>
+cudaError_t configure_f32(int n_sm) {
+    using G = GeoF<TJ_E>;
+    cudaError_t e = set_smem(stage_f32_kernel<STAGE, FLUX, TJ_E, 0>, G::bytes);
+    if (e == cudaSuccess) e = set_smem(stage_f32_kernel<STAGE, FLUX, TJ_E, 1>, G::bytes);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, stage_f32_kernel<STAGE, FLUX, TJ_E, 1>, G::NT, G::bytes);
+    if (e != cudaSuccess) return e;
+    resident_f32<STAGE, FLUX, 1>() = per_sm * n_sm;
+    return cudaSuccess;
+}
+#endif
+
 template <int STAGE, bool MHD, int FLUX>
 cudaError_t launch_one(const StageArgs& A, cudaStream_t s) {
+#if GDFV_FLOAT_EULER_PATH
+    if constexpr (!MHD && STAGE >= 1) {
+        if (A.prim[0] && float_euler_path(A.P)) return launch_f32<STAGE, FLUX>(A, s);
+    }
+#endif
     if constexpr (STAGE == 2 && rows_corrector<MHD>() != rows<MHD>()) {
         if (A.n_tiles2 > 0) {   // the corrector's own tile table follows the first
             StageArgs A2 = A;
@@ -59,11 +106,6 @@ cudaError_t launch_one(const StageArgs& A, cudaStream_t s) {
         }
     }
     return launch_rows<STAGE, MHD, FLUX, rows<MHD>()>(A, s);
-}
-
-template <class K>
-cudaError_t set_smem(K k, size_t bytes) {
-    return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
 template <int STAGE, bool MHD, int FLUX, int TJ>
@@ -84,6 +126,10 @@ cudaError_t configure_rows(int n_sm) {
 template <int STAGE, bool MHD, int FLUX>
 cudaError_t configure_one(int n_sm) {
     cudaError_t e = configure_rows<STAGE, MHD, FLUX, rows<MHD>()>(n_sm);
+#if GDFV_FLOAT_EULER_PATH
+    if constexpr (!MHD && STAGE >= 1)
+        if (e == cudaSuccess) e = configure_f32<STAGE, FLUX>(n_sm);
+#endif
     if constexpr (STAGE == 2 && rows_corrector<MHD>() != rows<MHD>())
         if (e == cudaSuccess) e = configure_rows<2, MHD, FLUX, rows_corrector<MHD>()>(n_sm);
     return e;
@@ -118,6 +164,12 @@ cudaError_t GDFV_LAUNCH(int stage, int flux, bool mhd, const StageArgs& A, cudaS
     }
     return cudaErrorInvalidValue;
 }
+
+#if GDFV_FLOAT_EULER_PATH
+void prims_f32(const double* U, long long total, const NumParams& P, float* Pout, cudaStream_t s) {
+    prims_f32_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(U, total, P, Pout);
+}
+#endif
 
 cudaError_t GDFV_CONFIGURE() {
     int dev = 0, n_sm = 0;

@@ -363,11 +363,12 @@ def test_get_conserved_into_caller_buffer():
 
 
 @pytest.mark.parametrize("flux", ["ausmdv", "hllc"])
-def test_corrector_tile_rows(flux):
-    """The float Euler corrector runs over tiles of its own rows when they fill the
-    block better (here 56 rows: 8 tiles of 7); the results match the oracle as the
-    other float tests do, in the per-tile and the persistent launch form, and the two
-    forms agree to float rounding.  A block height of 16 keeps the shared rows."""
+def test_float_euler_path_launch_forms(flux):
+    """The float Euler stages of the default options run on decoded float primitives
+    over one tile table of 8 rows in both stages (56 rows here: the stencil-decoding
+    kernels would give their corrector 7-row tiles of its own); the results match the
+    oracle as the other float tests do, in the per-tile and the persistent launch form,
+    and the two forms agree to float rounding."""
     case = cases.c2_inflow_box(n=(40, 56, 24), flux=flux)
     orc = cases.build_oracle(case)
     assert orc.run(20) == 0
@@ -375,7 +376,7 @@ def test_corrector_tile_rows(flux):
     states = {}
     for pers in (False, True):
         sim = cases.build_gpu(case, flux_precision="fp32", persistent=pers)
-        assert sim.option("tile_rows") == 8 and sim.option("tile_rows_corrector") == 7
+        assert sim.option("tile_rows") == 8 and sim.option("tile_rows_corrector") == 8
         assert sim.run(max_step=20) == 20
         Ug = sim.get_conserved(0)
         errs = [cases.rel_l2(Ug[0], Uo[0]), cases.rel_l2(Ug[1:4].ravel(), Uo[1:4].ravel()), cases.rel_l2(Ug[4], Uo[4])]
@@ -388,9 +389,6 @@ def test_corrector_tile_rows(flux):
     assert cases.rel_l2(a[0], b[0]) <= 1e-6
     assert cases.rel_l2(a[1:4].ravel(), b[1:4].ravel()) <= 1e-6
     assert cases.rel_l2(a[4], b[4]) <= 1e-6
-    sim = cases.build_gpu(cases.c2_inflow_box(n=(40, 16, 24)), flux_precision="fp32")
-    assert sim.option("tile_rows_corrector") == 8
-    sim.close()
 
 
 def test_calls_with_nothing_to_do():
