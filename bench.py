@@ -47,17 +47,45 @@ def measured_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and throttle reasons sampled during the timed region: NVML polled every
+    2 ms from a thread (nvidia-smi's loop, at 100 ms, when NVML is missing)."""
 
-    def __init__(self, index):
+    REASONS = (("hw_slowdown", 0x8), ("sw_thermal_slowdown", 0x20), ("hw_thermal_slowdown", 0x40),
+               ("sw_power_cap", 0x4))
+
+    def __init__(self, index, interval=0.002):
         self.index = index
-        self.samples = []
+        self.interval = interval
+        self.samples = []   # (sm_mhz, sm_max_mhz, reason bits)
         self.proc = None
+        self._stop = threading.Event()
+        self.thread = None
 
     def __enter__(self):
-        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            smax = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+
+            def poll():
+                while not self._stop.is_set():
+                    try:
+                        sm = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+                        bits = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                        self.samples.append((float(sm), float(smax), int(bits)))
+                    except Exception:
+                        pass
+                    time.sleep(self.interval)
+
+            self.thread = threading.Thread(target=poll, daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            pass
+        q = ("index,clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
                                           "--format=csv,noheader,nounits", "-lms", "100"],
@@ -70,29 +98,31 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.samples.append([x.strip() for x in line.split(",")])
+            f = [x.strip() for x in line.split(",")]
+            try:
+                bits = sum(b for (_, b), v in zip(self.REASONS, f[3:7]) if v.lower() == "active")
+                self.samples.append((float(f[1]), float(f[2]), bits))
+            except Exception:
+                pass
 
     def __exit__(self, *a):
+        self._stop.set()
         if self.proc:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
+        if self.thread is not None:
+            self.thread.join(timeout=2)
 
     def summary(self):
         if not self.samples:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = set()
-        for s in self.samples:
-            for n, v in zip(names, s[5:9]):
-                if v.strip().lower() == "active":
-                    reasons.add(n)
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(self.samples)}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [s[0] for s in self.samples]
+        reasons = sorted({n for s in self.samples for n, b in self.REASONS if s[2] & b})
+        return {"sm_mhz": float(np.median(sm)), "sm_min_mhz": float(min(sm)), "sm_max_mhz": max(s[1] for s in self.samples),
+                "reasons": reasons, "samples": len(self.samples)}
 
 
 def max_over_ranks(value, device="cpu"):
@@ -133,6 +163,26 @@ def chicken_baseline(steps, warmup):
     except Exception:
         return None
     return chicken_job.bench(exe, steps=steps, warmup=warmup)
+
+
+def chicken_gpu_leg(n=128, steps=1000, warmup=20):
+    """The reference's own GPU solver (chicken's CUDA build for sm_100a,
+    oracle/_ref/chkn-run-gpu: FP64, AUSMDV x_order 2, TVD-RK3, one thread per cell and
+    per face) on the same M=3 inflow box as one block, timed on this GPU: per-step time
+    from the difference of a short and a long run (start-up and binary job I/O cancel).
+    Reported per step and per stage (TVD-RK3 takes 3 stages a step, the
+    predictor-corrector 2)."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "chkn-run-gpu")
+    if not os.path.exists(exe):
+        return {"unavailable": "oracle/_ref/chkn-run-gpu not built (make -C oracle chicken_gpu)"}
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import chicken_job
+    r = chicken_job.bench(exe, steps=steps, warmup=warmup, n=n, nblk=(1, 1, 1))
+    per_step = r["value"]
+    return dict(value=per_step, unit=UNIT, value_per_stage=per_step * 3,
+                workload=f"M=3 inflow box {n}^3 as one block, FP64, TVD-RK3 (3 stages per step)",
+                how=r["cpu_baseline"]["sample"].replace("reference chicken CPU build (oracle/_ref/chkn-run, "
+                                                        "OpenMP over blocks)", "reference chicken GPU build"))
 
 
 def adjoint_over_forward(nsteps=50, checkpoint_every=10, shape=(128, 128, 64), autotune=False):
@@ -429,15 +479,14 @@ def main():
     peak, peak_kind = measured_peaks()
     ach2 = BYTES_STAGE2 * cells / (st2 * 1e-3) / 1e9
     traffic = None
-    # ncu DRAM bytes per cell of the corrector the run launches (its own 7-row tiles or
-    # the shared 8-row ones), captured on a smaller case
-    tf = os.path.join(ROOT, "profiles", "stage_kernel_fp32_corrector7_128x112x128.md"
-                      if sim32.option("tile_rows_corrector") == 7 else "stage_kernel_fp32_128cube.md")
+    # ncu DRAM bytes per cell of the corrector (float Euler kernel on decoded primitives),
+    # captured on a 256x128x128 case with the same tiles, scaled to this launch's cells
+    tf = os.path.join(ROOT, "profiles", "stage_f32_kernel_256x128x128.md")
     if os.path.exists(tf):
         import re
         with open(tf) as f:
             m = re.search(r"stage2_dram_bytes_per_cell:\s*([0-9.]+)", f.read())
-        if m:   # ncu DRAM bytes per cell of the corrector at 128^3, scaled to this launch
+        if m:
             traffic = float(m.group(1)) * cells
 
     # end to end through the public API: host state in, K steps, host state out
@@ -480,7 +529,7 @@ def main():
         "fp32_over_fp64": val32 / val64,
         "rel_l2_vs_fp64": err,
         "adjoint_over_forward": None,
-        "roofline": {"bound": "hbm", "kernel": "stage_kernel<2,float> (corrector)", "achieved": ach2,
+        "roofline": {"bound": "hbm", "kernel": "stage_f32_kernel<2> (corrector)", "achieved": ach2,
                      "peak": peak, "unit": "GB/s", "frac": ach2 / peak, "traffic": traffic,
                      "peak_source": peak_kind, "algorithmic_bytes_per_cell": BYTES_STAGE2,
                      "stage_ms": [st1, st2]},
@@ -504,7 +553,8 @@ def main():
                 ("accuracy_other_flux", lambda: accuracy_leg(None, n, "hllc" if args.flux == "ausmdv" else "ausmdv",
                                                              acc_steps, stream)),
                 ("multiblock", lambda: multiblock_leg(stream)),
-                ("mhd", lambda: mhd_leg(stream))]
+                ("mhd", lambda: mhd_leg(stream)),
+                ("chicken_gpu", chicken_gpu_leg)]
         for name, fn in legs:
             try:
                 line[name] = fn()
@@ -513,6 +563,10 @@ def main():
             torch.cuda.empty_cache()
         if isinstance(line.get("adjoint"), dict) and "ratio" in line["adjoint"]:
             line["adjoint_over_forward"] = line["adjoint"]["ratio"]
+        cg = line.get("chicken_gpu")
+        if isinstance(cg, dict) and "value" in cg:   # this library's FP64 form against the reference's GPU code
+            cg["fp64_plain_over_chicken_gpu_per_step"] = line["fp64_plain"]["value"] / cg["value"]
+            cg["fp64_plain_over_chicken_gpu_per_stage"] = 2 * line["fp64_plain"]["value"] / cg["value_per_stage"]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         # the reference's own CPU build when present (kind "reference"), the oracle port beside it
         try:
