@@ -301,9 +301,12 @@ __global__ void __launch_bounds__(32 * (TJ + 1), GDFV_MINB_F32E) stage_f32_kerne
             // ---------------- A: copies of the lead plane k+3 (own columns) and the halo of plane
             // k+1 into the ring, in flight during B (slot k+3 held plane k-1, last read in C of
             // plane k-1; the halo positions of slot k+1 are read first in B of plane k+1)
-            const bool lead_in = active && k + 3 < n2;
+            // (only while a plane k+1 follows in this tile: then k+3 <= n2+1, a ghost at most one
+            // layer deep, and k+1 < n2 lies inside the block)
+            const bool more = k + 1 < t.k1;
+            const bool lead_in = active && more && k + 3 < n2;
             if (lead_in) cp_async_pf(slot(k + 3), PLANE, pidx, Pin, total, boff + (c_own + 3 * pstride));
-            if (h_in) cp_async_pf(nx1, PLANE, h_dst, Pin, total, boff + c_halo);
+            if (h_in && more) cp_async_pf(nx1, PLANE, h_dst, Pin, total, boff + c_halo);
             cp_async_commit();
 
             // ---------------- B: i and j reconstruction
@@ -364,8 +367,9 @@ __global__ void __launch_bounds__(32 * (TJ + 1), GDFV_MINB_F32E) stage_f32_kerne
                 }
             }
             // ghosts of A (boundary tiles), then the copies complete
-            if (active && !lead_in) put_pf(slot(k + 3), PLANE, pidx, ghost_pf(A, Pin, B, t.i0 + lane, t.j0 + warp, k + 3));
-            if (h_on && !h_in) put_pf(nx1, PLANE, h_dst, ghost_pf(A, Pin, B, h_ci, h_cj, k + 1));
+            if (active && more && !lead_in)
+                put_pf(slot(k + 3), PLANE, pidx, ghost_pf(A, Pin, B, t.i0 + lane, t.j0 + warp, k + 3));
+            if (h_on && more && !h_in) put_pf(nx1, PLANE, h_dst, ghost_pf(A, Pin, B, h_ci, h_cj, k + 1));
             cp_async_wait<0>();
             __syncthreads();
 
