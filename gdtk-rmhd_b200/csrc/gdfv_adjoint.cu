@@ -649,6 +649,10 @@ bool vjp_supported(int ctx, const AdjView& v) {
                                "and van_albada_variant=e4");
         return false;
     }
+    if (v.P.graded) {
+        adjoint_set_error(ctx, "the adjoint supports uniform Cartesian blocks (no graded blocks)");
+        return false;
+    }
     for (const BlockDesc& B : v.h_blocks)
         for (int f = 0; f < 6; ++f)
             if (B.bc_type[f] == BC_FIXED_P || B.bc_type[f] == BC_FIXED_PT || B.bc_type[f] == BC_SIMPLE_FLUX) {

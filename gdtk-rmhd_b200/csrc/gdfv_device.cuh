@@ -23,6 +23,17 @@ enum : int { ST_OK = 0, ST_DECODE_FAILED = 1, ST_TOO_MANY_BAD_CELLS = 2 };
 // weights of the l2r2 reconstruction for one index direction (e4/onedinterp.d:338-355),
 // precomputed on the host because every cell of a block has the same lengths
 enum : int { W_AL0 = 0, W_AR0, W_LENL0, W_LENR0, W_TOL, W_TOC, W_TOR, W_TWOL, W_TWOR, W_N };
+// per-cell weights of a graded block along one index direction: the two interface values
+// of cell c (face c+1/2 left state, face c-1/2 right state) come from l2r2_prepare's
+// weights of those two faces, which are these expressions of len(c-1), len(c), len(c+1)
+enum : int { GW_TOL = 0,  // 2/(len_c + len_{c-1})
+             GW_TOC,      // 2/(len_{c+1} + len_c)
+             GW_A,        // 0.5 len_c / (len_{c-1} + 2 len_c + len_{c+1})  (aL0 of face c+1/2, aR0 of c-1/2)
+             GW_TWOL,     // 2 len_c + len_{c-1}
+             GW_LENR0,    // len_{c+1}
+             GW_LENL0,    // len_{c-1}
+             GW_TWOR,     // 2 len_c + len_{c+1}
+             GW_N };
 
 struct GasParams {
     double R, gamma, Cv, Cvinv;
@@ -38,6 +49,7 @@ struct NumParams {
     int nq;
     int lmr_epsilon;    // van Albada epsilon scaled per face (lmr/onedinterp.d:147-151)
     int outflow_bcs;    // some face has OutFlowBC_FixedP, _FixedPT or _SimpleFlux
+    int graded;         // some block has cell lengths varying along an axis
 };
 
 // Fixed ghost state of a supersonic-inflow face (FlowStateCopy, flow_state_copy.d:92-107)
@@ -56,7 +68,11 @@ struct BlockDesc {
     double x0, y0, z0;
     double w[3][W_N];     // l2r2 weights per direction
     int bc_type[6], bc_xorder[6], bc_other[6], bc_other_face[6], bc_inflow[6];
-    int pad1_;
+    int graded;           // rectilinear block with cell lengths varying along each axis
+    // graded: cell lengths of cells -2 .. n+1 (index c + 2), ghosts as the boundary gives
+    // them, and the l2r2 weights of cells -1 .. n (index (c + 1) * GW_N), per direction
+    const double* glen[3];
+    const double* gw[3];
 };
 
 struct TileDesc {
@@ -87,6 +103,17 @@ struct Prim {
 };
 
 // ---------------------------------------------------------------- small helpers
+// Cell lengths of cell (i, j, k) of a block (the same for every cell of a uniform block).
+__device__ __forceinline__ void cell_lengths(const BlockDesc& B, int i, int j, int k, double* L) {
+    if (B.graded) {
+        L[0] = B.glen[0][i + 2];
+        L[1] = B.glen[1][j + 2];
+        L[2] = B.glen[2][k + 2];
+    } else {
+        L[0] = B.len[0]; L[1] = B.len[1]; L[2] = B.len[2];
+    }
+}
+
 __device__ __forceinline__ double d_add(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ double d_mul(double a, double b) { return __dmul_rn(a, b); }
 
@@ -389,8 +416,9 @@ __device__ __forceinline__ bool check_data(const NumParams& P, const Prim<double
 }
 
 // e4/fvcell.d:975-1059 signal_frequency on a Cartesian structured block
-__device__ __forceinline__ double signal_frequency(const NumParams& P, const BlockDesc& B, const Prim<double>& s) {
-    const double iL = B.len[0], jL = B.len[1], kL = B.len[2];
+// L: the cell's lengths in the i, j and k directions.
+__device__ __forceinline__ double signal_frequency(const NumParams& P, const double* L, const Prim<double>& s) {
+    const double iL = L[0], jL = L[1], kL = L[2];
     double signal = 0.0;
     double un_N = fabs(s.v[1]);
     double un_E = fabs(s.v[0]);
@@ -417,7 +445,8 @@ __device__ __forceinline__ double signal_frequency(const NumParams& P, const Blo
         double B_mag_sq = s.B[0] * s.B[0] + s.B[1] * s.B[1] + s.B[2] * s.B[2];
         double ca2 = B_mag_sq / s.rho;
         double cfast = sqrt(ca2 + s.a * s.a);
-        signal = fmax(signal, (u_mag + cfast) / B.L_min);
+        const double L_min = P.dims == 3 ? fmin(fmin(iL, jL), kL) : fmin(iL, jL);
+        signal = fmax(signal, (u_mag + cfast) / L_min);
     }
     return signal;
 }

@@ -55,9 +55,10 @@ inline int tile_rows_corrector(int precision, bool mhd) {
 // Options under which the float-flux Euler stages run the kernel on decoded float
 // primitives (gdfv_stage_f32.cuh) when the arguments carry primitive buffers: the
 // defaults (limiter and extrema clipping on, e4 epsilon), no outflow boundary with a
-// flux or ghost rule of its own, 3D.
+// flux or ghost rule of its own, no graded block, 3D.
 inline bool float_euler_path(const NumParams& P) {
-    return !P.mhd && P.apply_limiter && P.extrema_clipping && !P.lmr_epsilon && !P.outflow_bcs && P.dims == 3;
+    return !P.mhd && P.apply_limiter && P.extrema_clipping && !P.lmr_epsilon && !P.outflow_bcs && !P.graded &&
+           P.dims == 3;
 }
 
 // Launch one stage (0 = residual only, 1 = predictor, 2 = corrector) over A.n_tiles tiles.

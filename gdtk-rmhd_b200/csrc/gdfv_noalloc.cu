@@ -85,7 +85,11 @@ __global__ void noalloc_signal_kernel(const double* U, long long total, const Bl
         for (int q = 0; q < P.nq; ++q) u[q] = U[q * total + B.offset + c];
         Prim<double> s;
         double p, T;
-        if (decode(P, u, s, p, T) == 0) sig = fmax(sig, signal_frequency(P, B, s));
+        if (decode(P, u, s, p, T) == 0) {
+            double L[3];
+            cell_lengths(B, (int)(c % B.n[0]), (int)((c / B.n[0]) % B.n[1]), (int)(c / ((long long)B.n[0] * B.n[1])), L);
+            sig = fmax(sig, signal_frequency(P, L, s));
+        }
     }
     for (int o = 16; o > 0; o >>= 1) sig = fmax(sig, __shfl_xor_sync(0xffffffffu, sig, o));
     if ((threadIdx.x & 31) == 0) atomicMax(&maxsig[blk], (unsigned long long)__double_as_longlong(sig));

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <climits>
 #include <cmath>
 #include <cstdio>
@@ -171,7 +172,9 @@ __global__ void signal_scan_kernel(const double* U, long long total, const Block
         Prim<double> s;
         double p, T;
         if (decode(P, u, s, p, T) == 0) {
-            sig = signal_frequency(P, B, s);
+            double L[3];
+            cell_lengths(B, (int)(c % B.n[0]), (int)((c / B.n[0]) % B.n[1]), (int)(c / ((long long)B.n[0] * B.n[1])), L);
+            sig = signal_frequency(P, L, s);
             if (c == n - 1) lastsig[blk] = sig;
         } else {
             atomicAdd(bad, 1);
@@ -195,6 +198,9 @@ struct HostBlock {
     double origin[3];
     HostBC bc[6];
     long long offset = 0;
+    std::vector<double> vert[3];   // graded: vertex coordinates along each axis (n + 1 each)
+    bool graded() const { return !vert[0].empty(); }
+    double cell_len(int d, int c) const { return graded() ? vert[d][c + 1] - vert[d][c] : len[d]; }
 };
 
 struct Config {
@@ -249,6 +255,7 @@ struct Context {
     double* adj_scratch = nullptr;     // adjoint work arrays, allocated on first use
     double* jvp_scratch = nullptr;     // Frechet JVP work arrays (U + sigma v, R0, R1, partial sums)
     double* norm_scratch = nullptr;    // per-CTA partials and result of gdfv_residual_norms
+    double* d_geom = nullptr;          // graded blocks: cell lengths and l2r2 weights per direction
     int adj_ready = 0;
     long long adj_scratch_n = 0;
     cudaStream_t aux_stream[2] = {nullptr, nullptr};  // lowest / highest priority streams of the rollout adjoint
@@ -265,7 +272,7 @@ struct Context {
         if (graph) cudaGraphExecDestroy(graph);
         for (void* p : {(void*)U[0], (void*)U[1], (void*)dU0, (void*)d_blocks, (void*)d_tiles, (void*)d_inflow,
                         (void*)d_ctl, (void*)d_maxsig, (void*)d_lastsig, (void*)d_bad, (void*)adj_scratch, (void*)jvp_scratch,
-                        (void*)norm_scratch, (void*)prim[0], (void*)prim[1], (void*)prim1,
+                        (void*)norm_scratch, (void*)prim[0], (void*)prim[1], (void*)prim1, (void*)d_geom,
                         (void*)step_ctl, (void*)step_maxsig, (void*)step_lastsig})
             if (p) cudaFree(p);
         if (h_ctl) cudaFreeHost(h_ctl);
@@ -606,6 +613,54 @@ int do_prepare(Context* c) {
         inflows.push_back(fx.state);
     }
     c->total = off;
+    // graded blocks: cell lengths of cells -2 .. n+1 per direction (ghosts: the partner's
+    // cells across an exchange face, else the block's own interior cell n, as SFluidBlock
+    // gives them, e4/sfluidblock.d:884-1090, simcore_exchange.d:44-70) and the l2r2 weights
+    // of cells -1 .. n; one device buffer for all of them
+    std::vector<double> geom;
+    std::vector<std::array<long long, 6>> geom_at(c->blocks.size());
+    int any_graded = 0;
+    for (size_t b = 0; b < c->blocks.size(); ++b) {
+        const HostBlock& hb = c->blocks[b];
+        if (!hb.graded()) continue;
+        any_graded = 1;
+        if (g.mhd) return fail(c, GDFV_ERR_ARG, "graded blocks are not offered with MHD");
+        if (g.lmr_epsilon) return fail(c, GDFV_ERR_ARG, "graded blocks are not offered with van_albada_variant lmr");
+        double lmin[3];
+        for (int d = 0; d < 3; ++d) {
+            const int n = hb.n[d];
+            std::vector<double> L((size_t)n + 4);
+            for (int cc = 0; cc < n; ++cc) L[(size_t)cc + 2] = hb.cell_len(d, cc);
+            lmin[d] = *std::min_element(L.begin() + 2, L.begin() + 2 + n);
+            for (int side = 0; side < 2; ++side) {
+                const HostBC& bc = hb.bc[2 * d + side];
+                for (int m = 0; m < 2; ++m) {
+                    double v;
+                    if (bc.type == BC_EXCHANGE && 2 * d + side < nfaces) {
+                        const HostBlock& ob = c->blocks[bc.other];
+                        v = ob.cell_len(d, (bc.other_face & 1) ? ob.n[d] - 1 - m : m);
+                    } else {
+                        v = hb.cell_len(d, side ? n - 1 - m : m);
+                    }
+                    L[(size_t)(side ? n + m : -1 - m) + 2] = v;
+                }
+            }
+            geom_at[b][d] = (long long)geom.size();
+            geom.insert(geom.end(), L.begin(), L.end());
+            geom_at[b][3 + d] = (long long)geom.size();
+            for (int cc = -1; cc <= n; ++cc) {
+                const double lm = L[(size_t)cc + 1], l0 = L[(size_t)cc + 2], lp = L[(size_t)cc + 3];
+                // l2r2_prepare (e4/onedinterp.d:338-355) of faces c+1/2 and c-1/2
+                const double wv[GW_N] = {2.0 / (l0 + lm), 2.0 / (lp + l0), 0.5 * l0 / (lm + 2.0 * l0 + lp),
+                                         2.0 * l0 + lm, lp, lm, 2.0 * l0 + lp};
+                geom.insert(geom.end(), wv, wv + GW_N);
+            }
+        }
+        BlockDesc& B = c->h_blocks[b];
+        B.graded = 1;
+        B.x0 = hb.vert[0][0]; B.y0 = hb.vert[1][0]; B.z0 = hb.vert[2][0];
+        B.L_min = g.dims == 3 ? std::min(std::min(lmin[0], lmin[1]), lmin[2]) : std::min(lmin[0], lmin[1]);
+    }
     build_tiles(c, g.tile_kchunk, tiles, c->n_tiles, c->n_tiles2);
     NumParams& P = c->P;
     P.gas.R = g.R; P.gas.gamma = g.gamma; P.gas.Cv = Cv; P.gas.Cvinv = 1.0 / Cv;
@@ -617,6 +672,7 @@ int do_prepare(Context* c) {
     P.mhd = g.mhd; P.divergence_cleaning = g.divergence_cleaning; P.dims = g.dims;
     P.stringent_cfl = g.stringent_cfl; P.nq = c->nq; P.lmr_epsilon = g.lmr_epsilon;
     P.outflow_bcs = outflow_bcs;
+    P.graded = any_graded;
     StepParams& sp = c->sp;
     sp.cfl_count = g.cfl_count; sp.n_stages = 2; sp.fixed_time_step = g.fixed_time_step;
     sp.mhd_cleaning = g.mhd && g.divergence_cleaning;
@@ -648,6 +704,17 @@ int do_prepare(Context* c) {
         CK(cudaMalloc(&c->prim1, pbytes));
     }
     c->prims_valid = false;
+    if (!geom.empty()) {
+        CK(cudaMalloc(&c->d_geom, sizeof(double) * geom.size()));
+        CK(cudaMemcpy(c->d_geom, geom.data(), sizeof(double) * geom.size(), cudaMemcpyHostToDevice));
+        for (size_t b = 0; b < c->h_blocks.size(); ++b) {
+            if (!c->h_blocks[b].graded) continue;
+            for (int d = 0; d < 3; ++d) {
+                c->h_blocks[b].glen[d] = c->d_geom + geom_at[b][d];
+                c->h_blocks[b].gw[d] = c->d_geom + geom_at[b][3 + d];
+            }
+        }
+    }
     CK(cudaMalloc(&c->d_blocks, sizeof(BlockDesc) * c->h_blocks.size()));
     CK(cudaMemcpy(c->d_blocks, c->h_blocks.data(), sizeof(BlockDesc) * c->h_blocks.size(), cudaMemcpyHostToDevice));
     CK(cudaMalloc(&c->d_tiles, sizeof(TileDesc) * tiles.size()));
@@ -1041,6 +1108,27 @@ int gdfv_block_new(int ctx, int nic, int njc, int nkc, double dx, double dy, dou
     b.n[0] = nic; b.n[1] = njc; b.n[2] = nkc;
     b.len[0] = dx; b.len[1] = dy; b.len[2] = dz;
     b.origin[0] = x0; b.origin[1] = y0; b.origin[2] = z0;
+    c->blocks.push_back(b);
+    return (int)c->blocks.size() - 1;
+}
+
+int gdfv_block_new_graded(int ctx, int nic, int njc, int nkc, const double* xv, const double* yv, const double* zv) {
+    Context* c = get_ctx(ctx);
+    if (!c) return fail(nullptr, GDFV_ERR_ARG, "bad context");
+    if (c->prepared) return fail(c, GDFV_ERR_STATE, "blocks are frozen after gdfv_prepare");
+    if (nic < 1 || njc < 1 || nkc < 1 || !xv || !yv || !zv) return fail(c, GDFV_ERR_ARG, "bad block size or vertices");
+    if ((long long)nic * njc * nkc > (1ll << 34)) return fail(c, GDFV_ERR_ARG, "block too large");
+    HostBlock b;
+    b.n[0] = nic; b.n[1] = njc; b.n[2] = nkc;
+    const double* v[3] = {xv, yv, zv};
+    for (int d = 0; d < 3; ++d) {
+        b.vert[d].assign(v[d], v[d] + b.n[d] + 1);
+        for (int cc = 0; cc < b.n[d]; ++cc)
+            if (!(b.vert[d][cc + 1] - b.vert[d][cc] > 0.0))
+                return fail(c, GDFV_ERR_ARG, "vertex coordinates must increase along each axis");
+        b.len[d] = b.vert[d][1] - b.vert[d][0];
+        b.origin[d] = b.vert[d][0];
+    }
     c->blocks.push_back(b);
     return (int)c->blocks.size() - 1;
 }

@@ -447,6 +447,33 @@ __device__ __forceinline__ void recon_cell(const R* w, const R* wf, const NumPar
     }
 }
 
+// recon_cell for a cell of a graded block: the weights g[GW_*] of the cell's position
+// along the direction (e4/onedinterp.d:338-386 with the lengths of cells c-1, c, c+1;
+// the two scaled differences are those of both faces of the cell, as on a uniform grid).
+template <class R, int NRS, bool MHD>
+__device__ __forceinline__ void recon_cell_graded(const double* g, const NumParams& P, const R* qm1, const R* q0,
+                                                  const R* qp1, R* qm, R* qp) {
+    const R tol = R(g[GW_TOL]), toc = R(g[GW_TOC]), a = R(g[GW_A]);
+    const R twoL = R(g[GW_TWOL]), lenR0 = R(g[GW_LENR0]), lenL0 = R(g[GW_LENL0]), twoR = R(g[GW_TWOR]);
+    const R eps = R(P.eps_van_albada);
+#pragma unroll
+    for (int s = 0; s < NRS; ++s) {
+        if (MHD && s == 8 && !P.divergence_cleaning) { qm[s] = q0[s]; qp[s] = q0[s]; continue; }
+        R dm = (q0[s] - qm1[s]) * tol;
+        R dp = (qp1[s] - q0[s]) * toc;
+        R sl = R(1.0);
+        if (P.apply_limiter) sl = (dm * dp + rabs(dm * dp) + eps) / (dm * dm + dp * dp + eps);
+        R vp = q0[s] + sl * a * (dp * twoL + dm * lenR0);
+        R vm = q0[s] - sl * a * (dp * lenL0 + dm * twoR);
+        if (P.extrema_clipping) {
+            vp = clip_fast(vp, q0[s], qp1[s]);
+            vm = clip_fast(vm, qm1[s], q0[s]);
+        }
+        qp[s] = vp;
+        qm[s] = vm;
+    }
+}
+
 // AUSMDV (e4/fluxcalc.d:477-651) for the float-flux ideal-gas variant.  The
 // ideal-gas identities p/rho = (gamma-1) e and H = e + p/rho + ke = gamma e + ke
 // replace the divisions of the general form: alpha = 2 e_L/(e_L + e_R), the
@@ -821,6 +848,14 @@ __global__ void __launch_bounds__(32 * (TJ + 1), MHD ? (sizeof(R) == 4 ? GDFV_MI
         __syncthreads();
 
         auto slot = [&](int kk) -> R* { return ring + (((kk % 3) + 3) % 3) * NPV * PLANE; };
+        // reconstruction of the cell at position pos along direction D (graded blocks take
+        // the weights of that position; only the general kernels have graded blocks)
+        auto recon = [&](int D, int pos, const R* qm1, const R* q0, const R* qp1, R* qm, R* qp) {
+            if (OPT == 0 && B.graded)
+                recon_cell_graded<R, NRS, MHD>(B.gw[D] + (pos + 1) * GW_N, P, qm1, q0, qp1, qm, qp);
+            else
+                recon_cell<R, NRS, MHD, OPT>(w[D], wf[D], P, qm1, q0, qp1, qm, qp);
+        };
 
         R kq_prev_p[NRS];        // k-direction q+ of the current plane (left state of its top face)
         R fB[NQ];                // flux through the bottom face of the owner's cell
@@ -846,7 +881,7 @@ __global__ void __launch_bounds__(32 * (TJ + 1), MHD ? (sizeof(R) == 4 ? GDFV_MI
                 gather<R, NRS, 2>(slot(t.k0 - 2), PLANE, pidx, qm1);
                 gather<R, NRS, 2>(slot(t.k0 - 1), PLANE, pidx, q0);
                 gather<R, NRS, 2>(slot(t.k0), PLANE, pidx, qp1);
-                recon_cell<R, NRS, MHD, OPT>(w[2], wf[2], P, qm1, q0, qp1, qm, kq_prev_p);
+                recon(2, t.k0 - 1, qm1, q0, qp1, qm, kq_prev_p);
                 // plane k0+1 replaces k0-2 in the ring
                 int ck3[2] = {t.k0 + 1, 0};
                 load_two<STAGE, FAST, MHD, NQ, OPT == 0>(A, Uin, B, dt, damp, true, false, ci, cj, ck3, pr);
@@ -855,7 +890,7 @@ __global__ void __launch_bounds__(32 * (TJ + 1), MHD ? (sizeof(R) == 4 ? GDFV_MI
                 gather<R, NRS, 2>(slot(t.k0 - 1), PLANE, pidx, qm1);
                 gather<R, NRS, 2>(slot(t.k0), PLANE, pidx, q0);
                 gather<R, NRS, 2>(slot(t.k0 + 1), PLANE, pidx, qp1);
-                recon_cell<R, NRS, MHD, OPT>(w[2], wf[2], P, qm1, q0, qp1, qkm, qkp);
+                recon(2, t.k0, qm1, q0, qp1, qkm, qkp);
                 face_flux<R, MHD, FLUX, 2, NPV>(P, c_hR, kq_prev_p, qkm, slot(t.k0 - 1), pidx, slot(t.k0), pidx, PLANE,
                                                 fB);
 #pragma unroll
@@ -871,7 +906,6 @@ __global__ void __launch_bounds__(32 * (TJ + 1), MHD ? (sizeof(R) == 4 ? GDFV_MI
         }
 
         double sig_max = 0.0;
-        const double Ai = B.area[0], Aj = B.area[1], Ak = B.area[2];
         double inv_len[3] = {0.0, 0.0, 0.0};
         if (FAST && !MHD && STAGE == 2) { inv_len[0] = 1.0 / B.len[0]; inv_len[1] = 1.0 / B.len[1]; inv_len[2] = 1.0 / B.len[2]; }
         // halo cell of this thread in every plane (4 columns beside, 4 rows above/below
@@ -950,7 +984,7 @@ __global__ void __launch_bounds__(32 * (TJ + 1), MHD ? (sizeof(R) == 4 ? GDFV_MI
                 gather<R, NRS, 2>(cur, PLANE, pidx, qm1);
                 gather<R, NRS, 2>(nx1, PLANE, pidx, q0);
                 gather<R, NRS, 2>(nx2, PLANE, pidx, qp1);
-                recon_cell<R, NRS, MHD, OPT>(w[2], wf[2], P, qm1, q0, qp1, kq_m, kq_p);
+                recon(2, k + 1, qm1, q0, qp1, kq_m, kq_p);
             }
             for (int f = f0; f < NRI + NRJ && f < fend; f += fstride) {
                 R qm1[NRS], q0[NRS], qp1[NRS], qm[NRS], qp[NRS];
@@ -961,7 +995,7 @@ __global__ void __launch_bounds__(32 * (TJ + 1), MHD ? (sizeof(R) == 4 ? GDFV_MI
                     gather<R, NRS, 0>(cur, PLANE, p - 1, qm1);
                     gather<R, NRS, 0>(cur, PLANE, p, q0);
                     gather<R, NRS, 0>(cur, PLANE, p + 1, qp1);
-                    recon_cell<R, NRS, MHD, OPT>(w[0], wf[0], P, qm1, q0, qp1, qm, qp);
+                    recon(0, t.i0 + ci, qm1, q0, qp1, qm, qp);
 #pragma unroll
                     for (int s = 0; s < NRS; ++s) { RI[s * NRI + f] = qm[s]; RI[(NRS + s) * NRI + f] = qp[s]; }
                 } else {
@@ -972,7 +1006,7 @@ __global__ void __launch_bounds__(32 * (TJ + 1), MHD ? (sizeof(R) == 4 ? GDFV_MI
                     gather<R, NRS, 1>(cur, PLANE, p - PW, qm1);
                     gather<R, NRS, 1>(cur, PLANE, p, q0);
                     gather<R, NRS, 1>(cur, PLANE, p + PW, qp1);
-                    recon_cell<R, NRS, MHD, OPT>(w[1], wf[1], P, qm1, q0, qp1, qm, qp);
+                    recon(1, t.j0 + cj, qm1, q0, qp1, qm, qp);
 #pragma unroll
                     for (int s = 0; s < NRS; ++s) { RJ[s * NRJ + g] = qm[s]; RJ[(NRS + s) * NRJ + g] = qp[s]; }
                 }
@@ -1049,10 +1083,24 @@ __global__ void __launch_bounds__(32 * (TJ + 1), MHD ? (sizeof(R) == 4 ? GDFV_MI
             if (active) {
                 const long long g = B.offset + c_own;
                 double dU[NQ];
+                double Ai = B.area[0], Aj = B.area[1], Ak = B.area[2], vol_inv = B.vol_inv;
+                double clen[3] = {B.len[0], B.len[1], B.len[2]};
+                if (OPT == 0 && B.graded) {
+                    // face areas and volume of the own cell from its lengths (uniform: dy dz,
+                    // dz dx, dx dy and 1/(dx dy dz) as the block's own)
+                    cell_lengths(B, t.i0 + ti, t.j0 + tj, k, clen);
+                    if (has_k) {
+                        Ai = d_mul(clen[1], clen[2]); Aj = d_mul(clen[2], clen[0]); Ak = d_mul(clen[0], clen[1]);
+                        vol_inv = 1.0 / d_mul(d_mul(clen[0], clen[1]), clen[2]);
+                    } else {
+                        Ai = clen[1]; Aj = clen[0];
+                        vol_inv = 1.0 / d_mul(clen[0], clen[1]);
+                    }
+                }
                 if (FAST) {
                     // float path: differences of opposite faces in float (same-signed,
                     // nearly equal fluxes subtract exactly), accumulation in FP64
-                    const double Vi = B.vol_inv;
+                    const double Vi = vol_inv;
 #pragma unroll
                     for (int q = 0; q < NQ; ++q) {
                         R dI = FI[q * NFI + ti + (TI + 1) * tj] - FI[q * NFI + ti + 1 + (TI + 1) * tj];
@@ -1077,7 +1125,7 @@ __global__ void __launch_bounds__(32 * (TJ + 1), MHD ? (sizeof(R) == 4 ? GDFV_MI
                         si = __dsub_rn(si, d_mul((double)fB[q], -Ak));
                         si = __dsub_rn(si, d_mul((double)fT[q], Ak));
                     }
-                    dU[q] = d_add(d_mul(B.vol_inv, si), 0.0);
+                    dU[q] = d_add(d_mul(vol_inv, si), 0.0);
                 }
                 if (STAGE == 0) {
 #pragma unroll
@@ -1122,7 +1170,10 @@ __global__ void __launch_bounds__(32 * (TJ + 1), MHD ? (sizeof(R) == 4 ? GDFV_MI
                                       (unsigned long long)g);
                         }
                         if (STAGE == 2) {
-                            double sig = (FAST && !MHD) ? signal_fast(P, inv_len, s) : signal_frequency(P, B, s);
+                            if (FAST && !MHD && OPT == 0 && B.graded) {
+                                inv_len[0] = 1.0 / clen[0]; inv_len[1] = 1.0 / clen[1]; inv_len[2] = 1.0 / clen[2];
+                            }
+                            double sig = (FAST && !MHD) ? signal_fast(P, inv_len, s) : signal_frequency(P, clen, s);
                             sig_max = fmax(sig_max, sig);
                             if (c_own == pstride * B.n[2] - 1) A.last_signal[blk] = sig;
                         }

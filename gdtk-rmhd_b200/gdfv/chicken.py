@@ -13,8 +13,8 @@ chicken (the reference's structured-grid CUDA solver) keeps a job as a directory
   times.data                   "tindx time" lines (simulate.cu:133-147, :176-177)
 
 `load_job` builds a `Simulation` from such a directory: each block becomes a
-uniform Cartesian block (the grid must be axis-aligned with constant spacing per
-block and direction), the face tags map onto this library's boundary conditions
+uniform Cartesian block, or a graded rectilinear one where the spacing varies along
+an axis (the grid must be axis-aligned), the face tags map onto this library's boundary conditions
 (exchange -> full-face exchange with the lattice neighbour, wrapping periodically
 at the lattice edge as chicken's index wrap does (face.cu:22-36); inflow -> supersonic
 inflow of the tagged flow state; outflow -> extrapolation, xOrder 0; wall_with_slip
@@ -80,6 +80,21 @@ def uniform_geometry(verts, path=""):
     if np.max(np.abs(verts - expect)) > 1e-9 * max(d) * max(verts.shape):
         raise ValueError(f"{path}: grid is not an axis-aligned Cartesian block")
     return tuple(d), tuple(float(v) for v in verts[0, 0, 0])
+
+
+def rectilinear_vertices(verts, path=""):
+    """(xv, yv, zv) of an axis-aligned grid whose spacing may vary along each axis (each
+    vertex coordinate depends on its own index only)."""
+    xv, yv, zv = verts[0, 0, :, 0], verts[0, :, 0, 1], verts[:, 0, 0, 2]
+    for axis, line in enumerate((xv, yv, zv)):
+        if not np.all(np.diff(line) > 0):
+            raise ValueError(f"{path}: vertex coordinates along axis {axis} do not increase")
+    Z, Y, X = np.meshgrid(zv, yv, xv, indexing="ij")
+    expect = np.stack([X, Y, Z], axis=-1)
+    scale = max(np.ptp(xv), np.ptp(yv), np.ptp(zv))
+    if np.max(np.abs(verts - expect)) > 1e-12 * scale:
+        raise ValueError(f"{path}: grid is not an axis-aligned rectilinear block")
+    return xv.copy(), yv.copy(), zv.copy()
 
 
 def read_flow(path, ncells, iovars):
@@ -168,9 +183,15 @@ def load_job(jobdir, tindx=0, **config_overrides):
     for b in job.active_blocks():
         nic, njc, nkc = job.shape(b)
         path = os.path.join(jobdir, "grid", _name("grid", *b, job.binary))
-        d, origin = uniform_geometry(read_grid(path, nic, njc, nkc), path)
-        geom[b] = (d, origin)
-        index[b] = sim.add_block(nic, njc, nkc, *d, *origin)
+        verts = read_grid(path, nic, njc, nkc)
+        try:
+            d, origin = uniform_geometry(verts, path)
+            geom[b] = (d, origin)
+            index[b] = sim.add_block(nic, njc, nkc, *d, *origin)
+        except ValueError:   # stretched spacing: a graded rectilinear block
+            xv, yv, zv = rectilinear_vertices(verts, path)
+            geom[b] = (xv, yv, zv)
+            index[b] = sim.add_block_graded(xv, yv, zv)
     for b in job.active_blocks():
         for face in FACES:
             bc = job.blocks[b]["bcs"].get(face, {"tag": "wall_with_slip"})
@@ -216,17 +237,23 @@ def write_flow(sim, job, tindx, time=None):
     cv = R / (g - 1.0)
     for b in job.active_blocks():
         nic, njc, nkc = job.shape(b)
-        (dx, dy, dz), (x0, y0, z0) = job.geom[b]
+        gb = job.geom[b]
+        if len(gb) == 3:   # graded: vertex coordinates per axis
+            cx, cy, cz = (0.5 * (v[1:] + v[:-1]) for v in gb)
+            vol = np.einsum("k,j,i->kji", np.diff(gb[2]), np.diff(gb[1]), np.diff(gb[0])).ravel()
+        else:
+            (dx, dy, dz), (x0, y0, z0) = gb
+            cx, cy, cz = (o + h * (np.arange(m) + 0.5) for o, h, m in ((x0, dx, nic), (y0, dy, njc), (z0, dz, nkc)))
+            vol = np.full(nic * njc * nkc, dx * dy * dz)
         U = sim.get_conserved(job.index[b])
         rho = U[0]
         vel = U[1:4] / rho
         e = U[4] / rho - 0.5 * np.sum(vel * vel, axis=0)
         T = e / cv
         p = rho * R * T
-        zc, yc, xc = np.meshgrid(z0 + dz * (np.arange(nkc) + 0.5), y0 + dy * (np.arange(njc) + 0.5),
-                                 x0 + dx * (np.arange(nic) + 0.5), indexing="ij")
+        zc, yc, xc = np.meshgrid(cz, cy, cx, indexing="ij")
         n = nic * njc * nkc
-        values = dict(posx=xc.ravel(), posy=yc.ravel(), posz=zc.ravel(), vol=np.full(n, dx * dy * dz), p=p, T=T,
+        values = dict(posx=xc.ravel(), posy=yc.ravel(), posz=zc.ravel(), vol=vol, p=p, T=T,
                       rho=rho, e=e, YB=np.zeros(n), a=np.sqrt(g * R * T), velx=vel[0], vely=vel[1], velz=vel[2])
         data = np.concatenate([np.asarray(values[v], dtype=np.float64).ravel() for v in job.iovars])
         path = os.path.join(outdir, _name("flow", *b, job.binary))

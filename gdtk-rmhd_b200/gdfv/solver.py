@@ -228,6 +228,21 @@ class Simulation:
         check(self.ctx, self.L.gdfv_last_bad_cell(self.ctx, blk, ijk, pos))
         return blk[0], (ijk[0], ijk[1], ijk[2]), (pos[0], pos[1], pos[2])
 
+    def add_block_graded(self, xv, yv, zv, bcList=None):
+        """A rectilinear block from its vertex coordinates along each axis (stretched
+        grids): cell (i, j, k) spans [xv[i], xv[i+1]] x [yv[j], yv[j+1]] x [zv[k], zv[k+1]]."""
+        xv, yv, zv = (np.ascontiguousarray(v, dtype=np.float64) for v in (xv, yv, zv))
+        n = (len(xv) - 1, len(yv) - 1, len(zv) - 1)
+        p = lambda a: ffi.cast("double*", a.ctypes.data)
+        b = self.L.gdfv_block_new_graded(self.ctx, *n, p(xv), p(yv), p(zv))
+        if b < 0:
+            check(self.ctx, b)
+        self.blocks.append(n)
+        self._bcs.append({})
+        for face, bc in (bcList or {}).items():
+            self.set_bc(b, face, bc)
+        return b
+
     def set_bc(self, blk, face, bc):
         f = FACE_INDEX[face] if isinstance(face, str) else int(face)
         x_order, other, other_face = 0, -1, -1

@@ -75,6 +75,20 @@ int gdfv_config_get_double(int ctx, const char* key, double* value);
 int gdfv_block_new(int ctx, int nic, int njc, int nkc, double dx, double dy, double dz,
                    double x0, double y0, double z0);
 
+/* A rectilinear structured block of nic x njc x nkc cells from its vertex coordinates
+ * along each axis (xv: nic+1, yv: njc+1, zv: nkc+1 values, increasing; 2D: zv two values):
+ * cell (i, j, k) spans [xv[i], xv[i+1]] x [yv[j], yv[j+1]] x [zv[k], zv[k+1]]; returns
+ * the block id.  Replaces SFluidBlock construction from a StructuredGrid
+ * (e4/sfluidblock.d:440-700, geometry of src/geom/elements/properties.d:97-140) for
+ * axis-aligned grids with stretched spacing: face areas and volumes are products of the
+ * cell's lengths, the l2r2 weights come from the lengths of the cells in each stencil
+ * (e4/onedinterp.d:338-355; ghost cells take the lengths of interior cell n, or of the
+ * partner's cell across an exchange, e4/sfluidblock.d:884-1090), and the CFL signal
+ * takes each cell's own lengths (e4/fvcell.d:975-1059).  Not with MHD or
+ * van_albada_variant=lmr; the adjoint rejects contexts with graded blocks. */
+int gdfv_block_new_graded(int ctx, int nic, int njc, int nkc, const double* xv, const double* yv,
+                          const double* zv);
+
 /* Boundary condition of one face, by the reference's BC type names:
  *   "wall_with_slip"             WallBC_WithSlip (e4/bc.lua:733-757)
  *   "outflow_simple_extrapolate" OutFlowBC_SimpleExtrapolate, x_order 0 or 1 (:1511-1530)

@@ -189,12 +189,14 @@ static void fill_ghosts(const Sim& sim, std::vector<std::vector<FlowState<T>>>& 
 }
 
 // ------------------------------------------------------------------ residual
-static inline double face_area(const Block& b, int d, int dims) {
-    if (dims == 2) return d == 0 ? b.dy : b.dx;
-    return d == 0 ? b.dy * b.dz : (d == 1 ? b.dz * b.dx : b.dx * b.dy);
+// Face areas and volume of cell (i, j, k) of a Cartesian block from its cell lengths
+// (a uniform block: dy dz, dz dx, dx dy and dx dy dz).
+static inline double face_area(const Block& b, int d, int dims, int i, int j, int k) {
+    if (dims == 2) return d == 0 ? b.L(1, j) : b.L(0, i);
+    return d == 0 ? b.L(1, j) * b.L(2, k) : (d == 1 ? b.L(2, k) * b.L(0, i) : b.L(0, i) * b.L(1, j));
 }
-static inline double cell_volume(const Block& b, int dims) {
-    return dims == 2 ? b.dx * b.dy : b.dx * b.dy * b.dz;
+static inline double cell_volume(const Block& b, int dims, int i, int j, int k) {
+    return dims == 2 ? b.L(0, i) * b.L(1, j) : b.L(0, i) * b.L(1, j) * b.L(2, k);
 }
 
 // boundary_flux_effect.d:504-645 BFE_SimpleOutflowFlux.compute_outflow_flux on a fixed
@@ -242,9 +244,6 @@ static void eval_dUdt(const Sim& sim, std::vector<std::vector<FlowState<T>>>& fs
             nf[d] += 1;
             size_t total = (size_t)nf[0] * nf[1] * nf[2];
             flux[d].assign(total * nq, T(0.0));
-            T len = b.length(d);
-            T lenL1 = len, lenL0 = len, lenR0 = len, lenR1 = len;
-            if (cfg.chicken_compat) { lenL1 = lenL0 = lenR0 = lenR1 = 1.0; }
 #pragma omp parallel for schedule(static)
             for (long long f = 0; f < (long long)total; ++f) {
                 int i = (int)(f % nf[0]);
@@ -257,6 +256,9 @@ static void eval_dUdt(const Sim& sim, std::vector<std::vector<FlowState<T>>>& fs
                 const FlowState<T>& cR0 = F[b.pidx(i, j, k)];
                 const FlowState<T>& cR1 = F[b.pidx(i + o[0], j + o[1], k + o[2])];
                 FlowState<T> Lft, Rght;
+                const int idx0 = d == 0 ? i : (d == 1 ? j : k);   // the face lies between cells idx0-1 and idx0
+                T lenL1 = b.L(d, idx0 - 2), lenL0 = b.L(d, idx0 - 1), lenR0 = b.L(d, idx0), lenR1 = b.L(d, idx0 + 1);
+                if (cfg.chicken_compat) { lenL1 = lenL0 = lenR0 = lenR1 = 1.0; }
                 interp_l2r2(cfg, g, d, cL1, cL0, cR0, cR1, lenL1, lenL0, lenR0, lenR1, Lft, Rght);
                 interface_flux(cfg, g, sim.c_h, d, Lft, Rght, &flux[d][(size_t)f * nq]);
                 const int idx = d == 0 ? i : (d == 1 ? j : k);
@@ -266,9 +268,6 @@ static void eval_dUdt(const Sim& sim, std::vector<std::vector<FlowState<T>>>& fs
                     simple_outflow_flux(cfg, cL0, d, 1, &flux[d][(size_t)f * nq]);
             }
         }
-        double area[3] = {face_area(b, 0, cfg.dimensions), face_area(b, 1, cfg.dimensions),
-                          cfg.dimensions == 3 ? face_area(b, 2, 3) : 0.0};
-        double vol_inv = 1.0 / cell_volume(b, cfg.dimensions);
         auto& R = dUdt[bi];
         R.assign(b.ncells() * nq, T(0.0));
 #pragma omp parallel for schedule(static)
@@ -276,6 +275,9 @@ static void eval_dUdt(const Sim& sim, std::vector<std::vector<FlowState<T>>>& fs
             int i = (int)(c % b.nic);
             int j = (int)((c / b.nic) % b.njc);
             int k = (int)(c / ((long long)b.nic * b.njc));
+            const double area[3] = {face_area(b, 0, cfg.dimensions, i, j, k), face_area(b, 1, cfg.dimensions, i, j, k),
+                                    cfg.dimensions == 3 ? face_area(b, 2, 3, i, j, k) : 0.0};
+            const double vol_inv = 1.0 / cell_volume(b, cfg.dimensions, i, j, k);
             // faces in the order W, E, S, N, B, T with outsigns -1, +1 (sfluidblock.d:684-696)
             size_t fidx[6];
             fidx[0] = (size_t)i + (size_t)(n[0] + 1) * ((size_t)j + (size_t)n[1] * k);
@@ -302,8 +304,8 @@ static void eval_dUdt(const Sim& sim, std::vector<std::vector<FlowState<T>>>& fs
 }
 
 // ------------------------------------------------------------------ signal frequency
-static double signal_frequency(const Config& cfg, const Block& b, const FlowState<double>& fs) {
-    double iL = b.dx, jL = b.dy, kL = b.dz;
+static double signal_frequency(const Config& cfg, const Block& b, int i, int j, int k, const FlowState<double>& fs) {
+    double iL = b.L(0, i), jL = b.L(1, j), kL = b.L(2, k);
     double L_min = cfg.dimensions == 3 ? std::min(std::min(iL, jL), kL) : std::min(iL, jL);
     double signal = 0.0;
     double un_N = std::fabs(fs.vel[1]);
@@ -339,8 +341,8 @@ static double signal_frequency(const Config& cfg, const Block& b, const FlowStat
     return signal;
 }
 
-static double block_L_min(const Config& cfg, const Block& b) {
-    return cfg.dimensions == 3 ? std::min(std::min(b.dx, b.dy), b.dz) : std::min(b.dx, b.dy);
+static double cell_L_min(const Config& cfg, const Block& b, int i, int j, int k) {
+    return cfg.dimensions == 3 ? std::min(std::min(b.L(0, i), b.L(1, j)), b.L(2, k)) : std::min(b.L(0, i), b.L(1, j));
 }
 
 // e4/simcore_gasdynamic_step.d:60-160 with e4/fluidblock.d:998-1095
@@ -357,9 +359,9 @@ static void chicken_time_step_size(Sim& sim) {
             for (int j = 0; j < b.njc; ++j)
                 for (int i = 0; i < b.nic; ++i) {
                     const FlowState<double>& fs = b.fs[b.pidx(i, j, k)];
-                    const double isig = b.dx / (std::fabs(fs.vel[0]) + fs.a);
-                    const double jsig = b.dy / (std::fabs(fs.vel[1]) + fs.a);
-                    const double ksig = b.dz / (std::fabs(fs.vel[2]) + fs.a);
+                    const double isig = b.L(0, i) / (std::fabs(fs.vel[0]) + fs.a);
+                    const double jsig = b.L(1, j) / (std::fabs(fs.vel[1]) + fs.a);
+                    const double ksig = b.L(2, k) / (std::fabs(fs.vel[2]) + fs.a);
                     smallest = std::fmin(smallest, cfg.cfl * std::fmin(std::fmin(isig, jsig), ksig));
                 }
     sim.dt_allow = smallest;
@@ -382,7 +384,7 @@ static void determine_time_step_size(Sim& sim) {
         for (int k = 0; k < b.nkc; ++k)
             for (int j = 0; j < b.njc; ++j)
                 for (int i = 0; i < b.nic; ++i) {
-                    signal = signal_frequency(cfg, b, b.fs[b.pidx(i, j, k)]);
+                    signal = signal_frequency(cfg, b, i, j, k, b.fs[b.pidx(i, j, k)]);
                     double cfl_local = sim.dt_global * signal;
                     double dt_local = cfg.cfl / signal;
                     if (first) {
@@ -421,8 +423,8 @@ static void update_ch(Sim& sim) {
         for (int k = 0; k < b.nkc; ++k)
             for (int j = 0; j < b.njc; ++j)
                 for (int i = 0; i < b.nic; ++i) {
-                    double L = block_L_min(sim.cfg, b);
-                    double cfl_local = signal_frequency(sim.cfg, b, b.fs[b.pidx(i, j, k)]) * sim.dt_global;
+                    double L = cell_L_min(sim.cfg, b, i, j, k);
+                    double cfl_local = signal_frequency(sim.cfg, b, i, j, k, b.fs[b.pidx(i, j, k)]) * sim.dt_global;
                     if (bfirst) { min_L = L; cfl_max = cfl_local; bfirst = false; }
                     else { min_L = std::fmin(L, min_L); cfl_max = std::fmax(cfl_local, cfl_max); }
                 }
@@ -646,6 +648,33 @@ int orc_add_block(int h, int nic, int njc, int nkc, double dx, double dy, double
     Block b;
     b.nic = nic; b.njc = njc; b.nkc = nkc;
     b.dx = dx; b.dy = dy; b.dz = dz; b.x0 = x0; b.y0 = y0; b.z0 = z0;
+    const int n[3] = {nic, njc, nkc};
+    const double d[3] = {dx, dy, dz};
+    for (int a = 0; a < 3; ++a) b.len[a].assign((size_t)n[a] + 4, d[a]);
+    b.fs.assign((size_t)b.pi() * b.pj() * b.pk(), FlowState<double>());
+    s->blocks.push_back(std::move(b));
+    return (int)s->blocks.size() - 1;
+}
+
+// A rectilinear block from its vertex coordinates along each axis (n+1 each, increasing):
+// cell lengths x[c+1] - x[c]; the ghost lengths follow at orc_init from the boundaries.
+int orc_add_block_graded(int h, int nic, int njc, int nkc, const double* xv, const double* yv, const double* zv) {
+    Sim* s = get(h);
+    if (!s || !xv || !yv || !zv) return -1;
+    Block b;
+    b.nic = nic; b.njc = njc; b.nkc = nkc;
+    const int n[3] = {nic, njc, nkc};
+    const double* v[3] = {xv, yv, zv};
+    for (int a = 0; a < 3; ++a) {
+        b.len[a].assign((size_t)n[a] + 4, 0.0);
+        for (int c = 0; c < n[a]; ++c) {
+            b.len[a][(size_t)c + 2] = v[a][c + 1] - v[a][c];
+            if (!(b.len[a][(size_t)c + 2] > 0.0)) { s->last_error = "vertex coordinates must increase"; return -1; }
+        }
+    }
+    b.graded = true;
+    b.dx = b.len[0][2]; b.dy = b.len[1][2]; b.dz = b.len[2][2];
+    b.x0 = xv[0]; b.y0 = yv[0]; b.z0 = zv[0];
     b.fs.assign((size_t)b.pi() * b.pj() * b.pk(), FlowState<double>());
     s->blocks.push_back(std::move(b));
     return (int)s->blocks.size() - 1;
@@ -740,6 +769,28 @@ int orc_init(int h) {
     Sim* s = get(h);
     if (!s) return -1;
     const int nq = s->nq();
+    // ghost cell lengths of graded blocks: the partner's cells across an exchange face,
+    // else the block's own interior cell n (e4/sfluidblock.d:884-1090)
+    for (auto& b : s->blocks) {
+        if (!b.graded) continue;
+        const int n[3] = {b.nic, b.njc, b.nkc};
+        for (int face = 0; face < 6; ++face) {
+            const int d = face / 2, plus = face & 1;
+            const BoundaryCondition& bc = b.bc[face];
+            for (int m = 0; m < 2; ++m) {
+                const int ghost = plus ? n[d] + m : -1 - m;
+                double L;
+                if (bc.type == BC_EXCHANGE) {
+                    const Block& ob = s->blocks[bc.other_block];
+                    const int on = d == 0 ? ob.nic : (d == 1 ? ob.njc : ob.nkc);
+                    L = ob.L(d, (bc.other_face & 1) ? on - 1 - m : m);
+                } else {
+                    L = b.L(d, plus ? n[d] - 1 - m : m);
+                }
+                b.len[d][(size_t)(ghost + 2)] = L;
+            }
+        }
+    }
     for (auto& b : s->blocks) {
         for (int l = 0; l < 4; ++l) { b.U[l].assign(b.ncells() * nq, 0.0); b.dUdt[l].assign(b.ncells() * nq, 0.0); }
         for (int k = 0; k < b.nkc; ++k)

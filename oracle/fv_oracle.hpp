@@ -591,6 +591,14 @@ struct Block {
     std::vector<double> dUdt[4];
     std::vector<double> Q;               // fixed source term per cell, cell-major (empty: none)
     double length(int d) const { return d == 0 ? dx : (d == 1 ? dy : dz); }
+    // Cell lengths per index direction, cells -2 .. n+1 (index c + 2): the block's own cells
+    // from its grid, the two ghost layers beyond each face as SFluidBlock gives them
+    // (e4/sfluidblock.d:884-1090: ghost n copies the lengths of interior cell n; across a
+    // full-face exchange, the partner's cell n, simcore_exchange.d:44-70).  Uniform blocks
+    // hold their spacing everywhere.
+    bool graded = false;
+    std::vector<double> len[3];
+    double L(int d, int c) const { return len[d][(size_t)(c + 2)]; }
 };
 
 } // namespace orc

@@ -51,6 +51,7 @@ def lib():
         L.orc_last_error.argtypes = [ctypes.c_int, ctypes.c_char_p, ctypes.c_int]
         L.orc_set_ghost_states.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, dp]
         L.orc_set_source.argtypes = [ctypes.c_int, ctypes.c_int, dp]
+        L.orc_add_block_graded.argtypes = [ctypes.c_int] * 4 + [dp] * 3
         _LIB = L
     return _LIB
 
@@ -98,6 +99,18 @@ class OracleSim:
         b = self.L.orc_add_block(self.h, nic, njc, nkc, dx, dy, dz, x0, y0, z0)
         self.blocks.append((nic, njc, nkc))
         self.geometry = getattr(self, "geometry", []) + [((dx, dy, dz), (x0, y0, z0))]
+        return b
+
+    def add_block_graded(self, xv, yv, zv):
+        """A rectilinear block from vertex coordinates along each axis (n+1 each)."""
+        xv, yv, zv = (np.ascontiguousarray(v, dtype=np.float64) for v in (xv, yv, zv))
+        n = (len(xv) - 1, len(yv) - 1, len(zv) - 1)
+        b = self.L.orc_add_block_graded(self.h, *n, _p(xv), _p(yv), _p(zv))
+        if b < 0:
+            raise ValueError(self.last_error())
+        self.blocks.append(n)
+        self.geometry = getattr(self, "geometry", []) + [((xv[1] - xv[0], yv[1] - yv[0], zv[1] - zv[0]),
+                                                          (xv[0], yv[0], zv[0]))]
         return b
 
     def ghost_positions(self, blk, face):

@@ -28,8 +28,11 @@ class Case:
         self.gamma = gamma
         self.blocks = []
 
-    def add_block(self, n, d, origin, bcs, rho, vel, T, B=None, psi=None):
-        self.blocks.append(dict(n=n, d=d, origin=origin, bcs=bcs, rho=rho, vel=vel, T=T, B=B, psi=psi))
+    def add_block(self, n, d, origin, bcs, rho, vel, T, B=None, psi=None, vertices=None):
+        """vertices: (xv, yv, zv) of a graded (rectilinear) block; d and origin are then
+        those of its first cell."""
+        self.blocks.append(dict(n=n, d=d, origin=origin, bcs=bcs, rho=rho, vel=vel, T=T, B=B, psi=psi,
+                                vertices=vertices))
         return len(self.blocks) - 1
 
     @property
@@ -72,7 +75,7 @@ def inflow_state_m3():
     return dict(p=5.0e3, T=T, vel=(3.0 * a, 0.0, 0.0))
 
 
-def c2_inflow_box(n=(256, 256, 256), flux="ausmdv", seed=4321, precision="fp64", noise_all=False):
+def c2_inflow_box(n=(256, 256, 256), flux="ausmdv", seed=4321, precision="fp64", noise_all=False, d=1e-3):
     """Single block, M=3 inflow on x-min, extrapolate outflow on x-max, slip walls
     on y and z faces, inflow state everywhere plus 1% density noise (dx = 1 mm).
     noise_all: also 1% noise on T and on the velocity components, so that no
@@ -94,7 +97,7 @@ def c2_inflow_box(n=(256, 256, 256), flux="ausmdv", seed=4321, precision="fp64",
            "east": ("outflow_simple_extrapolate", dict(x_order=0)),
            "south": ("wall_with_slip", {}), "north": ("wall_with_slip", {}),
            "bottom": ("wall_with_slip", {}), "top": ("wall_with_slip", {})}
-    c.add_block(n, (1e-3, 1e-3, 1e-3), (0, 0, 0), bcs, rho, vel, T)
+    c.add_block(n, (d, d, d), (0, 0, 0), bcs, rho, vel, T)
     return c
 
 
@@ -241,6 +244,70 @@ def mhd_slip_dipole(n=(64, 48, 4), seed=31, precision="fp64"):
     return c
 
 
+def stretched(n, d0, ratio, x0=0.0):
+    """n+1 vertex coordinates from x0 with first cell d0 and cell-to-cell growth ratio."""
+    return x0 + np.concatenate([[0.0], np.cumsum(d0 * ratio ** np.arange(n))])
+
+
+def graded_inflow_box(n=(40, 28, 20), seed=17, precision="fp64", flux="ausmdv", uniform=False):
+    """The M=3 inflow box on a stretched rectilinear grid: cells growing by 3% along x from
+    0.8 mm, shrinking by 2% along y from 1.2 mm, 1 mm along z; inflow on x-min, extrapolation on x-max, slip
+    walls on y and z, 1% density noise.  uniform=True: 1/1024 m everywhere (vertices i/1024
+    are exact, so the cell lengths are too), built as a graded block."""
+    c = Case("graded_box", dict(flux_calculator=flux, flux_precision=precision), R_AIR_CHICKEN, 1.4)
+    rng = np.random.default_rng(seed)
+    inf = inflow_state_m3()
+    nic, njc, nkc = n
+    if uniform:
+        verts = tuple(np.arange(m + 1) / 1024.0 for m in n)
+    else:
+        verts = (stretched(nic, 0.8e-3, 1.03), stretched(njc, 1.2e-3, 0.98), np.arange(nkc + 1) * 1e-3)
+    rho = _noisy_rho(rng, inf["p"] / (R_AIR_CHICKEN * inf["T"]), (nkc, njc, nic))
+    bcs = {"west": ("inflow_supersonic", dict(inflow=inf)),
+           "east": ("outflow_simple_extrapolate", dict(x_order=0)),
+           "south": ("wall_with_slip", {}), "north": ("wall_with_slip", {}),
+           "bottom": ("wall_with_slip", {}), "top": ("wall_with_slip", {})}
+    d = tuple(float(v[1] - v[0]) for v in verts)
+    c.add_block(n, d, tuple(float(v[0]) for v in verts), bcs, rho, inf["vel"], inf["T"], vertices=verts)
+    return c
+
+
+def graded_lattice(seed=23, precision="fp64"):
+    """2 x 2 x 1 blocks of stretched grids joined by full-face exchange (the ghost cells
+    across an exchange take the partner's cell lengths), a shock-box state (x < mid:
+    p 1e5, else 1e4; T 300) with 1% density noise, extrapolation on the outer x faces,
+    slip walls elsewhere."""
+    c = Case("graded_lattice", dict(flux_calculator="ausmdv", flux_precision=precision), R_AIR_CHICKEN, 1.4)
+    rng = np.random.default_rng(seed)
+    xs = [stretched(20, 1.0e-3, 1.04), None]
+    xs[1] = stretched(24, 0.7e-3, 0.99, x0=xs[0][-1])
+    ys = [stretched(18, 1.1e-3, 0.97), None]
+    ys[1] = stretched(16, 0.9e-3, 1.05, x0=ys[0][-1])
+    zv = stretched(12, 1.0e-3, 1.02)
+    xmid = 0.5 * (xs[0][0] + xs[1][-1])
+    idx = {(bi, bj): bi + 2 * bj for bj in range(2) for bi in range(2)}
+    for bj in range(2):
+        for bi in range(2):
+            xv, yv = xs[bi], ys[bj]
+            n = (len(xv) - 1, len(yv) - 1, len(zv) - 1)
+            xc = 0.5 * (xv[1:] + xv[:-1])
+            p = np.where(xc < xmid, 1.0e5, 1.0e4)
+            rho = _noisy_rho(rng, np.broadcast_to(p / (R_AIR_CHICKEN * 300.0), (n[2], n[1], n[0])), (n[2], n[1], n[0]))
+            bcs = {}
+            bcs["west"] = ("exchange_over_full_face", dict(other=idx[(0, bj)], other_face="east")) if bi == 1 else \
+                ("outflow_simple_extrapolate", dict(x_order=0))
+            bcs["east"] = ("exchange_over_full_face", dict(other=idx[(1, bj)], other_face="west")) if bi == 0 else \
+                ("outflow_simple_extrapolate", dict(x_order=0))
+            if bj == 1:
+                bcs["south"] = ("exchange_over_full_face", dict(other=idx[(bi, 0)], other_face="north"))
+            else:
+                bcs["north"] = ("exchange_over_full_face", dict(other=idx[(bi, 1)], other_face="south"))
+            d = (float(xv[1] - xv[0]), float(yv[1] - yv[0]), float(zv[1] - zv[0]))
+            c.add_block(n, d, (float(xv[0]), float(yv[0]), float(zv[0])), bcs, rho, (0.0, 0.0, 0.0), 300.0,
+                        vertices=(xv, yv, zv))
+    return c
+
+
 # ---------------------------------------------------------------- builders
 _ORACLE_BC = {"wall_with_slip": "wall_with_slip", "outflow_simple_extrapolate": "extrapolate",
               "inflow_supersonic": "inflow_supersonic", "exchange_over_full_face": "exchange",
@@ -254,7 +321,10 @@ def build_oracle(case):
     cfg = {k.replace("flowstate_limits_", ""): v for k, v in case.config.items() if k != "flux_precision"}
     s = OracleSim(R=case.R, gamma=case.gamma, **cfg)
     for b in case.blocks:
-        s.add_block(*b["n"], *b["d"], *b["origin"])
+        if b.get("vertices") is not None:
+            s.add_block_graded(*b["vertices"])
+        else:
+            s.add_block(*b["n"], *b["d"], *b["origin"])
     for bi, b in enumerate(case.blocks):
         for face, (kind, kw) in b["bcs"].items():
             inflow = kw.get("inflow")
@@ -272,7 +342,10 @@ def build_gpu(case, **extra_config):
     cfg = gdfv.Config(**{**case.config, **extra_config})
     sim = gdfv.Simulation(cfg, gas=gdfv.IdealGas(R=case.R, gamma=case.gamma))
     for b in case.blocks:
-        sim.add_block(*b["n"], *b["d"], *b["origin"])
+        if b.get("vertices") is not None:
+            sim.add_block_graded(*b["vertices"])
+        else:
+            sim.add_block(*b["n"], *b["d"], *b["origin"])
     for bi, b in enumerate(case.blocks):
         for face, (kind, kw) in b["bcs"].items():
             if kind == "wall_with_slip":

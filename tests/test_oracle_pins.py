@@ -214,3 +214,18 @@ def test_oracle_e4_mode_pinned_by_mms_euler():
     for k, ref in refs.items():
         assert abs(norms[k] - ref) / ref < 1.0e-3, (k, norms[k], ref, steps)
         assert abs(norms[k] - ref) / ref < 1.0e-9, (k, norms[k], ref)
+
+
+def test_oracle_graded_block_with_uniform_spacing_is_the_uniform_block():
+    """A graded (rectilinear) block whose vertices are evenly spaced -- at 1/1024 m, so the
+    cell lengths are exact -- computes the uniform block's results bit for bit: the
+    per-face l2r2 weights, areas, volumes and signal lengths of the graded path reduce to
+    the uniform ones."""
+    cu = cases.c2_inflow_box(n=(24, 16, 12), seed=17, d=1 / 1024.0)
+    cg = cases.graded_inflow_box(n=(24, 16, 12), uniform=True)
+    ou, og = cases.build_oracle(cu), cases.build_oracle(cg)
+    U = ou.get_U(0)
+    assert ou.set_U(0, U) == 0 and og.set_U(0, U) == 0
+    assert ou.run(6) == 0 and og.run(6) == 0
+    assert np.array_equal(ou.get_U(0), og.get_U(0))
+    assert ou.time()["dt"] == og.time()["dt"]
