@@ -308,7 +308,9 @@ def mhd_leg(stream, steps=2000, n=(512, 512, 4), dt=8.0e-5):
     """Ideal-MHD Orszag-Tang vortex (hlle + GLM divergence cleaning, periodic, gamma
     5/3, 1% seeded density noise): plain FP64 and FP32-flux forms at one fixed dt
     (so that both compare at the same times; 2000 x 8e-5 = 0.16), throughput over
-    the last 100 steps, error of the float form and max |div B| of both."""
+    the last 100 steps, error of the float form and max |div B| of both; beside the float
+    form's error, that of the FP64 form started from a density perturbed by float-epsilon
+    noise (the flow's sensitivity, which bounds what any float form can reach)."""
     import cases
     out = dict(workload=f"Orszag-Tang {n[0]}x{n[1]}x{n[2]} hlle+GLM, fixed dt {dt}", steps=steps)
     states = {}
@@ -326,6 +328,17 @@ def mhd_leg(stream, steps=2000, n=(512, 512, 4), dt=8.0e-5):
         sim.close()
     out["unit"] = UNIT
     out["rel_l2_vs_fp64"] = _l2_errors(states["fp32"], states["fp64"], mhd=True)
+    # the flow's own sensitivity: the FP64 form from a density perturbed once by float-epsilon
+    # noise (relative 6e-8), against the unperturbed FP64 run at the same time
+    case = cases.orszag_tang(n=n, precision="fp64")
+    sim = cases.build_gpu(case, fixed_time_step=True, dt_init=dt, dt_max=dt)
+    sim.set_stream(stream.cuda_stream)
+    U0 = sim.get_conserved(0)
+    U0[0] *= 1.0 + 6.0e-8 * np.random.default_rng(3).standard_normal(U0[0].shape)
+    sim.set_conserved(0, U0)
+    sim.run(max_step=steps)
+    out["fp64_perturbed_6e-8_rel_l2_vs_fp64"] = _l2_errors(sim.get_conserved(0), states["fp64"], mhd=True)
+    sim.close()
     return out
 
 
