@@ -494,7 +494,7 @@ def main():
     traffic = None
     # ncu DRAM bytes per cell of the corrector (float Euler kernel on decoded primitives),
     # captured on a 256x128x128 case with the same tiles, scaled to this launch's cells
-    tf = os.path.join(ROOT, "profiles", "stage_f32_kernel_256x128x128.md")
+    tf = os.path.join(ROOT, "profiles", "stage_prim_kernel_256x128x128.md")
     if os.path.exists(tf):
         import re
         with open(tf) as f:
@@ -542,7 +542,7 @@ def main():
         "fp32_over_fp64": val32 / val64,
         "rel_l2_vs_fp64": err,
         "adjoint_over_forward": None,
-        "roofline": {"bound": "hbm", "kernel": "stage_f32_kernel<2> (corrector)", "achieved": ach2,
+        "roofline": {"bound": "hbm", "kernel": "stage_prim_kernel<float,2> (corrector)", "achieved": ach2,
                      "peak": peak, "unit": "GB/s", "frac": ach2 / peak, "traffic": traffic,
                      "peak_source": peak_kind, "algorithmic_bytes_per_cell": BYTES_STAGE2,
                      "stage_ms": [st1, st2]},

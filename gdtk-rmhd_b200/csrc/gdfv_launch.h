@@ -52,11 +52,12 @@ inline int tile_rows_corrector(int precision, bool mhd) {
     return precision == 0 ? (mhd ? TJ_FP64_MHD : TJ_FP64_CORR) : (mhd ? TJ_FP32_MHD_CORR : TJ_FP32_CORR);
 }
 
-// Options under which the float-flux Euler stages run the kernel on decoded float
-// primitives (gdfv_stage_f32.cuh) when the arguments carry primitive buffers: the
+// Options under which the float-flux Euler stages run the kernel on decoded primitives
+// (gdfv_stage_prim.cuh) when the arguments carry primitive buffers (the FP64 form keeps
+// stage_kernel: measured faster there, see the design notes): the
 // defaults (limiter and extrema clipping on, e4 epsilon), no outflow boundary with a
 // flux or ghost rule of its own, no graded block, 3D.
-inline bool float_euler_path(const NumParams& P) {
+inline bool prim_path(const NumParams& P) {
     return !P.mhd && P.apply_limiter && P.extrema_clipping && !P.lmr_epsilon && !P.outflow_bcs && !P.graded &&
            P.dims == 3;
 }
@@ -64,9 +65,9 @@ inline bool float_euler_path(const NumParams& P) {
 // Launch one stage (0 = residual only, 1 = predictor, 2 = corrector) over A.n_tiles tiles.
 cudaError_t launch_stage_fp64(int stage, int flux, bool mhd, const StageArgs& A, cudaStream_t s);
 cudaError_t launch_stage_fp32(int stage, int flux, bool mhd, const StageArgs& A, cudaStream_t s);
-// Float primitives (rho, vel, u, a; SoA [6][total]) of the state U, for the float
-// Euler path, enqueued on stream s.
-void prims_f32(const double* U, long long total, const NumParams& P, float* Pout, cudaStream_t s);
+// Primitives (rho, vel, u, a; SoA [6][total], float or double) of the state U, for the
+// kernels on decoded primitives, enqueued on stream s.
+void prims_fp32(const double* U, long long total, const NumParams& P, void* Pout, cudaStream_t s);
 // Raise the dynamic shared-memory limit of every instantiation (once per device).
 cudaError_t configure_stage_fp64();
 cudaError_t configure_stage_fp32();

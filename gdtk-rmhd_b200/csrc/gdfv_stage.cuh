@@ -49,11 +49,12 @@ struct StageArgs {
     int max_invalid_cells;
     int persistent;           // grid of resident CTAs striding over the tiles
     int n_tiles2;             // > 0: the corrector's own tile table follows the first (other rows)
-    // float-flux Euler kernel of the default options (gdfv_stage_f32.cuh): float primitives
-    // (rho, vel, u, a; SoA [6][total]) of Ubuf[0], Ubuf[1] and of the predictor state;
-    // null: the stages decode their stencils from the conserved state
-    float* prim[2];
-    float* prim1;
+    // Euler kernel of the default options on decoded primitives (gdfv_stage_prim.cuh):
+    // primitives (rho, vel, u, a; SoA [6][total], in the flux precision) of Ubuf[0],
+    // Ubuf[1] and of the predictor state; null: the stages decode their stencils from the
+    // conserved state
+    void* prim[2];
+    void* prim1;
 };
 
 // Compile-time geometry of the tile and of the shared-memory layout.

@@ -9,5 +9,6 @@
 #define GDFV_TJ_MHD_CORR TJ_FP32_MHD_CORR
 #define GDFV_LAUNCH launch_stage_fp32
 #define GDFV_CONFIGURE configure_stage_fp32
-#define GDFV_FLOAT_EULER_PATH 1
+#define GDFV_PRIM_PATH 1
+#define GDFV_PRIMS prims_fp32
 #include "gdfv_stage_inst.cuh"

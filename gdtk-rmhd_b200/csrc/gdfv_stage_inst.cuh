@@ -4,8 +4,8 @@
 // corrector rows), GDFV_TJ_MHD, GDFV_TJ_MHD_CORR, GDFV_LAUNCH and
 // GDFV_CONFIGURE first.
 #include "gdfv_launch.h"
-#if GDFV_FLOAT_EULER_PATH
-#include "gdfv_stage_f32.cuh"
+#if GDFV_PRIM_PATH
+#include "gdfv_stage_prim.cuh"
 #endif
 
 namespace gdfv {
@@ -56,45 +56,46 @@ cudaError_t launch_rows(const StageArgs& A, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-#if GDFV_FLOAT_EULER_PATH
-// The float Euler kernel on decoded primitives (gdfv_stage_f32.cuh) over the first tile
+#if GDFV_PRIM_PATH
+// The Euler kernel on decoded primitives (gdfv_stage_prim.cuh) over the first tile
 // table (rows TJ_E in both stages).
 template <int STAGE, int FLUX, int PERS>
-int& resident_f32() {
+int& resident_prim() {
     static int v = 0;
     return v;
 }
 
 template <int STAGE, int FLUX>
-cudaError_t launch_f32(const StageArgs& A, cudaStream_t s) {
-    using G = GeoF<TJ_E>;
-    const int cap = resident_f32<STAGE, FLUX, 1>();
+cudaError_t launch_prim(const StageArgs& A, cudaStream_t s) {
+    using G = GeoF<Real, TJ_E>;
+    const int cap = resident_prim<STAGE, FLUX, 1>();
     if (A.persistent && cap > 0)
-        stage_f32_kernel<STAGE, FLUX, TJ_E, 1><<<cap < A.n_tiles ? cap : A.n_tiles, G::NT, G::bytes, s>>>(A);
+        stage_prim_kernel<Real, STAGE, FLUX, TJ_E, 1><<<cap < A.n_tiles ? cap : A.n_tiles, G::NT, G::bytes, s>>>(A);
     else
-        stage_f32_kernel<STAGE, FLUX, TJ_E, 0><<<A.n_tiles, G::NT, G::bytes, s>>>(A);
+        stage_prim_kernel<Real, STAGE, FLUX, TJ_E, 0><<<A.n_tiles, G::NT, G::bytes, s>>>(A);
     return cudaGetLastError();
 }
 
 template <int STAGE, int FLUX>
-cudaError_t configure_f32(int n_sm) {
-    using G = GeoF<TJ_E>;
-    cudaError_t e = set_smem(stage_f32_kernel<STAGE, FLUX, TJ_E, 0>, G::bytes);
-    if (e == cudaSuccess) e = set_smem(stage_f32_kernel<STAGE, FLUX, TJ_E, 1>, G::bytes);
+cudaError_t configure_prim(int n_sm) {
+    using G = GeoF<Real, TJ_E>;
+    cudaError_t e = set_smem(stage_prim_kernel<Real, STAGE, FLUX, TJ_E, 0>, G::bytes);
+    if (e == cudaSuccess) e = set_smem(stage_prim_kernel<Real, STAGE, FLUX, TJ_E, 1>, G::bytes);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, stage_f32_kernel<STAGE, FLUX, TJ_E, 1>, G::NT, G::bytes);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, stage_prim_kernel<Real, STAGE, FLUX, TJ_E, 1>, G::NT,
+                                                      G::bytes);
     if (e != cudaSuccess) return e;
-    resident_f32<STAGE, FLUX, 1>() = per_sm * n_sm;
+    resident_prim<STAGE, FLUX, 1>() = per_sm * n_sm;
     return cudaSuccess;
 }
 #endif
 
 template <int STAGE, bool MHD, int FLUX>
 cudaError_t launch_one(const StageArgs& A, cudaStream_t s) {
-#if GDFV_FLOAT_EULER_PATH
+#if GDFV_PRIM_PATH
     if constexpr (!MHD && STAGE >= 1) {
-        if (A.prim[0] && float_euler_path(A.P)) return launch_f32<STAGE, FLUX>(A, s);
+        if (A.prim[0] && prim_path(A.P)) return launch_prim<STAGE, FLUX>(A, s);
     }
 #endif
     if constexpr (STAGE == 2 && rows_corrector<MHD>() != rows<MHD>()) {
@@ -126,9 +127,9 @@ cudaError_t configure_rows(int n_sm) {
 template <int STAGE, bool MHD, int FLUX>
 cudaError_t configure_one(int n_sm) {
     cudaError_t e = configure_rows<STAGE, MHD, FLUX, rows<MHD>()>(n_sm);
-#if GDFV_FLOAT_EULER_PATH
+#if GDFV_PRIM_PATH
     if constexpr (!MHD && STAGE >= 1)
-        if (e == cudaSuccess) e = configure_f32<STAGE, FLUX>(n_sm);
+        if (e == cudaSuccess) e = configure_prim<STAGE, FLUX>(n_sm);
 #endif
     if constexpr (STAGE == 2 && rows_corrector<MHD>() != rows<MHD>())
         if (e == cudaSuccess) e = configure_rows<2, MHD, FLUX, rows_corrector<MHD>()>(n_sm);
@@ -165,9 +166,9 @@ cudaError_t GDFV_LAUNCH(int stage, int flux, bool mhd, const StageArgs& A, cudaS
     return cudaErrorInvalidValue;
 }
 
-#if GDFV_FLOAT_EULER_PATH
-void prims_f32(const double* U, long long total, const NumParams& P, float* Pout, cudaStream_t s) {
-    prims_f32_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(U, total, P, Pout);
+#if GDFV_PRIM_PATH
+void GDFV_PRIMS(const double* U, long long total, const NumParams& P, void* Pout, cudaStream_t s) {
+    prims_kernel<Real><<<(unsigned)((total + 255) / 256), 256, 0, s>>>(U, total, P, static_cast<Real*>(Pout));
 }
 #endif
 

@@ -1,16 +1,20 @@
-// gdfv_stage_f32.cuh -- the float-flux Euler stage kernel of the default options
-// (van Albada limiter and extrema clipping on, e4 epsilon, no outflow boundary with a
-// flux or ghost rule of its own, 3D).  Same stage semantics and the same per-face
-// arithmetic as stage_kernel's float path (recon_cell, face_flux; the stage update, the
-// decode checks and the signal reduction in FP64), with a leaner data flow:
+// gdfv_stage_prim.cuh -- the Euler stage kernel of the default options (van Albada
+// limiter and extrema clipping on, e4 epsilon, no outflow boundary with a flux or ghost
+// rule of its own, uniform blocks, 3D), in both flux precisions R: float (the FP32-flux /
+// FP64-update form) and double (the plain FP64 form, bit for bit the reference's
+// arithmetic as stage_kernel's FP64 path).  Same stage semantics and the same per-face
+// arithmetic as stage_kernel (recon_cell, face_flux; the stage update, the decode
+// checks and the signal reduction in FP64), with a leaner data flow:
 //
 // * Decoded primitives in HBM.  Every stage decodes the state it produces in its
 //   update phase anyway (the checks of decode_conserved, e4/fvcell.d:586-822); it also
-//   stores that state's primitives (rho, vel, u, a) in float, SoA [6][total]: the
-//   predictor those of U1 = U0 + dt dU0, the corrector those of U2.  The next stage
-//   loads its stencils -- own column, halo and prologue planes -- from these six floats
-//   instead of loading and decoding ten FP64 values (U0 and dU0) per stencil cell.
-//   P[b] holds the primitives of state buffer b; P1 those of the predictor state.
+//   stores that state's primitives (rho, vel, u, a) in R, SoA [6][total]: the predictor
+//   those of U1 = U0 + dt dU0, the corrector those of U2.  The next stage loads its
+//   stencils -- own column, halo and prologue planes -- from these six values instead of
+//   loading and decoding ten FP64 values (U0 and dU0) per stencil cell.  In FP64 the
+//   stored primitives are the bits the stencil decode would give (decode and
+//   decode_prim perform the same operations).  P[b] holds the primitives of state
+//   buffer b; P1 those of the predictor state.
 // * i direction in registers.  Warp w of the tile owns row w, lane l cell l.  The
 //   reconstruction of the lane's own cell gives both its interface values; the left
 //   state of face l-1/2 comes from lane l-1 by a warp shuffle, the flux of face
@@ -40,13 +44,15 @@
 
 namespace gdfv {
 
-// Float primitives of one cell as the ring stores them (rho, v0, v1, v2, u, a).
+// Primitives of one cell as the ring stores them (rho, v0, v1, v2, u, a).
+template <class R>
 struct PF {
-    float rho, v[3], u, a;
+    R rho, v[3], u, a;
 };
 
-__device__ __forceinline__ PF load_pf(const float* __restrict__ Pin, long long total, long long g) {
-    PF c;
+template <class R>
+__device__ __forceinline__ PF<R> load_pf(const R* __restrict__ Pin, long long total, long long g) {
+    PF<R> c;
     c.rho = __ldg(Pin + g);
     c.v[0] = __ldg(Pin + total + g);
     c.v[1] = __ldg(Pin + 2 * total + g);
@@ -56,7 +62,8 @@ __device__ __forceinline__ PF load_pf(const float* __restrict__ Pin, long long t
     return c;
 }
 
-__device__ __forceinline__ void put_pf(float* base, int stride, int idx, const PF& c) {
+template <class R>
+__device__ __forceinline__ void put_pf(R* base, int stride, int idx, const PF<R>& c) {
     base[idx] = c.rho;
     base[stride + idx] = c.v[0];
     base[2 * stride + idx] = c.v[1];
@@ -72,14 +79,15 @@ __device__ __forceinline__ void put_pf(float* base, int stride, int idx, const P
 // copy or linear extrapolation of rho, u and velocity with a from the boundary cell
 // (extrapolate_copy.d:124-201), the fixed inflow state (flow_state_copy.d), or the
 // partner block's cell (full_face_copy.d).
-__device__ __forceinline__ PF ghost_pf(const StageArgs& A, const float* __restrict__ Pin, const BlockDesc& B, int i, int j,
-                                    int k) {
+template <class R>
+__device__ __forceinline__ PF<R> ghost_pf(const StageArgs& A, const R* __restrict__ Pin, const BlockDesc& B, int i, int j,
+                                       int k) {
     const CellSrc s = resolve<false>(A, B, i, j, k);
-    PF c;
+    PF<R> c;
     if (s.kind == SRC_INFLOW) {
         const InflowState& in = A.inflow[s.inflow];
-        c.rho = (float)in.rho; c.u = (float)in.u; c.a = (float)in.a;
-        c.v[0] = (float)in.vel[0]; c.v[1] = (float)in.vel[1]; c.v[2] = (float)in.vel[2];
+        c.rho = (R)in.rho; c.u = (R)in.u; c.a = (R)in.a;
+        c.v[0] = (R)in.vel[0]; c.v[1] = (R)in.vel[1]; c.v[2] = (R)in.vel[2];
         return c;
     }
     c = load_pf(Pin, A.total, s.blk->offset + s.c0);
@@ -87,16 +95,16 @@ __device__ __forceinline__ PF ghost_pf(const StageArgs& A, const float* __restri
         c.v[s.axis] = -c.v[s.axis];
     } else if (s.kind == SRC_EXTRAP1_G0 || s.kind == SRC_EXTRAP1_G1) {
         // g0 = 2 e - f1, g1 = 2 g0 - e (e the boundary cell, f1 the cell inside it)
-        const PF f1 = load_pf(Pin, A.total, s.blk->offset + s.c1);
-        PF g = c;
-        g.rho = 2.0f * c.rho - f1.rho;
-        g.u = 2.0f * c.u - f1.u;
-        for (int m = 0; m < 3; ++m) g.v[m] = 2.0f * c.v[m] - f1.v[m];
+        const PF<R> f1 = load_pf(Pin, A.total, s.blk->offset + s.c1);
+        PF<R> g = c;
+        g.rho = R(2) * c.rho - f1.rho;
+        g.u = R(2) * c.u - f1.u;
+        for (int m = 0; m < 3; ++m) g.v[m] = R(2) * c.v[m] - f1.v[m];
         if (s.kind == SRC_EXTRAP1_G1) {
-            PF h = c;
-            h.rho = 2.0f * g.rho - c.rho;
-            h.u = 2.0f * g.u - c.u;
-            for (int m = 0; m < 3; ++m) h.v[m] = 2.0f * g.v[m] - c.v[m];
+            PF<R> h = c;
+            h.rho = R(2) * g.rho - c.rho;
+            h.u = R(2) * g.u - c.u;
+            for (int m = 0; m < 3; ++m) h.v[m] = R(2) * g.v[m] - c.v[m];
             return h;
         }
         return g;
@@ -107,12 +115,15 @@ __device__ __forceinline__ PF ghost_pf(const StageArgs& A, const float* __restri
 // Asynchronous copy of one cell's six primitives from P into a padded ring plane
 // (cp.async: global to shared memory without passing through registers; the copies of
 // a thread complete at cp_async_wait).
-__device__ __forceinline__ void cp_async_pf(float* base, int stride, int idx, const float* Pin, long long total,
-                                            long long g) {
+template <class R>
+__device__ __forceinline__ void cp_async_pf(R* base, int stride, int idx, const R* Pin, long long total, long long g) {
 #pragma unroll
     for (int q = 0; q < 6; ++q) {
         const unsigned d = (unsigned)__cvta_generic_to_shared(base + q * stride + idx);
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(Pin + q * total + g) : "memory");
+        if constexpr (sizeof(R) == 4)
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(Pin + q * total + g) : "memory");
+        else
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(Pin + q * total + g) : "memory");
     }
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
@@ -120,18 +131,19 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-// Float primitives of a decoded FP64 state (what the next stage loads).
-__device__ __forceinline__ void store_pf(float* __restrict__ Pout, long long total, long long g, const Prim<double>& s) {
-    Pout[g] = (float)s.rho;
-    Pout[total + g] = (float)s.v[0];
-    Pout[2 * total + g] = (float)s.v[1];
-    Pout[3 * total + g] = (float)s.v[2];
-    Pout[4 * total + g] = (float)s.u;
-    Pout[5 * total + g] = (float)s.a;
+// Primitives of a decoded FP64 state (what the next stage loads).
+template <class R>
+__device__ __forceinline__ void store_pf(R* __restrict__ Pout, long long total, long long g, const Prim<double>& s) {
+    Pout[g] = (R)s.rho;
+    Pout[total + g] = (R)s.v[0];
+    Pout[2 * total + g] = (R)s.v[1];
+    Pout[3 * total + g] = (R)s.v[2];
+    Pout[4 * total + g] = (R)s.u;
+    Pout[5 * total + g] = (R)s.a;
 }
 
-// Shared-memory layout (floats) of the kernel for TJ rows.
-template <int TJ_>
+// Shared-memory layout (values of R) of the kernel for TJ rows.
+template <class R, int TJ_>
 struct GeoF {
     static constexpr int TI = 32, TJ = TJ_;
     static constexpr int NT = 32 * (TJ + 1);
@@ -147,33 +159,38 @@ struct GeoF {
     static constexpr int O_FJ = O_EIL + NS * TJ;              // [NS][TJ+1][TI] flux of the S face of rows 0..nj
     static constexpr int O_FIE = O_FJ + NS * (TJ + 1) * TI;   // [NS][TJ]       flux of the E face of each row
     static constexpr int O_END = O_FIE + NS * TJ;
-    static constexpr size_t bytes = sizeof(float) * (size_t)O_END;
+    static constexpr size_t bytes = sizeof(R) * (size_t)O_END;
 };
 
-// Resident CTAs per SM the kernel is compiled for (its register budget).
-#ifndef GDFV_MINB_F32E
-#define GDFV_MINB_F32E 3
+// Resident CTAs per SM each precision's kernel is compiled for (its register budget).
+#ifndef GDFV_MINB_PRIM_FP32
+#define GDFV_MINB_PRIM_FP32 3
+#endif
+#ifndef GDFV_MINB_PRIM_FP64
+#define GDFV_MINB_PRIM_FP64 2
 #endif
 
-template <int STAGE, int FLUX, int TJ, int PERS>
-__global__ void __launch_bounds__(32 * (TJ + 1), GDFV_MINB_F32E) stage_f32_kernel(StageArgs A) {
+template <class R, int STAGE, int FLUX, int TJ, int PERS>
+__global__ void __launch_bounds__(32 * (TJ + 1), sizeof(R) == 4 ? GDFV_MINB_PRIM_FP32 : GDFV_MINB_PRIM_FP64)
+    stage_prim_kernel(StageArgs A) {
     static_assert(STAGE == 1 || STAGE == 2, "predictor or corrector");
-    using G = GeoF<TJ>;
+    constexpr bool FAST = sizeof(R) == 4;
+    using G = GeoF<R, TJ>;
     constexpr int TI = G::TI, PW = G::PW, PLANE = G::PLANE, NS = G::NS;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    float* sm = reinterpret_cast<float*>(smem_raw);
-    float* ring = sm + G::O_RING;
-    float* QPJ = sm + G::O_QPJ;
-    float* EJS = sm + G::O_EJS;
-    float* EJN = sm + G::O_EJN;
-    float* EIW = sm + G::O_EIW;
-    float* EIE = sm + G::O_EIE;
-    float* EIL = sm + G::O_EIL;
-    float* FJ = sm + G::O_FJ;
-    float* FIE = sm + G::O_FIE;
+    R* sm = reinterpret_cast<R*>(smem_raw);
+    R* ring = sm + G::O_RING;
+    R* QPJ = sm + G::O_QPJ;
+    R* EJS = sm + G::O_EJS;
+    R* EJN = sm + G::O_EJN;
+    R* EIW = sm + G::O_EIW;
+    R* EIE = sm + G::O_EIE;
+    R* EIL = sm + G::O_EIL;
+    R* FJ = sm + G::O_FJ;
+    R* FIE = sm + G::O_FIE;
     __shared__ double s_red[TJ + 1];
-    __shared__ float w[3][W_N];
-    __shared__ float wf[3][WF_N];
+    __shared__ R w[3][W_N];
+    __shared__ R wf[3][WF_N];
     __shared__ int s_tile;
     __shared__ double s_geo[4];   // 1/dx, 1/dy, 1/dz, 1/volume of the tile's block
 
@@ -184,8 +201,8 @@ __global__ void __launch_bounds__(32 * (TJ + 1), GDFV_MINB_F32E) stage_f32_kerne
     const double dt = ctl->dt_global;
     const double* __restrict__ Uin = A.Ubuf[parity];
     double* Uout = A.Ubuf[parity ^ 1];
-    const float* __restrict__ Pin = STAGE == 1 ? A.prim[parity] : A.prim1;
-    float* Pout = STAGE == 1 ? A.prim1 : A.prim[parity ^ 1];
+    const R* __restrict__ Pin = static_cast<const R*>(STAGE == 1 ? A.prim[parity] : A.prim1);
+    R* Pout = static_cast<R*>(STAGE == 1 ? A.prim1 : A.prim[parity ^ 1]);
     const long long total = A.total;
     const NumParams& P = A.P;
 
@@ -208,16 +225,16 @@ __global__ void __launch_bounds__(32 * (TJ + 1), GDFV_MINB_F32E) stage_f32_kerne
         const int nj_t = min(TJ, B.n[1] - t.j0);
         const bool active = !edge && warp < nj_t && lane < ni_t;
         const int pidx = (lane + 2) + PW * (warp + 2);     // own cell in a padded plane
-        if (tid < 3 * W_N) w[tid / W_N][tid % W_N] = (float)B.w[tid / W_N][tid % W_N];
+        if (tid < 3 * W_N) w[tid / W_N][tid % W_N] = (R)B.w[tid / W_N][tid % W_N];
         if (tid < 3) {
             s_geo[tid] = 1.0 / B.len[tid];
             const double* bw = B.w[tid];
             const double tc = bw[W_TOC];
-            wf[tid][WF_EPS] = (float)(P.eps_van_albada / (tc * tc));
-            wf[tid][WF_P1] = (float)(bw[W_AL0] * tc * bw[W_TWOL]);
-            wf[tid][WF_P2] = (float)(bw[W_AL0] * tc * bw[W_LENL0]);
-            wf[tid][WF_R1] = (float)(bw[W_AR0] * tc * bw[W_LENL0]);
-            wf[tid][WF_R2] = (float)(bw[W_AR0] * tc * bw[W_TWOL]);
+            wf[tid][WF_EPS] = (R)(P.eps_van_albada / (tc * tc));
+            wf[tid][WF_P1] = (R)(bw[W_AL0] * tc * bw[W_TWOL]);
+            wf[tid][WF_P2] = (R)(bw[W_AL0] * tc * bw[W_LENL0]);
+            wf[tid][WF_R1] = (R)(bw[W_AR0] * tc * bw[W_LENL0]);
+            wf[tid][WF_R2] = (R)(bw[W_AR0] * tc * bw[W_TWOL]);
         }
         if (tid == 3) s_geo[3] = B.vol_inv;
         __syncthreads();
@@ -226,7 +243,7 @@ __global__ void __launch_bounds__(32 * (TJ + 1), GDFV_MINB_F32E) stage_f32_kerne
         const int pstride = B.n[0] * B.n[1];
         const long long boff = B.offset;
         int c_own = (t.i0 + lane) + B.n[0] * ((t.j0 + warp) + B.n[1] * t.k0);
-        auto slot = [&](int kk) -> float* { return ring + (kk & 3) * (6 * PLANE); };
+        auto slot = [&](int kk) -> R* { return ring + (kk & 3) * (6 * PLANE); };
 
         double sig_max = 0.0;
         // halo cell of this thread in every plane: 2 columns beside each row, 2 rows
@@ -259,8 +276,8 @@ __global__ void __launch_bounds__(32 * (TJ + 1), GDFV_MINB_F32E) stage_f32_kerne
         // edge items of phases B and C (edge warp): reconstruction of 2 nj + 2 ni cells,
         // fluxes of nj east faces and ni north faces
         const int ne_rec = 2 * nj_t + 2 * ni_t, ne_flux = nj_t + ni_t;
-        float kq_prev_p[NS];   // k plus-side state of the current plane (left state of its top face)
-        float fB[NS];          // flux through the bottom face of the own cell
+        R kq_prev_p[NS];   // k plus-side state of the current plane (left state of its top face)
+        R fB[NS];          // flux through the bottom face of the own cell
         // ---------------- prologue: planes k0-2 .. k0+2 of the own column, halo of plane k0
         if (h_in) {
             put_pf(slot(t.k0), PLANE, h_dst, load_pf(Pin, total, boff + c_halo));
@@ -270,7 +287,7 @@ __global__ void __launch_bounds__(32 * (TJ + 1), GDFV_MINB_F32E) stage_f32_kerne
         c_halo += pstride;
         if (active) {
             const int gi = t.i0 + lane, gj = t.j0 + warp;
-            PF c[5];
+            PF<R> c[5];
 #pragma unroll
             for (int m = 0; m < 5; ++m) {
                 const int kk = t.k0 - 2 + m;
@@ -281,23 +298,23 @@ __global__ void __launch_bounds__(32 * (TJ + 1), GDFV_MINB_F32E) stage_f32_kerne
             put_pf(slot(t.k0), PLANE, pidx, c[2]);
             put_pf(slot(t.k0 + 1), PLANE, pidx, c[3]);
             put_pf(slot(t.k0 + 2), PLANE, pidx, c[4]);
-            float qm1[NS], q0[NS], qp1[NS], qm[NS], qpkm1[NS];
+            R qm1[NS], q0[NS], qp1[NS], qm[NS], qpkm1[NS];
             // face-local order for k: v2, v0, v1, rho, u
-            auto fr = [](const PF& x, float* q) { q[0] = x.v[2]; q[1] = x.v[0]; q[2] = x.v[1]; q[3] = x.rho; q[4] = x.u; };
+            auto fr = [](const PF<R>& x, R* q) { q[0] = x.v[2]; q[1] = x.v[0]; q[2] = x.v[1]; q[3] = x.rho; q[4] = x.u; };
             fr(c[0], qm1); fr(c[1], q0); fr(c[2], qp1);
-            recon_cell<float, NS, false, 1>(w[2], wf[2], P, qm1, q0, qp1, qm, qpkm1);
+            recon_cell<R, NS, false, 1>(w[2], wf[2], P, qm1, q0, qp1, qm, qpkm1);
             fr(c[1], qm1); fr(c[2], q0); fr(c[3], qp1);
-            recon_cell<float, NS, false, 1>(w[2], wf[2], P, qm1, q0, qp1, qm, kq_prev_p);
-            face_flux<float, false, FLUX, 2, 6>(P, 0.0f, qpkm1, qm, slot(t.k0 - 1), pidx, slot(t.k0), pidx, PLANE, fB);
+            recon_cell<R, NS, false, 1>(w[2], wf[2], P, qm1, q0, qp1, qm, kq_prev_p);
+            face_flux<R, false, FLUX, 2, 6>(P, R(0), qpkm1, qm, slot(t.k0 - 1), pidx, slot(t.k0), pidx, PLANE, fB);
         }
 
 
         __syncthreads();
 
         for (int k = t.k0; k < t.k1; ++k) {
-            float* cur = slot(k);
-            float* nx1 = slot(k + 1);
-            float* nx2 = slot(k + 2);
+            R* cur = slot(k);
+            R* nx1 = slot(k + 1);
+            R* nx2 = slot(k + 2);
             // ---------------- A: copies of the lead plane k+3 (own columns) and the halo of plane
             // k+1 into the ring, in flight during B (slot k+3 held plane k-1, last read in C of
             // plane k-1; the halo positions of slot k+1 are read first in B of plane k+1)
@@ -310,28 +327,28 @@ __global__ void __launch_bounds__(32 * (TJ + 1), GDFV_MINB_F32E) stage_f32_kerne
             cp_async_commit();
 
             // ---------------- B: i and j reconstruction
-            float qLi[NS], qmi[NS], qmj[NS];
+            R qLi[NS], qmi[NS], qmj[NS];
             {
-                float qpi[NS];
+                R qpi[NS];
                 if (active) {
-                    float qm1[NS], q0[NS], qp1[NS], qpj[NS];
-                    gather<float, NS, 0>(cur, PLANE, pidx - 1, qm1);
-                    gather<float, NS, 0>(cur, PLANE, pidx, q0);
-                    gather<float, NS, 0>(cur, PLANE, pidx + 1, qp1);
-                    recon_cell<float, NS, false, 1>(w[0], wf[0], P, qm1, q0, qp1, qmi, qpi);
+                    R qm1[NS], q0[NS], qp1[NS], qpj[NS];
+                    gather<R, NS, 0>(cur, PLANE, pidx - 1, qm1);
+                    gather<R, NS, 0>(cur, PLANE, pidx, q0);
+                    gather<R, NS, 0>(cur, PLANE, pidx + 1, qp1);
+                    recon_cell<R, NS, false, 1>(w[0], wf[0], P, qm1, q0, qp1, qmi, qpi);
                     if (lane == ni_t - 1) {
 #pragma unroll
                         for (int s = 0; s < NS; ++s) EIL[s * TJ + warp] = qpi[s];
                     }
-                    gather<float, NS, 1>(cur, PLANE, pidx - PW, qm1);
-                    gather<float, NS, 1>(cur, PLANE, pidx, q0);
-                    gather<float, NS, 1>(cur, PLANE, pidx + PW, qp1);
-                    recon_cell<float, NS, false, 1>(w[1], wf[1], P, qm1, q0, qp1, qmj, qpj);
+                    gather<R, NS, 1>(cur, PLANE, pidx - PW, qm1);
+                    gather<R, NS, 1>(cur, PLANE, pidx, q0);
+                    gather<R, NS, 1>(cur, PLANE, pidx + PW, qp1);
+                    recon_cell<R, NS, false, 1>(w[1], wf[1], P, qm1, q0, qp1, qmj, qpj);
 #pragma unroll
                     for (int s = 0; s < NS; ++s) QPJ[(s * TJ + warp) * TI + lane] = qpj[s];
                 } else {
 #pragma unroll
-                    for (int s = 0; s < NS; ++s) qpi[s] = 0.0f;
+                    for (int s = 0; s < NS; ++s) qpi[s] = R(0);
                 }
                 // left state of the W face: the plus-side state of the lane to the left
 #pragma unroll
@@ -339,16 +356,16 @@ __global__ void __launch_bounds__(32 * (TJ + 1), GDFV_MINB_F32E) stage_f32_kerne
             }
             if (edge) {
                 for (int e = lane; e < ne_rec; e += 32) {
-                    float qm1[NS], q0[NS], qp1[NS], qm[NS], qp[NS];
+                    R qm1[NS], q0[NS], qp1[NS], qm[NS], qp[NS];
                     if (e < 2 * nj_t) {            // column -1 (plus side) or ni (minus side) of row r
                         const bool east = e >= nj_t;
                         const int r = east ? e - nj_t : e;
                         const int p = (east ? ni_t + 2 : 1) + PW * (r + 2);
-                        gather<float, NS, 0>(cur, PLANE, p - 1, qm1);
-                        gather<float, NS, 0>(cur, PLANE, p, q0);
-                        gather<float, NS, 0>(cur, PLANE, p + 1, qp1);
-                        recon_cell<float, NS, false, 1>(w[0], wf[0], P, qm1, q0, qp1, qm, qp);
-                        float* dst = east ? EIE : EIW;
+                        gather<R, NS, 0>(cur, PLANE, p - 1, qm1);
+                        gather<R, NS, 0>(cur, PLANE, p, q0);
+                        gather<R, NS, 0>(cur, PLANE, p + 1, qp1);
+                        recon_cell<R, NS, false, 1>(w[0], wf[0], P, qm1, q0, qp1, qm, qp);
+                        R* dst = east ? EIE : EIW;
 #pragma unroll
                         for (int s = 0; s < NS; ++s) dst[s * TJ + r] = east ? qm[s] : qp[s];
                     } else {                       // row -1 (plus side) or nj (minus side) of column c
@@ -356,11 +373,11 @@ __global__ void __launch_bounds__(32 * (TJ + 1), GDFV_MINB_F32E) stage_f32_kerne
                         const bool north = e2 >= ni_t;
                         const int c = north ? e2 - ni_t : e2;
                         const int p = (c + 2) + PW * (north ? nj_t + 2 : 1);
-                        gather<float, NS, 1>(cur, PLANE, p - PW, qm1);
-                        gather<float, NS, 1>(cur, PLANE, p, q0);
-                        gather<float, NS, 1>(cur, PLANE, p + PW, qp1);
-                        recon_cell<float, NS, false, 1>(w[1], wf[1], P, qm1, q0, qp1, qm, qp);
-                        float* dst = north ? EJN : EJS;
+                        gather<R, NS, 1>(cur, PLANE, p - PW, qm1);
+                        gather<R, NS, 1>(cur, PLANE, p, q0);
+                        gather<R, NS, 1>(cur, PLANE, p + PW, qp1);
+                        recon_cell<R, NS, false, 1>(w[1], wf[1], P, qm1, q0, qp1, qm, qp);
+                        R* dst = north ? EJN : EJS;
 #pragma unroll
                         for (int s = 0; s < NS; ++s) dst[s * TI + c] = north ? qm[s] : qp[s];
                     }
@@ -374,44 +391,44 @@ __global__ void __launch_bounds__(32 * (TJ + 1), GDFV_MINB_F32E) stage_f32_kerne
             __syncthreads();
 
             // ---------------- C: fluxes (W, S faces; k reconstruction and the T face)
-            float fW[NS], fT[NS];
+            R fW[NS], fT[NS];
             if (active) {
                 if (lane == 0) {
 #pragma unroll
                     for (int s = 0; s < NS; ++s) qLi[s] = EIW[s * TJ + warp];
                 }
-                face_flux<float, false, FLUX, 0, 6>(P, 0.0f, qLi, qmi, cur, pidx - 1, cur, pidx, PLANE, fW);
+                face_flux<R, false, FLUX, 0, 6>(P, R(0), qLi, qmi, cur, pidx - 1, cur, pidx, PLANE, fW);
                 {
-                    float qL[NS], fS[NS];
+                    R qL[NS], fS[NS];
 #pragma unroll
                     for (int s = 0; s < NS; ++s)
                         qL[s] = warp == 0 ? EJS[s * TI + lane] : QPJ[(s * TJ + warp - 1) * TI + lane];
-                    face_flux<float, false, FLUX, 1, 6>(P, 0.0f, qL, qmj, cur, pidx - PW, cur, pidx, PLANE, fS);
+                    face_flux<R, false, FLUX, 1, 6>(P, R(0), qL, qmj, cur, pidx - PW, cur, pidx, PLANE, fS);
 #pragma unroll
                     for (int s = 0; s < NS; ++s) FJ[(s * (TJ + 1) + warp) * TI + lane] = fS[s];
                 }
                 {
-                    float qm1[NS], q0[NS], qp1[NS], kq_m[NS], kq_p[NS];
-                    gather<float, NS, 2>(cur, PLANE, pidx, qm1);
-                    gather<float, NS, 2>(nx1, PLANE, pidx, q0);
-                    gather<float, NS, 2>(nx2, PLANE, pidx, qp1);
-                    recon_cell<float, NS, false, 1>(w[2], wf[2], P, qm1, q0, qp1, kq_m, kq_p);
-                    face_flux<float, false, FLUX, 2, 6>(P, 0.0f, kq_prev_p, kq_m, cur, pidx, nx1, pidx, PLANE, fT);
+                    R qm1[NS], q0[NS], qp1[NS], kq_m[NS], kq_p[NS];
+                    gather<R, NS, 2>(cur, PLANE, pidx, qm1);
+                    gather<R, NS, 2>(nx1, PLANE, pidx, q0);
+                    gather<R, NS, 2>(nx2, PLANE, pidx, qp1);
+                    recon_cell<R, NS, false, 1>(w[2], wf[2], P, qm1, q0, qp1, kq_m, kq_p);
+                    face_flux<R, false, FLUX, 2, 6>(P, R(0), kq_prev_p, kq_m, cur, pidx, nx1, pidx, PLANE, fT);
 #pragma unroll
                     for (int s = 0; s < NS; ++s) kq_prev_p[s] = kq_p[s];
                 }
             } else {
 #pragma unroll
-                for (int s = 0; s < NS; ++s) fW[s] = 0.0f;
+                for (int s = 0; s < NS; ++s) fW[s] = R(0);
             }
             if (edge) {
                 for (int e = lane; e < ne_flux; e += 32) {
-                    float qL[NS], qR[NS], F[NS];
+                    R qL[NS], qR[NS], F[NS];
                     if (e < nj_t) {                // E face of row e
                         const int p = (ni_t + 2) + PW * (e + 2);
 #pragma unroll
                         for (int s = 0; s < NS; ++s) { qL[s] = EIL[s * TJ + e]; qR[s] = EIE[s * TJ + e]; }
-                        face_flux<float, false, FLUX, 0, 6>(P, 0.0f, qL, qR, cur, p - 1, cur, p, PLANE, F);
+                        face_flux<R, false, FLUX, 0, 6>(P, R(0), qL, qR, cur, p - 1, cur, p, PLANE, F);
 #pragma unroll
                         for (int s = 0; s < NS; ++s) FIE[s * TJ + e] = F[s];
                     } else {                       // N face of the top row, column c
@@ -422,7 +439,7 @@ __global__ void __launch_bounds__(32 * (TJ + 1), GDFV_MINB_F32E) stage_f32_kerne
                             qL[s] = QPJ[(s * TJ + nj_t - 1) * TI + c];
                             qR[s] = EJN[s * TI + c];
                         }
-                        face_flux<float, false, FLUX, 1, 6>(P, 0.0f, qL, qR, cur, p - PW, cur, p, PLANE, F);
+                        face_flux<R, false, FLUX, 1, 6>(P, R(0), qL, qR, cur, p - PW, cur, p, PLANE, F);
 #pragma unroll
                         for (int s = 0; s < NS; ++s) FJ[(s * (TJ + 1) + nj_t) * TI + c] = F[s];
                     }
@@ -433,7 +450,7 @@ __global__ void __launch_bounds__(32 * (TJ + 1), GDFV_MINB_F32E) stage_f32_kerne
             // ---------------- D: residual (e4/fvcell.d:824-856, faces W, E, S, N, B, T) and update
             {
                 // flux of the E face: the W face of the lane to the right
-                float fE[NS];
+                R fE[NS];
 #pragma unroll
                 for (int s = 0; s < NS; ++s) fE[s] = __shfl_down_sync(0xffffffffu, fW[s], 1);
                 if (active) {
@@ -441,19 +458,36 @@ __global__ void __launch_bounds__(32 * (TJ + 1), GDFV_MINB_F32E) stage_f32_kerne
 #pragma unroll
                         for (int s = 0; s < NS; ++s) fE[s] = FIE[s * TJ + warp];
                     }
+                    // face_flux turned the face-local flux (mass, normal and tangential momentum,
+                    // energy) back to the global frame: F[MASS], F[XMOM..ZMOM], F[TOTENERGY]
                     const long long g = boff + c_own;
                     const double Vi = s_geo[3];
                     const double Ai = B.area[0], Aj = B.area[1], Ak = B.area[2];
                     double dU[5];
 #pragma unroll
                     for (int q = 0; q < 5; ++q) {
-                        const float fS = FJ[(q * (TJ + 1) + warp) * TI + lane];
-                        const float fN = FJ[(q * (TJ + 1) + warp + 1) * TI + lane];
-                        const float dI = fW[q] - fE[q];
-                        const float dJ = fS - fN;
-                        double si = (double)dI * Ai + (double)dJ * Aj;
-                        si += (double)(fB[q] - fT[q]) * Ak;
-                        dU[q] = Vi * si;
+                        const R fS = FJ[(q * (TJ + 1) + warp) * TI + lane];
+                        const R fN = FJ[(q * (TJ + 1) + warp + 1) * TI + lane];
+                        if constexpr (FAST) {
+                            // float: differences of opposite faces in float (same-signed, nearly
+                            // equal fluxes subtract exactly), the sum in FP64
+                            const R dI = fW[q] - fE[q];
+                            const R dJ = fS - fN;
+                            double si = (double)dI * Ai + (double)dJ * Aj;
+                            si += (double)(fB[q] - fT[q]) * Ak;
+                            dU[q] = Vi * si;
+                        } else {
+                            // FP64: the reference's sum over the faces in their order, without
+                            // contraction (time_derivatives, e4/fvcell.d:824-856)
+                            double si = 0.0;
+                            si = __dsub_rn(si, d_mul(fW[q], -Ai));
+                            si = __dsub_rn(si, d_mul(fE[q], Ai));
+                            si = __dsub_rn(si, d_mul(fS, -Aj));
+                            si = __dsub_rn(si, d_mul(fN, Aj));
+                            si = __dsub_rn(si, d_mul(fB[q], -Ak));
+                            si = __dsub_rn(si, d_mul(fT[q], Ak));
+                            dU[q] = d_add(d_mul(Vi, si), 0.0);
+                        }
                     }
                     double U[5];
 #pragma unroll
@@ -474,7 +508,7 @@ __global__ void __launch_bounds__(32 * (TJ + 1), GDFV_MINB_F32E) stage_f32_kerne
                     }
                     Prim<double> s;
                     double p, T;
-                    const int st = decode_fast(P, U, s, p, T);
+                    const int st = FAST ? decode_fast(P, U, s, p, T) : decode(P, U, s, p, T);
                     if (st != 0) {
                         atomicAdd(&A.ctl->n_fail, 1);
                         atomicMin(reinterpret_cast<unsigned long long*>(&A.ctl->first_bad_cell),
@@ -488,7 +522,7 @@ __global__ void __launch_bounds__(32 * (TJ + 1), GDFV_MINB_F32E) stage_f32_kerne
                         }
                         if (STAGE == 2) {
                             const double inv_len[3] = {s_geo[0], s_geo[1], s_geo[2]};
-                            const double sig = signal_fast(P, inv_len, s);
+                            const double sig = FAST ? signal_fast(P, inv_len, s) : signal_frequency(P, B.len, s);
                             sig_max = fmax(sig_max, sig);
                             if (c_own == pstride * n2 - 1) A.last_signal[blk] = sig;
                         }
@@ -527,16 +561,17 @@ __global__ void __launch_bounds__(32 * (TJ + 1), GDFV_MINB_F32E) stage_f32_kerne
     }
 }
 
-// Float primitives of the state U (decode_prim with the float-flux reciprocal and
+// Primitives of the state U (decode_prim; for float, with the float-flux reciprocal and
 // square root), for P[b] of a state set from outside a stage.
-__global__ void prims_f32_kernel(const double* __restrict__ U, long long total, NumParams P, float* __restrict__ Pout) {
+template <class R>
+__global__ void prims_kernel(const double* __restrict__ U, long long total, NumParams P, R* __restrict__ Pout) {
     const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (g >= total) return;
     double u[5];
 #pragma unroll
     for (int q = 0; q < 5; ++q) u[q] = U[q * total + g];
     Prim<double> s;
-    decode_prim<true, false>(P, u, s);
+    decode_prim<sizeof(R) == 4, false>(P, u, s);
     store_pf(Pout, total, g, s);
 }
 
