@@ -185,13 +185,17 @@ def chicken_gpu_leg(n=128, steps=1000, warmup=20):
                                                         "OpenMP over blocks)", "reference chicken GPU build"))
 
 
-def adjoint_over_forward(nsteps=50, checkpoint_every=10, shape=(128, 128, 64), autotune=False):
+def adjoint_over_forward(nsteps=50, shape=(128, 128, 64), autotune=True, forms=(("resident", None), ("checkpointed", 10))):
     """Adjoint configuration: 128x128x64 M=3 inflow box (FP64, ausmdv), J = pressure
     integral over the y-min wall after 50 steps, gradient w.r.t. U0 and the inflow
-    state through the checkpointed rollout (every 10 steps).  Returns the ratio of
-    the backward time (recomputation + adjoint steps) to the forward time of the
-    same 50 steps run by gdfv_run, both with CUDA events on the device and both
-    warm (a 10-step rollout and its backward run first)."""
+    state through the rollout.  Returns the ratio of the backward time to the forward
+    time of the same 50 steps run by gdfv_run with the autotuned schedule (the forward
+    the library runs by default), both with CUDA events on the device and both warm (a
+    10-step rollout and its backward run first).  Two backward forms: the trajectory
+    resident in device memory (rollout's default when it fits: 100 states, 4.2 GB here),
+    which recomputes nothing, and a checkpoint every 10 steps with each segment
+    recomputed.  Also the time of the rollout's own forward, which keeps the trajectory
+    (one launch and one host round trip per step)."""
     import torch
     import cases
     from gdfv.autograd import rollout
@@ -212,24 +216,34 @@ def adjoint_over_forward(nsteps=50, checkpoint_every=10, shape=(128, 128, 64), a
     e1.record(stream)
     torch.cuda.synchronize()
     fwd_ms = e0.elapsed_time(e1)
-    theta = torch.tensor([inf["p"], inf["T"], inf["vel"][0]], dtype=torch.float64, requires_grad=True)
-    adj_ms = None
-    for rep in range(2):   # the first pass warms the adjoint (scratch allocation, face tables)
-        theta.grad = None
-        U0r = U0.clone().requires_grad_(True)
-        with torch.cuda.stream(stream):
-            UN = rollout(sim, U0r, theta, nsteps if rep else checkpoint_every, checkpoint_every)
-            J = wall_pressure(case, UN, case.R)
-        torch.cuda.synchronize()
-        b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        b0.record()
-        J.backward()
-        b1.record()
-        torch.cuda.synchronize()
+    out = dict(forward_ms=fwd_ms, steps=nsteps, workload=f"M=3 inflow box {shape[0]}x{shape[1]}x{shape[2]} FP64",
+               forward_schedule="autotuned" if autotune else "default tiles")
+    for label, K in forms:
+        theta = torch.tensor([inf["p"], inf["T"], inf["vel"][0]], dtype=torch.float64, requires_grad=True)
+        for rep in range(2):   # the first pass warms the adjoint (scratch allocation, face tables)
+            theta.grad = None
+            U0r = U0.clone().requires_grad_(True)
+            f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            f0.record(stream)
+            with torch.cuda.stream(stream):
+                UN = rollout(sim, U0r, theta, nsteps if rep else 10, K)
+            f1.record(stream)
+            with torch.cuda.stream(stream):
+                J = wall_pressure(case, UN, case.R)
+            torch.cuda.synchronize()
+            b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            b0.record()
+            J.backward()
+            b1.record()
+            torch.cuda.synchronize()
         adj_ms = b0.elapsed_time(b1)
-    return dict(ratio=adj_ms / fwd_ms, forward_ms=fwd_ms, adjoint_ms=adj_ms, steps=nsteps,
-                checkpoint_every=checkpoint_every, workload=f"M=3 inflow box {shape[0]}x{shape[1]}x{shape[2]} FP64",
-                dJ_dp_inflow=float(theta.grad[0]), grad_U0_norm=float(U0r.grad.norm()))
+        out[label] = dict(ratio=adj_ms / fwd_ms, adjoint_ms=adj_ms, checkpoint_every=K or nsteps,
+                          rollout_forward_ms=f0.elapsed_time(f1), dJ_dp_inflow=float(theta.grad[0]),
+                          grad_U0_norm=float(U0r.grad.norm()))
+    first = out[forms[0][0]]
+    out.update(ratio=first["ratio"], adjoint_ms=first["adjoint_ms"], checkpoint_every=first["checkpoint_every"])
+    return out
 
 
 def _timed_run(sim, stream, steps):
@@ -453,7 +467,7 @@ def main():
         torch.cuda.synchronize()
         return 0
     if args.profile_case == "adjoint":
-        adjoint_over_forward(nsteps=10, checkpoint_every=10)
+        adjoint_over_forward(nsteps=10, forms=(("checkpointed", 10),))
         torch.cuda.synchronize()
         return 0
 

@@ -1,9 +1,9 @@
 // gdfv_adjoint.cu -- hand-written vector-Jacobian product of the residual,
-// g = (dR/dU)^T w, for the Euler path with the ausmdv flux (FP64).
+// g = (dR/dU)^T w, for the Euler path (2D or 3D) with the ausmdv or hllc flux (FP64).
 //
 // The residual (e4/fvcell.d:824-856) is R_c = (1/V) sum_faces +-A F_f, each face
 // flux F_f a function of the four stencil states (e4/onedinterp.d:751-989 and
-// e4/fluxcalc.d:477-651), each state a function of U through decode_conserved
+// e4/fluxcalc.d:477-651 or :653-820), each state a function of U through decode_conserved
 // (e4/fvcell.d:586-822) or through a boundary condition (ghost cells).  The VJP
 // runs in three kernels:
 //   1. per cell: decode U -> primitive state P = (rho, v0, v1, v2, u, a);
@@ -279,6 +279,123 @@ __device__ void ausmdv_vjp(const NumParams& P, const FS& L, const FS& R, const d
     gR = FS{gr_R, gp_R, gu_R, gv_R, gw_R, ge_R, ga_R};
 }
 
+// hllc (e4/fluxcalc.d:653-820, factor 1, one gas) forward with the quantities the reverse
+// needs, then its reverse.  The Roe-averaged ratio of specific heats is gamma itself for
+// one gas (its derivative vanishes); the wave-speed min/max and the star/side switches
+// take the branches the primal values took.
+__device__ void hllc_vjp(const NumParams& P, const FS& L, const FS& R, const double* gF, FS& gL, FS& gR) {
+    // ---- forward
+    const double g = P.gas.gamma;
+    const double keL = 0.5 * (L.u * L.u + L.v * L.v + L.w * L.w);
+    const double keR = 0.5 * (R.u * R.u + R.v * R.v + R.w * R.w);
+    const double EL = L.r * L.e + L.r * keL, ER = R.r * R.e + R.r * keR;
+    const double srL = sqrt(L.r), srR = sqrt(R.r);
+    const double D = srL + srR, iD = rcp(D);
+    const double uhat = (srL * L.u + srR * R.u) * iD;
+    const double ghat = (srL * g + srR * g) * iD;
+    const double N1 = srL * L.a * L.a + srR * R.a * R.a;
+    const double sD = sqrt(D);
+    const double T = D / sD;
+    const double du = R.u - L.u;
+    const double c2 = 0.5 * (ghat - 1.0);
+    const double ahat2 = N1 * iD + c2 * T * du * du;
+    const double ahat = sqrt(ahat2);
+    const bool SLfromL = fmin(L.u - L.a, uhat - ahat) == L.u - L.a;
+    const double SL = fmin(L.u - L.a, uhat - ahat);
+    const bool SRfromR = fmax(R.u + R.a, uhat + ahat) == R.u + R.a;
+    const double SR = fmax(R.u + R.a, uhat + ahat);
+    const double num = R.p - L.p + L.r * L.u * (SL - L.u) - R.r * R.u * (SR - R.u);
+    const double den = L.r * (SL - L.u) - R.r * (SR - R.u);
+    const double iden = rcp(den);
+    const double Ss = num * iden;
+    const bool left = Ss > 0.0;
+    const FS& X = left ? L : R;
+    const double E = left ? EL : ER, S = left ? SL : SR;
+    const bool star = left ? !(SL > 0.0) : !(SR < 0.0);
+    const double dn = S - Ss, idn = star ? rcp(dn) : 0.0;
+    const double coeff = star ? X.r * (S - X.u) * idn : 0.0;
+    // ---- reverse (cotangents of the chosen side's r, p, u, v, w, E, S; of coeff, S*)
+    double gr = 0, gp = 0, gu = 0, gv = 0, gw = 0, gE = 0, gS = 0, gc = 0, gSs = 0;
+    // mass: r u (+ S (coeff - r))
+    gr += gF[MASS] * X.u; gu += gF[MASS] * X.r;
+    // momentum: r u u + p, r u v, r u w (+ S (coeff S* - r u), S (coeff - r) v, S (coeff - r) w)
+    gr += gF[XMOM] * X.u * X.u; gu += gF[XMOM] * 2.0 * X.r * X.u; gp += gF[XMOM];
+    gr += gF[YMOM] * X.u * X.v; gu += gF[YMOM] * X.r * X.v; gv += gF[YMOM] * X.r * X.u;
+    gr += gF[ZMOM] * X.u * X.w; gu += gF[ZMOM] * X.r * X.w; gw += gF[ZMOM] * X.r * X.u;
+    // energy: u (E + p) (+ S (U* - E))
+    gu += gF[TOTENERGY] * (E + X.p); gE += gF[TOTENERGY] * X.u; gp += gF[TOTENERGY] * X.u;
+    if (star) {
+        gS += gF[MASS] * (coeff - X.r); gc += gF[MASS] * S; gr -= gF[MASS] * S;
+        gS += gF[XMOM] * (coeff * Ss - X.r * X.u); gc += gF[XMOM] * S * Ss; gSs += gF[XMOM] * S * coeff;
+        gr -= gF[XMOM] * S * X.u; gu -= gF[XMOM] * S * X.r;
+        gS += gF[YMOM] * (coeff - X.r) * X.v; gc += gF[YMOM] * S * X.v; gr -= gF[YMOM] * S * X.v;
+        gv += gF[YMOM] * S * (coeff - X.r);
+        gS += gF[ZMOM] * (coeff - X.r) * X.w; gc += gF[ZMOM] * S * X.w; gr -= gF[ZMOM] * S * X.w;
+        gw += gF[ZMOM] * S * (coeff - X.r);
+        // U* = coeff (E/r + (S* - u) (S* + p/(r (S - u))))
+        const double ir = rcp(X.r), Su = S - X.u, iSu = rcp(Su);
+        const double Z = X.p * ir * iSu;
+        const double Bq = Ss - X.u, Cq = Ss + Z;
+        const double Xs = E * ir + Bq * Cq;
+        const double Ust = coeff * Xs;
+        gS += gF[TOTENERGY] * (Ust - E);
+        gE -= gF[TOTENERGY] * S;
+        const double gU = gF[TOTENERGY] * S;
+        gc += gU * Xs;
+        const double gX = gU * coeff;
+        gE += gX * ir; gr -= gX * E * ir * ir;
+        gSs += gX * Cq; gu -= gX * Cq;
+        const double gZ = gX * Bq;
+        gSs += gZ;
+        gp += gZ * ir * iSu; gr -= gZ * Z * ir;
+        const double gSu = -gZ * Z * iSu;
+        gS += gSu; gu -= gSu;
+        // coeff = r (S - u) / (S - S*)
+        gr += gc * Su * idn;
+        gS += gc * X.r * idn; gu -= gc * X.r * idn;
+        const double gdn = -gc * coeff * idn;
+        gS += gdn; gSs -= gdn;
+    }
+    // E = r e + r ke on the chosen side
+    const double ke = left ? keL : keR;
+    gr += gE * (X.e + ke);
+    double ge = gE * X.r;
+    gu += gE * X.r * X.u; gv += gE * X.r * X.v; gw += gE * X.r * X.w;
+    double gr_L = 0, gp_L = 0, gu_L = 0, gv_L = 0, gw_L = 0, ge_L = 0, ga_L = 0;
+    double gr_R = 0, gp_R = 0, gu_R = 0, gv_R = 0, gw_R = 0, ge_R = 0, ga_R = 0;
+    double gSL = 0, gSR = 0;
+    if (left) { gr_L += gr; gp_L += gp; gu_L += gu; gv_L += gv; gw_L += gw; ge_L += ge; gSL += gS; }
+    else { gr_R += gr; gp_R += gp; gu_R += gu; gv_R += gv; gw_R += gw; ge_R += ge; gSR += gS; }
+    // S* = num / den
+    const double gnum = gSs * iden, gden = -gSs * Ss * iden;
+    gp_R += gnum; gp_L -= gnum;
+    gr_L += gnum * L.u * (SL - L.u); gu_L += gnum * L.r * (SL - 2.0 * L.u); gSL += gnum * L.r * L.u;
+    gr_R -= gnum * R.u * (SR - R.u); gu_R -= gnum * R.r * (SR - 2.0 * R.u); gSR -= gnum * R.r * R.u;
+    gr_L += gden * (SL - L.u); gSL += gden * L.r; gu_L -= gden * L.r;
+    gr_R -= gden * (SR - R.u); gSR -= gden * R.r; gu_R += gden * R.r;
+    // SL = min(uL - aL, uhat - ahat), SR = max(uR + aR, uhat + ahat)
+    double guhat = 0.0, gahat = 0.0;
+    if (SLfromL) { gu_L += gSL; ga_L -= gSL; } else { guhat += gSL; gahat -= gSL; }
+    if (SRfromR) { gu_R += gSR; ga_R += gSR; } else { guhat += gSR; gahat += gSR; }
+    // ahat2 = N1 / D + c2 T du^2, T = D / sqrt(D); ahat = sqrt(ahat2)
+    const double gah2 = gahat * 0.5 / ahat;
+    const double gN1 = gah2 * iD;
+    double gD = -gah2 * N1 * iD * iD;
+    double gsrL = gN1 * L.a * L.a, gsrR = gN1 * R.a * R.a;
+    ga_L += gN1 * 2.0 * srL * L.a; ga_R += gN1 * 2.0 * srR * R.a;
+    gD += gah2 * c2 * du * du * 0.5 / sD;
+    const double gdu = gah2 * c2 * T * 2.0 * du;
+    gu_R += gdu; gu_L -= gdu;
+    // uhat = (srL uL + srR uR) / D
+    gsrL += guhat * L.u * iD; gu_L += guhat * srL * iD;
+    gsrR += guhat * R.u * iD; gu_R += guhat * srR * iD;
+    gD -= guhat * uhat * iD;
+    gsrL += gD; gsrR += gD;
+    gr_L += gsrL * 0.5 / srL; gr_R += gsrR * 0.5 / srR;
+    gL = FS{gr_L, gp_L, gu_L, gv_L, gw_L, ge_L, ga_L};
+    gR = FS{gr_R, gp_R, gu_R, gv_R, gw_R, ge_R, ga_R};
+}
+
 struct AdjArgs {
     const BlockDesc* blocks;
     const InflowState* inflow;
@@ -288,6 +405,7 @@ struct AdjArgs {
     double* gP;        // [6][total]
     double* gU;        // [nq][total]
     double* gInflow;   // [ninflow][6]
+    const double* rot; // rotations of exchange faces with an Rmatrix (9 doubles each)
     const long long* face_off;  // [3][nblocks+1] prefix counts of faces per direction
     double* lam;       // [nq][total] adjoint state of a fused step (modes 1, 2)
     double* bbuf;      // [nq][total] b = dt/2 lam + dt mu (mode 1 writes, mode 2 is its W)
@@ -321,13 +439,17 @@ struct Src {
     int kind, axis, inflow;
 };
 
+// ROT: some exchange rotates its ghosts' vectors (the face kernels without it carry
+// none of that code)
+template <bool ROT>
 __device__ Src adj_resolve(const AdjArgs& a, const BlockDesc& B, int i, int j, int k) {
     StageArgs A{};
     A.blocks = a.blocks;
-    CellSrc s = resolve<false>(A, B, i, j, k);   // no outflow boundaries with their own rule here
+    CellSrc s = resolve<false, ROT>(A, B, i, j, k);   // no outflow boundaries with their own rule here
     return Src{s.blk, s.c0, s.c1, s.kind, s.axis, s.inflow};
 }
 
+template <bool ROT>
 __device__ void adj_load(const AdjArgs& a, const Src& s, double* c) {
     if (s.kind == SRC_INFLOW) {
         const InflowState& in = a.inflow[s.inflow];
@@ -351,8 +473,13 @@ __device__ void adj_load(const AdjArgs& a, const Src& s, double* c) {
     }
     for (int m = 0; m < NP; ++m) c[m] = e[m];
     if (s.kind == SRC_MIRROR) c[1 + s.axis] = -c[1 + s.axis];
+    if (ROT && s.kind == SRC_ROTATE) {   // ghost velocity R v (flowstate.d:393-400)
+        const double* R = a.rot + 9 * s.inflow;
+        for (int r = 0; r < 3; ++r) c[1 + r] = R[3 * r] * e[1] + R[3 * r + 1] * e[2] + R[3 * r + 2] * e[3];
+    }
 }
 
+template <bool ROT>
 __device__ void adj_scatter(const AdjArgs& a, const Src& s, const double* gc) {
     if (s.kind == SRC_INFLOW) {
         for (int m = 0; m < NP; ++m) atomicAdd(&a.gInflow[s.inflow * NP + m], gc[m]);
@@ -367,6 +494,16 @@ __device__ void adj_scatter(const AdjArgs& a, const Src& s, const double* gc) {
             atomicAdd(&a.gP[m * a.total + g1], cf * gc[m]);
         }
         atomicAdd(&a.gP[5 * a.total + g0], gc[5]);
+        return;
+    }
+    if (ROT && s.kind == SRC_ROTATE) {   // the transpose of the ghost's rotation R v
+        const double* R = a.rot + 9 * s.inflow;
+        for (int m = 0; m < NP; ++m) {
+            const double v = (m >= 1 && m <= 3)
+                                 ? R[m - 1] * gc[1] + R[3 + m - 1] * gc[2] + R[6 + m - 1] * gc[3]
+                                 : gc[m];
+            atomicAdd(&a.gP[m * a.total + g0], v);
+        }
         return;
     }
     for (int m = 0; m < NP; ++m) {
@@ -397,7 +534,7 @@ __device__ __forceinline__ int face_coords(const AdjArgs& a, long long f, int& i
 // Source of stencil cell m (index -2, -1, 0, +1 along D from the face).  A face
 // whose four stencil cells lie inside its block (the other two indices always do)
 // takes them directly; the boundary rules apply to the others.
-template <int D>
+template <int D, bool ROT>
 __device__ __forceinline__ Src stencil_src(const AdjArgs& a, const BlockDesc& B, int i, int j, int k, int m) {
     const int idxD = D == 0 ? i : (D == 1 ? j : k);
     if (idxD >= 2 && idxD + 1 < B.n[D]) {
@@ -405,7 +542,7 @@ __device__ __forceinline__ Src stencil_src(const AdjArgs& a, const BlockDesc& B,
         const int c = i + B.n[0] * (j + B.n[1] * k) + (m - 2) * sD;
         return Src{&B, (long long)c, -1, SRC_CELL, D, 0};
     }
-    return adj_resolve(a, B, i - (D == 0 ? 2 - m : 0), j - (D == 1 ? 2 - m : 0), k - (D == 2 ? 2 - m : 0));
+    return adj_resolve<ROT>(a, B, i - (D == 0 ? 2 - m : 0), j - (D == 1 ? 2 - m : 0), k - (D == 2 ? 2 - m : 0));
 }
 
 // The reverse sweep of face f of direction D: cotangents gc[m] of the stencil
@@ -413,17 +550,17 @@ __device__ __forceinline__ Src stencil_src(const AdjArgs& a, const BlockDesc& B,
 // stencil reaches (if any).  Only these small records stay live: the sources
 // themselves are resolved again when the cotangents are scattered.
 // rowid identifies the line of faces (block and the two other indices).
-template <int D>
+template <int D, int FLUX, bool ROT>
 __device__ __forceinline__ void face_vjp(const AdjArgs& a, int b, int i, int j, int k, int* kind, int& inflow,
                                          double (*gc)[NP], long long& rowid) {
     const BlockDesc& B = a.blocks[b];
     rowid = (long long)b * 0x100000000ll + (D == 0 ? (long long)j + (long long)B.n[1] * k : (long long)i);
     double c[4][NP];
     for (int m = 0; m < 4; ++m) {
-        const Src sm = stencil_src<D>(a, B, i, j, k, m);
+        const Src sm = stencil_src<D, ROT>(a, B, i, j, k, m);
         kind[m] = sm.kind;
         if (sm.kind == SRC_INFLOW) inflow = sm.inflow;
-        adj_load(a, sm, c[m]);
+        adj_load<ROT>(a, sm, c[m]);
     }
     // cotangent of the face flux: F enters R_right with +A/V and R_left with -A/V
     const double AV = B.area[D] * B.vol_inv * a.w_scale;
@@ -458,7 +595,8 @@ __device__ __forceinline__ void face_vjp(const AdjArgs& a, int b, int i, int j, 
     else Rs = FS{qR[3], qR[3] * Rg * (qR[4] * Cvinv), qR[0], qR[1], qR[2], qR[4], c[2][5]};
     // ---- reverse
     FS gL, gR;
-    ausmdv_vjp(P, L, Rs, gF, gL, gR);
+    if constexpr (FLUX == FLUX_HLLC) hllc_vjp(P, L, Rs, gF, gL, gR);
+    else ausmdv_vjp(P, L, Rs, gF, gL, gR);
     gc[1][5] += gL.a;
     gc[2][5] += gR.a;
     double gqL[5] = {0, 0, 0, 0, 0}, gqR[5] = {0, 0, 0, 0, 0};
@@ -498,7 +636,7 @@ __device__ __forceinline__ void face_vjp(const AdjArgs& a, int b, int i, int j, 
 #ifndef GDFV_ADJ_MINB
 #define GDFV_ADJ_MINB 3
 #endif
-template <int D>
+template <int D, int FLUX, bool ROT>
 __device__ __forceinline__ void face_thread(const AdjArgs& a, long long f) {
     const long long* off = a.face_off + D * (a.nblocks + 1);
     const bool act = f < off[a.nblocks];
@@ -511,7 +649,7 @@ __device__ __forceinline__ void face_thread(const AdjArgs& a, long long f) {
     int b = 0, i = 0, j = 0, k = 0;
     if (act) {
         b = face_coords<D>(a, f, i, j, k);
-        face_vjp<D>(a, b, i, j, k, kind, inflow, gc, rowid);
+        face_vjp<D, FLUX, ROT>(a, b, i, j, k, kind, inflow, gc, rowid);
     }
     if (D == 0) {
         const unsigned full = 0xffffffffu;
@@ -575,17 +713,18 @@ __device__ __forceinline__ void face_thread(const AdjArgs& a, long long f) {
     if (!act) return;
     const BlockDesc& B = a.blocks[b];
     for (int m = 0; m < 4; ++m)
-        if (kind[m] >= 0) adj_scatter(a, stencil_src<D>(a, B, i, j, k, m), gc[m]);
+        if (kind[m] >= 0) adj_scatter<ROT>(a, stencil_src<D, ROT>(a, B, i, j, k, m), gc[m]);
 }
 
 // All faces of the three directions in one launch: CTAs [0, nb0) take the i faces,
 // [nb0, nb0 + nb1) the j faces, the rest the k faces (128 faces per CTA).
 constexpr int FACE_CTA = 128;
+template <int FLUX, bool ROT>
 __global__ void __launch_bounds__(FACE_CTA, GDFV_ADJ_MINB) adj_faces_kernel(AdjArgs a, unsigned nb0, unsigned nb1) {
     const unsigned bid = blockIdx.x;
-    if (bid < nb0) face_thread<0>(a, (long long)bid * FACE_CTA + threadIdx.x);
-    else if (bid < nb0 + nb1) face_thread<1>(a, (long long)(bid - nb0) * FACE_CTA + threadIdx.x);
-    else face_thread<2>(a, (long long)(bid - nb0 - nb1) * FACE_CTA + threadIdx.x);
+    if (bid < nb0) face_thread<0, FLUX, ROT>(a, (long long)bid * FACE_CTA + threadIdx.x);
+    else if (bid < nb0 + nb1) face_thread<1, FLUX, ROT>(a, (long long)(bid - nb0) * FACE_CTA + threadIdx.x);
+    else face_thread<2, FLUX, ROT>(a, (long long)(bid - nb0 - nb1) * FACE_CTA + threadIdx.x);
 }
 
 // gU = (dP/dU)^T gP for P = decode(U) (e4/fvcell.d:586-822 with ideal_gas.d:98-139)
@@ -642,10 +781,24 @@ using namespace gdfv;
 
 namespace {
 
+// The face kernel of the context's flux calculator (and rotating exchanges, if any) over
+// nb[d] CTAs of each direction.
+template <int FLUX>
+void launch_faces_flux(const AdjArgs& a, bool rot, const unsigned* nb, cudaStream_t s) {
+    const unsigned n = nb[0] + nb[1] + nb[2];
+    if (rot) adj_faces_kernel<FLUX, true><<<n, FACE_CTA, 0, s>>>(a, nb[0], nb[1]);
+    else adj_faces_kernel<FLUX, false><<<n, FACE_CTA, 0, s>>>(a, nb[0], nb[1]);
+}
+
+void launch_faces(const AdjArgs& a, int flux, const unsigned* nb, cudaStream_t s) {
+    if (flux == FLUX_HLLC) launch_faces_flux<FLUX_HLLC>(a, a.P.rotating, nb, s);
+    else launch_faces_flux<FLUX_AUSMDV>(a, a.P.rotating, nb, s);
+}
+
 bool vjp_supported(int ctx, const AdjView& v) {
     if (!v.prepared) { adjoint_set_error(ctx, "call gdfv_prepare first"); return false; }
-    if (v.mhd || v.flux != FLUX_AUSMDV || v.dims != 3 || v.P.lmr_epsilon) {
-        adjoint_set_error(ctx, "the adjoint supports the 3D Euler path with flux_calculator=ausmdv "
+    if (v.mhd || (v.flux != FLUX_AUSMDV && v.flux != FLUX_HLLC) || v.P.lmr_epsilon) {
+        adjoint_set_error(ctx, "the adjoint supports the Euler path with flux_calculator=ausmdv or hllc "
                                "and van_albada_variant=e4");
         return false;
     }
@@ -682,6 +835,7 @@ cudaError_t vjp_setup(const AdjView& v, AdjArgs& a, std::vector<long long>& off)
     a = AdjArgs{};
     a.blocks = v.d_blocks;
     a.inflow = v.d_inflow;
+    a.rot = v.d_rot;
     a.Pp = base;
     a.gP = base + 6 * total;
     a.bbuf = base + 12 * total;
@@ -695,7 +849,9 @@ cudaError_t vjp_setup(const AdjView& v, AdjArgs& a, std::vector<long long>& off)
     for (int d = 0; d < 3; ++d) {
         for (int b = 0; b < v.nblocks; ++b) {
             const BlockDesc& B = v.h_blocks[b];
-            long long nf = (long long)(B.n[0] + (d == 0)) * (B.n[1] + (d == 1)) * (B.n[2] + (d == 2));
+            // 2D blocks have no k faces (the residual sums four faces)
+            long long nf = (v.dims == 2 && d == 2) ? 0
+                                                   : (long long)(B.n[0] + (d == 0)) * (B.n[1] + (d == 1)) * (B.n[2] + (d == 2));
             off[d * (v.nblocks + 1) + b + 1] = off[d * (v.nblocks + 1) + b] + nf;
         }
     }
@@ -716,7 +872,7 @@ cudaError_t enqueue_vjp(const AdjView& v, const AdjArgs& a, const std::vector<lo
     if (e == cudaSuccess) {
         unsigned nb[3];
         for (int d = 0; d < 3; ++d) nb[d] = (unsigned)((off[d * (v.nblocks + 1) + v.nblocks] + 127) / 128);
-        adj_faces_kernel<<<nb[0] + nb[1] + nb[2], FACE_CTA, 0, v.stream>>>(a, nb[0], nb[1]);
+        launch_faces(a, v.flux, nb, v.stream);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) {
@@ -766,7 +922,7 @@ struct VjpChain {
         if (e == cudaSuccess) {
             unsigned nb[3];
             for (int d = 0; d < 3; ++d) nb[d] = (unsigned)((off[d * (v.nblocks + 1) + v.nblocks] + 127) / 128);
-            adj_faces_kernel<<<nb[0] + nb[1] + nb[2], FACE_CTA, 0, v.stream>>>(a, nb[0], nb[1]);
+            launch_faces(a, v.flux, nb, v.stream);
             e = cudaGetLastError();
         }
         back = a;

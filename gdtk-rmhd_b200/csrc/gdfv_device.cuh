@@ -50,6 +50,7 @@ struct NumParams {
     int lmr_epsilon;    // van Albada epsilon scaled per face (lmr/onedinterp.d:147-151)
     int outflow_bcs;    // some face has OutFlowBC_FixedP, _FixedPT or _SimpleFlux
     int graded;         // some block has cell lengths varying along an axis
+    int rotating;       // some exchange face rotates its ghosts' vectors (Rmatrix)
 };
 
 // Fixed ghost state of a supersonic-inflow face (FlowStateCopy, flow_state_copy.d:92-107)
@@ -68,6 +69,13 @@ struct BlockDesc {
     double x0, y0, z0;
     double w[3][W_N];     // l2r2 weights per direction
     int bc_type[6], bc_xorder[6], bc_other[6], bc_other_face[6], bc_inflow[6];
+    // exchange faces: the partner's cell (index within its block) that feeds the ghost
+    // (i, j, k) is x[0] + x[1] i + x[2] j + x[3] k (every partner index is this block's
+    // i, j, k or the ghost's depth, possibly counted from the far end: affine in i, j, k);
+    // bc_xrot = 1 + the index of the rotation of the ghost's vectors in StageArgs::rot,
+    // 0 for none
+    int bc_xlin[6][4];
+    int bc_xrot[6];
     int graded;           // rectilinear block with cell lengths varying along each axis
     // graded: cell lengths of cells -2 .. n+1 (index c + 2), ghosts as the boundary gives
     // them, and the l2r2 weights of cells -1 .. n (index (c + 1) * GW_N), per direction

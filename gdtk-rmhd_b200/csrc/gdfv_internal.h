@@ -15,6 +15,7 @@ struct NoallocView {
     const BlockDesc* d_blocks;
     const TileDesc* d_tiles;
     const InflowState* d_inflow;
+    const double* d_rot;         // exchange rotations (9 doubles each), null if none
     NumParams P;
     double c_h;
     cudaStream_t stream;
@@ -33,6 +34,7 @@ struct AdjView {
     long long total;
     const BlockDesc* d_blocks;
     const InflowState* d_inflow;
+    const double* d_rot;    // exchange rotations (9 doubles each), null if none
     NumParams P;
     cudaStream_t stream;
     std::vector<BlockDesc> h_blocks;

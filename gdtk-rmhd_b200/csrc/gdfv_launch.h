@@ -54,12 +54,12 @@ inline int tile_rows_corrector(int precision, bool mhd) {
 
 // Options under which the float-flux Euler stages run the kernel on decoded primitives
 // (gdfv_stage_prim.cuh) when the arguments carry primitive buffers (the FP64 form keeps
-// stage_kernel: measured faster there, see the design notes): the
+// stage_kernel, which ran faster than an FP64 build of the primitive kernel): the
 // defaults (limiter and extrema clipping on, e4 epsilon), no outflow boundary with a
-// flux or ghost rule of its own, no graded block, 3D.
+// flux or ghost rule of its own, no graded block, no exchange with an Rmatrix, 3D.
 inline bool prim_path(const NumParams& P) {
     return !P.mhd && P.apply_limiter && P.extrema_clipping && !P.lmr_epsilon && !P.outflow_bcs && !P.graded &&
-           P.dims == 3;
+           !P.rotating && P.dims == 3;
 }
 
 // Launch one stage (0 = residual only, 1 = predictor, 2 = corrector) over A.n_tiles tiles.

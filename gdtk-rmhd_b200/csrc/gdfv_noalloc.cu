@@ -165,6 +165,7 @@ extern "C" int gdfv_step_noalloc(int ctx, const double* U_in_dev, double* U_out_
     A.blocks = v.d_blocks;
     A.tiles = v.d_tiles;
     A.inflow = v.d_inflow;
+    A.rot = v.d_rot;
     A.Ubuf[0] = const_cast<double*>(U_in_dev);  // read by both stages (step parity 0)
     A.Ubuf[1] = U_out_dev;                      // written by the corrector
     A.dU0 = base;

@@ -189,6 +189,9 @@ struct HostBC {
     int type = BC_SLIP_WALL;
     int x_order = 0;
     int other = -1, other_face = -1;
+    int orientation = 0;      // exchange: ExchangeBC_FullFace orientation 0..3
+    int rotate = 0;           // exchange: rot holds an Rmatrix for the ghosts' vectors
+    double rot[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
     double inflow[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
 };
 
@@ -256,6 +259,7 @@ struct Context {
     double* jvp_scratch = nullptr;     // Frechet JVP work arrays (U + sigma v, R0, R1, partial sums)
     double* norm_scratch = nullptr;    // per-CTA partials and result of gdfv_residual_norms
     double* d_geom = nullptr;          // graded blocks: cell lengths and l2r2 weights per direction
+    double* d_rot = nullptr;           // rotations of exchange faces with an Rmatrix, 9 doubles each
     int adj_ready = 0;
     long long adj_scratch_n = 0;
     cudaStream_t aux_stream[2] = {nullptr, nullptr};  // lowest / highest priority streams of the rollout adjoint
@@ -272,7 +276,7 @@ struct Context {
         if (graph) cudaGraphExecDestroy(graph);
         for (void* p : {(void*)U[0], (void*)U[1], (void*)dU0, (void*)d_blocks, (void*)d_tiles, (void*)d_inflow,
                         (void*)d_ctl, (void*)d_maxsig, (void*)d_lastsig, (void*)d_bad, (void*)adj_scratch, (void*)jvp_scratch,
-                        (void*)norm_scratch, (void*)prim[0], (void*)prim[1], (void*)prim1, (void*)d_geom,
+                        (void*)norm_scratch, (void*)prim[0], (void*)prim[1], (void*)prim1, (void*)d_geom, (void*)d_rot,
                         (void*)step_ctl, (void*)step_maxsig, (void*)step_lastsig})
             if (p) cudaFree(p);
         if (h_ctl) cudaFreeHost(h_ctl);
@@ -358,6 +362,7 @@ StageArgs stage_args(Context* c) {
     A.blocks = c->d_blocks;
     A.tiles = c->d_tiles;
     A.inflow = c->d_inflow;
+    A.rot = c->d_rot;
     A.Ubuf[0] = c->U[0];
     A.Ubuf[1] = c->U[1];
     A.U_in = nullptr;
@@ -512,6 +517,64 @@ void build_tiles(Context* c, int kchunk, std::vector<TileDesc>& tiles, int& n1, 
     }
 }
 
+// The cell that feeds each ghost of an ExchangeBC_FullFace, as a map word: for the
+// partner's index along axis d, bits 3d..3d+1 select this block's i, j, k or the ghost's
+// depth (0..3), and bit 3d+2 counts it from the partner's far end.  GhostCellFullFaceCopy.set_up_cell_mapping_phase0
+// (e4/bc/ghost_cell_effect/full_face_copy.d:680-1409) spells it out for 6 x 6 face pairs
+// and 4 orientations; every case there follows one rule, restated here.  Each face has
+// a tangential frame of two axes with signs, right-handed about its outward normal:
+// west (-j, k), east (j, k), south (i, k), north (-i, k), bottom (-i, j), top (i, j).
+// Seen from the partner the ghost's frame is mirrored (first axis reversed), then turned
+// by `orientation` quarter turns ((a, b) -> (-b, a) each); its coordinates are then the
+// source's coordinates in the partner face's frame.  Along the partner's normal the
+// source lies `depth` cells inside the face.  2D blocks take orientation 0, as there.
+const int kFaceAxis[6][2] = {{1, 2}, {1, 2}, {0, 2}, {0, 2}, {0, 1}, {0, 1}};
+const int kFaceSign[6][2] = {{-1, 1}, {1, 1}, {1, 1}, {-1, 1}, {-1, 1}, {1, 1}};
+
+int exchange_map(int dims, int face, int other_face, int orientation) {
+    int ax[2] = {kFaceAxis[face][0], kFaceAxis[face][1]};
+    int sg[2] = {-kFaceSign[face][0], kFaceSign[face][1]};
+    const int turns = dims == 2 ? 0 : orientation;
+    for (int t = 0; t < turns; ++t) {
+        const int a0 = ax[0], s0 = sg[0];
+        ax[0] = ax[1]; sg[0] = -sg[1];
+        ax[1] = a0; sg[1] = s0;
+    }
+    int sel[3], flip[3];
+    sel[other_face / 2] = 3;
+    flip[other_face / 2] = other_face & 1;
+    for (int r = 0; r < 2; ++r) {
+        const int d = kFaceAxis[other_face][r];
+        sel[d] = ax[r];
+        flip[d] = kFaceSign[other_face][r] * sg[r] < 0;
+    }
+    int xm = 0;
+    for (int d = 0; d < 3; ++d) xm |= (sel[d] | (flip[d] << 2)) << (3 * d);
+    return xm;
+}
+
+// The map as the kernels evaluate it: partner cell = x[0] + x[1] i + x[2] j + x[3] k for
+// the ghost (i, j, k) beyond face `face` (depth = -1 - index on a minus face, index - n
+// on a plus face).  Block cell counts are below 2^31, so the coefficients fit an int.
+void exchange_linear(int xm, int face, const int* n, const int* on, int* x) {
+    const int ax = face / 2, plus = face & 1;
+    const long long stride[3] = {1, (long long)on[0], (long long)on[0] * on[1]};
+    long long c[4] = {0, 0, 0, 0};
+    for (int d = 0; d < 3; ++d) {
+        const int sel = (xm >> (3 * d)) & 3, flip = (xm >> (3 * d + 2)) & 1;
+        // v = a + b * (this block's index along axis `src`)
+        const int src = sel == 3 ? ax : sel;
+        long long a = 0, b = 1;
+        if (sel == 3) { a = plus ? -(long long)n[ax] : -1; b = plus ? 1 : -1; }
+        // p = flip ? on[d] - 1 - v : v
+        long long pa = flip ? on[d] - 1 - a : a, pb = flip ? -b : b;
+        c[0] += stride[d] * pa;
+        c[1 + src] += stride[d] * pb;
+    }
+    // kept modulo 2^32: the kernels evaluate the sum in 32-bit wrap-around arithmetic
+    for (int m = 0; m < 4; ++m) x[m] = (int)(unsigned)(unsigned long long)c[m];
+}
+
 int do_prepare(Context* c) {
     Config& g = c->cfg;
     if (c->blocks.empty()) return fail(c, GDFV_ERR_STATE, "no blocks");
@@ -524,6 +587,7 @@ int do_prepare(Context* c) {
     std::vector<InflowState> inflows;
     struct FixedState { int block, face; InflowState state; };
     std::vector<FixedState> fixed;
+    std::vector<double> rots;   // Rmatrix of each rotating exchange face
     int outflow_bcs = 0;
     c->h_blocks.clear();
     c->h_inflow.clear();
@@ -562,15 +626,29 @@ int do_prepare(Context* c) {
             B.bc_other_face[f] = bc.other_face;
             B.bc_inflow[f] = -1;
             if (f >= nfaces) continue;
+            for (int m = 0; m < 4; ++m) B.bc_xlin[f][m] = 0;
+            B.bc_xrot[f] = 0;
             if (bc.type == BC_EXCHANGE) {
                 if (bc.other < 0 || bc.other >= (int)c->blocks.size())
                     return fail(c, GDFV_ERR_ARG, "exchange partner block does not exist");
-                if (bc.other_face / 2 != f / 2 || bc.other_face == f)
-                    return fail(c, GDFV_ERR_ARG, "exchange (orientation 0) joins opposite faces of the same index direction");
+                if (bc.other_face < 0 || bc.other_face >= nfaces)
+                    return fail(c, GDFV_ERR_ARG, "exchange partner face does not exist");
+                if (bc.orientation < 0 || bc.orientation > 3)
+                    return fail(c, GDFV_ERR_ARG, "exchange orientation must be 0..3");
                 const HostBlock& ob = c->blocks[bc.other];
-                for (int d = 0; d < 3; ++d)
-                    if (d != f / 2 && ob.n[d] != hb.n[d]) return fail(c, GDFV_ERR_ARG, "exchange faces differ in size");
-                if (ob.n[f / 2] < 2) return fail(c, GDFV_ERR_ARG, "exchange partner is too thin");
+                const int xm = exchange_map(g.dims, f, bc.other_face, bc.orientation);
+                for (int d = 0; d < 3; ++d) {
+                    const int sel = (xm >> (3 * d)) & 3;
+                    if (sel < 3 && ob.n[d] != hb.n[sel])
+                        return fail(c, GDFV_ERR_ARG, "exchange faces differ in size (block " + std::to_string(b) +
+                                                         " face " + std::to_string(f) + ")");
+                }
+                if (ob.n[bc.other_face / 2] < 2) return fail(c, GDFV_ERR_ARG, "exchange partner is too thin");
+                exchange_linear(xm, f, hb.n, ob.n, B.bc_xlin[f]);
+                if (bc.rotate) {
+                    B.bc_xrot[f] = (int)(1 + rots.size() / 9);
+                    rots.insert(rots.end(), bc.rot, bc.rot + 9);
+                }
             }
             if (bc.type == BC_EXTRAPOLATE && (bc.x_order < 0 || bc.x_order > 1))
                 return fail(c, GDFV_ERR_ARG, "x_order must be 0 or 1");
@@ -637,8 +715,10 @@ int do_prepare(Context* c) {
                 for (int m = 0; m < 2; ++m) {
                     double v;
                     if (bc.type == BC_EXCHANGE && 2 * d + side < nfaces) {
+                        // the partner's cell m layers inside its face, along its normal
                         const HostBlock& ob = c->blocks[bc.other];
-                        v = ob.cell_len(d, (bc.other_face & 1) ? ob.n[d] - 1 - m : m);
+                        const int od = bc.other_face / 2;
+                        v = ob.cell_len(od, (bc.other_face & 1) ? ob.n[od] - 1 - m : m);
                     } else {
                         v = hb.cell_len(d, side ? n - 1 - m : m);
                     }
@@ -673,6 +753,7 @@ int do_prepare(Context* c) {
     P.stringent_cfl = g.stringent_cfl; P.nq = c->nq; P.lmr_epsilon = g.lmr_epsilon;
     P.outflow_bcs = outflow_bcs;
     P.graded = any_graded;
+    P.rotating = !rots.empty();
     StepParams& sp = c->sp;
     sp.cfl_count = g.cfl_count; sp.n_stages = 2; sp.fixed_time_step = g.fixed_time_step;
     sp.mhd_cleaning = g.mhd && g.divergence_cleaning;
@@ -716,6 +797,10 @@ int do_prepare(Context* c) {
                 c->h_blocks[b].gw[d] = c->d_geom + geom_at[b][3 + d];
             }
         }
+    }
+    if (!rots.empty()) {
+        CK(cudaMalloc(&c->d_rot, sizeof(double) * rots.size()));
+        CK(cudaMemcpy(c->d_rot, rots.data(), sizeof(double) * rots.size(), cudaMemcpyHostToDevice));
     }
     CK(cudaMalloc(&c->d_blocks, sizeof(BlockDesc) * c->h_blocks.size()));
     CK(cudaMemcpy(c->d_blocks, c->h_blocks.data(), sizeof(BlockDesc) * c->h_blocks.size(), cudaMemcpyHostToDevice));
@@ -788,6 +873,7 @@ bool noalloc_view(int ctx, NoallocView* v) {
     v->d_blocks = c->d_blocks;
     v->d_tiles = c->d_tiles;
     v->d_inflow = c->d_inflow;
+    v->d_rot = c->d_rot;
     v->P = c->P;
     v->c_h = c->h_ctl ? c->h_ctl->c_h : 0.0;
     v->stream = c->stream;
@@ -822,6 +908,7 @@ bool adjoint_view(int ctx, AdjView* v) {
     v->total = c->total;
     v->d_blocks = c->d_blocks;
     v->d_inflow = c->d_inflow;
+    v->d_rot = c->d_rot;
     v->P = c->P;
     v->stream = c->stream;
     v->h_blocks = c->h_blocks;
@@ -1165,6 +1252,46 @@ int gdfv_block_set_bc(int ctx, int blk, int face, const char* bc_type, int x_ord
         bc.inflow[1] = bc.type == BC_FIXED_PT ? inflow[1] : 0.0;
     }
     c->blocks[blk].bc[face] = bc;
+    return GDFV_OK;
+}
+
+int gdfv_block_set_exchange(int ctx, int blk, int face, int other_blk, int other_face, int orientation,
+                            const double* Rmatrix) {
+    const int rc = gdfv_block_set_bc(ctx, blk, face, "exchange_over_full_face", 0, other_blk, other_face, nullptr);
+    if (rc != GDFV_OK) return rc;
+    Context* c = get_ctx(ctx);
+    if (orientation < 0 || orientation > 3) return fail(c, GDFV_ERR_ARG, "exchange orientation must be 0..3");
+    HostBC& bc = c->blocks[blk].bc[face];
+    bc.orientation = orientation;
+    if (Rmatrix) {
+        for (int m = 0; m < 9; ++m)
+            if (!std::isfinite(Rmatrix[m])) return fail(c, GDFV_ERR_ARG, "Rmatrix entries must be finite");
+        bc.rotate = 1;
+        for (int m = 0; m < 9; ++m) bc.rot[m] = Rmatrix[m];
+    }
+    return GDFV_OK;
+}
+
+int gdfv_exchange_source(int dims, int face, int other_face, int orientation, const int* n_this, const int* n_other,
+                         const int* ijk, int* src) {
+    const int nf = dims == 3 ? 6 : 4;
+    if ((dims != 2 && dims != 3) || face < 0 || face >= nf || other_face < 0 || other_face >= nf || orientation < 0 ||
+        orientation > 3 || !n_this || !n_other || !ijk || !src)
+        return fail(nullptr, GDFV_ERR_ARG, "gdfv_exchange_source: bad dims, face, orientation or pointer");
+    const int ax = face / 2;
+    const int depth = (face & 1) ? ijk[ax] - n_this[ax] : -1 - ijk[ax];
+    for (int d = 0; d < 3; ++d)
+        if (d != ax && (ijk[d] < 0 || ijk[d] >= n_this[d]))
+            return fail(nullptr, GDFV_ERR_ARG, "gdfv_exchange_source: ghost cell not beside the face");
+    if (depth < 0 || depth > 1) return fail(nullptr, GDFV_ERR_ARG, "gdfv_exchange_source: ghost depth must be 0 or 1");
+    const int xm = exchange_map(dims, face, other_face, orientation);
+    for (int d = 0; d < 3; ++d) {
+        const int sel = (xm >> (3 * d)) & 3;
+        const int v = sel == 3 ? depth : ijk[sel];
+        src[d] = ((xm >> (3 * d + 2)) & 1) ? n_other[d] - 1 - v : v;
+        if (src[d] < 0 || src[d] >= n_other[d])
+            return fail(nullptr, GDFV_ERR_ARG, "gdfv_exchange_source: the faces differ in size under this map");
+    }
     return GDFV_OK;
 }
 

@@ -55,6 +55,8 @@ struct StageArgs {
     // conserved state
     void* prim[2];
     void* prim1;
+    // rotations of exchange faces with an Rmatrix (9 doubles each, row major)
+    const double* rot;
 };
 
 // Compile-time geometry of the tile and of the shared-memory layout.
@@ -93,7 +95,7 @@ __device__ __forceinline__ long long cell_index(const BlockDesc& B, int i, int j
 
 // Where the state of block cell (i,j,k) comes from.
 enum : int { SRC_CELL = 0, SRC_MIRROR = 1, SRC_EXTRAP1_G0 = 2, SRC_EXTRAP1_G1 = 3, SRC_INFLOW = 4, SRC_FIXEDP = 5,
-             SRC_FIXEDPT = 6 };
+             SRC_FIXEDPT = 6, SRC_ROTATE = 7 };
 struct CellSrc {
     const BlockDesc* blk;  // block holding the source cell(s)
     long long c0, c1;      // source cell (and the depth-1 cell for xOrder 1)
@@ -103,8 +105,9 @@ struct CellSrc {
 // At most one index may lie outside the block; the boundary condition of that
 // face supplies the ghost (e4/bc/ghost_cell_effect/*.d).
 // OUTF false: no face of the launch has an OutFlowBC_FixedP, _FixedPT or _SimpleFlux
-// boundary (those branches are left out).
-template <bool OUTF = true>
+// boundary (those branches are left out).  ROT false: no exchange face rotates its
+// ghosts' vectors (SRC_ROTATE is never returned).
+template <bool OUTF = true, bool ROT = true>
 __device__ __forceinline__ CellSrc resolve(const StageArgs& A, const BlockDesc& B, int i, int j, int k) {
     CellSrc s;
     s.blk = &B; s.c1 = -1; s.kind = SRC_CELL; s.axis = 0; s.inflow = 0;
@@ -147,13 +150,19 @@ __device__ __forceinline__ CellSrc resolve(const StageArgs& A, const BlockDesc& 
         s.kind = SRC_INFLOW;
         s.c0 = -1;
         s.inflow = B.bc_inflow[face];
-    } else {                            // full_face_copy.d: partner's interior cell n from its face
-        const BlockDesc& O = A.blocks[B.bc_other[face]];
-        const int of = B.bc_other_face[face];
-        const int onax = axis == 0 ? O.n[0] : (axis == 1 ? O.n[1] : O.n[2]);
-        int a = (of & 1) ? (onax - 1 - depth) : depth;
-        s.blk = &O;
-        s.c0 = cell_index(O, axis == 0 ? a : i, axis == 1 ? a : j, axis == 2 ? a : k);
+    } else {
+        // full_face_copy.d:680-1409: the partner's cell `depth` layers inside its face,
+        // at the tangential position the face pair and orientation give (bc_xlin; 32-bit
+        // wrap-around arithmetic, exact since the result is a cell index below 2^31)
+        const int* x = B.bc_xlin[face];
+        s.blk = &A.blocks[B.bc_other[face]];
+        s.c0 = (int)((unsigned)x[0] + (unsigned)x[1] * (unsigned)i + (unsigned)x[2] * (unsigned)j +
+                     (unsigned)x[3] * (unsigned)k);
+        const int rot = ROT ? B.bc_xrot[face] : 0;
+        if (rot) {                      // full_face_copy.d:2403-2405 reorient_vector_quantities
+            s.kind = SRC_ROTATE;
+            s.inflow = rot - 1;
+        }
     }
     return s;
 }
@@ -209,6 +218,27 @@ __device__ __forceinline__ void decode_prim_g(double Cvinv, double gR, const dou
 template <bool FAST, bool MHD>
 __device__ __forceinline__ void decode_prim(const NumParams& P, const double* U, Prim<double>& s) {
     decode_prim_g<FAST, MHD>(P.gas.Cvinv, P.gas.gamma * P.gas.R, U, s);
+}
+
+// flowstate.d:393-400 reorient_vector_quantities: velocity (and B) times the row-major
+// matrix R (vector3.d:453-460 apply_matrix_transform, its operation order).  Rare path,
+// out of line, with the state passed by value (no caller state needs an address).
+template <bool MHD>
+__device__ __noinline__ Prim<double> rotate_vectors(const double* R, Prim<double> s) {
+    double r[9];
+#pragma unroll
+    for (int m = 0; m < 9; ++m) r[m] = __ldg(R + m);
+    const double x = s.v[0], y = s.v[1], z = s.v[2];
+    s.v[0] = d_add(d_add(d_mul(r[0], x), d_mul(r[1], y)), d_mul(r[2], z));
+    s.v[1] = d_add(d_add(d_mul(r[3], x), d_mul(r[4], y)), d_mul(r[5], z));
+    s.v[2] = d_add(d_add(d_mul(r[6], x), d_mul(r[7], y)), d_mul(r[8], z));
+    if (MHD) {
+        const double bx = s.B[0], by = s.B[1], bz = s.B[2];
+        s.B[0] = d_add(d_add(d_mul(r[0], bx), d_mul(r[1], by)), d_mul(r[2], bz));
+        s.B[1] = d_add(d_add(d_mul(r[3], bx), d_mul(r[4], by)), d_mul(r[5], bz));
+        s.B[2] = d_add(d_add(d_mul(r[6], bx), d_mul(r[7], by)), d_mul(r[8], bz));
+    }
+    return s;
 }
 
 // extrapolate_copy.d:171-201 linearly_extrapolate_flowstate; fields the
@@ -290,7 +320,9 @@ __device__ __forceinline__ void finish_cell(const StageArgs& A, const double* Ui
             if (x > -0.4136 && x < 0.4136) dipole_field(x, y, out.B[0], out.B[1]);
         }
     } else if (s.kind > SRC_MIRROR) {   // the rare kinds, out of line (SRC_INFLOW returned above)
-        if (OUTF && s.kind >= SRC_FIXEDP) {
+        if (OUTF && s.kind == SRC_ROTATE) {
+            out = rotate_vectors<MHD>(A.rot + 9 * s.inflow, out);
+        } else if (OUTF && s.kind >= SRC_FIXEDP) {
             const InflowState& o = A.inflow[s.inflow];
             out = fixed_ghost(out, s.kind == SRC_FIXEDP, o.p, o.rho, o.u, A.P.gas.Cvinv, A.P.gas.Cv, A.P.gas.R);
         } else {
@@ -708,7 +740,8 @@ __device__ __forceinline__ double signal_fast(const NumParams& P, const double* 
 }
 
 // Load the state of up to two cells per thread (on[m] says which): resolve, issue
-// every global load, then decode (keeps the loads in flight together).
+// every global load, then decode (keeps the loads in flight together).  OUTF false:
+// no outflow boundary with a rule of its own and no rotating exchange in the launch.
 template <int STAGE, bool FAST, bool MHD, int NQ, bool OUTF>
 __device__ __forceinline__ void load_two(const StageArgs& A, const double* Uin, const BlockDesc& B, double dt,
                                          double damp, bool on0, bool on1, const int* ci, const int* cj, const int* ck,
@@ -719,7 +752,7 @@ __device__ __forceinline__ void load_two(const StageArgs& A, const double* Uin, 
 #pragma unroll
     for (int m = 0; m < 2; ++m) {
         if (on[m]) {
-            s[m] = resolve<OUTF>(A, B, ci[m], cj[m], ck[m]);
+            s[m] = resolve<OUTF, OUTF>(A, B, ci[m], cj[m], ck[m]);
             if (s[m].kind != SRC_INFLOW) fetch_U<STAGE, NQ>(A, Uin, *s[m].blk, s[m].c0, dt, damp, U0[m]);
         }
     }

@@ -42,9 +42,10 @@ template <int STAGE, bool MHD, int FLUX, int TJ>
 cudaError_t launch_rows(const StageArgs& A, cudaStream_t s) {
     using G = Geo<Real, MHD, TJ>;
     // defaults (limiter and extrema clipping on, e4 epsilon, none of the outflow
-    // boundaries with their own ghost or flux rule, uniform blocks) take the specialised
-    // path, which also has the persistent form
-    if (A.P.apply_limiter && A.P.extrema_clipping && !A.P.lmr_epsilon && !A.P.outflow_bcs && !A.P.graded) {
+    // boundaries with their own ghost or flux rule, uniform blocks, no exchange with an
+    // Rmatrix) take the specialised path, which also has the persistent form
+    if (A.P.apply_limiter && A.P.extrema_clipping && !A.P.lmr_epsilon && !A.P.outflow_bcs && !A.P.graded &&
+        !A.P.rotating) {
         const int cap = resident<STAGE, MHD, FLUX, TJ>();
         if (A.persistent && cap > 0)
             stage_kernel<STAGE, Real, MHD, FLUX, TJ, 1, 1><<<cap < A.n_tiles ? cap : A.n_tiles, G::NT, G::bytes, s>>>(A);

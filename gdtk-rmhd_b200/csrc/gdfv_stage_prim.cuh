@@ -78,11 +78,11 @@ __device__ __forceinline__ void put_pf(R* base, int stride, int idx, const PF<R>
 // synthesis: mirror with negated normal velocity (internal_copy_then_reflect.d),
 // copy or linear extrapolation of rho, u and velocity with a from the boundary cell
 // (extrapolate_copy.d:124-201), the fixed inflow state (flow_state_copy.d), or the
-// partner block's cell (full_face_copy.d).
+// partner block's cell (full_face_copy.d; exchanges with an Rmatrix run stage_kernel).
 template <class R>
 __device__ __forceinline__ PF<R> ghost_pf(const StageArgs& A, const R* __restrict__ Pin, const BlockDesc& B, int i, int j,
                                        int k) {
-    const CellSrc s = resolve<false>(A, B, i, j, k);
+    const CellSrc s = resolve<false, false>(A, B, i, j, k);
     PF<R> c;
     if (s.kind == SRC_INFLOW) {
         const InflowState& in = A.inflow[s.inflow];

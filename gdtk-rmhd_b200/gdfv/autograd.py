@@ -3,12 +3,14 @@
 * `residual(sim, U)`: R(U) with backward = gdfv_residual_vjp.
 * `jvp(sim, U, v)`: J v by the real Frechet derivative (gdfv_residual_jvp), the
   Jacobian-vector product of a Newton-Krylov solver.
-* `rollout(sim, U0, theta, nsteps, checkpoint_every)`: nsteps predictor-corrector
+* `rollout(sim, U0, theta, nsteps, checkpoint_every=None)`: nsteps predictor-corrector
   steps of the GPU solver from U0, differentiable in U0 and in the supersonic-
   inflow state theta = (p, T, vel.x), which the forward sets on every supersonic-
   inflow face (the other components of each face's state stay as configured), so
   that dJ/dtheta sums the cotangents of all those faces.  The forward records each step's dt and
-  keeps a copy of the state every `checkpoint_every` steps; the backward
+  keeps a copy of the state every `checkpoint_every` steps (None: the whole
+  trajectory stays resident in device memory when it fits, see resident_steps, and
+  the backward recomputes nothing); the backward
   (gdfv_rollout_adjoint) recomputes each segment from its checkpoint
   (bit-identical to the forward steps) on a second stream while it applies the
   adjoint of the predictor-corrector step (e4/simcore_gasdynamic_step.d:1245-1333)
@@ -126,11 +128,12 @@ class Rollout(torch.autograd.Function):
     @staticmethod
     def forward(ctx, U0, theta, sim, nsteps, checkpoint_every):
         U0 = U0.contiguous()
-        K = checkpoint_every
+        K = min(checkpoint_every, nsteps)
         dts, ckpts = [], {0: U0.clone()}
         # work arrays of the backward (two sets of K states and K predictor states);
-        # the first set keeps the last segment's steps as the forward takes them
-        work = [torch.empty_like(U0) for _ in range(4 * K)]
+        # the first set keeps the last segment's steps as the forward takes them.  One
+        # segment (K = nsteps) needs only that set: the backward reads no other.
+        work = [torch.empty_like(U0) for _ in range((2 if K == nsteps else 4) * K)]
         outs0, preds0 = work[:K], work[K:2 * K]
         s_last = ((nsteps + K - 1) // K - 1) * K
         # theta is the state of every supersonic-inflow face for this rollout
@@ -170,7 +173,8 @@ class Rollout(torch.autograd.Function):
         gin = torch.zeros((max(1, getattr(sim, "n_inflow", 1)), 6), dtype=torch.float64, device=lam.device)
         nseg = (len(dts) + K - 1) // K
         pc = ffi.new("double*[]", [_p(ckpts[s * K]) for s in range(nseg)])
-        pw = ffi.new("double*[]", [_p(t) for t in ctx.work])
+        sets = ctx.work if len(ctx.work) == 4 * K else ctx.work + ctx.work
+        pw = ffi.new("double*[]", [_p(t) for t in sets])
         pd = ffi.new("double[]", [float(d) for d in dts])
         torch.cuda.synchronize()
         check(sim.ctx, sim.L.gdfv_rollout_adjoint(sim.ctx, pc, nseg, pd, len(dts), K, pw, 1, _p(lam), _p(gin)))
@@ -196,5 +200,17 @@ def _from_ptr(ptr, shape):
     return torch.as_tensor(_Holder(), device="cuda").view(*shape)
 
 
-def rollout(sim, U0, theta, nsteps, checkpoint_every=10):
-    return Rollout.apply(U0, theta, sim, int(nsteps), int(checkpoint_every))
+def resident_steps(sim, nsteps, fraction=0.5):
+    """The checkpoint interval that keeps a whole rollout of nsteps resident (nsteps), when
+    its states and predictor states fit in `fraction` of the free device memory and
+    nsteps <= 64 (8.4 GB for 50 steps of 1M Euler cells); else 10."""
+    state_bytes = 8 * sim.nq * sim.total_cells()
+    free, _ = torch.cuda.mem_get_info()
+    if nsteps <= 64 and 2 * nsteps * state_bytes <= fraction * free:
+        return int(nsteps)
+    return 10
+
+
+def rollout(sim, U0, theta, nsteps, checkpoint_every=None):
+    K = resident_steps(sim, nsteps) if checkpoint_every is None else int(checkpoint_every)
+    return Rollout.apply(U0, theta, sim, int(nsteps), K)

@@ -149,11 +149,19 @@ class InFlowBC_Supersonic:
 
 
 class ExchangeBC_FullFace:
+    """bc.lua:1603-1625: the ghost cells copy the partner block's cells inside face
+    otherFace, placed by the face pair and orientation (full_face_copy.d:680-1409); with
+    reorient_vector_quantities their velocity and magnetic field are multiplied by the
+    row-major 3x3 Rmatrix (flowstate.d:393-400)."""
     name = "exchange_over_full_face"
 
-    def __init__(self, otherBlock, otherFace):
+    def __init__(self, otherBlock, otherFace, orientation=0, reorient_vector_quantities=False,
+                 Rmatrix=(1.0, 0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0, 1.0)):
         self.otherBlock = int(otherBlock)
         self.otherFace = FACE_INDEX[otherFace] if isinstance(otherFace, str) else int(otherFace)
+        self.orientation = int(orientation)
+        self.reorient_vector_quantities = bool(reorient_vector_quantities)
+        self.Rmatrix = np.asarray(Rmatrix, dtype=np.float64).reshape(9)
 
 
 class Simulation:
@@ -251,7 +259,14 @@ class Simulation:
         if isinstance(bc, OutFlowBC_SimpleExtrapolate):
             x_order = bc.xOrder
         elif isinstance(bc, ExchangeBC_FullFace):
-            other, other_face = bc.otherBlock, bc.otherFace
+            R = ffi.NULL
+            if bc.reorient_vector_quantities:
+                arr = np.ascontiguousarray(bc.Rmatrix, dtype=np.float64)
+                self._bcs[blk][f] = arr
+                R = ffi.cast("double*", arr.ctypes.data)
+            check(self.ctx, self.L.gdfv_block_set_exchange(self.ctx, blk, f, bc.otherBlock, bc.otherFace,
+                                                            bc.orientation, R))
+            return
         elif isinstance(bc, InFlowBC_Supersonic):
             arr = np.array(bc.flowState.as_array(), dtype=np.float64)
             self._bcs[blk][f] = arr  # keep alive

@@ -94,8 +94,11 @@ int gdfv_block_new_graded(int ctx, int nic, int njc, int nkc, const double* xv, 
  *   "outflow_simple_extrapolate" OutFlowBC_SimpleExtrapolate, x_order 0 or 1 (:1511-1530)
  *   "inflow_supersonic"          InFlowBC_Supersonic; inflow = {p, T, vel.x, vel.y, vel.z,
  *                                B.x, B.y, B.z, psi} as FlowState:new{p=,T=,...} (:1251-1280)
- *   "exchange_over_full_face"    ExchangeBC_FullFace with orientation 0 onto the opposite
- *                                face other_face of block other_blk (:1603)
+ *   "exchange_over_full_face"    ExchangeBC_FullFace (:1603-1625) with orientation 0 onto
+ *                                face other_face of block other_blk (any face: the ghost
+ *                                cells copy the partner's cells inside that face); for
+ *                                another orientation or a rotation see
+ *                                gdfv_block_set_exchange
  *   "outflow_simple_flux"        OutFlowBC_SimpleFlux (:1532-1556): ghosts copy the boundary
  *                                cell, the boundary face's flux is the interior cell's
  *                                (boundary_flux_effect.d:504-645); not with MHD
@@ -104,6 +107,27 @@ int gdfv_block_new_graded(int ctx, int nic, int njc, int nkc, const double* xv, 
  * Ghost cells are never stored: the kernels synthesise them (ghost_cell_effect/*.d). */
 int gdfv_block_set_bc(int ctx, int blk, int face, const char* bc_type, int x_order,
                       int other_blk, int other_face, const double* inflow);
+
+/* ExchangeBC_FullFace{otherBlock, otherFace, orientation, reorient_vector_quantities,
+ * Rmatrix} (e4/bc.lua:1603-1625) on face `face` of block `blk`.  The ghost cell at depth
+ * n beyond the face copies the partner's cell n layers inside face other_face, at the
+ * tangential position that GhostCellFullFaceCopy.set_up_cell_mapping_phase0 gives for
+ * the face pair and orientation 0..3 (e4/bc/ghost_cell_effect/full_face_copy.d:680-1409;
+ * 2D blocks ignore the orientation, as there); gdfv_exchange_source evaluates that map.
+ * Rmatrix: NULL, or 9 doubles (row major) applied to the ghost's velocity and magnetic
+ * field (flowstate.d:393-400 reorient_vector_quantities, full_face_copy.d:2403-2405).
+ * The faces' cell counts must match under the map and the partner must be at least 2
+ * cells deep; checked at gdfv_prepare.  The adjoint rejects a context with an Rmatrix. */
+int gdfv_block_set_exchange(int ctx, int blk, int face, int other_blk, int other_face, int orientation,
+                            const double* Rmatrix);
+
+/* The partner cell that feeds a ghost cell of an exchange face, by the map above, without
+ * a context: dims 2 or 3, faces 0..5 (0..3 in 2D), n_other = the partner's cell counts,
+ * ijk = the ghost cell's indices in its own block (one index outside [0, n), at depth 0
+ * or 1 beyond `face`); writes the partner's cell indices to src.  Returns GDFV_OK, or
+ * GDFV_ERR_ARG for a bad face, orientation or ghost position. */
+int gdfv_exchange_source(int dims, int face, int other_face, int orientation, const int* n_this,
+                         const int* n_other, const int* ijk, int* src);
 
 /* Validate the configuration and allocate device memory.  After this call
  * blocks and options are frozen. */
@@ -171,11 +195,12 @@ int gdfv_residual_jvp(int ctx, const double* U_dev, const double* v_dev, const d
 
 /* Vector-Jacobian product of the residual: G = (dR/dU)^T W at the state U, device
  * arrays [nq][total] over all blocks (the adjoint of gdfv_residual, hand-written:
- * reverse of decode_conserved, interp_l2r2 and ausmdv, with the branches of the
- * primal values).  g_inflow_host (may be NULL) receives, per supersonic-inflow face
+ * reverse of decode_conserved, interp_l2r2 and ausmdv or hllc, with the branches of
+ * the primal values).  g_inflow_host (may be NULL) receives, per supersonic-inflow face
  * state in the order the faces were defined, the cotangent of its ghost state
- * (rho, vel.x, vel.y, vel.z, u, a), 6 doubles each.  3D Euler with
- * flux_calculator=ausmdv.  It is the transpose of the Jacobian-vector products of
+ * (rho, vel.x, vel.y, vel.z, u, a), 6 doubles each.  Euler (2D or 3D) with
+ * flux_calculator=ausmdv or hllc; exchanges of any orientation, with or without an
+ * Rmatrix (the cotangent goes back through its transpose).  It is the transpose of the Jacobian-vector products of
  * e4/steadystate_core.d:1870-2060 (evalJacobianVecProd), which it is checked against. */
 int gdfv_residual_vjp(int ctx, const double* U_dev, const double* W_dev, double* G_dev, double* g_inflow_host);
 

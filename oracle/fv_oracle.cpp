@@ -69,6 +69,64 @@ static inline size_t depth_index(const Block& b, int face, int m, int p, int q) 
     return b.pidx(ijk[0], ijk[1], ijk[2]);
 }
 
+// full_face_copy.d:680-1409 (GhostCellFullFaceCopy.set_up_cell_mapping_phase0): the
+// partner cell that the ghost at depth m beyond `face` copies.  The reference writes the
+// map out for each face pair and orientation; restated here as geometry.  A face carries
+// a frame of two signed axes, right-handed about its outward normal (table below).  The
+// ghost's position in its face's frame, in centred doubled coordinates (2 x - (n - 1):
+// reversing an axis negates it), is mirrored across the shared face and turned by
+// `orientation` quarter turns ((a, b) -> (-b, a)), giving the source's position in the
+// partner face's frame; normal to that face the source lies m cells inside.  In 2D the
+// orientation is ignored, as there.  ijk: the ghost's indices (the one along the face's
+// normal is not used); returns false when the source falls outside the partner.
+static bool exchange_source(int dims, int face, int other_face, int orientation, const int n[3], const int on[3],
+                            int m, const int ijk[3], int src[3]) {
+    static const int frame[6][2][2] = {
+        {{1, -1}, {2, 1}},   // west:   (-j, k)
+        {{1, 1}, {2, 1}},    // east:   (j, k)
+        {{0, 1}, {2, 1}},    // south:  (i, k)
+        {{0, -1}, {2, 1}},   // north:  (-i, k)
+        {{0, -1}, {1, 1}},   // bottom: (-i, j)
+        {{0, 1}, {1, 1}}};   // top:    (i, j)
+    int w[2];
+    for (int r = 0; r < 2; ++r) {
+        const int ax = frame[face][r][0];
+        w[r] = frame[face][r][1] * (2 * ijk[ax] - (n[ax] - 1));
+    }
+    int a = -w[0], b = w[1];
+    for (int t = 0; t < (dims == 3 ? orientation : 0); ++t) {
+        const int a2 = -b;
+        b = a;
+        a = a2;
+    }
+    const int v[2] = {a, b};
+    for (int r = 0; r < 2; ++r) {
+        const int ax = frame[other_face][r][0];
+        const int twice = frame[other_face][r][1] * v[r] + (on[ax] - 1);
+        if (twice < 0 || twice > 2 * (on[ax] - 1) || (twice & 1)) return false;
+        src[ax] = twice / 2;
+    }
+    const int od = other_face / 2;
+    src[od] = (other_face & 1) ? on[od] - 1 - m : m;
+    return src[od] >= 0 && src[od] < on[od];
+}
+
+// flowstate.d:393-400 reorient_vector_quantities: vel (and B) times the row-major R,
+// vector3.d:453-460 apply_matrix_transform
+template <class T>
+static void reorient(FlowState<T>& s, const double* R, bool mhd) {
+    const T x = s.vel[0], y = s.vel[1], z = s.vel[2];
+    s.vel[0] = R[0] * x + R[1] * y + R[2] * z;
+    s.vel[1] = R[3] * x + R[4] * y + R[5] * z;
+    s.vel[2] = R[6] * x + R[7] * y + R[8] * z;
+    if (mhd) {
+        const T bx = s.B[0], by = s.B[1], bz = s.B[2];
+        s.B[0] = R[0] * bx + R[1] * by + R[2] * bz;
+        s.B[1] = R[3] * bx + R[4] * by + R[5] * bz;
+        s.B[2] = R[6] * bx + R[7] * by + R[8] * bz;
+    }
+}
+
 static inline void face_extent(const Block& b, int face, int& np, int& nq_) {
     int d = face / 2;
     int n[3] = {b.nic, b.njc, b.nkc};
@@ -174,11 +232,20 @@ static void fill_ghosts(const Sim& sim, std::vector<std::vector<FlowState<T>>>& 
                         F[depth_index(b, face, -1, p, q)] = s;
                         F[depth_index(b, face, -2, p, q)] = s;
                     } break;
-                    case BC_EXCHANGE: {
+                    case BC_EXCHANGE: {   // full_face_copy.d:2397-2410
                         const Block& ob = sim.blocks[bc.other_block];
+                        const int n3[3] = {b.nic, b.njc, b.nkc}, on3[3] = {ob.nic, ob.njc, ob.nkc};
+                        const int d = face / 2;
+                        int ijk[3];
+                        ijk[d] = 0;
+                        ijk[(d + 1) % 3] = p;
+                        ijk[(d + 2) % 3] = q;
                         for (int n = 0; n < 2; ++n) {
-                            F[depth_index(b, face, -1 - n, p, q)] =
-                                fs[bc.other_block][depth_index(ob, bc.other_face, n, p, q)];
+                            int src[3];
+                            exchange_source(cfg.dimensions, face, bc.other_face, bc.orientation, n3, on3, n, ijk, src);
+                            FlowState<T> s = fs[bc.other_block][ob.pidx(src[0], src[1], src[2])];
+                            if (bc.rotate) reorient(s, bc.R, cfg.mhd);
+                            F[depth_index(b, face, -1 - n, p, q)] = s;
                         }
                     } break;
                     }
@@ -713,6 +780,31 @@ int orc_set_bc(int h, int blk, int face, int type, int x_order, int other_blk, i
     return 0;
 }
 
+// ExchangeBC_FullFace{otherBlock, otherFace, orientation, reorient_vector_quantities,
+// Rmatrix} (bc.lua:1603-1625); R null: no reorientation
+int orc_set_exchange(int h, int blk, int face, int other_blk, int other_face, int orientation, const double* R) {
+    Sim* s = get(h);
+    if (!s || blk < 0 || blk >= (int)s->blocks.size() || face < 0 || face > 5 || orientation < 0 || orientation > 3)
+        return -1;
+    BoundaryCondition& bc = s->blocks[blk].bc[face];
+    bc.type = BC_EXCHANGE; bc.other_block = other_blk; bc.other_face = other_face; bc.orientation = orientation;
+    bc.rotate = R != nullptr;
+    if (R) for (int m = 0; m < 9; ++m) bc.R[m] = R[m];
+    return 0;
+}
+
+// The map of exchange_source for a ghost (i, j, k) of `face` (one index outside the block
+// at depth 0 or 1); 0 and src filled, or -1.
+int orc_exchange_source(int dims, int face, int other_face, int orientation, const int* n, const int* on,
+                        const int* ijk, int* src) {
+    const int nf = dims == 3 ? 6 : 4;
+    if (face < 0 || face >= nf || other_face < 0 || other_face >= nf || orientation < 0 || orientation > 3) return -1;
+    const int d = face / 2;
+    const int m = (face & 1) ? ijk[d] - n[d] : -1 - ijk[d];
+    if (m < 0 || m > 1) return -1;
+    return exchange_source(dims, face, other_face, orientation, n, on, m, ijk, src) ? 0 : -1;
+}
+
 // Ghost states of a face from the caller (UserDefinedGhostCell): pTv[(layer*nq_ + q)*np + p][5] =
 // p, T, vel.x, vel.y, vel.z; each becomes a FlowState by update_thermo_from_pT and
 // update_sound_speed (user_defined_effects.d:175-240).
@@ -769,6 +861,38 @@ int orc_init(int h) {
     Sim* s = get(h);
     if (!s) return -1;
     const int nq = s->nq();
+    // exchange faces: the partner exists, its face has as many cells, and every ghost's
+    // source lies inside it (full_face_copy.d:160-680 checks the cell counts)
+    const int nfaces = s->cfg.dimensions == 3 ? 6 : 4;
+    for (auto& b : s->blocks) {
+        for (int face = 0; face < nfaces; ++face) {
+            const BoundaryCondition& bc = b.bc[face];
+            if (bc.type != BC_EXCHANGE) continue;
+            if (bc.other_block < 0 || bc.other_block >= (int)s->blocks.size() || bc.other_face < 0 ||
+                bc.other_face >= nfaces) {
+                s->last_error = "exchange partner does not exist";
+                return -1;
+            }
+            const Block& ob = s->blocks[bc.other_block];
+            const int n3[3] = {b.nic, b.njc, b.nkc}, on3[3] = {ob.nic, ob.njc, ob.nkc};
+            const int d = face / 2, od = bc.other_face / 2;
+            if ((long long)n3[(d + 1) % 3] * n3[(d + 2) % 3] != (long long)on3[(od + 1) % 3] * on3[(od + 2) % 3]) {
+                s->last_error = "exchange faces differ in size";
+                return -1;
+            }
+            for (int q = 0; q < n3[(d + 2) % 3]; ++q)
+                for (int p = 0; p < n3[(d + 1) % 3]; ++p)
+                    for (int m = 0; m < 2; ++m) {
+                        int ijk[3], src[3];
+                        ijk[d] = 0; ijk[(d + 1) % 3] = p; ijk[(d + 2) % 3] = q;
+                        if (!exchange_source(s->cfg.dimensions, face, bc.other_face, bc.orientation, n3, on3, m, ijk,
+                                             src)) {
+                            s->last_error = "exchange faces differ in size under this orientation";
+                            return -1;
+                        }
+                    }
+        }
+    }
     // ghost cell lengths of graded blocks: the partner's cells across an exchange face,
     // else the block's own interior cell n (e4/sfluidblock.d:884-1090)
     for (auto& b : s->blocks) {
@@ -780,10 +904,11 @@ int orc_init(int h) {
             for (int m = 0; m < 2; ++m) {
                 const int ghost = plus ? n[d] + m : -1 - m;
                 double L;
-                if (bc.type == BC_EXCHANGE) {
+                if (bc.type == BC_EXCHANGE) {   // the partner's cell m inside its face, along its normal
                     const Block& ob = s->blocks[bc.other_block];
-                    const int on = d == 0 ? ob.nic : (d == 1 ? ob.njc : ob.nkc);
-                    L = ob.L(d, (bc.other_face & 1) ? on - 1 - m : m);
+                    const int od = bc.other_face / 2;
+                    const int on = od == 0 ? ob.nic : (od == 1 ? ob.njc : ob.nkc);
+                    L = ob.L(od, (bc.other_face & 1) ? on - 1 - m : m);
                 } else {
                     L = b.L(d, plus ? n[d] - 1 - m : m);
                 }

@@ -563,8 +563,11 @@ inline bool check_data(const Config& cfg, const FlowState<double>& fs) {
 struct BoundaryCondition {
     int type = BC_SLIP_WALL;
     int x_order = 0;                 // ExtrapolateCopy xOrder (bc.lua:135)
-    int other_block = -1;            // FullFaceCopy partner, orientation 0
+    int other_block = -1;            // FullFaceCopy partner (full_face_copy.d:65-160)
     int other_face = -1;
+    int orientation = 0;             // 0..3 (ignored in 2D)
+    bool rotate = false;             // reorient_vector_quantities with Rmatrix R (row major)
+    double R[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
     FlowState<double> inflow;        // FlowStateCopy state
     double p_out = 0.0, T_out = 0.0; // GhostCellFixedP / GhostCellFixedPT (fixed_p.d, fixed_pt.d)
     // UserDefinedGhostCell (e4/bc/ghost_cell_effect/user_defined_effects.d:108-308): ghost

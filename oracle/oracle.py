@@ -52,6 +52,9 @@ def lib():
         L.orc_set_ghost_states.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, dp]
         L.orc_set_source.argtypes = [ctypes.c_int, ctypes.c_int, dp]
         L.orc_add_block_graded.argtypes = [ctypes.c_int] * 4 + [dp] * 3
+        L.orc_set_exchange.argtypes = [ctypes.c_int] * 6 + [dp]
+        ip = ctypes.POINTER(ctypes.c_int)
+        L.orc_exchange_source.argtypes = [ctypes.c_int] * 4 + [ip] * 4
         _LIB = L
     return _LIB
 
@@ -160,6 +163,16 @@ class OracleSim:
         if rc != 0:
             raise ValueError("set_bc failed")
 
+    def set_exchange(self, blk, face, other_block, other_face, orientation=0, Rmatrix=None):
+        """ExchangeBC_FullFace{otherBlock, otherFace, orientation, reorient_vector_quantities,
+        Rmatrix} (bc.lua:1603-1625); Rmatrix: 9 numbers, row major, or None."""
+        f = FACES[face] if isinstance(face, str) else face
+        of = FACES[other_face] if isinstance(other_face, str) else other_face
+        R = None if Rmatrix is None else np.ascontiguousarray(Rmatrix, dtype=np.float64).reshape(9)
+        rc = self.L.orc_set_exchange(self.h, blk, f, other_block, of, orientation, None if R is None else _p(R))
+        if rc != 0:
+            raise ValueError("set_exchange failed")
+
     def set_flow_rhoT(self, blk, rho, vel, T, B=None, psi=None):
         """Arrays shaped (nkc, njc, nic) (i fastest); vel (3, ...)."""
         nic, njc, nkc = self.blocks[blk]
@@ -253,3 +266,14 @@ class OracleSim:
             self.L.orc_free(self.h)
         except Exception:
             pass
+
+
+def exchange_source(dims, face, other_face, orientation, n, n_other, ijk):
+    """The partner cell (i, j, k) that the exchange ghost ijk copies (full_face_copy.d:680-1409),
+    or None for a ghost the map does not place inside the partner."""
+    L = lib()
+    arr = lambda v: (ctypes.c_int * 3)(*[int(x) for x in v])
+    src = (ctypes.c_int * 3)()
+    rc = L.orc_exchange_source(dims, face, other_face, orientation, arr(n), arr(n_other), arr(ijk), src)
+    return None if rc != 0 else tuple(src)
+

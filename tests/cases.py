@@ -308,6 +308,114 @@ def graded_lattice(seed=23, precision="fp64"):
     return c
 
 
+R90 = (0.0, -1.0, 0.0, 1.0, 0.0, 0.0, 0.0, 0.0, 1.0)    # +90 degrees about z: (x, y) -> (-y, x)
+R270 = (0.0, 1.0, 0.0, -1.0, 0.0, 0.0, 0.0, 0.0, 1.0)   # -90 degrees about z
+
+
+def exchange_pair(orientation, precision="fp64", seed=41, graded=False):
+    """Two blocks joined by a full-face exchange between block 0's east face and block
+    1's north face, both ways with the same orientation 0..3 (the map of one direction
+    is then the inverse of the other's; full_face_copy.d:680-1409).  The faces are 16 x 16
+    cells, so every orientation fits.  The library's blocks are axis-aligned, so the join
+    is not geometric: the case tests the ghost map on a flow that stays valid, a
+    two-state box (p 1e5 / 3e4, T 300 / 350) with 1% noise on density and on all three
+    velocity components about (40, -25, 30) m/s, extrapolation on the other faces.
+    graded: block 1 stretched along j (the normal of its exchange face), so the ghosts
+    of block 0's east face take block 1's j lengths."""
+    c = Case(f"exchange_pair_o{orientation}", dict(flux_calculator="ausmdv", flux_precision=precision),
+             R_AIR_CHICKEN, 1.4)
+    rng = np.random.default_rng(seed + orientation)
+    d = 1.0e-3
+    ext = {f: ("outflow_simple_extrapolate", dict(x_order=0)) for f in
+           ("west", "east", "south", "north", "bottom", "top")}
+    for blk, (n, origin, p, T, face, other_face) in enumerate(
+            [((20, 16, 16), (0.0, 0.0, 0.0), 1.0e5, 300.0, "east", "north"),
+             ((16, 12, 16), (0.03, 0.0, 0.0), 3.0e4, 350.0, "north", "east")]):
+        shp = (n[2], n[1], n[0])
+        rho = _noisy_rho(rng, p / (R_AIR_CHICKEN * T), shp)
+        vel = tuple(v * (1.0 + 0.01 * rng.standard_normal(shp)) for v in (40.0, -25.0, 30.0))
+        bcs = dict(ext)
+        bcs[face] = ("exchange_over_full_face", dict(other=1 - blk, other_face=other_face, orientation=orientation))
+        vertices = None
+        if graded and blk == 1:
+            vertices = (origin[0] + d * np.arange(n[0] + 1), stretched(n[1], 0.8e-3, 1.05),
+                        d * np.arange(n[2] + 1))
+        c.add_block(n, (d, d, d), origin, bcs, rho, vel, T, vertices=vertices)
+    return c
+
+
+def quarter_rotational(n=(24, 24, 4), precision="fp64", mhd=False, seed=None):
+    """The quadrant x, y >= 0 of a flow with four-fold rotational symmetry about the z
+    axis: the ghosts beyond x = 0 copy the cells inside y = 0 turned by +90 degrees, and
+    the ghosts beyond y = 0 the cells inside x = 0 turned by -90 degrees (ExchangeBC_FullFace
+    west <-> south with reorient_vector_quantities; the vectors turn with the cells).
+    Euler: air, a density and pressure bump of 30% and a swirl of up to 80 m/s about the
+    axis, slip walls at x = L, y = L and on the z faces.  mhd: hlle + GLM (gamma 5/3, R 1)
+    with an azimuthal magnetic field on top of a uniform B_z, extrapolation at x = L and
+    y = L and periodic in z (this fork's MHD slip-wall ghosts carry a dipole field for
+    |x| < 0.4136, internal_copy_then_reflect.d:140-143, which walls through the axis would
+    meet at its singular point).  seed: 1% density noise (breaks the symmetry; the parity
+    tests), None: the smooth field."""
+    nic, njc, nkc = n
+    if mhd:
+        c = Case("quarter_rotational_mhd", dict(flux_calculator="hlle", MHD=1, divergence_cleaning=1, stringent_cfl=1,
+                                                flux_precision=precision, dt_init=2e-3, dt_max=1e-2), 1.0, 5.0 / 3.0)
+        L = 1.0
+    else:
+        c = Case("quarter_rotational", dict(flux_calculator="ausmdv", flux_precision=precision), R_AIR_CHICKEN, 1.4)
+        L = 0.024
+    dx = L / nic
+    x = (np.arange(nic) + 0.5) * dx
+    y = (np.arange(njc) + 0.5) * dx
+    X = np.broadcast_to(x[None, None, :], (nkc, njc, nic))
+    Y = np.broadcast_to(y[None, :, None], (nkc, njc, nic))
+    g = np.exp(-(X * X + Y * Y) / (0.4 * L) ** 2)
+    if mhd:
+        rho = 1.0 + 0.3 * g
+        T = (1.0 + 0.3 * g) / rho
+        w = 0.5 * g / L
+        B = (-0.2 * g * Y / L, 0.2 * g * X / L, np.full(X.shape, 0.1))
+    else:
+        rho = 1.2 * (1.0 + 0.3 * g)
+        T = 300.0 * (1.0 + 0.1 * g)
+        w = 80.0 * g / L
+        B = None
+    if seed is not None:
+        rho = _noisy_rho(np.random.default_rng(seed), rho, rho.shape)
+    vel = (-w * Y, w * X, np.zeros(X.shape))
+    bcs = {"west": ("exchange_over_full_face", dict(other=0, other_face="south", Rmatrix=R90)),
+           "south": ("exchange_over_full_face", dict(other=0, other_face="west", Rmatrix=R270)),
+           "east": ("wall_with_slip", {}), "north": ("wall_with_slip", {}),
+           "bottom": ("wall_with_slip", {}), "top": ("wall_with_slip", {})}
+    if mhd:
+        bcs.update(east=("outflow_simple_extrapolate", dict(x_order=0)),
+                   north=("outflow_simple_extrapolate", dict(x_order=0)),
+                   bottom=("exchange_over_full_face", dict(other=0, other_face="top")),
+                   top=("exchange_over_full_face", dict(other=0, other_face="bottom")))
+    c.add_block(n, (dx, dx, dx), (0.0, 0.0, 0.0), bcs, rho, vel, T, B=B)
+    return c
+
+
+def full_rotational(n=(24, 24, 4)):
+    """quarter_rotational's Euler flow (smooth) on the whole square [-L, L]^2 as one block,
+    slip walls all round: its quadrant x, y >= 0 is the quarter case."""
+    nic, njc, nkc = n
+    c = Case("full_rotational", dict(flux_calculator="ausmdv"), R_AIR_CHICKEN, 1.4)
+    L = 0.024
+    dx = L / nic
+    x = (np.arange(2 * nic) + 0.5) * dx - L
+    y = (np.arange(2 * njc) + 0.5) * dx - L
+    X = np.broadcast_to(x[None, None, :], (nkc, 2 * njc, 2 * nic))
+    Y = np.broadcast_to(y[None, :, None], (nkc, 2 * njc, 2 * nic))
+    g = np.exp(-(X * X + Y * Y) / (0.4 * L) ** 2)
+    rho = 1.2 * (1.0 + 0.3 * g)
+    T = 300.0 * (1.0 + 0.1 * g)
+    w = 80.0 * g / L
+    bcs = {f: ("wall_with_slip", {}) for f in ("west", "east", "south", "north", "bottom", "top")}
+    c.add_block((2 * nic, 2 * njc, nkc), (dx, dx, dx), (-L, -L, 0.0), bcs, rho, (-w * Y, w * X, np.zeros(X.shape)), T)
+    return c
+
+
 # ---------------------------------------------------------------- builders
 _ORACLE_BC = {"wall_with_slip": "wall_with_slip", "outflow_simple_extrapolate": "extrapolate",
               "inflow_supersonic": "inflow_supersonic", "exchange_over_full_face": "exchange",
@@ -330,6 +438,9 @@ def build_oracle(case):
             inflow = kw.get("inflow")
             if kind in ("outflow_fixed_p", "outflow_fixed_p_and_t"):
                 inflow = dict(p=kw["p_outside"], T=kw.get("T_outside", 0.0))
+            if kind == "exchange_over_full_face":
+                s.set_exchange(bi, face, kw["other"], kw["other_face"], kw.get("orientation", 0), kw.get("Rmatrix"))
+                continue
             s.set_bc(bi, face, _ORACLE_BC[kind], x_order=kw.get("x_order", 0),
                      other_block=kw.get("other", -1), other_face=kw.get("other_face", -1), inflow=inflow)
         s.set_flow_rhoT(bi, b["rho"], b["vel"], b["T"], B=b["B"])
@@ -362,8 +473,11 @@ def build_gpu(case, **extra_config):
                 inf = kw["inflow"]
                 bc = gdfv.InFlowBC_Supersonic(gdfv.FlowState(p=inf["p"], T=inf["T"], velx=inf["vel"][0],
                                                              vely=inf["vel"][1], velz=inf["vel"][2]))
+            elif kw.get("Rmatrix") is not None:
+                bc = gdfv.ExchangeBC_FullFace(kw["other"], kw["other_face"], orientation=kw.get("orientation", 0),
+                                              reorient_vector_quantities=True, Rmatrix=kw["Rmatrix"])
             else:
-                bc = gdfv.ExchangeBC_FullFace(kw["other"], kw["other_face"])
+                bc = gdfv.ExchangeBC_FullFace(kw["other"], kw["other_face"], orientation=kw.get("orientation", 0))
             sim.set_bc(bi, face, bc)
     sim.prepare()
     for bi, b in enumerate(case.blocks):

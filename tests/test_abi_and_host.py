@@ -149,7 +149,42 @@ def test_prepare_rejects_invalid_layouts_before_touching_the_device():
     assert L.gdfv_prepare(h) == GDFV_ERR_ARG
     assert "differ in size" in last_error(h)
     L.gdfv_context_free(h)
+    # east onto north: the partner's i runs along this face's j (orientation 0) or along
+    # its k (orientation 1); a 16 x 8 x 16 partner fits the first, an 8 x 16 x 12 one neither
+    for nb1, orientation, ok in (((16, 8, 16), 0, True), ((8, 16, 12), 0, False), ((8, 16, 12), 1, False)):
+        h, b0 = _ctx_with_block(L, (16, 16, 16))
+        b1 = L.gdfv_block_new(h, *nb1, 1e-3, 1e-3, 1e-3, 0.016, 0, 0)
+        assert L.gdfv_block_set_exchange(h, b0, 1, b1, 3, orientation, ffi.NULL) == GDFV_OK
+        assert L.gdfv_block_set_exchange(h, b1, 3, b0, 1, orientation, ffi.NULL) == GDFV_OK
+        if ok:
+            assert L.gdfv_prepare(h) != GDFV_ERR_ARG   # valid: no GPU here, so it fails later
+        else:
+            assert L.gdfv_prepare(h) == GDFV_ERR_ARG
+            assert "differ in size" in last_error(h)
+        L.gdfv_context_free(h)
     h, b0 = _ctx_with_block(L, (16, 16, 16))
-    assert L.gdfv_block_set_bc(h, b0, 1, b"exchange_over_full_face", 0, b0, 1, ffi.NULL) == GDFV_OK
-    assert L.gdfv_prepare(h) == GDFV_ERR_ARG
+    assert L.gdfv_block_set_exchange(h, b0, 1, b0, 0, 4, ffi.NULL) == GDFV_ERR_ARG
+    bad = ffi.new("double[9]", [1.0, 0.0, 0.0, 0.0, float("nan"), 0.0, 0.0, 0.0, 1.0])
+    assert L.gdfv_block_set_exchange(h, b0, 1, b0, 0, 0, bad) == GDFV_ERR_ARG
+    assert L.gdfv_block_set_exchange(h, b0, 1, 5, 0, 0, ffi.NULL) == GDFV_OK
+    assert L.gdfv_prepare(h) == GDFV_ERR_ARG                     # no block 5
     L.gdfv_context_free(h)
+
+
+def test_exchange_map_is_the_reference_map():
+    """gdfv_exchange_source (the map the kernels evaluate, from the same rule) against
+    the reference's own map of every face pair and orientation
+    (full_face_copy.d:680-1409, tests/golden/exchange_map.json), every ghost."""
+    import test_oracle_pins as pins
+    L = gdfv.lib()
+    maps = pins.exchange_maps()
+    src = ffi.new("int[3]")
+    for rec in maps:
+        for n, on, ijk, want in pins.exchange_ghosts(rec):
+            rc = L.gdfv_exchange_source(rec["dims"], rec["face"], rec["other_face"], rec["orientation"],
+                                        ffi.new("int[3]", n), ffi.new("int[3]", on), ffi.new("int[3]", ijk), src)
+            assert rc == GDFV_OK and tuple(src) == want, (rec, ijk)
+    n, on = ffi.new("int[3]", [3, 4, 5]), ffi.new("int[3]", [4, 6, 5])
+    assert L.gdfv_exchange_source(3, 1, 3, 0, n, on, ffi.new("int[3]", [5, 0, 0]), src) == GDFV_ERR_ARG   # depth 2
+    assert L.gdfv_exchange_source(3, 1, 3, 1, n, on, ffi.new("int[3]", [3, 3, 4]), src) == GDFV_ERR_ARG   # too small
+    assert L.gdfv_exchange_source(2, 4, 3, 0, n, on, ffi.new("int[3]", [0, 0, -1]), src) == GDFV_ERR_ARG  # 2D k face

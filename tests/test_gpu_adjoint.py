@@ -1,7 +1,7 @@
 """GPU adjoint: the hand-written VJP of R(U) (gdfv_residual_vjp) and the
 checkpointed rollout adjoint behind torch.autograd.Function.
 
-Checks, all in FP64:
+Checks, all in FP64 (ausmdv, and hllc where named):
 * <w, J v> from the oracle's complex-step JVP (e4/steadystate_core.d:1972-2060
   restated, src/ntypes/complex.d semantics) equals <J^T w, v> from the VJP kernel;
 * the same against the oracle's real Frechet JVP with the Knoll-McHugh step
@@ -66,6 +66,32 @@ def test_vjp_transpose_of_complex_step_jvp_shock_box():
 
 def test_vjp_transpose_multiblock_exchange():
     _dot_check(cases.multiblock_lattice(nb=(2, 1, 2), sizes=(16, 24), seed=3), 4, 1e-10, seed=2)
+
+
+def test_vjp_transpose_hllc():
+    """hllc (e4/fluxcalc.d:653-820): the reverse of its Roe-averaged wave speeds, the
+    star state and the side and star switches; the supersonic inflow box (mostly the
+    upwind side alone) and the subsonic shock box (star states on both sides)."""
+    _dot_check(cases.c2_inflow_box(n=(24, 16, 12), flux="hllc", noise_all=True), 6, 1e-10, seed=8)
+    box = cases.c1_shock_box(n=16)
+    box.config["flux_calculator"] = "hllc"
+    _dot_check(box, 8, 1e-10, seed=9)
+
+
+@pytest.mark.parametrize("flux", ["ausmdv", "hllc"])
+def test_vjp_transpose_2d(flux):
+    """2D blocks: four faces per cell (no k faces), areas and volumes per unit depth."""
+    case = cases.c2_inflow_box(n=(40, 24, 1), flux=flux, noise_all=True)
+    case.config["dimensions"] = 2
+    _dot_check(case, 6, 1e-10, seed=10)
+
+
+def test_vjp_transpose_oriented_and_rotating_exchanges():
+    """Exchange ghosts placed by orientation 3 (the cotangent goes to the partner cell
+    the map names), and ghosts whose velocity the exchange turns by +-90 degrees
+    (the cotangent goes back through the transpose of the rotation)."""
+    _dot_check(cases.exchange_pair(3), 4, 1e-10, seed=5)
+    _dot_check(cases.quarter_rotational(n=(16, 16, 4), seed=7), 4, 1e-10, seed=6)
 
 
 def test_vjp_against_reference_frechet_jvp():
@@ -146,6 +172,12 @@ def test_rollout_gradients_against_finite_differences():
     with a small derivative).  Asserted with margins above those; the strict check
     is the smooth configuration below."""
     _rollout_fd_check({}, ((1e-6, 2e-2), (1e-8, 1e-3)), ((1e-6, 2e-2), (1e-8, 1e-3)))
+
+
+def test_rollout_gradients_hllc_smooth_configuration():
+    """The same with hllc: the checkpointed rollout adjoint through the hllc VJP."""
+    _rollout_fd_check(dict(flux_calculator="hllc", apply_limiter=False, extrema_clipping=False),
+                      ((1e-6, 1e-4), (1e-7, 2e-5)), ((1e-6, 1e-4), (1e-7, 2e-5)))
 
 
 def test_rollout_gradients_smooth_configuration():
@@ -294,6 +326,30 @@ def test_pipelined_rollout_adjoint_matches_sequential():
         torch.cuda.synchronize()
         assert torch.allclose(lam, lam2, rtol=1e-12, atol=1e-12 * float(lam.abs().max())), last_ready
         assert torch.allclose(gin, gin2, rtol=1e-12, atol=0.0), last_ready
+
+
+def test_resident_trajectory_rollout_matches_checkpointed():
+    """rollout's default keeps the whole trajectory on the device when it fits (one
+    segment, nothing recomputed); its gradients equal those of the checkpointed form (a
+    checkpoint every 4 steps, segments recomputed) to the rounding of the FP64 atomic
+    accumulation."""
+    from gdfv.autograd import resident_steps, rollout
+    case = cases.c2_inflow_box(n=(40, 24, 20), noise_all=True)
+    inf = cases.inflow_state_m3()
+    _, sim = cases.build_pair(case)
+    U0 = torch.from_numpy(sim.get_conserved(0)).cuda()
+    nsteps = 11
+    assert resident_steps(sim, nsteps) == nsteps
+    grads = []
+    for K in (None, 4):
+        theta = torch.tensor([inf["p"], inf["T"], inf["vel"][0]], dtype=torch.float64, requires_grad=True)
+        U0r = U0.clone().requires_grad_(True)
+        UN = rollout(sim, U0r, theta, nsteps, K)
+        wall_pressure(case, UN, case.R).backward()
+        grads.append((U0r.grad.clone(), theta.grad.clone()))
+    (gr, tr), (gc, tc) = grads
+    assert torch.allclose(gr, gc, rtol=1e-11, atol=1e-11 * float(gc.abs().max()))
+    assert torch.allclose(tr, tc, rtol=1e-11, atol=0.0)
 
 
 @pytest.mark.parametrize("case_name", ["inflow", "multiblock"])

@@ -249,6 +249,47 @@ def test_graded_fp32_flux():
         assert max(errs) <= TOL_FP32_L2, (case.name, errs)
 
 
+@pytest.mark.parametrize("orientation", [0, 1, 2, 3])
+def test_exchange_orientations_fp64(orientation):
+    """One block's east face joined to another's north face in each orientation
+    (full_face_copy.d:680-1409): every ghost of both faces from the partner cell the map
+    names, bit for bit with the oracle."""
+    case = cases.exchange_pair(orientation)
+    orc, sim = run_both(case, 10)
+    assert compare_fp64(case, orc, sim) <= TOL_FP64
+
+
+def test_exchange_orientation_graded_fp64():
+    """The same join with the partner stretched along its face normal: the ghosts take
+    the partner's lengths along its own normal axis."""
+    case = cases.exchange_pair(1, graded=True)
+    orc, sim = run_both(case, 10)
+    assert compare_fp64(case, orc, sim) <= TOL_FP64
+
+
+@pytest.mark.parametrize("mhd", [False, True])
+def test_rotating_exchange_fp64(mhd):
+    """A quarter domain closed by exchanges that turn the ghosts' velocity (and magnetic
+    field) by +-90 degrees (reorient_vector_quantities, flowstate.d:393-400)."""
+    case = cases.quarter_rotational(n=(24, 24, 4), seed=11, mhd=mhd)
+    orc, sim = run_both(case, 12)
+    assert compare_fp64(case, orc, sim) <= TOL_FP64
+
+
+def test_oriented_and_rotating_exchanges_fp32():
+    """The float forms: oriented exchanges on the kernel on decoded primitives, rotating
+    ones on the general float kernel."""
+    for case in [cases.exchange_pair(o, precision="fp32") for o in range(4)] + \
+            [cases.quarter_rotational(n=(24, 24, 4), seed=11, precision="fp32")]:
+        orc, sim = cases.build_pair(case)
+        assert orc.run(20) == 0
+        assert sim.run(max_step=20) == 20
+        Uo = np.concatenate([orc.get_U(b) for b in range(len(case.blocks))], axis=1)
+        Ug = np.concatenate([sim.get_conserved(b) for b in range(len(case.blocks))], axis=1)
+        errs = [cases.rel_l2(Ug[0], Uo[0]), cases.rel_l2(Ug[1:4].ravel(), Uo[1:4].ravel()), cases.rel_l2(Ug[4], Uo[4])]
+        assert max(errs) <= TOL_FP32_L2, (case.name, errs)
+
+
 def test_graded_block_with_uniform_spacing_is_the_uniform_block():
     """On the GPU too, a graded block with evenly spaced vertices (1/1024 m) gives the
     uniform block's results bit for bit (the general kernel's graded path against the

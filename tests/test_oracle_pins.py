@@ -10,7 +10,11 @@
   speed kept through the rhou update, predictor-corrector);
 * the reference's own compiled chicken solver: a golden run committed in
   tests/golden/chicken_lattice.npz (made by tests/golden/make_golden.py), and a
-  live run when oracle/_ref/chkn-run has been built here.
+  live run when oracle/_ref/chkn-run has been built here;
+* the ExchangeBC_FullFace ghost map of every face pair and orientation, read from the
+  reference's source (tests/golden/exchange_map.json, made by
+  tests/golden/make_exchange_map.py), and the rotation of the ghosts' vectors against
+  the flow it stands for (a quarter domain against the whole).
 """
 import json
 import os
@@ -229,3 +233,72 @@ def test_oracle_graded_block_with_uniform_spacing_is_the_uniform_block():
     assert ou.run(6) == 0 and og.run(6) == 0
     assert np.array_equal(ou.get_U(0), og.get_U(0))
     assert ou.time()["dt"] == og.time()["dt"]
+
+
+def exchange_maps():
+    with open(os.path.join(GOLDEN, "exchange_map.json")) as f:
+        return json.load(f)["maps"]
+
+
+def exchange_ghosts(rec):
+    """Every ghost of a map's face on small blocks (3 x 4 x 5 cells, 3 x 4 x 1 in 2D; the
+    partner sized as the map needs) with the partner cell the reference's map names."""
+    dims, f, src = rec["dims"], rec["face"], rec["src"]
+    n = [3, 4, 5] if dims == 3 else [3, 4, 1]
+    on = [6 if sel == 3 else n[sel] for sel, _ in src]
+    ax = f // 2
+    t = [d for d in range(3) if d != ax]
+    for m in range(2):
+        for a in range(n[t[0]]):
+            for b in range(n[t[1]]):
+                ijk = [0, 0, 0]
+                ijk[t[0]], ijk[t[1]] = a, b
+                ijk[ax] = n[ax] + m if f & 1 else -1 - m
+                want = tuple(on[d] - 1 - (m if sel == 3 else ijk[sel]) if flip else (m if sel == 3 else ijk[sel])
+                             for d, (sel, flip) in enumerate(src))
+                yield n, on, ijk, want
+
+
+def test_oracle_exchange_map_is_the_reference_map():
+    """full_face_copy.d:680-1409 spells out the ghost-to-source map for 4 x 4 face pairs
+    in 2D and 6 x 6 pairs x 4 orientations in 3D; the oracle restates it as one rule.
+    Every ghost of every case agrees."""
+    import oracle
+    maps = exchange_maps()
+    assert len(maps) == 160
+    for rec in maps:
+        for n, on, ijk, want in exchange_ghosts(rec):
+            got = oracle.exchange_source(rec["dims"], rec["face"], rec["other_face"], rec["orientation"], n, on, ijk)
+            assert got == want, (rec, ijk)
+    # a ghost two layers out, and a partner too small for the map
+    assert oracle.exchange_source(3, 1, 3, 0, [3, 4, 5], [4, 6, 5], [5, 0, 0]) is None
+    assert oracle.exchange_source(3, 1, 3, 1, [3, 4, 5], [4, 6, 5], [3, 3, 4]) is None
+
+
+def test_oracle_rotational_exchange_is_the_whole_domain():
+    """A flow with four-fold rotational symmetry on the quadrant x, y >= 0, its x = 0 and
+    y = 0 faces joined by exchanges that turn the ghosts' velocity by +-90 degrees
+    (reorient_vector_quantities, flowstate.d:393-400), against the same flow on the whole
+    square: after 40 steps (the momentum changes by O(1) relative to its maximum) the
+    quadrant agrees to rounding; without the rotation it does not."""
+    q, f = cases.quarter_rotational(n=(16, 16, 2)), cases.full_rotational(n=(16, 16, 2))
+    for c in (q, f):
+        c.config.update(dt_init=4e-7, dt_max=4e-7)
+    oq, of = cases.build_oracle(q), cases.build_oracle(f)
+    U0 = of.get_U(0).reshape(5, 2, 32, 32)[:, :, 16:, 16:].copy()
+    assert oq.run(40) == 0 and of.run(40) == 0
+    Uq = oq.get_U(0).reshape(5, 2, 16, 16)
+    Uf = of.get_U(0).reshape(5, 2, 32, 32)[:, :, 16:, 16:]
+    for qv in (0, 1, 2, 4):   # z momentum stays 0
+        scale = np.max(np.abs(Uf[qv]))
+        assert np.max(np.abs(Uq[qv] - Uf[qv])) <= 1e-13 * scale, qv
+    assert np.max(np.abs(Uf[1] - U0[1])) >= 0.5 * np.max(np.abs(Uf[1]))
+    plain = cases.quarter_rotational(n=(16, 16, 2))
+    plain.config.update(dt_init=4e-7, dt_max=4e-7)
+    for face in ("west", "south"):
+        plain.blocks[0]["bcs"][face][1].pop("Rmatrix")
+    op = cases.build_oracle(plain)
+    assert op.run(40) == 0
+    Up = op.get_U(0).reshape(5, 2, 16, 16)
+    assert np.max(np.abs(Up[1] - Uf[1])) >= 0.1 * np.max(np.abs(Uf[1]))
+
