@@ -283,6 +283,9 @@ def accuracy_leg(sims, n, flux, total_steps, stream):
             sim.run(max_step=total_steps - done)
     Uf, Ud = sims["fp32"].get_conserved(0), sims["fp64"].get_conserved(0)
     out["steps"] = total_steps
+    out["flux_calculator"] = flux
+    if flux == "hllc":   # both forms equal the oracle; the oracle's hllc has no reference-held check
+        out["pinned"] = "unpinned by the reference: no reference run, test or job uses hllc"
     out["rel_l2_vs_fp64"] = _l2_errors(Uf, Ud)
     out["time_fp32"], out["time_fp64"] = sims["fp32"].time()["time"], sims["fp64"].time()["time"]
     return out

@@ -171,6 +171,30 @@ def test_prepare_rejects_invalid_layouts_before_touching_the_device():
     L.gdfv_context_free(h)
 
 
+def test_block_size_limits():
+    """The largest blocks: the kernels index a block's cells and faces in 32-bit
+    arithmetic, so gdfv_prepare refuses a block whose faces of some direction (bounded
+    by (nic+1)(njc+1)(nkc+1)) pass 2^31 - 1, before any device allocation; 1289^3 cells
+    pass that check, 1290 x 1290 x 1289 do not.  gdfv_block_new refuses more than 2^34
+    cells outright."""
+    L = gdfv.lib()
+    h = L.gdfv_context_new()
+    assert L.gdfv_block_new(h, 4096, 4096, 1025, 1e-3, 1e-3, 1e-3, 0, 0, 0) == GDFV_ERR_ARG
+    assert "too large" in last_error(h)
+    L.gdfv_context_free(h)
+    import torch
+    # on a machine with a GPU the valid case would go on to allocate 3 x 86 GB
+    cases_ = [((1290, 1290, 1289), False)] + ([] if torch.cuda.is_available() else [((1289, 1289, 1289), True)])
+    for n, ok in cases_:
+        h, b = _ctx_with_block(L, n)
+        rc = L.gdfv_prepare(h)
+        if ok:
+            assert rc != GDFV_ERR_ARG, last_error(h)   # valid: no GPU here, so it fails later
+        else:
+            assert rc == GDFV_ERR_ARG and "2^31 - 1" in last_error(h)
+        L.gdfv_context_free(h)
+
+
 def test_exchange_map_is_the_reference_map():
     """gdfv_exchange_source (the map the kernels evaluate, from the same rule) against
     the reference's own map of every face pair and orientation
