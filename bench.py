@@ -191,11 +191,12 @@ def adjoint_over_forward(nsteps=50, shape=(128, 128, 64), autotune=True, forms=(
     state through the rollout.  Returns the ratio of the backward time to the forward
     time of the same 50 steps run by gdfv_run with the autotuned schedule (the forward
     the library runs by default), both with CUDA events on the device and both warm (a
-    10-step rollout and its backward run first).  Two backward forms: the trajectory
-    resident in device memory (rollout's default when it fits: 100 states, 4.2 GB here),
-    which recomputes nothing, and a checkpoint every 10 steps with each segment
-    recomputed.  Also the time of the rollout's own forward, which keeps the trajectory
-    (one launch and one host round trip per step)."""
+    rollout of the same length and its backward run first, so that torch's caching
+    allocator holds the trajectory buffers).  Two backward forms: the trajectory resident
+    in device memory (rollout's default when it fits: 100 states, 4.2 GB here), which
+    recomputes nothing, and a checkpoint every 10 steps with each segment recomputed.
+    Also the time of the rollout's own forward, which keeps the trajectory (one gdfv_run
+    call and host round trip per step)."""
     import torch
     import cases
     from gdfv.autograd import rollout
@@ -227,7 +228,7 @@ def adjoint_over_forward(nsteps=50, shape=(128, 128, 64), autotune=True, forms=(
             torch.cuda.synchronize()
             f0.record(stream)
             with torch.cuda.stream(stream):
-                UN = rollout(sim, U0r, theta, nsteps if rep else 10, K)
+                UN = rollout(sim, U0r, theta, nsteps, K)
             f1.record(stream)
             with torch.cuda.stream(stream):
                 J = wall_pressure(case, UN, case.R)

@@ -215,6 +215,7 @@ struct Config {
     int stringent_cfl = 0, cfl_count = 10, max_attempts = 3, max_invalid_cells = 0;
     int fixed_time_step = 0;
     int tile_kchunk = 0;  // 0: chosen per block
+    int tile_width = 32;  // kernel on decoded primitives: tiles 32 or 16 cells wide (build_tiles)
     int persistent = 0;   // 1: stage kernels as a resident grid taking tiles from a queue
     int autotune = 0;     // time tile shapes and the launch form on the first run, keep the fastest
     int lmr_epsilon = 0;  // van_albada_variant = lmr
@@ -235,6 +236,7 @@ struct Context {
     int nq = 5;
     int n_tiles = 0;
     int n_tiles2 = 0;   // > 0: the corrector's tile table (other rows) follows the first in d_tiles
+    int n_prim_wide = 0, n_prim_narrow = 0;   // the primitive kernel's tables after those
     double* U[2] = {nullptr, nullptr};
     double* dU0 = nullptr;
     BlockDesc* d_blocks = nullptr;
@@ -248,7 +250,8 @@ struct Context {
     std::vector<BlockDesc> h_blocks;
     NumParams P{};
     StepParams sp{};
-    cudaGraphExec_t graph = nullptr;
+    cudaGraphExec_t graph = nullptr;    // kGraphSteps step slots
+    cudaGraphExec_t graph1 = nullptr;   // one step slot (the tail of a run)
     int graph_steps = 0;
     bool signal_valid = false;
     int n_inflow = 0;
@@ -274,6 +277,7 @@ struct Context {
 
     ~Context() {
         if (graph) cudaGraphExecDestroy(graph);
+        if (graph1) cudaGraphExecDestroy(graph1);
         for (void* p : {(void*)U[0], (void*)U[1], (void*)dU0, (void*)d_blocks, (void*)d_tiles, (void*)d_inflow,
                         (void*)d_ctl, (void*)d_maxsig, (void*)d_lastsig, (void*)d_bad, (void*)adj_scratch, (void*)jvp_scratch,
                         (void*)norm_scratch, (void*)prim[0], (void*)prim[1], (void*)prim1, (void*)d_geom, (void*)d_rot,
@@ -375,6 +379,8 @@ StageArgs stage_args(Context* c) {
     A.P = c->P;
     A.n_tiles = c->n_tiles;
     A.n_tiles2 = c->n_tiles2;
+    A.n_prim_wide = c->n_prim_wide;
+    A.n_prim_narrow = c->n_prim_narrow;
     A.max_invalid_cells = c->cfg.max_invalid_cells;
     A.persistent = c->cfg.persistent;
     return A;
@@ -463,7 +469,10 @@ void fill_weights(double len, double* w) {
 // block's nkc up to 32).  Ordered by decreasing work (cells), so that a grid
 // taking tiles in order -- the hardware's CTA order, or the persistent stride --
 // starts the long tiles of uneven blocks first.
-void build_tiles_rows(Context* c, int kchunk, int TJ, std::vector<TileDesc>& tiles) {
+// Tiles of TI x TJ cells (k chunks of kchunk planes) over the i strips (i0 a multiple of
+// TI) that pick(block, i0) selects, sorted by decreasing work.
+template <class Pick>
+void build_tiles_strips(Context* c, int kchunk, int TI, int TJ, Pick pick, std::vector<TileDesc>& tiles) {
     tiles.clear();
     for (size_t b = 0; b < c->blocks.size(); ++b) {
         const HostBlock& hb = c->blocks[b];
@@ -471,7 +480,8 @@ void build_tiles_rows(Context* c, int kchunk, int TJ, std::vector<TileDesc>& til
         if (c->cfg.dims == 2) kc = 1;
         for (int k0 = 0; k0 < hb.n[2]; k0 += kc)
             for (int j0 = 0; j0 < hb.n[1]; j0 += TJ)
-                for (int i0 = 0; i0 < hb.n[0]; i0 += 32) {
+                for (int i0 = 0; i0 < hb.n[0]; i0 += TI) {
+                    if (!pick(hb, i0)) continue;
                     TileDesc t{};
                     t.block = (int)b; t.i0 = i0; t.j0 = j0; t.k0 = k0; t.k1 = std::min(k0 + kc, hb.n[2]);
                     tiles.push_back(t);
@@ -479,9 +489,13 @@ void build_tiles_rows(Context* c, int kchunk, int TJ, std::vector<TileDesc>& til
     }
     auto work = [&](const TileDesc& t) {
         const HostBlock& hb = c->blocks[t.block];
-        return (long long)std::min(32, hb.n[0] - t.i0) * std::min(TJ, hb.n[1] - t.j0) * (t.k1 - t.k0);
+        return (long long)std::min(TI, hb.n[0] - t.i0) * std::min(TJ, hb.n[1] - t.j0) * (t.k1 - t.k0);
     };
     std::stable_sort(tiles.begin(), tiles.end(), [&](const TileDesc& a, const TileDesc& b) { return work(a) > work(b); });
+}
+
+void build_tiles_rows(Context* c, int kchunk, int TJ, std::vector<TileDesc>& tiles) {
+    build_tiles_strips(c, kchunk, 32, TJ, [](const HostBlock&, int) { return true; }, tiles);
 }
 
 // Fraction of the tile rows of all blocks that hold cells, weighted by cells per row.
@@ -503,11 +517,18 @@ double row_use(const Context* c, int TJ) {
 // four-plane prologue of each tile weighs more: a 64-block lattice of 32-128 rows with
 // 96% row use ran 2.5% slower.  So the corrector gets its own table only when its rows
 // leave at most about 3% more empty row slots than the shared ones.
-void build_tiles(Context* c, int kchunk, std::vector<TileDesc>& tiles, int& n1, int& n2) {
+//
+// The kernel on decoded primitives (float Euler defaults) takes tiles 32 or 16 cells wide
+// (GeoF; 16 wide: two rows per warp, twice the rows), by cfg.tile_width.  With 16 its
+// table follows the others: n3 = 0 tiles 32 wide, n4 tiles 16 wide.  n3 = n4 = 0: it runs
+// over the first table.  The other kernels (and the no-alloc step, which runs them) keep
+// the first tables.  (Both widths in one stage, 16-wide tiles only for the strip left at
+// a block's i end, ran slower: the second, small launch waits for the first to drain.)
+void build_tiles(Context* c, int kchunk, std::vector<TileDesc>& tiles, int& n1, int& n2, int& n3, int& n4) {
     const int TJ = tile_rows(c->cfg.precision, c->cfg.mhd);
     build_tiles_rows(c, kchunk, TJ, tiles);
     n1 = (int)tiles.size();
-    n2 = 0;
+    n2 = n3 = n4 = 0;
     const int TJ2 = tile_rows_corrector(c->cfg.precision, c->cfg.mhd);
     if (TJ2 != TJ && row_use(c, TJ2) * 1.03 > row_use(c, TJ)) {
         std::vector<TileDesc> t2;
@@ -515,13 +536,19 @@ void build_tiles(Context* c, int kchunk, std::vector<TileDesc>& tiles, int& n1, 
         n2 = (int)t2.size();
         tiles.insert(tiles.end(), t2.begin(), t2.end());
     }
+    if (!(c->cfg.precision == 1 && prim_path(c->P)) || c->cfg.tile_width != 16) return;
+    std::vector<TileDesc> t4;
+    build_tiles_strips(c, kchunk, 16, 2 * TJ, [](const HostBlock&, int) { return true; }, t4);
+    n4 = (int)t4.size();
+    tiles.insert(tiles.end(), t4.begin(), t4.end());
 }
 
 // The cell that feeds each ghost of an ExchangeBC_FullFace, as a map word: for the
 // partner's index along axis d, bits 3d..3d+1 select this block's i, j, k or the ghost's
-// depth (0..3), and bit 3d+2 counts it from the partner's far end.  GhostCellFullFaceCopy.set_up_cell_mapping_phase0
-// (e4/bc/ghost_cell_effect/full_face_copy.d:680-1409) spells it out for 6 x 6 face pairs
-// and 4 orientations; every case there follows one rule, restated here.  Each face has
+// depth (0..3), and bit 3d+2 counts it from the partner's far end.
+// GhostCellFullFaceCopy.set_up_cell_mapping_phase0 (e4/bc/ghost_cell_effect/
+// full_face_copy.d:680-1409) spells it out for 6 x 6 face pairs and 4 orientations;
+// every case there follows one rule, restated here.  Each face has
 // a tangential frame of two axes with signs, right-handed about its outward normal:
 // west (-j, k), east (j, k), south (i, k), north (-i, k), bottom (-i, j), top (i, j).
 // Seen from the partner the ghost's frame is mirrored (first axis reversed), then turned
@@ -741,7 +768,6 @@ int do_prepare(Context* c) {
         B.x0 = hb.vert[0][0]; B.y0 = hb.vert[1][0]; B.z0 = hb.vert[2][0];
         B.L_min = g.dims == 3 ? std::min(std::min(lmin[0], lmin[1]), lmin[2]) : std::min(lmin[0], lmin[1]);
     }
-    build_tiles(c, g.tile_kchunk, tiles, c->n_tiles, c->n_tiles2);
     NumParams& P = c->P;
     P.gas.R = g.R; P.gas.gamma = g.gamma; P.gas.Cv = Cv; P.gas.Cvinv = 1.0 / Cv;
     P.eps_van_albada = g.eps_van_albada;
@@ -760,6 +786,8 @@ int do_prepare(Context* c) {
     sp.max_attempts = g.max_attempts; sp.max_invalid_cells = g.max_invalid_cells;
     sp.nblocks = (int)c->blocks.size();
     sp.cfl_value = g.cfl_value; sp.dt_init = g.dt_init; sp.dt_max = g.dt_max;
+    // (after the options: the tables depend on which kernels run)
+    build_tiles(c, g.tile_kchunk, tiles, c->n_tiles, c->n_tiles2, c->n_prim_wide, c->n_prim_narrow);
 
     CK(cudaGetDevice(&c->device));
     if (c->device < 64 && !g_configured[c->device]) {
@@ -839,18 +867,27 @@ int write_ctl(Context* c) {
 
 constexpr int kGraphSteps = 8;
 
-int build_graph(Context* c) {
+void drop_graphs(Context* c) {
     if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
-    cudaGraph_t g = nullptr;
-    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    cudaError_t e = cudaSuccess;
-    for (int s = 0; s < kGraphSteps && e == cudaSuccess; ++s) e = enqueue_step(c);
-    cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
-    if (e != cudaSuccess) { if (g) cudaGraphDestroy(g); return cuda_fail(c, e, "capture step"); }
-    if (e2 != cudaSuccess) return cuda_fail(c, e2, "cudaStreamEndCapture");
-    e = cudaGraphInstantiate(&c->graph, g, 0);
-    cudaGraphDestroy(g);
-    if (e != cudaSuccess) return cuda_fail(c, e, "cudaGraphInstantiate");
+    if (c->graph1) { cudaGraphExecDestroy(c->graph1); c->graph1 = nullptr; }
+}
+
+// The step slots of a run, captured once: kGraphSteps of them, and one alone for the
+// tail of a run (a slot past the halt is a no-op, but still launches its kernels).
+int build_graph(Context* c) {
+    drop_graphs(c);
+    for (int n : {kGraphSteps, 1}) {
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e = cudaSuccess;
+        for (int s = 0; s < n && e == cudaSuccess; ++s) e = enqueue_step(c);
+        cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
+        if (e != cudaSuccess) { if (g) cudaGraphDestroy(g); return cuda_fail(c, e, "capture step"); }
+        if (e2 != cudaSuccess) return cuda_fail(c, e2, "cudaStreamEndCapture");
+        e = cudaGraphInstantiate(n == 1 ? &c->graph1 : &c->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return cuda_fail(c, e, "cudaGraphInstantiate");
+    }
     c->graph_steps = kGraphSteps;
     return GDFV_OK;
 }
@@ -1137,6 +1174,10 @@ int gdfv_config_set_int(int ctx, const char* key, long long value) {
     else if (k == "fixed_time_step") g.fixed_time_step = v != 0;
     else if (k == "tile_kchunk") { if (v < 0) return fail(c, GDFV_ERR_ARG, "tile_kchunk >= 0"); g.tile_kchunk = v; }
     else if (k == "persistent") g.persistent = v != 0;
+    else if (k == "tile_width") {
+        if (v != 16 && v != 32) return fail(c, GDFV_ERR_ARG, "tile_width is 16 or 32");
+        g.tile_width = (int)v;
+    }
     else if (k == "autotune") g.autotune = v != 0;
     else return fail(c, GDFV_ERR_ARG, "unknown integer option: " + k);
     return GDFV_OK;
@@ -1176,6 +1217,7 @@ int gdfv_config_get_double(int ctx, const char* key, double* value) {
     else if (k == "divB_damping_length" || k == "divb_damping_length") *value = g.divB_damping_length;
     else if (k == "tile_kchunk") *value = g.tile_kchunk;
     else if (k == "persistent") *value = g.persistent;
+    else if (k == "tile_width") *value = g.tile_width;
     else if (k == "autotune") *value = g.autotune;
     else if (k == "autotune_stage_ms") *value = c->tune_ms;
     else if (k == "tile_rows") *value = tile_rows(g.precision, g.mhd);
@@ -1493,7 +1535,7 @@ cudaStream_t context_aux_stream(int ctx, int which) {
     return c->aux_stream[which];
 }
 
-int upload_tiles(Context* c, const std::vector<TileDesc>& tiles, int n1, int n2) {
+int upload_tiles(Context* c, const std::vector<TileDesc>& tiles, int n1, int n2, int n3, int n4) {
     CK(cudaStreamSynchronize(c->stream));
     if (tiles.size() > c->tiles_cap) {
         if (c->d_tiles) cudaFree(c->d_tiles);
@@ -1505,12 +1547,15 @@ int upload_tiles(Context* c, const std::vector<TileDesc>& tiles, int n1, int n2)
     CK(cudaMemcpy(c->d_tiles, tiles.data(), sizeof(TileDesc) * tiles.size(), cudaMemcpyHostToDevice));
     c->n_tiles = n1;
     c->n_tiles2 = n2;
-    if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }  // captured the old table
+    c->n_prim_wide = n3;
+    c->n_prim_narrow = n4;
+    drop_graphs(c);  // captured the old table
     return GDFV_OK;
 }
 
 // Autotuner: for each tile k-chunk and launch form (persistent grid or one CTA
-// per tile), time stage 1 + stage 2 on the current state and keep the fastest.
+// per tile) -- and for the kernel on decoded primitives, both tile widths -- time
+// stage 1 + stage 2 on the current state and keep the fastest.
 // The trial steps use a scratch control record with dt = 0 and write only the
 // idle state buffer and dU0, so the solution is not changed.
 int autotune(Context* c) {
@@ -1533,14 +1578,19 @@ int autotune(Context* c) {
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
     double best = 1e30;
-    int best_kc = c->cfg.tile_kchunk, best_p = c->cfg.persistent;
+    int best_kc = c->cfg.tile_kchunk, best_p = c->cfg.persistent, best_w = c->cfg.tile_width;
+    // tile widths of the kernel on decoded primitives
+    std::vector<int> widths = {c->cfg.tile_width};
+    if (c->prim[0]) widths = {32, 16};
     std::vector<TileDesc> tiles;
     cudaError_t e = cudaSuccess;
     const int reps = 3;
+    for (int tw : widths)
     for (int kc : kcs) {
-        int n1 = 0, n2 = 0;
-        build_tiles(c, kc, tiles, n1, n2);
-        int st = upload_tiles(c, tiles, n1, n2);
+        c->cfg.tile_width = tw;
+        int n1 = 0, n2 = 0, n3 = 0, n4 = 0;
+        build_tiles(c, kc, tiles, n1, n2, n3, n4);
+        int st = upload_tiles(c, tiles, n1, n2, n3, n4);
         if (st) { cudaEventDestroy(e0); cudaEventDestroy(e1); return st; }
         for (int pers = 1; pers >= 0 && e == cudaSuccess; --pers) {
             StageArgs A = stage_args_run(c, parity);
@@ -1561,7 +1611,7 @@ int autotune(Context* c) {
             if (e == cudaSuccess) e = cudaEventSynchronize(e1);
             float ms = 0.0f;
             if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
-            if (e == cudaSuccess && ms / reps < best) { best = ms / reps; best_kc = kc; best_p = pers; }
+            if (e == cudaSuccess && ms / reps < best) { best = ms / reps; best_kc = kc; best_p = pers; best_w = tw; }
         }
         if (e != cudaSuccess) break;
     }
@@ -1570,9 +1620,10 @@ int autotune(Context* c) {
     if (e != cudaSuccess) return cuda_fail(c, e, "autotune");
     c->cfg.tile_kchunk = best_kc;
     c->cfg.persistent = best_p;
-    int n1 = 0, n2 = 0;
-    build_tiles(c, best_kc, tiles, n1, n2);
-    int st = upload_tiles(c, tiles, n1, n2);
+    c->cfg.tile_width = best_w;
+    int n1 = 0, n2 = 0, n3 = 0, n4 = 0;
+    build_tiles(c, best_kc, tiles, n1, n2, n3, n4);
+    int st = upload_tiles(c, tiles, n1, n2, n3, n4);
     if (st) return st;
     c->tuned = true;
     c->tune_ms = best;
@@ -1618,9 +1669,13 @@ int gdfv_run(int ctx, int max_steps, double max_time, int* steps_taken) {
             if (est < (double)remaining) remaining = (long long)std::max(1.0, est);
         }
         if (c->h_ctl->retrying) remaining += 1;
-        int graphs = (int)std::min<long long>(64, std::max<long long>(1, (remaining + c->graph_steps - 1) / c->graph_steps));
+        // whole batches, then single slots for the rest
+        remaining = std::max<long long>(1, remaining);
+        const int graphs = (int)std::min<long long>(64, remaining / c->graph_steps);
+        const int singles = graphs < 64 ? (int)(remaining % c->graph_steps) : 0;
         for (int g = 0; g < graphs; ++g) CK(cudaGraphLaunch(c->graph, c->stream));
-        launched += (long long)graphs * c->graph_steps;
+        for (int g = 0; g < singles; ++g) CK(cudaGraphLaunch(c->graph1, c->stream));
+        launched += (long long)graphs * c->graph_steps + singles;
         if (read_ctl(c)) return GDFV_ERR_CUDA;
     }
     if (steps_taken) *steps_taken = c->h_ctl->step - start_step;
@@ -1878,7 +1933,7 @@ int gdfv_set_stream(int ctx, void* stream) {
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
     c->stream = (cudaStream_t)stream;
     c->own_stream = false;
-    if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
+    drop_graphs(c);
     return GDFV_OK;
 }
 

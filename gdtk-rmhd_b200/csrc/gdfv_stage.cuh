@@ -55,6 +55,10 @@ struct StageArgs {
     // conserved state
     void* prim[2];
     void* prim1;
+    // that kernel's own tile tables after the first two (n_tiles + n_tiles2 entries on):
+    // n_prim_wide tiles 32 cells wide, then n_prim_narrow tiles 16 wide; both 0: it runs
+    // over the first table
+    int n_prim_wide, n_prim_narrow;
     // rotations of exchange faces with an Rmatrix (9 doubles each, row major)
     const double* rot;
 };

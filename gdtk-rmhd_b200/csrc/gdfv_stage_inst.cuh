@@ -58,37 +58,64 @@ cudaError_t launch_rows(const StageArgs& A, cudaStream_t s) {
 }
 
 #if GDFV_PRIM_PATH
-// The Euler kernel on decoded primitives (gdfv_stage_prim.cuh) over the first tile
-// table (rows TJ_E in both stages).
-template <int STAGE, int FLUX, int PERS>
+// The Euler kernel on decoded primitives (gdfv_stage_prim.cuh): TJ_E row warps, tiles 32
+// or 16 cells wide (TW).
+template <int STAGE, int FLUX, int TW>
 int& resident_prim() {
     static int v = 0;
     return v;
 }
 
+template <int STAGE, int FLUX, int TW>
+cudaError_t launch_prim_w(const StageArgs& A, cudaStream_t s) {
+    using G = GeoF<Real, TJ_E, TW>;
+    const int cap = resident_prim<STAGE, FLUX, TW>();
+    if (A.persistent && cap > 0)
+        stage_prim_kernel<Real, STAGE, FLUX, TJ_E, 1, TW><<<cap < A.n_tiles ? cap : A.n_tiles, G::NT, G::bytes, s>>>(A);
+    else
+        stage_prim_kernel<Real, STAGE, FLUX, TJ_E, 0, TW><<<A.n_tiles, G::NT, G::bytes, s>>>(A);
+    return cudaGetLastError();
+}
+
+// Over the first tile table (rows TJ_E in both stages), or over its own tables: tiles 32
+// wide, then (a second launch; a persistent launch leaves the tile queue at zero) tiles
+// 16 wide.  The runtime fills one of the two.
 template <int STAGE, int FLUX>
 cudaError_t launch_prim(const StageArgs& A, cudaStream_t s) {
-    using G = GeoF<Real, TJ_E>;
-    const int cap = resident_prim<STAGE, FLUX, 1>();
-    if (A.persistent && cap > 0)
-        stage_prim_kernel<Real, STAGE, FLUX, TJ_E, 1><<<cap < A.n_tiles ? cap : A.n_tiles, G::NT, G::bytes, s>>>(A);
-    else
-        stage_prim_kernel<Real, STAGE, FLUX, TJ_E, 0><<<A.n_tiles, G::NT, G::bytes, s>>>(A);
-    return cudaGetLastError();
+    if (A.n_prim_wide + A.n_prim_narrow == 0) return launch_prim_w<STAGE, FLUX, 32>(A, s);
+    cudaError_t e = cudaSuccess;
+    StageArgs Ap = A;
+    Ap.tiles = A.tiles + A.n_tiles + A.n_tiles2;
+    if (A.n_prim_wide > 0) {
+        Ap.n_tiles = A.n_prim_wide;
+        e = launch_prim_w<STAGE, FLUX, 32>(Ap, s);
+        Ap.tiles += A.n_prim_wide;
+    }
+    if (e == cudaSuccess && A.n_prim_narrow > 0) {
+        Ap.n_tiles = A.n_prim_narrow;
+        e = launch_prim_w<STAGE, FLUX, 16>(Ap, s);
+    }
+    return e;
+}
+
+template <int STAGE, int FLUX, int TW>
+cudaError_t configure_prim_w(int n_sm) {
+    using G = GeoF<Real, TJ_E, TW>;
+    cudaError_t e = set_smem(stage_prim_kernel<Real, STAGE, FLUX, TJ_E, 0, TW>, G::bytes);
+    if (e == cudaSuccess) e = set_smem(stage_prim_kernel<Real, STAGE, FLUX, TJ_E, 1, TW>, G::bytes);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, stage_prim_kernel<Real, STAGE, FLUX, TJ_E, 1, TW>,
+                                                      G::NT, G::bytes);
+    if (e != cudaSuccess) return e;
+    resident_prim<STAGE, FLUX, TW>() = per_sm * n_sm;
+    return cudaSuccess;
 }
 
 template <int STAGE, int FLUX>
 cudaError_t configure_prim(int n_sm) {
-    using G = GeoF<Real, TJ_E>;
-    cudaError_t e = set_smem(stage_prim_kernel<Real, STAGE, FLUX, TJ_E, 0>, G::bytes);
-    if (e == cudaSuccess) e = set_smem(stage_prim_kernel<Real, STAGE, FLUX, TJ_E, 1>, G::bytes);
-    if (e != cudaSuccess) return e;
-    int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, stage_prim_kernel<Real, STAGE, FLUX, TJ_E, 1>, G::NT,
-                                                      G::bytes);
-    if (e != cudaSuccess) return e;
-    resident_prim<STAGE, FLUX, 1>() = per_sm * n_sm;
-    return cudaSuccess;
+    cudaError_t e = configure_prim_w<STAGE, FLUX, 32>(n_sm);
+    return e == cudaSuccess ? configure_prim_w<STAGE, FLUX, 16>(n_sm) : e;
 }
 #endif
 

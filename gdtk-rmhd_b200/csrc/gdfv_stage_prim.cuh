@@ -142,23 +142,26 @@ __device__ __forceinline__ void store_pf(R* __restrict__ Pout, long long total, 
     Pout[5 * total + g] = (R)s.a;
 }
 
-// Shared-memory layout (values of R) of the kernel for TJ rows.
-template <class R, int TJ_>
+// Shared-memory layout (values of R) of the kernel for TJ row warps and tiles TW cells
+// wide: TW = 32, one row per warp; TW = 16, two rows per warp (lanes 0-15 and 16-31),
+// NR = TJ * 32 / TW rows.
+template <class R, int TJ_, int TW = 32>
 struct GeoF {
-    static constexpr int TI = 32, TJ = TJ_;
+    static_assert(TW == 32 || TW == 16, "tiles 32 or 16 cells wide");
+    static constexpr int TI = TW, TJ = TJ_, NR = TJ_ * (32 / TW);
     static constexpr int NT = 32 * (TJ + 1);
-    static constexpr int PW = TI + 4, PH = TJ + 4, PLANE = PW * PH;
+    static constexpr int PW = TI + 4, PH = NR + 4, PLANE = PW * PH;
     static constexpr int NS = 5;                              // reconstructed scalars
     static constexpr int O_RING = 0;                          // [4][6][PLANE]
-    static constexpr int O_QPJ = O_RING + 4 * 6 * PLANE;      // [NS][TJ][TI]   j plus-side state of each cell
-    static constexpr int O_EJS = O_QPJ + NS * TJ * TI;        // [NS][TI]       j plus-side state of row -1
+    static constexpr int O_QPJ = O_RING + 4 * 6 * PLANE;      // [NS][NR][TI]   j plus-side state of each cell
+    static constexpr int O_EJS = O_QPJ + NS * NR * TI;        // [NS][TI]       j plus-side state of row -1
     static constexpr int O_EJN = O_EJS + NS * TI;             // [NS][TI]       j minus-side state of row nj
-    static constexpr int O_EIW = O_EJN + NS * TI;             // [NS][TJ]       i plus-side state of column -1
-    static constexpr int O_EIE = O_EIW + NS * TJ;             // [NS][TJ]       i minus-side state of column ni
-    static constexpr int O_EIL = O_EIE + NS * TJ;             // [NS][TJ]       i plus-side state of column ni-1
-    static constexpr int O_FJ = O_EIL + NS * TJ;              // [NS][TJ+1][TI] flux of the S face of rows 0..nj
-    static constexpr int O_FIE = O_FJ + NS * (TJ + 1) * TI;   // [NS][TJ]       flux of the E face of each row
-    static constexpr int O_END = O_FIE + NS * TJ;
+    static constexpr int O_EIW = O_EJN + NS * TI;             // [NS][NR]       i plus-side state of column -1
+    static constexpr int O_EIE = O_EIW + NS * NR;             // [NS][NR]       i minus-side state of column ni
+    static constexpr int O_EIL = O_EIE + NS * NR;             // [NS][NR]       i plus-side state of column ni-1
+    static constexpr int O_FJ = O_EIL + NS * NR;              // [NS][NR+1][TI] flux of the S face of rows 0..nj
+    static constexpr int O_FIE = O_FJ + NS * (NR + 1) * TI;   // [NS][NR]       flux of the E face of each row
+    static constexpr int O_END = O_FIE + NS * NR;
     static constexpr size_t bytes = sizeof(R) * (size_t)O_END;
 };
 
@@ -170,13 +173,13 @@ struct GeoF {
 #define GDFV_MINB_PRIM_FP64 2
 #endif
 
-template <class R, int STAGE, int FLUX, int TJ, int PERS>
+template <class R, int STAGE, int FLUX, int TJ, int PERS, int TW = 32>
 __global__ void __launch_bounds__(32 * (TJ + 1), sizeof(R) == 4 ? GDFV_MINB_PRIM_FP32 : GDFV_MINB_PRIM_FP64)
     stage_prim_kernel(StageArgs A) {
     static_assert(STAGE == 1 || STAGE == 2, "predictor or corrector");
     constexpr bool FAST = sizeof(R) == 4;
-    using G = GeoF<R, TJ>;
-    constexpr int TI = G::TI, PW = G::PW, PLANE = G::PLANE, NS = G::NS;
+    using G = GeoF<R, TJ, TW>;
+    constexpr int TI = G::TI, NR = G::NR, PW = G::PW, PLANE = G::PLANE, NS = G::NS;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R* sm = reinterpret_cast<R*>(smem_raw);
     R* ring = sm + G::O_RING;
@@ -209,6 +212,9 @@ __global__ void __launch_bounds__(32 * (TJ + 1), sizeof(R) == 4 ? GDFV_MINB_PRIM
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
     const bool edge = warp == TJ;   // the edge warp
+    // own column and row in the tile: lane and warp (32 wide), or two rows per warp (16 wide)
+    const int ti = TW == 32 ? lane : (lane & (TW - 1));
+    const int tj = TW == 32 ? warp : warp * (32 / TW) + lane / TW;
 
     Control* qctl = const_cast<Control*>(ctl);
     int tix = blockIdx.x;
@@ -222,9 +228,9 @@ __global__ void __launch_bounds__(32 * (TJ + 1), sizeof(R) == 4 ? GDFV_MINB_PRIM
         const int blk = t.block;
         const BlockDesc& B = A.blocks[blk];
         const int ni_t = min(TI, B.n[0] - t.i0);
-        const int nj_t = min(TJ, B.n[1] - t.j0);
-        const bool active = !edge && warp < nj_t && lane < ni_t;
-        const int pidx = (lane + 2) + PW * (warp + 2);     // own cell in a padded plane
+        const int nj_t = min(NR, B.n[1] - t.j0);
+        const bool active = !edge && tj < nj_t && ti < ni_t;
+        const int pidx = (ti + 2) + PW * (tj + 2);         // own cell in a padded plane
         if (tid < 3 * W_N) w[tid / W_N][tid % W_N] = (R)B.w[tid / W_N][tid % W_N];
         if (tid < 3) {
             s_geo[tid] = 1.0 / B.len[tid];
@@ -242,7 +248,7 @@ __global__ void __launch_bounds__(32 * (TJ + 1), sizeof(R) == 4 ? GDFV_MINB_PRIM
         const int n2 = B.n[2];
         const int pstride = B.n[0] * B.n[1];
         const long long boff = B.offset;
-        int c_own = (t.i0 + lane) + B.n[0] * ((t.j0 + warp) + B.n[1] * t.k0);
+        int c_own = (t.i0 + ti) + B.n[0] * ((t.j0 + tj) + B.n[1] * t.k0);
         auto slot = [&](int kk) -> R* { return ring + (kk & 3) * (6 * PLANE); };
 
         double sig_max = 0.0;
@@ -286,7 +292,7 @@ __global__ void __launch_bounds__(32 * (TJ + 1), sizeof(R) == 4 ? GDFV_MINB_PRIM
         }
         c_halo += pstride;
         if (active) {
-            const int gi = t.i0 + lane, gj = t.j0 + warp;
+            const int gi = t.i0 + ti, gj = t.j0 + tj;
             PF<R> c[5];
 #pragma unroll
             for (int m = 0; m < 5; ++m) {
@@ -336,23 +342,23 @@ __global__ void __launch_bounds__(32 * (TJ + 1), sizeof(R) == 4 ? GDFV_MINB_PRIM
                     gather<R, NS, 0>(cur, PLANE, pidx, q0);
                     gather<R, NS, 0>(cur, PLANE, pidx + 1, qp1);
                     recon_cell<R, NS, false, 1>(w[0], wf[0], P, qm1, q0, qp1, qmi, qpi);
-                    if (lane == ni_t - 1) {
+                    if (ti == ni_t - 1) {
 #pragma unroll
-                        for (int s = 0; s < NS; ++s) EIL[s * TJ + warp] = qpi[s];
+                        for (int s = 0; s < NS; ++s) EIL[s * NR + tj] = qpi[s];
                     }
                     gather<R, NS, 1>(cur, PLANE, pidx - PW, qm1);
                     gather<R, NS, 1>(cur, PLANE, pidx, q0);
                     gather<R, NS, 1>(cur, PLANE, pidx + PW, qp1);
                     recon_cell<R, NS, false, 1>(w[1], wf[1], P, qm1, q0, qp1, qmj, qpj);
 #pragma unroll
-                    for (int s = 0; s < NS; ++s) QPJ[(s * TJ + warp) * TI + lane] = qpj[s];
+                    for (int s = 0; s < NS; ++s) QPJ[(s * NR + tj) * TI + ti] = qpj[s];
                 } else {
 #pragma unroll
                     for (int s = 0; s < NS; ++s) qpi[s] = R(0);
                 }
                 // left state of the W face: the plus-side state of the lane to the left
 #pragma unroll
-                for (int s = 0; s < NS; ++s) qLi[s] = __shfl_up_sync(0xffffffffu, qpi[s], 1);
+                for (int s = 0; s < NS; ++s) qLi[s] = __shfl_up_sync(0xffffffffu, qpi[s], 1, TI);
             }
             if (edge) {
                 for (int e = lane; e < ne_rec; e += 32) {
@@ -367,7 +373,7 @@ __global__ void __launch_bounds__(32 * (TJ + 1), sizeof(R) == 4 ? GDFV_MINB_PRIM
                         recon_cell<R, NS, false, 1>(w[0], wf[0], P, qm1, q0, qp1, qm, qp);
                         R* dst = east ? EIE : EIW;
 #pragma unroll
-                        for (int s = 0; s < NS; ++s) dst[s * TJ + r] = east ? qm[s] : qp[s];
+                        for (int s = 0; s < NS; ++s) dst[s * NR + r] = east ? qm[s] : qp[s];
                     } else {                       // row -1 (plus side) or nj (minus side) of column c
                         const int e2 = e - 2 * nj_t;
                         const bool north = e2 >= ni_t;
@@ -385,7 +391,7 @@ __global__ void __launch_bounds__(32 * (TJ + 1), sizeof(R) == 4 ? GDFV_MINB_PRIM
             }
             // ghosts of A (boundary tiles), then the copies complete
             if (active && more && !lead_in)
-                put_pf(slot(k + 3), PLANE, pidx, ghost_pf(A, Pin, B, t.i0 + lane, t.j0 + warp, k + 3));
+                put_pf(slot(k + 3), PLANE, pidx, ghost_pf(A, Pin, B, t.i0 + ti, t.j0 + tj, k + 3));
             if (h_on && more && !h_in) put_pf(nx1, PLANE, h_dst, ghost_pf(A, Pin, B, h_ci, h_cj, k + 1));
             cp_async_wait<0>();
             __syncthreads();
@@ -393,19 +399,19 @@ __global__ void __launch_bounds__(32 * (TJ + 1), sizeof(R) == 4 ? GDFV_MINB_PRIM
             // ---------------- C: fluxes (W, S faces; k reconstruction and the T face)
             R fW[NS], fT[NS];
             if (active) {
-                if (lane == 0) {
+                if (ti == 0) {
 #pragma unroll
-                    for (int s = 0; s < NS; ++s) qLi[s] = EIW[s * TJ + warp];
+                    for (int s = 0; s < NS; ++s) qLi[s] = EIW[s * NR + tj];
                 }
                 face_flux<R, false, FLUX, 0, 6>(P, R(0), qLi, qmi, cur, pidx - 1, cur, pidx, PLANE, fW);
                 {
                     R qL[NS], fS[NS];
 #pragma unroll
                     for (int s = 0; s < NS; ++s)
-                        qL[s] = warp == 0 ? EJS[s * TI + lane] : QPJ[(s * TJ + warp - 1) * TI + lane];
+                        qL[s] = tj == 0 ? EJS[s * TI + ti] : QPJ[(s * NR + tj - 1) * TI + ti];
                     face_flux<R, false, FLUX, 1, 6>(P, R(0), qL, qmj, cur, pidx - PW, cur, pidx, PLANE, fS);
 #pragma unroll
-                    for (int s = 0; s < NS; ++s) FJ[(s * (TJ + 1) + warp) * TI + lane] = fS[s];
+                    for (int s = 0; s < NS; ++s) FJ[(s * (NR + 1) + tj) * TI + ti] = fS[s];
                 }
                 {
                     R qm1[NS], q0[NS], qp1[NS], kq_m[NS], kq_p[NS];
@@ -427,21 +433,21 @@ __global__ void __launch_bounds__(32 * (TJ + 1), sizeof(R) == 4 ? GDFV_MINB_PRIM
                     if (e < nj_t) {                // E face of row e
                         const int p = (ni_t + 2) + PW * (e + 2);
 #pragma unroll
-                        for (int s = 0; s < NS; ++s) { qL[s] = EIL[s * TJ + e]; qR[s] = EIE[s * TJ + e]; }
+                        for (int s = 0; s < NS; ++s) { qL[s] = EIL[s * NR + e]; qR[s] = EIE[s * NR + e]; }
                         face_flux<R, false, FLUX, 0, 6>(P, R(0), qL, qR, cur, p - 1, cur, p, PLANE, F);
 #pragma unroll
-                        for (int s = 0; s < NS; ++s) FIE[s * TJ + e] = F[s];
+                        for (int s = 0; s < NS; ++s) FIE[s * NR + e] = F[s];
                     } else {                       // N face of the top row, column c
                         const int c = e - nj_t;
                         const int p = (c + 2) + PW * (nj_t + 2);
 #pragma unroll
                         for (int s = 0; s < NS; ++s) {
-                            qL[s] = QPJ[(s * TJ + nj_t - 1) * TI + c];
+                            qL[s] = QPJ[(s * NR + nj_t - 1) * TI + c];
                             qR[s] = EJN[s * TI + c];
                         }
                         face_flux<R, false, FLUX, 1, 6>(P, R(0), qL, qR, cur, p - PW, cur, p, PLANE, F);
 #pragma unroll
-                        for (int s = 0; s < NS; ++s) FJ[(s * (TJ + 1) + nj_t) * TI + c] = F[s];
+                        for (int s = 0; s < NS; ++s) FJ[(s * (NR + 1) + nj_t) * TI + c] = F[s];
                     }
                 }
             }
@@ -452,11 +458,11 @@ __global__ void __launch_bounds__(32 * (TJ + 1), sizeof(R) == 4 ? GDFV_MINB_PRIM
                 // flux of the E face: the W face of the lane to the right
                 R fE[NS];
 #pragma unroll
-                for (int s = 0; s < NS; ++s) fE[s] = __shfl_down_sync(0xffffffffu, fW[s], 1);
+                for (int s = 0; s < NS; ++s) fE[s] = __shfl_down_sync(0xffffffffu, fW[s], 1, TI);
                 if (active) {
-                    if (lane == ni_t - 1) {
+                    if (ti == ni_t - 1) {
 #pragma unroll
-                        for (int s = 0; s < NS; ++s) fE[s] = FIE[s * TJ + warp];
+                        for (int s = 0; s < NS; ++s) fE[s] = FIE[s * NR + tj];
                     }
                     // face_flux turned the face-local flux (mass, normal and tangential momentum,
                     // energy) back to the global frame: F[MASS], F[XMOM..ZMOM], F[TOTENERGY]
@@ -466,8 +472,8 @@ __global__ void __launch_bounds__(32 * (TJ + 1), sizeof(R) == 4 ? GDFV_MINB_PRIM
                     double dU[5];
 #pragma unroll
                     for (int q = 0; q < 5; ++q) {
-                        const R fS = FJ[(q * (TJ + 1) + warp) * TI + lane];
-                        const R fN = FJ[(q * (TJ + 1) + warp + 1) * TI + lane];
+                        const R fS = FJ[(q * (NR + 1) + tj) * TI + ti];
+                        const R fN = FJ[(q * (NR + 1) + tj + 1) * TI + ti];
                         if constexpr (FAST) {
                             // float: differences of opposite faces in float (same-signed, nearly
                             // equal fluxes subtract exactly), the sum in FP64

@@ -27,7 +27,8 @@ _STR_KEYS = ("flux_calculator", "gasdynamic_update_scheme", "thermo_interpolator
 _INT_KEYS = ("interpolation_order", "dimensions", "MHD", "divergence_cleaning", "apply_limiter",
              "extrema_clipping", "apply_entropy_fix", "interpolate_in_local_frame", "stringent_cfl",
              "cfl_count", "max_attempts_for_step", "max_invalid_cells", "fixed_time_step",
-             "n_ghost_cell_layers", "glm_reference_indexing", "tile_kchunk", "persistent", "autotune")
+             "n_ghost_cell_layers", "glm_reference_indexing", "tile_kchunk", "persistent", "tile_width",
+             "autotune")
 _DBL_KEYS = ("cfl_value", "dt_init", "dt_max", "epsilon_van_albada", "divB_damping_length",
              "flowstate_limits_max_velocity", "flowstate_limits_max_temp", "flowstate_limits_min_temp")
 
@@ -60,6 +61,7 @@ class Config:
         self.glm_reference_indexing = True
         self.tile_kchunk = 0          # planes per tile (0: the block's nkc up to 32)
         self.persistent = False       # True: stage kernels as a resident grid over the tile queue
+        self.tile_width = 32          # float Euler kernel: tiles 32 or 16 cells wide
         self.autotune = False         # time tile shapes and launch forms on the first run
         self.cfl_value = 0.5
         self.dt_init = 1.0e-3
@@ -390,7 +392,7 @@ class Simulation:
 
     def option(self, key):
         """Current value of a numeric option as the library holds it (after an
-        autotuned run: tile_kchunk, persistent and autotune_stage_ms)."""
+        autotuned run: tile_kchunk, persistent, tile_width and autotune_stage_ms)."""
         v = ffi.new("double*")
         check(self.ctx, self.L.gdfv_config_get_double(self.ctx, key.encode(), v))
         return v[0]

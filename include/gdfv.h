@@ -58,10 +58,12 @@ int gdfv_context_free(int ctx);
  * Scheduling integers with no reference counterpart (results do not depend on them):
  * tile_kchunk (planes per tile, 0: the block's nkc up to 32), persistent (1: each
  * stage is one resident grid taking the tiles of all blocks from a queue; default 0:
- * one CTA per tile),
- * autotune (1: the first gdfv_run times the tile k-chunks and both launch forms and
- * keeps the fastest).  gdfv_config_get_double also reads tile_kchunk, persistent,
- * autotune and autotune_stage_ms (stage 1 + stage 2 time of the tuned choice), and after
+ * one CTA per tile), tile_width (float-flux Euler defaults: 32, the default, tiles 32
+ * cells wide, one row per warp; 16: tiles 16 wide with two rows per warp, which leave
+ * fewer lanes idle on blocks whose width is not a multiple of 32),
+ * autotune (1: the first gdfv_run times the tile k-chunks, both launch forms and both
+ * tile widths, and keeps the fastest).  gdfv_config_get_double also reads
+ * tile_kchunk, persistent, tile_width, autotune and autotune_stage_ms (stage 1 + stage 2 time of the tuned choice), and after
  * gdfv_prepare tile_rows and tile_rows_corrector (rows per column tile of the stages
  * and of the corrector, which may take taller or shorter tiles of its own). */
 int gdfv_config_set_str(int ctx, const char* key, const char* value);

@@ -487,29 +487,35 @@ def test_get_conserved_into_caller_buffer():
 def test_float_euler_path_launch_forms(flux):
     """The float Euler stages of the default options run on decoded float primitives
     over one tile table of 8 rows in both stages (56 rows here: the stencil-decoding
-    kernels would give their corrector 7-row tiles of its own); the results match the
-    oracle as the other float tests do, in the per-tile and the persistent launch form,
-    and the two forms agree to float rounding."""
+    kernels would give their corrector 7-row tiles of its own), in tiles 32 cells wide or
+    16 wide with two rows per warp (40 x 56 here: a ragged 8-wide strip, three full
+    16-row tiles and a ragged one); the results match the oracle as the other float tests
+    do, in the per-tile and the persistent launch form, and all forms agree to float
+    rounding."""
     case = cases.c2_inflow_box(n=(40, 56, 24), flux=flux)
     orc = cases.build_oracle(case)
     assert orc.run(20) == 0
     Uo = orc.get_U(0)
     states = {}
     for pers in (False, True):
-        sim = cases.build_gpu(case, flux_precision="fp32", persistent=pers)
-        assert sim.option("tile_rows") == 8 and sim.option("tile_rows_corrector") == 8
-        assert sim.run(max_step=20) == 20
-        Ug = sim.get_conserved(0)
-        errs = [cases.rel_l2(Ug[0], Uo[0]), cases.rel_l2(Ug[1:4].ravel(), Uo[1:4].ravel()), cases.rel_l2(Ug[4], Uo[4])]
-        assert max(errs) <= TOL_FP32_L2, (pers, errs)
-        states[pers] = Ug
-        sim.close()
+        for tw in (32, 16):
+            sim = cases.build_gpu(case, flux_precision="fp32", persistent=pers, tile_width=tw)
+            assert sim.option("tile_rows") == 8 and sim.option("tile_rows_corrector") == 8
+            assert sim.option("tile_width") == tw
+            assert sim.run(max_step=20) == 20
+            Ug = sim.get_conserved(0)
+            errs = [cases.rel_l2(Ug[0], Uo[0]), cases.rel_l2(Ug[1:4].ravel(), Uo[1:4].ravel()),
+                    cases.rel_l2(Ug[4], Uo[4])]
+            assert max(errs) <= TOL_FP32_L2, (pers, tw, errs)
+            states[(pers, tw)] = Ug
+            sim.close()
     # mass, momentum pooled over its components (y and z momentum alone are near zero
     # in this x-directed flow), energy
-    a, b = states[True], states[False]
-    assert cases.rel_l2(a[0], b[0]) <= 1e-6
-    assert cases.rel_l2(a[1:4].ravel(), b[1:4].ravel()) <= 1e-6
-    assert cases.rel_l2(a[4], b[4]) <= 1e-6
+    b = states[(False, 32)]
+    for key, a in states.items():
+        assert cases.rel_l2(a[0], b[0]) <= 1e-6, key
+        assert cases.rel_l2(a[1:4].ravel(), b[1:4].ravel()) <= 1e-6, key
+        assert cases.rel_l2(a[4], b[4]) <= 1e-6, key
 
 
 def test_calls_with_nothing_to_do():
