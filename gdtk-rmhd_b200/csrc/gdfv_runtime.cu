@@ -263,6 +263,8 @@ struct Context {
     double* norm_scratch = nullptr;    // per-CTA partials and result of gdfv_residual_norms
     double* d_geom = nullptr;          // graded blocks: cell lengths and l2r2 weights per direction
     double* d_rot = nullptr;           // rotations of exchange faces with an Rmatrix, 9 doubles each
+    double* d_rec = nullptr;           // gdfv_run_record: dt of each step, then a flag
+    int rec_cap = 0;
     int adj_ready = 0;
     long long adj_scratch_n = 0;
     cudaStream_t aux_stream[2] = {nullptr, nullptr};  // lowest / highest priority streams of the rollout adjoint
@@ -280,7 +282,7 @@ struct Context {
         if (graph1) cudaGraphExecDestroy(graph1);
         for (void* p : {(void*)U[0], (void*)U[1], (void*)dU0, (void*)d_blocks, (void*)d_tiles, (void*)d_inflow,
                         (void*)d_ctl, (void*)d_maxsig, (void*)d_lastsig, (void*)d_bad, (void*)adj_scratch, (void*)jvp_scratch,
-                        (void*)norm_scratch, (void*)prim[0], (void*)prim[1], (void*)prim1, (void*)d_geom, (void*)d_rot,
+                        (void*)norm_scratch, (void*)prim[0], (void*)prim[1], (void*)prim1, (void*)d_geom, (void*)d_rot, (void*)d_rec,
                         (void*)step_ctl, (void*)step_maxsig, (void*)step_lastsig})
             if (p) cudaFree(p);
         if (h_ctl) cudaFreeHost(h_ctl);
@@ -966,6 +968,28 @@ void adjoint_set_error(int ctx, const std::string& msg) {
 __global__ void predictor_state_kernel(const double* U0, const double* dU0, double dt, long long n, double* U1) {
     long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (x < n) U1[x] = __dadd_rn(U0[x], __dmul_rn(dt, dU0[x]));
+}
+
+// Record of the step that just completed (gdfv_run_record): the state after it (the
+// buffer the step counter's parity names), its predictor state U0 + dt dU0 (U0 in the
+// other buffer, the step's input, in the predictor's operation order) and its dt.  A step
+// counter other than `expect` means the step did not complete in its slot (a retry, or a
+// failure): *flag is set and nothing is written.
+__global__ void record_step_kernel(const Control* ctl, const double* U0buf, const double* U1buf, const double* dU0,
+                                   long long n, int expect, double* state_out, double* pred_out, double* dt_out,
+                                   int* flag) {
+    if (ctl->step != expect || ctl->status != ST_OK) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) *flag = 1;
+        return;
+    }
+    const double* cur = (ctl->step & 1) ? U1buf : U0buf;
+    const double* prev = (ctl->step & 1) ? U0buf : U1buf;
+    const double dt = ctl->dt_global;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *dt_out = dt;
+    for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < n; x += (long long)gridDim.x * blockDim.x) {
+        if (state_out) state_out[x] = cur[x];
+        if (pred_out) pred_out[x] = __dadd_rn(prev[x], __dmul_rn(dt, dU0[x]));
+    }
 }
 
 // Residual norms of dU/dt (e4/fluidblock.d:861-909): per CTA, the maximum of |dU/dt[q]|
@@ -1685,6 +1709,64 @@ int gdfv_run(int ctx, int max_steps, double max_time, int* steps_taken) {
     if (c->h_ctl->status == ST_DECODE_FAILED)
         return fail(c, GDFV_ERR_STEP_FAILED, "Explicit update failed after max_attempts_for_step attempts." +
                                                  bad_cell_text(c, c->h_ctl->first_bad_cell));
+    return GDFV_OK;
+}
+
+int gdfv_run_record(int ctx, int nsteps, double* const* states_dev, double* const* preds_dev, double* dts) {
+    Context* c = get_ctx(ctx);
+    int st = check_ready(c, -1);
+    if (st) return st;
+    if (nsteps < 1 || !states_dev || !preds_dev || !dts)
+        return fail(c, GDFV_ERR_ARG, "gdfv_run_record needs nsteps >= 1, the two pointer arrays and dts");
+    if (!c->signal_valid) {
+        if ((st = scan_signal(c)) != GDFV_OK) return st;
+    }
+    if ((st = ensure_prims(c)) != GDFV_OK) return st;
+    if (c->cfg.autotune && !c->tuned) {
+        if ((st = autotune(c)) != GDFV_OK) return st;
+    }
+    if (read_ctl(c)) return GDFV_ERR_CUDA;
+    if (c->h_ctl->status != ST_OK) return fail(c, GDFV_ERR_STATE, "a previous run failed; reset the state");
+    const int start_step = c->h_ctl->step;
+    c->h_ctl->step_limit = start_step + nsteps;
+    c->h_ctl->max_time = 0.0;
+    c->h_ctl->halted = 0;
+    c->h_ctl->steps_done = 0;
+    if (write_ctl(c)) return GDFV_ERR_CUDA;
+    if (!c->graph) {
+        if ((st = build_graph(c)) != GDFV_OK) return st;
+    }
+    if (c->rec_cap < nsteps) {
+        if (c->d_rec) cudaFree(c->d_rec);
+        c->d_rec = nullptr;
+        c->rec_cap = 0;
+        CK(cudaMalloc(&c->d_rec, sizeof(double) * ((size_t)nsteps + 1)));
+        c->rec_cap = nsteps;
+    }
+    int* flag = reinterpret_cast<int*>(c->d_rec + nsteps);
+    CK(cudaMemsetAsync(flag, 0, sizeof(int), c->stream));
+    const long long n = (long long)c->nq * c->total;
+    const unsigned grid = (unsigned)std::min<long long>((n + 255) / 256, 8LL * 148);
+    // one step slot per step, each followed by its record: no host round trip in between
+    for (int m = 0; m < nsteps; ++m) {
+        CK(cudaGraphLaunch(c->graph1, c->stream));
+        record_step_kernel<<<grid, 256, 0, c->stream>>>(c->d_ctl, c->U[0], c->U[1], c->dU0, n, start_step + m + 1,
+                                                        states_dev[m], preds_dev[m], c->d_rec + m, flag);
+        CK(cudaGetLastError());
+    }
+    int h_flag = 0;
+    CK(cudaMemcpyAsync(&h_flag, flag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(dts, c->d_rec, sizeof(double) * nsteps, cudaMemcpyDeviceToHost, c->stream));
+    if (read_ctl(c)) return GDFV_ERR_CUDA;   // synchronises the stream
+    if (c->h_ctl->status == ST_TOO_MANY_BAD_CELLS)
+        return fail(c, GDFV_ERR_BAD_CELLS, "Too many bad cells during explicit gasdynamic update." +
+                                               bad_cell_text(c, c->h_ctl->first_bad_cell));
+    if (c->h_ctl->status == ST_DECODE_FAILED)
+        return fail(c, GDFV_ERR_STEP_FAILED, "Explicit update failed after max_attempts_for_step attempts." +
+                                                 bad_cell_text(c, c->h_ctl->first_bad_cell));
+    if (h_flag || c->h_ctl->step != start_step + nsteps)
+        return fail(c, GDFV_ERR_STATE, "gdfv_run_record: a step was retried, so the record is incomplete (the "
+                                       "state has moved on; take the steps with gdfv_run instead)");
     return GDFV_OK;
 }
 

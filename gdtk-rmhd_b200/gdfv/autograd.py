@@ -24,7 +24,7 @@ Tensors are float64 on the simulation's device, shaped [nq, total cells].
 """
 import torch
 
-from ._lib import check, ffi
+from ._lib import GDFV_ERR_STATE, GDFV_OK, check, ffi
 
 
 def _p(t):
@@ -142,24 +142,48 @@ class Rollout(torch.autograd.Function):
             s = st.copy()
             s[0], s[1], s[2] = p, T, vx
             sim.set_inflow(i, s)
-        sim.set_time(0.0, 0, sim.config.dt_init)
-        torch.cuda.current_stream().synchronize()
-        state = _state_view(sim)
-        state.copy_(U0)
-        torch.cuda.synchronize()
+        # what each step leaves: a checkpoint, or (last segment) its state and predictor state
+        states, preds = [None] * nsteps, [None] * nsteps
         for n in range(nsteps):
-            sim.run(max_step=1)
-            dts.append(sim.time()["dt"])
-            if n >= s_last:
-                m = n - s_last
-                U0n = ckpts[s_last] if m == 0 else outs0[m - 1]
-                check(sim.ctx, sim.L.gdfv_last_predictor_state(sim.ctx, _p(U0n), _p(preds0[m])))
-                if n < nsteps - 1:
-                    outs0[m].copy_(_state_view(sim))
-                    torch.cuda.synchronize()
             if (n + 1) % K == 0 and n + 1 < nsteps:
-                ckpts[n + 1] = _state_view(sim).clone()
-                torch.cuda.synchronize()
+                ckpts[n + 1] = torch.empty_like(U0)
+                states[n] = ckpts[n + 1]
+            if n >= s_last:
+                preds[n] = preds0[n - s_last]
+                if n < nsteps - 1:
+                    states[n] = outs0[n - s_last]
+        ptr = lambda t: ffi.NULL if t is None else _p(t)
+        pst = ffi.new("double*[]", [ptr(t) for t in states])
+        ppr = ffi.new("double*[]", [ptr(t) for t in preds])
+        hdt = ffi.new("double[]", nsteps)
+        recorded = False
+        for attempt in range(2):
+            sim.set_time(0.0, 0, sim.config.dt_init)
+            torch.cuda.current_stream().synchronize()
+            state = _state_view(sim)
+            state.copy_(U0)
+            torch.cuda.synchronize()
+            if attempt == 0:
+                # all steps and their records on the device, one host round trip
+                rc = sim.L.gdfv_run_record(sim.ctx, nsteps, pst, ppr, hdt)
+                if rc == GDFV_OK:
+                    dts = [hdt[n] for n in range(nsteps)]
+                    recorded = True
+                    break
+                if rc != GDFV_ERR_STATE:
+                    check(sim.ctx, rc)
+                # a step was retried: take the steps one by one below
+        if not recorded:
+            for n in range(nsteps):
+                sim.run(max_step=1)
+                dts.append(sim.time()["dt"])
+                if n >= s_last:
+                    m = n - s_last
+                    U0n = ckpts[s_last] if m == 0 else outs0[m - 1]
+                    check(sim.ctx, sim.L.gdfv_last_predictor_state(sim.ctx, _p(U0n), _p(preds0[m])))
+                if states[n] is not None:
+                    states[n].copy_(_state_view(sim))
+                    torch.cuda.synchronize()
         UN = _state_view(sim).clone()
         torch.cuda.synchronize()
         ctx.sim, ctx.dts, ctx.ckpts, ctx.k, ctx.work = sim, dts, ckpts, K, work

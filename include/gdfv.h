@@ -248,6 +248,15 @@ int gdfv_rollout_adjoint(int ctx, const double* const* ckpt_dev, int n_ckpt, con
                          int checkpoint_every, double* const* work_dev, int last_ready, double* lam_dev,
                          double* g_inflow_dev);
 
+/* nsteps steps as gdfv_run takes them (the dt rule on the device), each recorded on the
+ * device as it completes, with no host round trip between steps: states_dev[n] (NULL:
+ * not kept) receives the state after step n, preds_dev[n] (NULL: not kept) its
+ * predictor state U1 = U0 + dt*dU0 (as gdfv_last_predictor_state forms it), and dts[n]
+ * (host) its dt; device arrays [nq][total].  What a differentiable rollout keeps of its
+ * trajectory.  A step that needed a retry leaves the record incomplete: GDFV_ERR_STATE,
+ * with the state moved on.  No reference counterpart. */
+int gdfv_run_record(int ctx, int nsteps, double* const* states_dev, double* const* preds_dev, double* dts);
+
 /* Predictor state U1 = U0 + dt*dU0 of the step gdfv_run took last, from the state U0
  * before it (device arrays): what a forward pass keeps to differentiate its last
  * steps without recomputing them.  Valid directly after the step.  No reference

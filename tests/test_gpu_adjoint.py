@@ -328,6 +328,47 @@ def test_pipelined_rollout_adjoint_matches_sequential():
         assert torch.allclose(gin, gin2, rtol=1e-12, atol=0.0), last_ready
 
 
+def test_run_record_is_the_stepwise_trajectory():
+    """gdfv_run_record (steps and their records on the device, one host round trip) keeps
+    the states, predictor states and dts that gdfv_run taken one step at a time with
+    gdfv_last_predictor_state gives, bit for bit; NULL entries keep nothing."""
+    from gdfv._lib import check, ffi
+    from gdfv.autograd import _p, _state_view
+    case = cases.c2_inflow_box(n=(40, 24, 20), noise_all=True)
+    _, sim = cases.build_pair(case)
+    U0 = torch.from_numpy(sim.get_conserved(0)).cuda()
+    nsteps = 7
+    states = [torch.full_like(U0, -1.0) for _ in range(nsteps)]
+    preds = [torch.full_like(U0, -1.0) for _ in range(nsteps)]
+    keep = [n != 3 for n in range(nsteps)]   # step 3's state is not asked for
+    sim.set_time(0.0, 0, sim.config.dt_init)
+    _state_view(sim).copy_(U0)
+    torch.cuda.synchronize()
+    dts = ffi.new("double[]", nsteps)
+    check(sim.ctx, sim.L.gdfv_run_record(sim.ctx, nsteps, ffi.new("double*[]", [_p(t) if k else ffi.NULL
+                                                                                  for t, k in zip(states, keep)]),
+                                         ffi.new("double*[]", [_p(t) for t in preds]), dts))
+    UN = _state_view(sim).clone()
+    sim.set_time(0.0, 0, sim.config.dt_init)
+    _state_view(sim).copy_(U0)
+    torch.cuda.synchronize()
+    prev = U0.clone()
+    for n in range(nsteps):
+        assert sim.run(max_step=1) == 1
+        assert sim.time()["dt"] == dts[n]
+        pred = torch.empty_like(U0)
+        check(sim.ctx, sim.L.gdfv_last_predictor_state(sim.ctx, _p(prev), _p(pred)))
+        cur = _state_view(sim).clone()
+        torch.cuda.synchronize()
+        assert torch.equal(pred, preds[n]), n
+        if keep[n]:
+            assert torch.equal(cur, states[n]), n
+        else:
+            assert bool((states[n] == -1.0).all())
+        prev = cur
+    assert torch.equal(prev, UN)
+
+
 def test_resident_trajectory_rollout_matches_checkpointed():
     """rollout's default keeps the whole trajectory on the device when it fits (one
     segment, nothing recomputed); its gradients equal those of the checkpointed form (a
