@@ -405,10 +405,11 @@ def main():
                     help="steps after which the FP32 form is compared with FP64 (0: at the timed steps)")
     ap.add_argument("--no-extra", action="store_true", help="skip the multi-block, MHD and adjoint legs")
     ap.add_argument("--profile-case", nargs="?", const="stage", default=None,
-                    choices=["stage", "corrector", "mhd", "adjoint", "norms"],
+                    choices=["stage", "corrector", "narrow", "mhd", "adjoint", "norms"],
                     help="small case for ncu captures, then exit: stage = the 128^3 inflow box "
-                         "(FP32 then FP64 form, warmup steps); corrector = the inflow box at 128x112x128, "
-                         "FP32 form, whose rows take the 7-row corrector tiles the 256^3 run uses; mhd = "
+                         "(FP32 then FP64 form, warmup steps); corrector = the inflow box at 256x128x128, "
+                         "FP32 form, with the 256^3 run's tile k-chunk; narrow = the inflow box at "
+                         "240x128x128, FP32 form in 16-wide tiles (the tuner's choice at 240^3); mhd = "
                          "Orszag-Tang 512x512x4 (both forms, warmup steps); adjoint = 128x128x64 FP64 "
                          "rollout of 10 steps and its backward; norms = the 256^3 box, FP32 form, warmup "
                          "steps then the residual norms twice")
@@ -450,6 +451,15 @@ def main():
         # same tile shape and grid fill per wave, 0.8 GB on the device
         case = cases.c2_inflow_box(n=(256, 128, 128), flux=args.flux, precision="fp32", seed=4321)
         sim = cases.build_gpu(case, tile_kchunk=12)
+        sim.set_stream(stream.cuda_stream)
+        sim.run(max_step=max(3, args.warmup))
+        torch.cuda.synchronize()
+        return 0
+    if args.profile_case == "narrow":
+        # the float Euler path in tiles 16 cells wide (two rows per warp) at 240 x 128 x 128,
+        # k-chunk 32 and the persistent form: what the autotuner picks at 240^3; 0.8 GB
+        case = cases.c2_inflow_box(n=(240, 128, 128), flux=args.flux, precision="fp32", seed=4321)
+        sim = cases.build_gpu(case, tile_kchunk=32, persistent=True, tile_width=16)
         sim.set_stream(stream.cuda_stream)
         sim.run(max_step=max(3, args.warmup))
         torch.cuda.synchronize()

@@ -396,6 +396,49 @@ __device__ void hllc_vjp(const NumParams& P, const FS& L, const FS& R, const dou
     gR = FS{gr_R, gp_R, gu_R, gv_R, gw_R, ge_R, ga_R};
 }
 
+// Reverse of the simple outflow flux of cell state q (rho, v0, v1, v2, u, a) through a
+// face of normal +axis D (simple_outflow_flux, boundary_flux_effect.d:504-645): F = the
+// cell's convective flux plus p n when the mass flux leaves (outsign m > 0), else p n
+// alone; g the cotangent of the global-frame flux, added into gq.
+template <int D>
+__device__ void simple_flux_vjp(const NumParams& P, const double* q, int outsign, const double* g, double* gq) {
+    const double rho = q[0], u = q[4];
+    const double v[3] = {q[1], q[2], q[3]};
+    const double T = u * P.gas.Cvinv;
+    const double p = rho * P.gas.R * T;
+    const double vn = v[D];
+    const double m = rho * vn;
+    double gp = 0.0, gm = 0.0, gvn = 0.0, gu = 0.0;
+    double gv[3] = {0.0, 0.0, 0.0};
+    if (outsign * m > 0.0) {
+        gm += g[MASS];
+        for (int d = 0; d < 3; ++d) {
+            if (d == 2 && P.dims != 3) continue;   // no z momentum flux in 2D
+            const double gd = g[XMOM + d];
+            if (d == D) gp += gd;
+            gv[d] += gd * m;
+            gm += gd * v[d];
+        }
+        const double utot = u + 0.5 * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        gm += g[TOTENERGY] * utot;
+        gu += g[TOTENERGY] * m;
+        for (int d = 0; d < 3; ++d) gv[d] += g[TOTENERGY] * m * v[d];
+        gp += g[TOTENERGY] * vn;
+        gvn += g[TOTENERGY] * p;
+    } else {
+        gp += g[XMOM + D];
+    }
+    gq[0] += gm * vn;                     // m = rho vn
+    gvn += gm * rho;
+    gv[D] += gvn;
+    gq[0] += gp * P.gas.R * T;            // p = rho R (u Cvinv)
+    gu += gp * rho * P.gas.R * P.gas.Cvinv;
+    gq[1] += gv[0];
+    gq[2] += gv[1];
+    gq[3] += gv[2];
+    gq[4] += gu;
+}
+
 struct AdjArgs {
     const BlockDesc* blocks;
     const InflowState* inflow;
@@ -439,17 +482,18 @@ struct Src {
     int kind, axis, inflow;
 };
 
-// ROT: some exchange rotates its ghosts' vectors (the face kernels without it carry
-// none of that code)
-template <bool ROT>
+// RARE: some exchange rotates its ghosts' vectors, or some face is an outflow boundary
+// with a ghost or flux rule of its own (the face kernels without it carry none of that
+// code)
+template <bool RARE>
 __device__ Src adj_resolve(const AdjArgs& a, const BlockDesc& B, int i, int j, int k) {
     StageArgs A{};
     A.blocks = a.blocks;
-    CellSrc s = resolve<false, ROT>(A, B, i, j, k);   // no outflow boundaries with their own rule here
+    CellSrc s = resolve<RARE, RARE>(A, B, i, j, k);
     return Src{s.blk, s.c0, s.c1, s.kind, s.axis, s.inflow};
 }
 
-template <bool ROT>
+template <bool RARE>
 __device__ void adj_load(const AdjArgs& a, const Src& s, double* c) {
     if (s.kind == SRC_INFLOW) {
         const InflowState& in = a.inflow[s.inflow];
@@ -473,13 +517,22 @@ __device__ void adj_load(const AdjArgs& a, const Src& s, double* c) {
     }
     for (int m = 0; m < NP; ++m) c[m] = e[m];
     if (s.kind == SRC_MIRROR) c[1 + s.axis] = -c[1 + s.axis];
-    if (ROT && s.kind == SRC_ROTATE) {   // ghost velocity R v (flowstate.d:393-400)
+    if (RARE && s.kind == SRC_ROTATE) {   // ghost velocity R v (flowstate.d:393-400)
         const double* R = a.rot + 9 * s.inflow;
         for (int r = 0; r < 3; ++r) c[1 + r] = R[3 * r] * e[1] + R[3 * r + 1] * e[2] + R[3 * r + 2] * e[3];
     }
+    if (RARE && s.kind == SRC_FIXEDP) {   // fixed_p.d:98-119: rho, u from p_outside at the cell's T
+        const double T = e[4] * a.P.gas.Cvinv;
+        c[0] = a.inflow[s.inflow].p / (T * a.P.gas.R);
+        c[4] = a.P.gas.Cv * T;
+    }
+    if (RARE && s.kind == SRC_FIXEDPT) {  // fixed_pt.d:105-128: rho, u from p_outside, T_outside
+        c[0] = a.inflow[s.inflow].rho;
+        c[4] = a.inflow[s.inflow].u;
+    }
 }
 
-template <bool ROT>
+template <bool RARE>
 __device__ void adj_scatter(const AdjArgs& a, const Src& s, const double* gc) {
     if (s.kind == SRC_INFLOW) {
         for (int m = 0; m < NP; ++m) atomicAdd(&a.gInflow[s.inflow * NP + m], gc[m]);
@@ -496,7 +549,24 @@ __device__ void adj_scatter(const AdjArgs& a, const Src& s, const double* gc) {
         atomicAdd(&a.gP[5 * a.total + g0], gc[5]);
         return;
     }
-    if (ROT && s.kind == SRC_ROTATE) {   // the transpose of the ghost's rotation R v
+    if (RARE && (s.kind == SRC_FIXEDP || s.kind == SRC_FIXEDPT)) {
+        // velocity and sound speed pass through; rho and u are the outside state's
+        // (FixedPT) or, FixedP, rho = p/(T R) and u = Cv T with T = u_cell / Cv
+        double gu = 0.0;
+        if (s.kind == SRC_FIXEDP) {
+            const double u = a.Pp[4 * a.total + g0];
+            const double T = u * a.P.gas.Cvinv;
+            const double rho = a.inflow[s.inflow].p / (T * a.P.gas.R);
+            gu = gc[0] * (-rho / T) * a.P.gas.Cvinv + gc[4] * a.P.gas.Cv * a.P.gas.Cvinv;
+        }
+        atomicAdd(&a.gP[1 * a.total + g0], gc[1]);
+        atomicAdd(&a.gP[2 * a.total + g0], gc[2]);
+        atomicAdd(&a.gP[3 * a.total + g0], gc[3]);
+        if (gu != 0.0) atomicAdd(&a.gP[4 * a.total + g0], gu);
+        atomicAdd(&a.gP[5 * a.total + g0], gc[5]);
+        return;
+    }
+    if (RARE && s.kind == SRC_ROTATE) {   // the transpose of the ghost's rotation R v
         const double* R = a.rot + 9 * s.inflow;
         for (int m = 0; m < NP; ++m) {
             const double v = (m >= 1 && m <= 3)
@@ -534,7 +604,7 @@ __device__ __forceinline__ int face_coords(const AdjArgs& a, long long f, int& i
 // Source of stencil cell m (index -2, -1, 0, +1 along D from the face).  A face
 // whose four stencil cells lie inside its block (the other two indices always do)
 // takes them directly; the boundary rules apply to the others.
-template <int D, bool ROT>
+template <int D, bool RARE>
 __device__ __forceinline__ Src stencil_src(const AdjArgs& a, const BlockDesc& B, int i, int j, int k, int m) {
     const int idxD = D == 0 ? i : (D == 1 ? j : k);
     if (idxD >= 2 && idxD + 1 < B.n[D]) {
@@ -542,7 +612,7 @@ __device__ __forceinline__ Src stencil_src(const AdjArgs& a, const BlockDesc& B,
         const int c = i + B.n[0] * (j + B.n[1] * k) + (m - 2) * sD;
         return Src{&B, (long long)c, -1, SRC_CELL, D, 0};
     }
-    return adj_resolve<ROT>(a, B, i - (D == 0 ? 2 - m : 0), j - (D == 1 ? 2 - m : 0), k - (D == 2 ? 2 - m : 0));
+    return adj_resolve<RARE>(a, B, i - (D == 0 ? 2 - m : 0), j - (D == 1 ? 2 - m : 0), k - (D == 2 ? 2 - m : 0));
 }
 
 // The reverse sweep of face f of direction D: cotangents gc[m] of the stencil
@@ -550,17 +620,17 @@ __device__ __forceinline__ Src stencil_src(const AdjArgs& a, const BlockDesc& B,
 // stencil reaches (if any).  Only these small records stay live: the sources
 // themselves are resolved again when the cotangents are scattered.
 // rowid identifies the line of faces (block and the two other indices).
-template <int D, int FLUX, bool ROT>
+template <int D, int FLUX, bool RARE>
 __device__ __forceinline__ void face_vjp(const AdjArgs& a, int b, int i, int j, int k, int* kind, int& inflow,
                                          double (*gc)[NP], long long& rowid) {
     const BlockDesc& B = a.blocks[b];
     rowid = (long long)b * 0x100000000ll + (D == 0 ? (long long)j + (long long)B.n[1] * k : (long long)i);
     double c[4][NP];
     for (int m = 0; m < 4; ++m) {
-        const Src sm = stencil_src<D, ROT>(a, B, i, j, k, m);
+        const Src sm = stencil_src<D, RARE>(a, B, i, j, k, m);
         kind[m] = sm.kind;
         if (sm.kind == SRC_INFLOW) inflow = sm.inflow;
-        adj_load<ROT>(a, sm, c[m]);
+        adj_load<RARE>(a, sm, c[m]);
     }
     // cotangent of the face flux: F enters R_right with +A/V and R_left with -A/V
     const double AV = B.area[D] * B.vol_inv * a.w_scale;
@@ -574,6 +644,16 @@ __device__ __forceinline__ void face_vjp(const AdjArgs& a, int b, int i, int j, 
         double wr = rightIn ? a.W[q * a.total + gr] : 0.0;
         double wl = leftIn ? a.W[q * a.total + gl] : 0.0;
         gFg[q] = AV * (wr - wl);
+    }
+    if constexpr (RARE) {
+        // OutFlowBC_SimpleFlux (boundary_flux_effect.d:504-645): the boundary face's flux is
+        // the interior cell's outflow flux, or only its pressure on a closed face
+        const int bface = idxD == 0 ? 2 * D : (idxD == nD ? 2 * D + 1 : -1);
+        if (bface >= 0 && B.bc_type[bface] == BC_SIMPLE_FLUX) {
+            const int in = (bface & 1) ? 1 : 2;   // the interior cell: left of a plus face
+            simple_flux_vjp<D>(a.P, c[in], (bface & 1) ? 1 : -1, gFg, gc[in]);
+            return;
+        }
     }
     constexpr int ax0 = D, ax1 = (D + 1) % 3, ax2 = (D + 2) % 3;
     double gF[5] = {gFg[MASS], gFg[XMOM + ax0], gFg[XMOM + ax1], gFg[XMOM + ax2], gFg[TOTENERGY]};
@@ -636,7 +716,7 @@ __device__ __forceinline__ void face_vjp(const AdjArgs& a, int b, int i, int j, 
 #ifndef GDFV_ADJ_MINB
 #define GDFV_ADJ_MINB 3
 #endif
-template <int D, int FLUX, bool ROT>
+template <int D, int FLUX, bool RARE>
 __device__ __forceinline__ void face_thread(const AdjArgs& a, long long f) {
     const long long* off = a.face_off + D * (a.nblocks + 1);
     const bool act = f < off[a.nblocks];
@@ -649,7 +729,7 @@ __device__ __forceinline__ void face_thread(const AdjArgs& a, long long f) {
     int b = 0, i = 0, j = 0, k = 0;
     if (act) {
         b = face_coords<D>(a, f, i, j, k);
-        face_vjp<D, FLUX, ROT>(a, b, i, j, k, kind, inflow, gc, rowid);
+        face_vjp<D, FLUX, RARE>(a, b, i, j, k, kind, inflow, gc, rowid);
     }
     if (D == 0) {
         const unsigned full = 0xffffffffu;
@@ -713,18 +793,18 @@ __device__ __forceinline__ void face_thread(const AdjArgs& a, long long f) {
     if (!act) return;
     const BlockDesc& B = a.blocks[b];
     for (int m = 0; m < 4; ++m)
-        if (kind[m] >= 0) adj_scatter<ROT>(a, stencil_src<D, ROT>(a, B, i, j, k, m), gc[m]);
+        if (kind[m] >= 0) adj_scatter<RARE>(a, stencil_src<D, RARE>(a, B, i, j, k, m), gc[m]);
 }
 
 // All faces of the three directions in one launch: CTAs [0, nb0) take the i faces,
 // [nb0, nb0 + nb1) the j faces, the rest the k faces (128 faces per CTA).
 constexpr int FACE_CTA = 128;
-template <int FLUX, bool ROT>
+template <int FLUX, bool RARE>
 __global__ void __launch_bounds__(FACE_CTA, GDFV_ADJ_MINB) adj_faces_kernel(AdjArgs a, unsigned nb0, unsigned nb1) {
     const unsigned bid = blockIdx.x;
-    if (bid < nb0) face_thread<0, FLUX, ROT>(a, (long long)bid * FACE_CTA + threadIdx.x);
-    else if (bid < nb0 + nb1) face_thread<1, FLUX, ROT>(a, (long long)(bid - nb0) * FACE_CTA + threadIdx.x);
-    else face_thread<2, FLUX, ROT>(a, (long long)(bid - nb0 - nb1) * FACE_CTA + threadIdx.x);
+    if (bid < nb0) face_thread<0, FLUX, RARE>(a, (long long)bid * FACE_CTA + threadIdx.x);
+    else if (bid < nb0 + nb1) face_thread<1, FLUX, RARE>(a, (long long)(bid - nb0) * FACE_CTA + threadIdx.x);
+    else face_thread<2, FLUX, RARE>(a, (long long)(bid - nb0 - nb1) * FACE_CTA + threadIdx.x);
 }
 
 // gU = (dP/dU)^T gP for P = decode(U) (e4/fvcell.d:586-822 with ideal_gas.d:98-139)
@@ -781,18 +861,20 @@ using namespace gdfv;
 
 namespace {
 
-// The face kernel of the context's flux calculator (and rotating exchanges, if any) over
-// nb[d] CTAs of each direction.
+// The face kernel of the context's flux calculator (with the rare boundary rules when
+// some exchange rotates or some face is an outflow boundary of its own) over nb[d] CTAs
+// of each direction.
 template <int FLUX>
-void launch_faces_flux(const AdjArgs& a, bool rot, const unsigned* nb, cudaStream_t s) {
+void launch_faces_flux(const AdjArgs& a, bool rare, const unsigned* nb, cudaStream_t s) {
     const unsigned n = nb[0] + nb[1] + nb[2];
-    if (rot) adj_faces_kernel<FLUX, true><<<n, FACE_CTA, 0, s>>>(a, nb[0], nb[1]);
+    if (rare) adj_faces_kernel<FLUX, true><<<n, FACE_CTA, 0, s>>>(a, nb[0], nb[1]);
     else adj_faces_kernel<FLUX, false><<<n, FACE_CTA, 0, s>>>(a, nb[0], nb[1]);
 }
 
 void launch_faces(const AdjArgs& a, int flux, const unsigned* nb, cudaStream_t s) {
-    if (flux == FLUX_HLLC) launch_faces_flux<FLUX_HLLC>(a, a.P.rotating, nb, s);
-    else launch_faces_flux<FLUX_AUSMDV>(a, a.P.rotating, nb, s);
+    const bool rare = a.P.rotating || a.P.outflow_bcs;
+    if (flux == FLUX_HLLC) launch_faces_flux<FLUX_HLLC>(a, rare, nb, s);
+    else launch_faces_flux<FLUX_AUSMDV>(a, rare, nb, s);
 }
 
 bool vjp_supported(int ctx, const AdjView& v) {
@@ -806,13 +888,6 @@ bool vjp_supported(int ctx, const AdjView& v) {
         adjoint_set_error(ctx, "the adjoint supports uniform Cartesian blocks (no graded blocks)");
         return false;
     }
-    for (const BlockDesc& B : v.h_blocks)
-        for (int f = 0; f < 6; ++f)
-            if (B.bc_type[f] == BC_FIXED_P || B.bc_type[f] == BC_FIXED_PT || B.bc_type[f] == BC_SIMPLE_FLUX) {
-                adjoint_set_error(ctx, "the adjoint supports slip-wall, extrapolate, supersonic-inflow and "
-                                       "exchange boundaries");
-                return false;
-            }
     return true;
 }
 

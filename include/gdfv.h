@@ -119,7 +119,7 @@ int gdfv_block_set_bc(int ctx, int blk, int face, const char* bc_type, int x_ord
  * Rmatrix: NULL, or 9 doubles (row major) applied to the ghost's velocity and magnetic
  * field (flowstate.d:393-400 reorient_vector_quantities, full_face_copy.d:2403-2405).
  * The faces' cell counts must match under the map and the partner must be at least 2
- * cells deep; checked at gdfv_prepare.  The adjoint rejects a context with an Rmatrix. */
+ * cells deep; checked at gdfv_prepare.  The adjoint follows both the map and the rotation. */
 int gdfv_block_set_exchange(int ctx, int blk, int face, int other_blk, int other_face, int orientation,
                             const double* Rmatrix);
 
@@ -201,8 +201,9 @@ int gdfv_residual_jvp(int ctx, const double* U_dev, const double* v_dev, const d
  * the primal values).  g_inflow_host (may be NULL) receives, per supersonic-inflow face
  * state in the order the faces were defined, the cotangent of its ghost state
  * (rho, vel.x, vel.y, vel.z, u, a), 6 doubles each.  Euler (2D or 3D) with
- * flux_calculator=ausmdv or hllc; exchanges of any orientation, with or without an
- * Rmatrix (the cotangent goes back through its transpose).  It is the transpose of the Jacobian-vector products of
+ * flux_calculator=ausmdv or hllc; every boundary condition of this library, exchanges
+ * of any orientation with or without an Rmatrix (the cotangent goes back through its
+ * transpose) and the outflow boundaries with their own ghost or flux rule included.  It is the transpose of the Jacobian-vector products of
  * e4/steadystate_core.d:1870-2060 (evalJacobianVecProd), which it is checked against. */
 int gdfv_residual_vjp(int ctx, const double* U_dev, const double* W_dev, double* G_dev, double* g_inflow_host);
 

@@ -86,6 +86,16 @@ def test_vjp_transpose_2d(flux):
     _dot_check(case, 6, 1e-10, seed=10)
 
 
+@pytest.mark.parametrize("bc", ["simple_flux", "fixed_p", "fixed_pt"])
+def test_vjp_transpose_outflow_boundaries(bc):
+    """OutFlowBC_SimpleFlux (the boundary face's flux from the interior cell alone, on
+    faces the flow leaves and on closed ones), OutFlowBC_FixedP and OutFlowBC_FixedPT
+    (ghost rho and u from the outside p, or p and T) on the subsonic shock box, whose flow
+    runs both ways through its x faces."""
+    from test_gpu_parity import OUTFLOW_BCS, _with_bcs
+    _dot_check(_with_bcs(cases.c1_shock_box(n=16), OUTFLOW_BCS[bc]), 8, 1e-10, seed=11)
+
+
 def test_vjp_transpose_oriented_and_rotating_exchanges():
     """Exchange ghosts placed by orientation 3 (the cotangent goes to the partner cell
     the map names), and ghosts whose velocity the exchange turns by +-90 degrees
