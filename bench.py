@@ -195,8 +195,10 @@ def adjoint_over_forward(nsteps=50, shape=(128, 128, 64), autotune=True, forms=(
     allocator holds the trajectory buffers).  Two backward forms: the trajectory resident
     in device memory (rollout's default when it fits: 100 states, 4.2 GB here), which
     recomputes nothing, and a checkpoint every 10 steps with each segment recomputed.
-    Also the time of the rollout's own forward, which keeps the trajectory (one gdfv_run
-    call and host round trip per step)."""
+    Also the time of the rollout's own forward, which keeps the trajectory (gdfv_run_record:
+    the steps and their records on the device, one host round trip), between events around
+    the call: the minimum and the maximum of two warm passes (host work between the events,
+    such as Python allocating the trajectory's tensors, adds to it and varies)."""
     import torch
     import cases
     from gdfv.autograd import rollout
@@ -221,7 +223,8 @@ def adjoint_over_forward(nsteps=50, shape=(128, 128, 64), autotune=True, forms=(
                forward_schedule="autotuned" if autotune else "default tiles")
     for label, K in forms:
         theta = torch.tensor([inf["p"], inf["T"], inf["vel"][0]], dtype=torch.float64, requires_grad=True)
-        for rep in range(2):   # the first pass warms the adjoint (scratch allocation, face tables)
+        fwd_reps = []
+        for rep in range(3):   # the first pass warms the adjoint (scratch allocation, face tables)
             theta.grad = None
             U0r = U0.clone().requires_grad_(True)
             f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -238,9 +241,13 @@ def adjoint_over_forward(nsteps=50, shape=(128, 128, 64), autotune=True, forms=(
             J.backward()
             b1.record()
             torch.cuda.synchronize()
+            if rep:
+                fwd_reps.append(f0.elapsed_time(f1))
         adj_ms = b0.elapsed_time(b1)
         out[label] = dict(ratio=adj_ms / fwd_ms, adjoint_ms=adj_ms, checkpoint_every=K or nsteps,
-                          rollout_forward_ms=f0.elapsed_time(f1), dJ_dp_inflow=float(theta.grad[0]),
+                          rollout_forward_ms=min(fwd_reps), rollout_forward_ms_max=max(fwd_reps),
+                          forward_recorded_on_device=bool(getattr(sim, "rollout_recorded", False)),
+                          dJ_dp_inflow=float(theta.grad[0]),
                           grad_U0_norm=float(U0r.grad.norm()))
     first = out[forms[0][0]]
     out.update(ratio=first["ratio"], adjoint_ms=first["adjoint_ms"], checkpoint_every=first["checkpoint_every"])
@@ -307,6 +314,7 @@ def multiblock_leg(stream, steps=20, seed=2024):
     out = dict(workload=f"64-block lattice (4x4x4, sizes by seed {seed} from 16..128), FP32 flux",
                cells=cells, steps=steps, value=cells * steps / (ms * 1e-3) / 1e6, unit=UNIT,
                tile_kchunk=sim.option("tile_kchunk"), persistent=bool(sim.option("persistent")),
+               tile_width=sim.option("tile_width"),
                autotune_stage_ms=sim.option("autotune_stage_ms"))
     sim.close()
     return out
@@ -583,7 +591,8 @@ def main():
         "clocks_fp64": results["fp64"]["clocks"],
     }
     line["config"].update(autotune=bool(args.autotune), tile_kchunk=sim32.option("tile_kchunk"),
-                          persistent=bool(sim32.option("persistent")), tile_rows=sim32.option("tile_rows"),
+                          persistent=bool(sim32.option("persistent")), tile_width=sim32.option("tile_width"),
+                          tile_rows=sim32.option("tile_rows"),
                           tile_rows_corrector=sim32.option("tile_rows_corrector"))
     line["accuracy"] = acc
     if not args.no_extra:

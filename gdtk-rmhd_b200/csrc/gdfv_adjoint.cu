@@ -66,15 +66,27 @@ __device__ __forceinline__ void clip_rev(double q, double A, double B, double g,
 // l2r2 for one scalar with equal lengths (e4/onedinterp.d:357-386), forward and reverse.
 struct L2R2Rec {
     double dLm, del, dRp, sL, sR, nL, dL, nR, dR, X, Y, qLr, qRr;
+    int eps_from;   // van_albada_variant lmr: epsilon from |q0| (1), |r0| (2) or the floor (0)
 };
 
+// LMR: the context may take van_albada_variant lmr (a face kernel with the rare rules)
+template <bool LMR>
 __device__ __forceinline__ void l2r2_fwd(const double* w, const NumParams& P, double q1, double q0, double r0,
                                          double r1, double& qL, double& qR, L2R2Rec& t) {
     t.dLm = (q0 - q1) * w[W_TOL];
     t.del = (r0 - q0) * w[W_TOC];
     t.dRp = (r1 - r0) * w[W_TOR];
     t.sL = 1.0; t.sR = 1.0;
-    const double eps = P.eps_van_albada;
+    double eps = P.eps_van_albada;
+    t.eps_from = 0;
+    if (LMR && P.lmr_epsilon) {
+        // lmr/onedinterp.d:147-151: the face's epsilon scaled by the larger of its two
+        // states (both limiter values of the face take it), as the forward kernels form it
+        const double tiny = 1e-12, a0 = fabs(q0), a1 = fabs(r0);
+        const double m = fmax(fmax(tiny, a0), fmax(tiny, a1));
+        t.eps_from = m == tiny ? 0 : (a0 >= a1 ? 1 : 2);
+        eps = m * eps * w[W_TOC];
+    }
     if (P.apply_limiter) {
         double pl = t.dLm * t.del, pr = t.del * t.dRp;
         t.nL = pl + fabs(pl) + eps; t.dL = t.dLm * t.dLm + t.del * t.del + eps; t.sL = t.nL * rcp(t.dL);
@@ -91,6 +103,7 @@ __device__ __forceinline__ void l2r2_fwd(const double* w, const NumParams& P, do
     }
 }
 
+template <bool LMR>
 __device__ __forceinline__ void l2r2_rev(const double* w, const NumParams& P, double q1, double q0, double r0,
                                          double r1, const L2R2Rec& t, double gqL, double gqR, double& g1,
                                          double& g0, double& h0, double& h1) {
@@ -128,10 +141,89 @@ __device__ __forceinline__ void l2r2_rev(const double* w, const NumParams& P, do
         double gpr = gnR * (1.0 + sgn(pr));
         gdel += gpr * t.dRp + gdR * 2.0 * t.del;
         gdRp += gpr * t.del + gdR * 2.0 * t.dRp;
+        if (LMR && t.eps_from) {   // lmr: epsilon enters nL, dL, nR and dR
+            const double geps = gnL + gdL + gnR + gdR;
+            const double d = geps * P.eps_van_albada * w[W_TOC];
+            if (t.eps_from == 1) g0 += d * sgn(q0);
+            else h0 += d * sgn(r0);
+        }
     }
     g0 += gdLm * w[W_TOL]; g1 -= gdLm * w[W_TOL];
     h0 += gdel * w[W_TOC]; g0 -= gdel * w[W_TOC];
     h1 += gdRp * w[W_TOR]; h0 -= gdRp * w[W_TOR];
+}
+
+// l2r2 on a graded block (recon_cell_graded's arithmetic): the left state of the face is
+// cell L's plus-face value with L's weights gL[GW_*], the right state cell R's minus-face
+// value with R's weights gR (e4/onedinterp.d:338-386 with each cell's own lengths); the
+// difference across the face is scaled by L's and by R's weight separately.
+struct L2R2G {
+    double dLm, delL, delR, dRp, sL, sR, dL, dR, X, Y, qLr, qRr;
+};
+
+__device__ __forceinline__ void l2r2g_fwd(const double* gL, const double* gR, const NumParams& P, double q1,
+                                          double q0, double r0, double r1, double& qL, double& qR, L2R2G& t) {
+    t.dLm = (q0 - q1) * gL[GW_TOL];
+    t.delL = (r0 - q0) * gL[GW_TOC];
+    t.delR = (r0 - q0) * gR[GW_TOL];
+    t.dRp = (r1 - r0) * gR[GW_TOC];
+    t.sL = 1.0; t.sR = 1.0;
+    const double eps = P.eps_van_albada;
+    if (P.apply_limiter) {
+        const double pl = t.dLm * t.delL, pr = t.delR * t.dRp;
+        t.dL = t.dLm * t.dLm + t.delL * t.delL + eps; t.sL = (pl + fabs(pl) + eps) * rcp(t.dL);
+        t.dR = t.delR * t.delR + t.dRp * t.dRp + eps; t.sR = (pr + fabs(pr) + eps) * rcp(t.dR);
+    }
+    t.X = t.delL * gL[GW_TWOL] + t.dLm * gL[GW_LENR0];
+    t.Y = t.dRp * gR[GW_LENL0] + t.delR * gR[GW_TWOR];
+    t.qLr = q0 + t.sL * gL[GW_A] * t.X;
+    t.qRr = r0 - t.sR * gR[GW_A] * t.Y;
+    qL = t.qLr; qR = t.qRr;
+    if (P.extrema_clipping) {
+        qL = clip_to_limits(qL, q0, r0);
+        qR = clip_to_limits(qR, q0, r0);
+    }
+}
+
+__device__ __forceinline__ void l2r2g_rev(const double* gL, const double* gR, const NumParams& P, double q0, double r0,
+                                          const L2R2G& t, double gqL, double gqR, double& g1, double& g0, double& h0,
+                                          double& h1) {
+    double gqLr = 0.0, gqRr = 0.0;
+    if (P.extrema_clipping) {
+        clip_rev(t.qLr, q0, r0, gqL, gqLr, g0, h0);
+        clip_rev(t.qRr, q0, r0, gqR, gqRr, g0, h0);
+    } else {
+        gqLr = gqL; gqRr = gqR;
+    }
+    double gdLm = 0.0, gdelL = 0.0, gdelR = 0.0, gdRp = 0.0;
+    g0 += gqLr;
+    const double gsL = gqLr * gL[GW_A] * t.X;
+    const double gX = gqLr * t.sL * gL[GW_A];
+    gdelL += gX * gL[GW_TWOL];
+    gdLm += gX * gL[GW_LENR0];
+    h0 += gqRr;
+    const double gsR = -gqRr * gR[GW_A] * t.Y;
+    const double gY = -gqRr * t.sR * gR[GW_A];
+    gdRp += gY * gR[GW_LENL0];
+    gdelR += gY * gR[GW_TWOR];
+    if (P.apply_limiter) {
+        // s = (p + |p| + eps) / d with p the product of the two differences, d their squares + eps
+        const double idL = rcp(t.dL), idR = rcp(t.dR);
+        const double gnL = gsL * idL, gdL = -gsL * t.sL * idL;
+        const double pl = t.dLm * t.delL;
+        const double gpl = gnL * (1.0 + sgn(pl));
+        gdLm += gpl * t.delL + gdL * 2.0 * t.dLm;
+        gdelL += gpl * t.dLm + gdL * 2.0 * t.delL;
+        const double gnR = gsR * idR, gdR = -gsR * t.sR * idR;
+        const double pr = t.delR * t.dRp;
+        const double gpr = gnR * (1.0 + sgn(pr));
+        gdelR += gpr * t.dRp + gdR * 2.0 * t.delR;
+        gdRp += gpr * t.delR + gdR * 2.0 * t.dRp;
+    }
+    g0 += gdLm * gL[GW_TOL]; g1 -= gdLm * gL[GW_TOL];
+    h0 += gdelL * gL[GW_TOC]; g0 -= gdelL * gL[GW_TOC];
+    h0 += gdelR * gR[GW_TOL]; g0 -= gdelR * gR[GW_TOL];
+    h1 += gdRp * gR[GW_TOC]; h0 -= gdRp * gR[GW_TOC];
 }
 
 // ausmdv (e4/fluxcalc.d:477-651) forward with the quantities the reverse needs,
@@ -482,9 +574,9 @@ struct Src {
     int kind, axis, inflow;
 };
 
-// RARE: some exchange rotates its ghosts' vectors, or some face is an outflow boundary
-// with a ghost or flux rule of its own (the face kernels without it carry none of that
-// code)
+// RARE: some exchange rotates its ghosts' vectors, some face is an outflow boundary
+// with a ghost or flux rule of its own, the limiter is lmr's, or some block is graded
+// (the face kernels without it carry none of that code)
 template <bool RARE>
 __device__ Src adj_resolve(const AdjArgs& a, const BlockDesc& B, int i, int j, int k) {
     StageArgs A{};
@@ -639,11 +731,37 @@ __device__ __forceinline__ void face_vjp(const AdjArgs& a, int b, int i, int j, 
     const bool leftIn = idxD - 1 >= 0, rightIn = idxD < nD;
     const long long gl = B.offset + (long long)(i - (D == 0)) + (long long)B.n[0] * ((long long)(j - (D == 1)) + (long long)B.n[1] * (k - (D == 2)));
     const long long gr = B.offset + (long long)i + (long long)B.n[0] * ((long long)j + (long long)B.n[1] * k);
+    double AVr = AV, AVl = AV;
+    bool graded = false;
+    const double* gwL = nullptr;
+    const double* gwR = nullptr;
+    if constexpr (RARE) {
+        if (B.graded) {
+            // graded block: the face's area from the lengths of its cells across it, each
+            // side's own volume (cell lengths glen[d][c + 2], weights of cells -1 .. n)
+            graded = true;
+            const int ic[3] = {i, j, k};
+            double Lr[3], Ll[3];
+            for (int d = 0; d < 3; ++d) {
+                Lr[d] = B.glen[d][ic[d] + 2];
+                Ll[d] = B.glen[d][ic[d] - (d == D) + 2];
+            }
+            const bool threeD = a.P.dims == 3;
+            const double Af = threeD ? (D == 0 ? Lr[1] * Lr[2] : (D == 1 ? Lr[2] * Lr[0] : Lr[0] * Lr[1]))
+                                     : (D == 0 ? Lr[1] : Lr[0]);
+            const double Vr = threeD ? Lr[0] * Lr[1] * Lr[2] : Lr[0] * Lr[1];
+            const double Vl = threeD ? Ll[0] * Ll[1] * Ll[2] : Ll[0] * Ll[1];
+            AVr = Af / Vr * a.w_scale;
+            AVl = Af / Vl * a.w_scale;
+            gwL = B.gw[D] + (long long)idxD * GW_N;
+            gwR = gwL + GW_N;
+        }
+    }
     double gFg[5];
     for (int q = 0; q < 5; ++q) {
         double wr = rightIn ? a.W[q * a.total + gr] : 0.0;
         double wl = leftIn ? a.W[q * a.total + gl] : 0.0;
-        gFg[q] = AV * (wr - wl);
+        gFg[q] = AVr * wr - AVl * wl;
     }
     if constexpr (RARE) {
         // OutFlowBC_SimpleFlux (boundary_flux_effect.d:504-645): the boundary face's flux is
@@ -663,8 +781,13 @@ __device__ __forceinline__ void face_vjp(const AdjArgs& a, int b, int i, int j, 
     const int pv[5] = {1 + ax0, 1 + ax1, 1 + ax2, 0, 4};
     double qL[5], qR[5];
     for (int sc = 0; sc < 5; ++sc) {
+        if (RARE && graded) {
+            L2R2G rg;
+            l2r2g_fwd(gwL, gwR, P, c[0][pv[sc]], c[1][pv[sc]], c[2][pv[sc]], c[3][pv[sc]], qL[sc], qR[sc], rg);
+            continue;
+        }
         L2R2Rec rec;  // recomputed in the reverse sweep rather than kept live
-        l2r2_fwd(w, P, c[0][pv[sc]], c[1][pv[sc]], c[2][pv[sc]], c[3][pv[sc]], qL[sc], qR[sc], rec);
+        l2r2_fwd<RARE>(w, P, c[0][pv[sc]], c[1][pv[sc]], c[2][pv[sc]], c[3][pv[sc]], qL[sc], qR[sc], rec);
     }
     const double Rg = P.gas.R, Cvinv = P.gas.Cvinv;
     bool badL = qL[4] <= 0.0 || qL[3] <= 0.0, badR = qR[4] <= 0.0 || qR[3] <= 0.0;
@@ -701,10 +824,17 @@ __device__ __forceinline__ void face_vjp(const AdjArgs& a, int b, int i, int j, 
     }
     for (int sc = 0; sc < 5; ++sc) {
         const int v = pv[sc];
+        if (RARE && graded) {
+            L2R2G rg;
+            double ql, qr;
+            l2r2g_fwd(gwL, gwR, P, c[0][v], c[1][v], c[2][v], c[3][v], ql, qr, rg);
+            l2r2g_rev(gwL, gwR, P, c[1][v], c[2][v], rg, gqL[sc], gqR[sc], gc[0][v], gc[1][v], gc[2][v], gc[3][v]);
+            continue;
+        }
         L2R2Rec rec;
         double ql, qr;
-        l2r2_fwd(w, P, c[0][v], c[1][v], c[2][v], c[3][v], ql, qr, rec);
-        l2r2_rev(w, P, c[0][v], c[1][v], c[2][v], c[3][v], rec, gqL[sc], gqR[sc], gc[0][v], gc[1][v], gc[2][v],
+        l2r2_fwd<RARE>(w, P, c[0][v], c[1][v], c[2][v], c[3][v], ql, qr, rec);
+        l2r2_rev<RARE>(w, P, c[0][v], c[1][v], c[2][v], c[3][v], rec, gqL[sc], gqR[sc], gc[0][v], gc[1][v], gc[2][v],
                  gc[3][v]);
     }
 }
@@ -861,9 +991,9 @@ using namespace gdfv;
 
 namespace {
 
-// The face kernel of the context's flux calculator (with the rare boundary rules when
-// some exchange rotates or some face is an outflow boundary of its own) over nb[d] CTAs
-// of each direction.
+// The face kernel of the context's flux calculator (with the rare rules when some
+// exchange rotates, some face is an outflow boundary of its own or the limiter is lmr's)
+// over nb[d] CTAs of each direction.
 template <int FLUX>
 void launch_faces_flux(const AdjArgs& a, bool rare, const unsigned* nb, cudaStream_t s) {
     const unsigned n = nb[0] + nb[1] + nb[2];
@@ -872,20 +1002,15 @@ void launch_faces_flux(const AdjArgs& a, bool rare, const unsigned* nb, cudaStre
 }
 
 void launch_faces(const AdjArgs& a, int flux, const unsigned* nb, cudaStream_t s) {
-    const bool rare = a.P.rotating || a.P.outflow_bcs;
+    const bool rare = a.P.rotating || a.P.outflow_bcs || a.P.lmr_epsilon || a.P.graded;
     if (flux == FLUX_HLLC) launch_faces_flux<FLUX_HLLC>(a, rare, nb, s);
     else launch_faces_flux<FLUX_AUSMDV>(a, rare, nb, s);
 }
 
 bool vjp_supported(int ctx, const AdjView& v) {
     if (!v.prepared) { adjoint_set_error(ctx, "call gdfv_prepare first"); return false; }
-    if (v.mhd || (v.flux != FLUX_AUSMDV && v.flux != FLUX_HLLC) || v.P.lmr_epsilon) {
-        adjoint_set_error(ctx, "the adjoint supports the Euler path with flux_calculator=ausmdv or hllc "
-                               "and van_albada_variant=e4");
-        return false;
-    }
-    if (v.P.graded) {
-        adjoint_set_error(ctx, "the adjoint supports uniform Cartesian blocks (no graded blocks)");
+    if (v.mhd || (v.flux != FLUX_AUSMDV && v.flux != FLUX_HLLC)) {
+        adjoint_set_error(ctx, "the adjoint supports the Euler path with flux_calculator=ausmdv or hllc");
         return false;
     }
     return true;

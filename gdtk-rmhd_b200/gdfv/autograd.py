@@ -186,6 +186,7 @@ class Rollout(torch.autograd.Function):
                     torch.cuda.synchronize()
         UN = _state_view(sim).clone()
         torch.cuda.synchronize()
+        sim.rollout_recorded = recorded   # False: a retried step sent the forward step by step
         ctx.sim, ctx.dts, ctx.ckpts, ctx.k, ctx.work = sim, dts, ckpts, K, work
         ctx.theta = theta.detach().clone()
         return UN

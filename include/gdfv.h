@@ -87,7 +87,7 @@ int gdfv_block_new(int ctx, int nic, int njc, int nkc, double dx, double dy, dou
  * (e4/onedinterp.d:338-355; ghost cells take the lengths of interior cell n, or of the
  * partner's cell across an exchange, e4/sfluidblock.d:884-1090), and the CFL signal
  * takes each cell's own lengths (e4/fvcell.d:975-1059).  Not with MHD or
- * van_albada_variant=lmr; the adjoint rejects contexts with graded blocks. */
+ * van_albada_variant=lmr; the adjoint takes them (per-cell weights, areas and volumes). */
 int gdfv_block_new_graded(int ctx, int nic, int njc, int nkc, const double* xv, const double* yv,
                           const double* zv);
 
@@ -201,7 +201,7 @@ int gdfv_residual_jvp(int ctx, const double* U_dev, const double* v_dev, const d
  * the primal values).  g_inflow_host (may be NULL) receives, per supersonic-inflow face
  * state in the order the faces were defined, the cotangent of its ghost state
  * (rho, vel.x, vel.y, vel.z, u, a), 6 doubles each.  Euler (2D or 3D) with
- * flux_calculator=ausmdv or hllc; every boundary condition of this library, exchanges
+ * flux_calculator=ausmdv or hllc, van_albada_variant e4 or lmr, uniform or graded blocks; every boundary condition of this library, exchanges
  * of any orientation with or without an Rmatrix (the cotangent goes back through its
  * transpose) and the outflow boundaries with their own ghost or flux rule included.  It is the transpose of the Jacobian-vector products of
  * e4/steadystate_core.d:1870-2060 (evalJacobianVecProd), which it is checked against. */

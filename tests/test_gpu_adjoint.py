@@ -86,6 +86,26 @@ def test_vjp_transpose_2d(flux):
     _dot_check(case, 6, 1e-10, seed=10)
 
 
+@pytest.mark.parametrize("flux", ["ausmdv", "hllc"])
+def test_vjp_transpose_graded_blocks(flux):
+    """Graded (stretched rectilinear) blocks: each side of a face reconstructs with its own
+    cell's l2r2 weights, the face's area comes from its cells' lengths and each side
+    divides by its own volume; the lattice joins four differently graded blocks by
+    exchange."""
+    _dot_check(cases.graded_inflow_box(flux=flux), 6, 1e-10, seed=13)
+    if flux == "ausmdv":
+        _dot_check(cases.graded_lattice(), 6, 1e-10, seed=14)
+
+
+def test_vjp_transpose_lmr_limiter():
+    """van_albada_variant lmr (lmr/onedinterp.d:147-151): each face's epsilon scales with
+    the larger of its two states, which adds a derivative through epsilon (taken at 1e-3
+    so that it weighs)."""
+    for case in (cases.c1_shock_box(n=16), cases.c2_inflow_box(n=(24, 16, 12), noise_all=True)):
+        case.config.update(van_albada_variant="lmr", epsilon_van_albada=1e-3)
+        _dot_check(case, 6, 1e-10, seed=12)
+
+
 @pytest.mark.parametrize("bc", ["simple_flux", "fixed_p", "fixed_pt"])
 def test_vjp_transpose_outflow_boundaries(bc):
     """OutFlowBC_SimpleFlux (the boundary face's flux from the interior cell alone, on
