@@ -531,6 +531,190 @@ __device__ void simple_flux_vjp(const NumParams& P, const double* q, int outsign
     gq[4] += gu;
 }
 
+// hlle for ideal MHD (e4/fluxcalc.d:1608-1780, mu0 = 1) forward with the quantities the
+// reverse needs, then its reverse.  Face-local states: r, p, u (normal), v, w
+// (tangential), B (normal, tangential, tangential), e (internal energy).  The
+// alpha-weighted Cv and R of one gas are Cv and R themselves (their derivatives vanish);
+// the wave-speed min/max and the switches at 0 take the branches the primal values took;
+// SAFESQRT's floor (|x| <= 1e-14: 0) has derivative 0.
+struct FSm { double r, p, u, v, w, Bx, By, Bz, e; };
+
+struct FastSpeed {   // cf = sqrt(0.5 (alf + sqrt(alf^2 - 4 a2 ca2))) with its pieces
+    double a2, ca2, alf, X, als, cf2, cf;
+    bool live;        // SAFESQRT took the root
+};
+__device__ __forceinline__ FastSpeed fast_speed(double gam, double p, double rho, double Bx, double By, double Bz) {
+    FastSpeed f;
+    const double BB = Bx * Bx + By * By + Bz * Bz;
+    f.a2 = gam * p / rho;
+    f.ca2 = Bx * Bx / rho;
+    f.alf = f.a2 + BB / rho;
+    f.X = f.alf * f.alf - 4.0 * f.a2 * f.ca2;
+    f.live = fabs(f.X) > 1.0e-14;
+    f.als = f.live ? sqrt(f.X) : 0.0;
+    f.cf2 = 0.5 * (f.alf + f.als);
+    f.cf = sqrt(f.cf2);
+    return f;
+}
+// reverse of fast_speed: gcf into the cotangents of p, rho and B (added)
+__device__ __forceinline__ void fast_speed_rev(const FastSpeed& f, double gam, double p, double rho, double Bx,
+                                               double By, double Bz, double gcf, double& gp, double& grho,
+                                               double& gBx, double& gBy, double& gBz) {
+    const double gcf2 = gcf * 0.5 / f.cf;
+    double galf = 0.5 * gcf2, gals = 0.5 * gcf2;
+    double ga2 = 0.0, gca2 = 0.0;
+    if (f.live) {
+        const double gX = gals * 0.5 / f.als;
+        galf += gX * 2.0 * f.alf;
+        ga2 += -4.0 * f.ca2 * gX;
+        gca2 += -4.0 * f.a2 * gX;
+    }
+    const double BB = Bx * Bx + By * By + Bz * Bz;
+    // alf = a2 + BB / rho
+    ga2 += galf;
+    const double gBB = galf / rho;
+    grho -= galf * BB / (rho * rho);
+    // ca2 = Bx^2 / rho
+    double gBx2 = gca2 / rho;
+    grho -= gca2 * f.ca2 / rho;
+    // a2 = gam p / rho
+    gp += ga2 * gam / rho;
+    grho -= ga2 * f.a2 / rho;
+    gBx2 += gBB;
+    gBx += 2.0 * Bx * gBx2;
+    gBy += 2.0 * By * gBB;
+    gBz += 2.0 * Bz * gBB;
+}
+
+// The one-sided fluxes of hlle_mhd: mass, x, y, z momentum, energy, By, Bz (Bx: 0).
+__device__ __forceinline__ void mhd_side_flux(const FSm& S, double* f) {
+    const double BB = S.Bx * S.Bx + S.By * S.By + S.Bz * S.Bz;
+    const double pt = S.p + 0.5 * BB;
+    const double uu = S.u * S.u + S.v * S.v + S.w * S.w;
+    f[0] = S.r * S.u;
+    f[1] = S.r * S.u * S.u - S.Bx * S.Bx + pt;
+    f[2] = S.r * S.u * S.v - S.Bx * S.By;
+    f[3] = S.r * S.u * S.w - S.Bx * S.Bz;
+    f[4] = (S.r * S.e + 0.5 * (S.r * uu + BB) + pt) * S.u - (S.u * S.Bx + S.v * S.By + S.w * S.Bz) * S.Bx;
+    f[5] = S.u * S.By - S.v * S.Bx;
+    f[6] = S.u * S.Bz - S.w * S.Bx;
+}
+// reverse of mhd_side_flux: cotangents gf[7] into gS (added)
+__device__ __forceinline__ void mhd_side_flux_rev(const FSm& S, const double* gf, FSm& gS) {
+    const double BB = S.Bx * S.Bx + S.By * S.By + S.Bz * S.Bz;
+    const double pt = S.p + 0.5 * BB;
+    const double uu = S.u * S.u + S.v * S.v + S.w * S.w;
+    double gpt = 0.0, guu = 0.0, gBB = 0.0;
+    // mass
+    gS.r += gf[0] * S.u; gS.u += gf[0] * S.r;
+    // x momentum r u^2 - Bx^2 + pt
+    gS.r += gf[1] * S.u * S.u; gS.u += gf[1] * 2.0 * S.r * S.u; gS.Bx -= gf[1] * 2.0 * S.Bx; gpt += gf[1];
+    // y, z momentum
+    gS.r += gf[2] * S.u * S.v; gS.u += gf[2] * S.r * S.v; gS.v += gf[2] * S.r * S.u;
+    gS.Bx -= gf[2] * S.By; gS.By -= gf[2] * S.Bx;
+    gS.r += gf[3] * S.u * S.w; gS.u += gf[3] * S.r * S.w; gS.w += gf[3] * S.r * S.u;
+    gS.Bx -= gf[3] * S.Bz; gS.Bz -= gf[3] * S.Bx;
+    // energy (H) u - (u Bx + v By + w Bz) Bx, H = r e + (r uu + BB)/2 + pt
+    const double H = S.r * S.e + 0.5 * (S.r * uu + BB) + pt;
+    const double Sd = S.u * S.Bx + S.v * S.By + S.w * S.Bz;
+    const double gH = gf[4] * S.u;
+    gS.u += gf[4] * H;
+    const double gSd = -gf[4] * S.Bx;
+    gS.Bx -= gf[4] * Sd;
+    gS.r += gH * (S.e + 0.5 * uu); gS.e += gH * S.r; guu += 0.5 * gH * S.r; gBB += 0.5 * gH; gpt += gH;
+    gS.u += gSd * S.Bx; gS.Bx += gSd * S.u; gS.v += gSd * S.By; gS.By += gSd * S.v;
+    gS.w += gSd * S.Bz; gS.Bz += gSd * S.w;
+    // By, Bz induction
+    gS.u += gf[5] * S.By; gS.By += gf[5] * S.u; gS.v -= gf[5] * S.Bx; gS.Bx -= gf[5] * S.v;
+    gS.u += gf[6] * S.Bz; gS.Bz += gf[6] * S.u; gS.w -= gf[6] * S.Bx; gS.Bx -= gf[6] * S.w;
+    // pt = p + BB/2, uu, BB
+    gS.p += gpt; gBB += 0.5 * gpt;
+    gS.u += 2.0 * S.u * guu; gS.v += 2.0 * S.v * guu; gS.w += 2.0 * S.w * guu;
+    gS.Bx += 2.0 * S.Bx * gBB; gS.By += 2.0 * S.By * gBB; gS.Bz += 2.0 * S.Bz * gBB;
+}
+
+// gF: cotangent of the face-local flux in the order MASS, XMOM, YMOM, ZMOM, TOTENERGY, XB,
+// YB, ZB; gL, gR receive the cotangents of the two states (added).
+__device__ void hlle_mhd_vjp(const NumParams& P, const FSm& L, const FSm& R, const double* gF, FSm& gL, FSm& gR) {
+    // ---- forward
+    const double gam = (P.gas.Cv + P.gas.R) / P.gas.Cv;
+    const double rho = 0.5 * (L.r + R.r), p = 0.5 * (L.p + R.p), u = 0.5 * (L.u + R.u);
+    const double Bx = 0.5 * (L.Bx + R.Bx), By = 0.5 * (L.By + R.By), Bz = 0.5 * (L.Bz + R.Bz);
+    const FastSpeed fm = fast_speed(gam, p, rho, Bx, By, Bz);
+    const FastSpeed fL = fast_speed(gam, L.p, L.r, L.Bx, L.By, L.Bz);
+    const FastSpeed fR = fast_speed(gam, R.p, R.r, R.Bx, R.By, R.Bz);
+    const double wp = u + fm.cf, wm = u - fm.cf, wmL = L.u - fL.cf, wpR = R.u + fR.cf;
+    const bool blL = wmL <= wm, brR = wpR >= wp;
+    const double bl = blL ? wmL : wm, br = brR ? wpR : wp;
+    const double blm = fmin(bl, 0.0), brp = fmax(br, 0.0);
+    double fl[7], fr[7];
+    mhd_side_flux(L, fl);
+    mhd_side_flux(R, fr);
+    const double uuL = L.u * L.u + L.v * L.v + L.w * L.w, uuR = R.u * R.u + R.v * R.v + R.w * R.w;
+    const double BBL = L.Bx * L.Bx + L.By * L.By + L.Bz * L.Bz, BBR = R.Bx * R.Bx + R.By * R.By + R.Bz * R.Bz;
+    // one-sided fluxes and jumps in the order of F (the Bx flux of either side is 0)
+    const double fLF[8] = {fl[0], fl[1], fl[2], fl[3], fl[4], 0.0, fl[5], fl[6]};
+    const double fRF[8] = {fr[0], fr[1], fr[2], fr[3], fr[4], 0.0, fr[5], fr[6]};
+    const double d[8] = {R.r - L.r, R.r * R.u - L.r * L.u, R.r * R.v - L.r * L.v, R.r * R.w - L.r * L.w,
+                         (R.p - L.p) / (gam - 1.0) + 0.5 * (R.r * uuR + BBR) - 0.5 * (L.r * uuL + BBL),
+                         R.Bx - L.Bx, R.By - L.By, R.Bz - L.Bz};
+    const double iden = 1.0 / (brp - blm), fac1 = brp * blm;
+    // ---- reverse
+    double gbrp = 0.0, gblm = 0.0, gfac1 = 0.0, giden = 0.0;
+    double gfLF[8], gfRF[8], gd[8];
+    for (int q = 0; q < 8; ++q) {
+        const double N = brp * fLF[q] - blm * fRF[q] + fac1 * d[q];
+        const double gN = gF[q] * iden;
+        giden += gF[q] * N;
+        gfLF[q] = gN * brp;
+        gfRF[q] = -gN * blm;
+        gd[q] = gN * fac1;
+        gbrp += gN * fLF[q];
+        gblm -= gN * fRF[q];
+        gfac1 += gN * d[q];
+    }
+    gbrp += -giden * iden * iden;
+    gblm += giden * iden * iden;
+    gbrp += gfac1 * blm;
+    gblm += gfac1 * brp;
+    // fmin(bl, 0), fmax(br, 0) keep their first argument on a tie (src/ntypes/complex.d)
+    const double gbl = bl <= 0.0 ? gblm : 0.0, gbr = br >= 0.0 ? gbrp : 0.0;
+    double gwm = 0.0, gwp = 0.0, gcfL = 0.0, gcfR = 0.0;
+    if (blL) { gL.u += gbl; gcfL -= gbl; } else gwm += gbl;
+    if (brR) { gR.u += gbr; gcfR += gbr; } else gwp += gbr;
+    // wp = u + cf, wm = u - cf of the averages
+    const double gu = gwp + gwm, gcf = gwp - gwm;
+    double gp = 0.0, grho = 0.0, gBx = 0.0, gBy = 0.0, gBz = 0.0;
+    fast_speed_rev(fm, gam, p, rho, Bx, By, Bz, gcf, gp, grho, gBx, gBy, gBz);
+    fast_speed_rev(fL, gam, L.p, L.r, L.Bx, L.By, L.Bz, gcfL, gL.p, gL.r, gL.Bx, gL.By, gL.Bz);
+    fast_speed_rev(fR, gam, R.p, R.r, R.Bx, R.By, R.Bz, gcfR, gR.p, gR.r, gR.Bx, gR.By, gR.Bz);
+    gL.r += 0.5 * grho; gR.r += 0.5 * grho;
+    gL.p += 0.5 * gp; gR.p += 0.5 * gp;
+    gL.u += 0.5 * gu; gR.u += 0.5 * gu;
+    gL.Bx += 0.5 * gBx; gR.Bx += 0.5 * gBx;
+    gL.By += 0.5 * gBy; gR.By += 0.5 * gBy;
+    gL.Bz += 0.5 * gBz; gR.Bz += 0.5 * gBz;
+    const double gfl[7] = {gfLF[0], gfLF[1], gfLF[2], gfLF[3], gfLF[4], gfLF[6], gfLF[7]};
+    const double gfr[7] = {gfRF[0], gfRF[1], gfRF[2], gfRF[3], gfRF[4], gfRF[6], gfRF[7]};
+    mhd_side_flux_rev(L, gfl, gL);
+    mhd_side_flux_rev(R, gfr, gR);
+    // jumps
+    gR.r += gd[0]; gL.r -= gd[0];
+    gR.r += gd[1] * R.u; gR.u += gd[1] * R.r; gL.r -= gd[1] * L.u; gL.u -= gd[1] * L.r;
+    gR.r += gd[2] * R.v; gR.v += gd[2] * R.r; gL.r -= gd[2] * L.v; gL.v -= gd[2] * L.r;
+    gR.r += gd[3] * R.w; gR.w += gd[3] * R.r; gL.r -= gd[3] * L.w; gL.w -= gd[3] * L.r;
+    const double ig = gd[4] / (gam - 1.0);
+    gR.p += ig; gL.p -= ig;
+    gR.r += 0.5 * gd[4] * uuR; gL.r -= 0.5 * gd[4] * uuL;
+    gR.u += gd[4] * R.r * R.u; gR.v += gd[4] * R.r * R.v; gR.w += gd[4] * R.r * R.w;
+    gL.u -= gd[4] * L.r * L.u; gL.v -= gd[4] * L.r * L.v; gL.w -= gd[4] * L.r * L.w;
+    gR.Bx += gd[4] * R.Bx; gR.By += gd[4] * R.By; gR.Bz += gd[4] * R.Bz;
+    gL.Bx -= gd[4] * L.Bx; gL.By -= gd[4] * L.By; gL.Bz -= gd[4] * L.Bz;
+    gR.Bx += gd[5]; gL.Bx -= gd[5];
+    gR.By += gd[6]; gL.By -= gd[6];
+    gR.Bz += gd[7]; gL.Bz -= gd[7];
+}
+
 struct AdjArgs {
     const BlockDesc* blocks;
     const InflowState* inflow;
@@ -550,6 +734,7 @@ struct AdjArgs {
     int nblocks;
     int mode;          // 0: gU = result; 1: mu -> bbuf, lam += mu; 2: lam += result
     NumParams P;
+    double c_h;        // MHD: the GLM wave speed of the residual (the context's current one)
 };
 
 __device__ __forceinline__ void decode_cell(const AdjArgs& a, long long g) {
@@ -673,6 +858,76 @@ __device__ void adj_scatter(const AdjArgs& a, const Src& s, const double* gc) {
         if (s.kind == SRC_MIRROR && m == 1 + s.axis) v = -v;
         atomicAdd(&a.gP[m * a.total + g0], v);
     }
+}
+
+// ---------------------------------------------------------------- MHD (residual VJP)
+// Primitives of an MHD cell: rho, v0, v1, v2, u, a, B0, B1, B2, psi.
+constexpr int NPM = 10;
+
+// Stencil state of an MHD source (the ghost rules of finish_cell): (x, y) is the centre
+// of the stencil cell, for the slip wall's dipole field (internal_copy_then_reflect.d:
+// 140-143: Bx, By of a slip-wall ghost with |x| < 0.4136 are the dipole's, constants).
+__device__ void adj_load_mhd(const AdjArgs& a, const Src& s, double x, double y, double* c) {
+    if (s.kind == SRC_INFLOW) {
+        const InflowState& in = a.inflow[s.inflow];
+        c[0] = in.rho; c[1] = in.vel[0]; c[2] = in.vel[1]; c[3] = in.vel[2]; c[4] = in.u; c[5] = in.a;
+        c[6] = in.B[0]; c[7] = in.B[1]; c[8] = in.B[2]; c[9] = in.psi;
+        return;
+    }
+    const long long g0 = s.blk->offset + s.c0;
+    double e[NPM];
+    for (int m = 0; m < NPM; ++m) e[m] = a.Pp[m * a.total + g0];
+    for (int m = 0; m < NPM; ++m) c[m] = e[m];
+    if (s.kind == SRC_EXTRAP1_G0 || s.kind == SRC_EXTRAP1_G1) {
+        // extrapolate_copy.d:171-201: rho, u, v, B extrapolated; a and psi of the edge cell
+        const long long g1 = s.blk->offset + s.c1;
+        for (int m = 0; m < NPM; ++m) {
+            if (m == 5 || m == 9) continue;
+            const double f = a.Pp[m * a.total + g1];
+            const double g0v = 2.0 * e[m] - f;
+            c[m] = (s.kind == SRC_EXTRAP1_G0) ? g0v : 2.0 * g0v - e[m];
+        }
+    } else if (s.kind == SRC_MIRROR) {
+        c[1 + s.axis] = -c[1 + s.axis];   // B is not reflected (ghost_cell.d:56-67)
+        if (x > -0.4136 && x < 0.4136) dipole_field(x, y, c[6], c[7]);
+    } else if (s.kind == SRC_ROTATE) {
+        const double* R = a.rot + 9 * s.inflow;
+        for (int r = 0; r < 3; ++r) {
+            c[1 + r] = R[3 * r] * e[1] + R[3 * r + 1] * e[2] + R[3 * r + 2] * e[3];
+            c[6 + r] = R[3 * r] * e[6] + R[3 * r + 1] * e[7] + R[3 * r + 2] * e[8];
+        }
+    }
+}
+
+__device__ void adj_scatter_mhd(const AdjArgs& a, const Src& s, double x, double y, const double* gc) {
+    if (s.kind == SRC_INFLOW) {
+        for (int m = 0; m < NPM; ++m) atomicAdd(&a.gInflow[s.inflow * NPM + m], gc[m]);
+        return;
+    }
+    const long long g0 = s.blk->offset + s.c0;
+    if (s.kind == SRC_EXTRAP1_G0 || s.kind == SRC_EXTRAP1_G1) {
+        const long long g1 = s.blk->offset + s.c1;
+        const double ce = (s.kind == SRC_EXTRAP1_G0) ? 2.0 : 3.0, cf = (s.kind == SRC_EXTRAP1_G0) ? -1.0 : -2.0;
+        for (int m = 0; m < NPM; ++m) {
+            if (m == 5 || m == 9) { atomicAdd(&a.gP[m * a.total + g0], gc[m]); continue; }
+            atomicAdd(&a.gP[m * a.total + g0], ce * gc[m]);
+            atomicAdd(&a.gP[m * a.total + g1], cf * gc[m]);
+        }
+        return;
+    }
+    double g[NPM];
+    for (int m = 0; m < NPM; ++m) g[m] = gc[m];
+    if (s.kind == SRC_MIRROR) {
+        g[1 + s.axis] = -g[1 + s.axis];
+        if (x > -0.4136 && x < 0.4136) { g[6] = 0.0; g[7] = 0.0; }   // the dipole's constants
+    } else if (s.kind == SRC_ROTATE) {
+        const double* R = a.rot + 9 * s.inflow;
+        for (int m = 0; m < 3; ++m) {
+            g[1 + m] = R[m] * gc[1] + R[3 + m] * gc[2] + R[6 + m] * gc[3];
+            g[6 + m] = R[m] * gc[6] + R[3 + m] * gc[7] + R[6 + m] * gc[8];
+        }
+    }
+    for (int m = 0; m < NPM; ++m) atomicAdd(&a.gP[m * a.total + g0], g[m]);
 }
 
 // Block and cell indices of face f of direction D (the face lies between cells
@@ -937,6 +1192,172 @@ __global__ void __launch_bounds__(FACE_CTA, GDFV_ADJ_MINB) adj_faces_kernel(AdjA
     else face_thread<2, FLUX, RARE>(a, (long long)(bid - nb0 - nb1) * FACE_CTA + threadIdx.x);
 }
 
+// The reverse sweep of MHD face f of direction D (face_flux with hlle_mhd and the GLM
+// terms, e4/fluxcalc.d:54-187, :1608-1780): cotangents of the four stencil cells'
+// primitives, scattered through the ghost rules.  The limiter's arithmetic is the Euler
+// path's; psi is reconstructed only with divergence cleaning (a copy of the cell's
+// otherwise); c_h is the residual's, frozen.
+template <int D>
+__device__ void face_mhd(const AdjArgs& a, long long f) {
+    const long long* off = a.face_off + D * (a.nblocks + 1);
+    if (f >= off[a.nblocks]) return;
+    int i = 0, j = 0, k = 0;
+    const int b = face_coords<D>(a, f, i, j, k);
+    const BlockDesc& B = a.blocks[b];
+    const NumParams& P = a.P;
+    Src src[4];
+    double xs[4], ys[4];
+    double c[4][NPM];
+    for (int m = 0; m < 4; ++m) {
+        src[m] = stencil_src<D, true>(a, B, i, j, k, m);
+        const int ci = i - (D == 0 ? 2 - m : 0), cj = j - (D == 1 ? 2 - m : 0);
+        xs[m] = B.x0 + ((double)ci + 0.5) * B.len[0];
+        ys[m] = B.y0 + ((double)cj + 0.5) * B.len[1];
+        adj_load_mhd(a, src[m], xs[m], ys[m], c[m]);
+    }
+    const double AV = B.area[D] * B.vol_inv * a.w_scale;
+    const int nD = B.n[D];
+    const int idxD = D == 0 ? i : (D == 1 ? j : k);
+    const bool leftIn = idxD - 1 >= 0, rightIn = idxD < nD;
+    const long long gl = B.offset + (long long)(i - (D == 0)) +
+                         (long long)B.n[0] * ((long long)(j - (D == 1)) + (long long)B.n[1] * (k - (D == 2)));
+    const long long gr = B.offset + (long long)i + (long long)B.n[0] * ((long long)j + (long long)B.n[1] * k);
+    double gFg[10];
+    for (int q = 0; q < 10; ++q) {
+        const double wr = rightIn ? a.W[q * a.total + gr] : 0.0;
+        const double wl = leftIn ? a.W[q * a.total + gl] : 0.0;
+        gFg[q] = AV * (wr - wl);
+    }
+    constexpr int ax0 = D, ax1 = (D + 1) % 3, ax2 = (D + 2) % 3;
+    double gF[10];
+    gF[MASS] = gFg[MASS]; gF[TOTENERGY] = gFg[TOTENERGY]; gF[PSI] = gFg[PSI]; gF[DIVB] = gFg[DIVB];
+    gF[XMOM] = gFg[XMOM + ax0]; gF[YMOM] = gFg[XMOM + ax1]; gF[ZMOM] = gFg[XMOM + ax2];
+    gF[XB] = gFg[XB + ax0]; gF[YB] = gFg[XB + ax1]; gF[ZB] = gFg[XB + ax2];
+    // ---- forward reconstruction: face-frame v, rho, u, face-frame B, psi
+    const double* w = B.w[D];
+    const int pv[9] = {1 + ax0, 1 + ax1, 1 + ax2, 0, 4, 6 + ax0, 6 + ax1, 6 + ax2, 9};
+    const bool clean = P.divergence_cleaning;
+    double qL[9], qR[9];
+    for (int sc = 0; sc < 9; ++sc) {
+        if (sc == 8 && !clean) { qL[8] = c[1][9]; qR[8] = c[2][9]; continue; }
+        L2R2Rec rec;
+        l2r2_fwd<true>(w, P, c[0][pv[sc]], c[1][pv[sc]], c[2][pv[sc]], c[3][pv[sc]], qL[sc], qR[sc], rec);
+    }
+    const double Rg = P.gas.R, Cvinv = P.gas.Cvinv;
+    const bool badL = qL[4] <= 0.0 || qL[3] <= 0.0, badR = qR[4] <= 0.0 || qR[3] <= 0.0;
+    auto state = [&](bool bad, const double* q, const double* cell, FSm& S, double& psi) {
+        if (bad) {   // e4/onedinterp.d:44-74: the cell-centre state
+            S = FSm{cell[0], cell[0] * Rg * (cell[4] * Cvinv), cell[pv[0]], cell[pv[1]], cell[pv[2]],
+                    cell[pv[5]], cell[pv[6]], cell[pv[7]], cell[4]};
+            psi = cell[9];
+        } else {
+            S = FSm{q[3], q[3] * Rg * (q[4] * Cvinv), q[0], q[1], q[2], q[5], q[6], q[7], q[4]};
+            psi = q[8];
+        }
+    };
+    FSm L, R;
+    double psiL, psiR;
+    state(badL, qL, c[1], L, psiL);
+    state(badR, qR, c[2], R, psiR);
+    // ---- reverse: F[divB] = (BxR - BxL)/2 and the GLM terms (fluxcalc.d:139-150, with the
+    // reference's third term added to F[xB] under glm_reference_indexing)
+    FSm gL{}, gR{};
+    double gpsiL = 0.0, gpsiR = 0.0;
+    gR.Bx += 0.5 * gF[DIVB]; gL.Bx -= 0.5 * gF[DIVB];
+    if (clean) {
+        const double ch = a.c_h;
+        const double gt3 = P.glm_reference_indexing ? gF[XB] : gF[ZB];
+        const double gpa = gF[XB] + gF[YB] + gt3;
+        gR.Bx -= 0.5 * ch * gF[XB]; gL.Bx += 0.5 * ch * gF[XB];
+        gR.By -= 0.5 * ch * gF[YB]; gL.By += 0.5 * ch * gF[YB];
+        gR.Bz -= 0.5 * ch * gt3; gL.Bz += 0.5 * ch * gt3;
+        gpsiL += 0.5 * gpa; gpsiR += 0.5 * gpa;
+        const double gps = gF[PSI] * ch * ch;
+        gL.Bx += 0.5 * gps; gR.Bx += 0.5 * gps;
+        gpsiR -= gps / (2.0 * ch); gpsiL += gps / (2.0 * ch);
+    }
+    const double gF8[8] = {gF[MASS], gF[XMOM], gF[YMOM], gF[ZMOM], gF[TOTENERGY], gF[XB], gF[YB], gF[ZB]};
+    hlle_mhd_vjp(P, L, R, gF8, gL, gR);
+    double gc[4][NPM];
+    for (int m = 0; m < 4; ++m)
+        for (int q = 0; q < NPM; ++q) gc[m][q] = 0.0;
+    double gqL[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, gqR[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    auto back = [&](bool bad, const FSm& S, const FSm& gS, double gpsi, double* gq, double* gcell) {
+        // p = rho R (u Cvinv)
+        const double gr_ = gS.r + gS.p * Rg * (S.e * Cvinv), ge_ = gS.e + gS.p * S.r * Rg * Cvinv;
+        if (bad) {
+            gcell[0] += gr_; gcell[4] += ge_;
+            gcell[pv[0]] += gS.u; gcell[pv[1]] += gS.v; gcell[pv[2]] += gS.w;
+            gcell[pv[5]] += gS.Bx; gcell[pv[6]] += gS.By; gcell[pv[7]] += gS.Bz; gcell[9] += gpsi;
+        } else {
+            gq[3] += gr_; gq[4] += ge_;
+            gq[0] += gS.u; gq[1] += gS.v; gq[2] += gS.w;
+            gq[5] += gS.Bx; gq[6] += gS.By; gq[7] += gS.Bz; gq[8] += gpsi;
+        }
+    };
+    back(badL, L, gL, gpsiL, gqL, gc[1]);
+    back(badR, R, gR, gpsiR, gqR, gc[2]);
+    for (int sc = 0; sc < 9; ++sc) {
+        const int v = pv[sc];
+        if (sc == 8 && !clean) { gc[1][9] += gqL[8]; gc[2][9] += gqR[8]; continue; }
+        L2R2Rec rec;
+        double ql, qr;
+        l2r2_fwd<true>(w, P, c[0][v], c[1][v], c[2][v], c[3][v], ql, qr, rec);
+        l2r2_rev<true>(w, P, c[0][v], c[1][v], c[2][v], c[3][v], rec, gqL[sc], gqR[sc], gc[0][v], gc[1][v], gc[2][v],
+                       gc[3][v]);
+    }
+    for (int m = 0; m < 4; ++m) adj_scatter_mhd(a, src[m], xs[m], ys[m], gc[m]);
+}
+
+__global__ void __launch_bounds__(128) adj_faces_mhd_kernel(AdjArgs a, unsigned nb0, unsigned nb1) {
+    const unsigned bid = blockIdx.x;
+    if (bid < nb0) face_mhd<0>(a, (long long)bid * 128 + threadIdx.x);
+    else if (bid < nb0 + nb1) face_mhd<1>(a, (long long)(bid - nb0) * 128 + threadIdx.x);
+    else face_mhd<2>(a, (long long)(bid - nb0 - nb1) * 128 + threadIdx.x);
+}
+
+// MHD decode (e4/fvcell.d:586-822): the ten primitives of each cell, gP cleared.
+__global__ void adj_decode_mhd_kernel(AdjArgs a) {
+    const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (g >= a.total) return;
+    double u[10];
+    for (int q = 0; q < 10; ++q) u[q] = a.U[q * a.total + g];
+    Prim<double> s;
+    double p, T;
+    decode(a.P, u, s, p, T);
+    const double v[NPM] = {s.rho, s.v[0], s.v[1], s.v[2], s.u, s.a, s.B[0], s.B[1], s.B[2], s.psi};
+    for (int m = 0; m < NPM; ++m) { a.Pp[m * a.total + g] = v[m]; a.gP[m * a.total + g] = 0.0; }
+}
+
+// gU = (dP/dU)^T gP for the MHD decode: u = (E - |B|^2/2)/rho - |v|^2/2, B and psi
+// copied, a = sqrt(gamma R u / Cv); divB does not enter the primitives.
+__global__ void adj_back_mhd_kernel(AdjArgs a) {
+    const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (g >= a.total) return;
+    double U[10], gp[NPM];
+    for (int q = 0; q < 10; ++q) U[q] = a.U[q * a.total + g];
+    for (int m = 0; m < NPM; ++m) gp[m] = a.gP[m * a.total + g];
+    const double rho = U[MASS], dinv = 1.0 / rho;
+    const double v0 = U[XMOM] * dinv, v1 = U[YMOM] * dinv, v2 = U[ZMOM] * dinv;
+    const double rE = U[TOTENERGY] - 0.5 * (U[XB] * U[XB] + U[YB] * U[YB] + U[ZB] * U[ZB]);
+    const double u = rE * dinv - 0.5 * (v0 * v0 + v1 * v1 + v2 * v2);
+    const double gR = a.P.gas.gamma * a.P.gas.R;
+    const double aa = sqrt(gR * u * a.P.gas.Cvinv);
+    const double gu = gp[4] + gp[5] * gR * a.P.gas.Cvinv / (2.0 * aa);
+    const double gv0 = gp[1] - gu * v0, gv1 = gp[2] - gu * v1, gv2 = gp[3] - gu * v2;
+    const double gdinv = gu * rE + gv0 * U[XMOM] + gv1 * U[YMOM] + gv2 * U[ZMOM];
+    double r[10];
+    r[MASS] = gp[0] - gdinv * dinv * dinv;
+    r[XMOM] = gv0 * dinv; r[YMOM] = gv1 * dinv; r[ZMOM] = gv2 * dinv;
+    r[TOTENERGY] = gu * dinv;
+    r[XB] = gp[6] - gu * dinv * U[XB];
+    r[YB] = gp[7] - gu * dinv * U[YB];
+    r[ZB] = gp[8] - gu * dinv * U[ZB];
+    r[PSI] = gp[9];
+    r[DIVB] = 0.0;
+    for (int q = 0; q < 10; ++q) a.gU[q * a.total + g] = r[q];
+}
+
 // gU = (dP/dU)^T gP for P = decode(U) (e4/fvcell.d:586-822 with ideal_gas.d:98-139)
 __device__ __forceinline__ void back_cell(const AdjArgs& a, long long g) {
     double U[5];
@@ -1007,20 +1428,39 @@ void launch_faces(const AdjArgs& a, int flux, const unsigned* nb, cudaStream_t s
     else launch_faces_flux<FLUX_AUSMDV>(a, rare, nb, s);
 }
 
-bool vjp_supported(int ctx, const AdjView& v) {
+// residual_only: gdfv_residual_vjp, which also takes MHD (the step and rollout adjoints
+// take the Euler path only)
+bool vjp_supported(int ctx, const AdjView& v, bool residual_only = false) {
     if (!v.prepared) { adjoint_set_error(ctx, "call gdfv_prepare first"); return false; }
-    if (v.mhd || (v.flux != FLUX_AUSMDV && v.flux != FLUX_HLLC)) {
-        adjoint_set_error(ctx, "the adjoint supports the Euler path with flux_calculator=ausmdv or hllc");
+    if (v.mhd) {
+        if (!residual_only) {
+            adjoint_set_error(ctx, "the step and rollout adjoints support the Euler path (the MHD residual "
+                                   "has gdfv_residual_vjp)");
+            return false;
+        }
+        for (const BlockDesc& B : v.h_blocks)
+            for (int f = 0; f < 6; ++f)
+                if (B.bc_type[f] == BC_FIXED_P || B.bc_type[f] == BC_FIXED_PT) {
+                    adjoint_set_error(ctx, "the MHD residual VJP does not take outflow_fixed_p boundaries");
+                    return false;
+                }
+        return true;
+    }
+    if (v.flux != FLUX_AUSMDV && v.flux != FLUX_HLLC) {
+        adjoint_set_error(ctx, "the adjoint supports flux_calculator=ausmdv or hllc (and hlle with MHD in "
+                               "gdfv_residual_vjp)");
         return false;
     }
     return true;
 }
 
-// Scratch layout: P [6][total] | gP [6][total] | b [5][total] | face offsets [3][nblocks+1]
-// | inflow cotangents [ninflow][6].  Face offsets are uploaded once per allocation.
+// Scratch layout, np = 6 primitives (Euler) or 10 (MHD), nq conserved quantities:
+// P [np][total] | gP [np][total] | b [nq][total] | face offsets [3][nblocks+1] | inflow
+// cotangents [ninflow][np].  Face offsets are uploaded once per allocation.
 cudaError_t vjp_setup(const AdjView& v, AdjArgs& a, std::vector<long long>& off) {
     const long long total = v.total;
-    const long long need = 17 * total + 3 * (v.nblocks + 1) + 6 * (long long)v.ninflow + 8;
+    const long long np = v.mhd ? NPM : NP, nq = v.mhd ? 10 : 5;
+    const long long need = (2 * np + nq) * total + 3 * (v.nblocks + 1) + np * (long long)v.ninflow + 8;
     cudaError_t e = cudaSuccess;
     if (*v.scratch_n < need) {
         if (*v.scratch) cudaFree(*v.scratch);
@@ -1037,10 +1477,11 @@ cudaError_t vjp_setup(const AdjView& v, AdjArgs& a, std::vector<long long>& off)
     a.inflow = v.d_inflow;
     a.rot = v.d_rot;
     a.Pp = base;
-    a.gP = base + 6 * total;
-    a.bbuf = base + 12 * total;
-    a.face_off = reinterpret_cast<const long long*>(base + 17 * total);
-    a.gInflow = base + 17 * total + 3 * (v.nblocks + 1);
+    a.gP = base + np * total;
+    a.bbuf = base + 2 * np * total;
+    a.face_off = reinterpret_cast<const long long*>(base + (2 * np + nq) * total);
+    a.gInflow = base + (2 * np + nq) * total + 3 * (v.nblocks + 1);
+    a.c_h = v.c_h;
     a.total = total;
     a.nblocks = v.nblocks;
     a.P = v.P;
@@ -1061,6 +1502,21 @@ cudaError_t vjp_setup(const AdjView& v, AdjArgs& a, std::vector<long long>& off)
         *v.scratch_ready = 1;
     }
     return cudaSuccess;
+}
+
+// The MHD residual VJP: decode, the face sweep of the three directions, reverse decode.
+cudaError_t enqueue_vjp_mhd(const AdjView& v, const AdjArgs& a, const std::vector<long long>& off) {
+    const int nt = 256;
+    const unsigned nb_cells = (unsigned)((v.total + nt - 1) / nt);
+    adj_decode_mhd_kernel<<<nb_cells, nt, 0, v.stream>>>(a);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    unsigned nb[3];
+    for (int d = 0; d < 3; ++d) nb[d] = (unsigned)((off[d * (v.nblocks + 1) + v.nblocks] + 127) / 128);
+    adj_faces_mhd_kernel<<<nb[0] + nb[1] + nb[2], 128, 0, v.stream>>>(a, nb[0], nb[1]);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    adj_back_mhd_kernel<<<nb_cells, nt, 0, v.stream>>>(a);
+    return cudaGetLastError();
 }
 
 // decode, the three face sweeps (cotangents scattered onto gP) and the reverse decode.
@@ -1088,7 +1544,7 @@ extern "C" int gdfv_residual_vjp(int ctx, const double* U_dev, const double* W_d
                                  double* g_inflow_host) {
     AdjView v;
     if (!adjoint_view(ctx, &v)) return GDFV_ERR_ARG;
-    if (!vjp_supported(ctx, v)) return v.prepared ? GDFV_ERR_ARG : GDFV_ERR_STATE;
+    if (!vjp_supported(ctx, v, true)) return v.prepared ? GDFV_ERR_ARG : GDFV_ERR_STATE;
     if (!U_dev || !W_dev || !G_dev) { adjoint_set_error(ctx, "null pointer"); return GDFV_ERR_ARG; }
     AdjArgs a;
     std::vector<long long> off;
@@ -1097,10 +1553,11 @@ extern "C" int gdfv_residual_vjp(int ctx, const double* U_dev, const double* W_d
     a.W = W_dev;
     a.gU = G_dev;
     a.mode = 0;
-    if (e == cudaSuccess && v.ninflow > 0) e = cudaMemsetAsync(a.gInflow, 0, sizeof(double) * 6 * v.ninflow, v.stream);
-    if (e == cudaSuccess) e = enqueue_vjp(v, a, off);
+    const int np = v.mhd ? NPM : NP;
+    if (e == cudaSuccess && v.ninflow > 0) e = cudaMemsetAsync(a.gInflow, 0, sizeof(double) * np * v.ninflow, v.stream);
+    if (e == cudaSuccess) e = v.mhd ? enqueue_vjp_mhd(v, a, off) : enqueue_vjp(v, a, off);
     if (e == cudaSuccess && g_inflow_host && v.ninflow > 0)
-        e = cudaMemcpyAsync(g_inflow_host, a.gInflow, sizeof(double) * 6 * v.ninflow, cudaMemcpyDeviceToHost, v.stream);
+        e = cudaMemcpyAsync(g_inflow_host, a.gInflow, sizeof(double) * np * v.ninflow, cudaMemcpyDeviceToHost, v.stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(v.stream);
     if (e != cudaSuccess) { adjoint_set_error(ctx, cudaGetErrorString(e)); return GDFV_ERR_CUDA; }
     return GDFV_OK;

@@ -36,6 +36,7 @@ struct AdjView {
     const InflowState* d_inflow;
     const double* d_rot;    // exchange rotations (9 doubles each), null if none
     NumParams P;
+    double c_h;             // the GLM wave speed the context holds (MHD residual)
     cudaStream_t stream;
     std::vector<BlockDesc> h_blocks;
     double** scratch;       // context-owned, lazily allocated adjoint buffers

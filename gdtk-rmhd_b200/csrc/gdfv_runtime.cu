@@ -949,6 +949,7 @@ bool adjoint_view(int ctx, AdjView* v) {
     v->d_inflow = c->d_inflow;
     v->d_rot = c->d_rot;
     v->P = c->P;
+    v->c_h = c->h_ctl ? c->h_ctl->c_h : 0.0;
     v->stream = c->stream;
     v->h_blocks = c->h_blocks;
     v->scratch = &c->adj_scratch;

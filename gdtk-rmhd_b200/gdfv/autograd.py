@@ -32,12 +32,13 @@ def _p(t):
 
 
 def vjp(sim, U, W):
-    """G = (dR/dU)^T W and the inflow-state cotangents [n_inflow, 6]."""
+    """G = (dR/dU)^T W and the inflow-state cotangents [n_inflow, 6] (rho, vel, u, a; MHD
+    [n_inflow, 10]: and B, psi)."""
     U = U.contiguous()
     W = W.contiguous()
     G = torch.empty_like(U)
     n_in = max(1, getattr(sim, "n_inflow", 1))
-    gin = torch.zeros((n_in, 6), dtype=torch.float64)
+    gin = torch.zeros((n_in, 10 if sim.nq == 10 else 6), dtype=torch.float64)
     torch.cuda.current_stream().synchronize()
     check(sim.ctx, sim.L.gdfv_residual_vjp(sim.ctx, _p(U), _p(W), _p(G), ffi.cast("double*", gin.data_ptr())))
     return G, gin

@@ -200,10 +200,14 @@ int gdfv_residual_jvp(int ctx, const double* U_dev, const double* v_dev, const d
  * reverse of decode_conserved, interp_l2r2 and ausmdv or hllc, with the branches of
  * the primal values).  g_inflow_host (may be NULL) receives, per supersonic-inflow face
  * state in the order the faces were defined, the cotangent of its ghost state
- * (rho, vel.x, vel.y, vel.z, u, a), 6 doubles each.  Euler (2D or 3D) with
- * flux_calculator=ausmdv or hllc, van_albada_variant e4 or lmr, uniform or graded blocks; every boundary condition of this library, exchanges
- * of any orientation with or without an Rmatrix (the cotangent goes back through its
- * transpose) and the outflow boundaries with their own ghost or flux rule included.  It is the transpose of the Jacobian-vector products of
+ * (rho, vel.x, vel.y, vel.z, u, a), 6 doubles each (MHD: and B.x, B.y, B.z, psi, 10
+ * each).  Euler (2D or 3D) with flux_calculator=ausmdv or hllc, van_albada_variant e4 or
+ * lmr, uniform or graded blocks, every boundary condition of this library: exchanges of
+ * any orientation with or without an Rmatrix (the cotangent goes back through its
+ * transpose) and the outflow boundaries with their own ghost or flux rule included.
+ * MHD with hlle and GLM, the context's current c_h held fixed, every boundary condition
+ * the MHD forward takes except outflow_fixed_p and outflow_fixed_p_and_t
+ * (GDFV_ERR_ARG).  It is the transpose of the Jacobian-vector products of
  * e4/steadystate_core.d:1870-2060 (evalJacobianVecProd), which it is checked against. */
 int gdfv_residual_vjp(int ctx, const double* U_dev, const double* W_dev, double* G_dev, double* g_inflow_host);
 

@@ -157,9 +157,13 @@ def sod_eilmer(nic=100):
     return c
 
 
-def mhd_shock_tube(N=512):
+def mhd_shock_tube(N=512, noise=0.0, seed=5):
     """examples/eilmer/2D/MHDShockTube/MHDShockTube.lua (Dai & Woodward problem 3):
-    2D, two 256x3 blocks, hlle MHD without cleaning, stringent CFL, ideal He."""
+    2D, two 256x3 blocks, hlle MHD without cleaning, stringent CFL, ideal He.
+    noise > 0 multiplies rho, T and every velocity and B component cell by cell by
+    (1 + noise * N(0, 1)): a state off the piecewise residual's switch points, where
+    the uniform regions would otherwise meet the disturbed ones one ulp apart."""
+    rng = np.random.default_rng(seed)
     c = Case("mhd_tube", dict(flux_calculator="hlle", MHD=1, divergence_cleaning=0, dimensions=2,
                               stringent_cfl=1, cfl_value=0.5, dt_init=1e-5), R_HE, 5.0 / 3.0)
     nic, njc = N // 2, 3
@@ -171,6 +175,11 @@ def mhd_shock_tube(N=512):
         B = (Bx, s4, -s4) if side == 0 else (Bx, s4, s4)
         rho, p = 1.0, 1.0
         T = p / (rho * R_HE)
+        if noise > 0.0:
+            shp = (1, njc, nic)
+            jit = lambda x: x * (1.0 + noise * rng.standard_normal(shp))
+            rho, T = jit(rho), jit(T)
+            vel, B = tuple(jit(x) for x in vel), tuple(jit(x) for x in B)
         bcs = {"north": ("exchange_over_full_face", dict(other=side, other_face="south")),
                "south": ("exchange_over_full_face", dict(other=side, other_face="north"))}
         if side == 0:

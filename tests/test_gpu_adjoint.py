@@ -32,6 +32,8 @@ def _gpu_to_oracle_layout(case, X):
 def _state_after(case, nsteps):
     orc, sim = cases.build_pair(case)
     assert sim.run(max_step=nsteps) == nsteps
+    if case.mhd:   # the oracle takes the same steps, so that both hold the same c_h
+        assert orc.run(nsteps) == 0
     U = np.concatenate([sim.get_conserved(b) for b in range(len(case.blocks))], axis=1)
     for b in range(len(case.blocks)):   # the oracle evaluates at the same state
         assert orc.set_U(b, sim.get_conserved(b)) == 0
@@ -95,6 +97,22 @@ def test_vjp_transpose_graded_blocks(flux):
     _dot_check(cases.graded_inflow_box(flux=flux), 6, 1e-10, seed=13)
     if flux == "ausmdv":
         _dot_check(cases.graded_lattice(), 6, 1e-10, seed=14)
+
+
+@pytest.mark.parametrize("case_name", ["orszag_tang", "orszag_tang_no_cleaning", "slip_dipole", "shock_tube_2d"])
+def test_vjp_transpose_mhd(case_name):
+    """The MHD residual (hlle with GLM, e4/fluxcalc.d:54-187, :1608-1780): the reverse of
+    the fast magnetosonic speeds, the one-sided fluxes and jumps, the GLM terms of F[B]
+    and F[psi] and F[divB], the MHD decode; periodic exchange (Orszag-Tang, with and
+    without divergence cleaning), slip walls whose ghosts carry the dipole field, and the
+    2D MHD shock tube (extrapolation and exchange; its states jittered, since the plain
+    tube's uniform regions meet the disturbed ones one ulp apart, where the clipping
+    switches follow each side's own rounding).  c_h is the context's, frozen."""
+    case = {"orszag_tang": lambda: cases.orszag_tang(n=(24, 24, 4)),
+            "orszag_tang_no_cleaning": lambda: cases.orszag_tang(n=(24, 24, 4), cleaning=False),
+            "slip_dipole": lambda: cases.mhd_slip_dipole(n=(24, 20, 4)),
+            "shock_tube_2d": lambda: cases.mhd_shock_tube(N=64, noise=0.01)}[case_name]()
+    _dot_check(case, 4, 1e-10, seed=16)
 
 
 def test_vjp_transpose_lmr_limiter():
