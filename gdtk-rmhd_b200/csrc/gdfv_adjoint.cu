@@ -1317,9 +1317,7 @@ __global__ void __launch_bounds__(128) adj_faces_mhd_kernel(AdjArgs a, unsigned 
 }
 
 // MHD decode (e4/fvcell.d:586-822): the ten primitives of each cell, gP cleared.
-__global__ void adj_decode_mhd_kernel(AdjArgs a) {
-    const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (g >= a.total) return;
+__device__ __forceinline__ void decode_cell_mhd(const AdjArgs& a, long long g) {
     double u[10];
     for (int q = 0; q < 10; ++q) u[q] = a.U[q * a.total + g];
     Prim<double> s;
@@ -1329,11 +1327,16 @@ __global__ void adj_decode_mhd_kernel(AdjArgs a) {
     for (int m = 0; m < NPM; ++m) { a.Pp[m * a.total + g] = v[m]; a.gP[m * a.total + g] = 0.0; }
 }
 
-// gU = (dP/dU)^T gP for the MHD decode: u = (E - |B|^2/2)/rho - |v|^2/2, B and psi
-// copied, a = sqrt(gamma R u / Cv); divB does not enter the primitives.
-__global__ void adj_back_mhd_kernel(AdjArgs a) {
+__global__ void adj_decode_mhd_kernel(AdjArgs a) {
     const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (g >= a.total) return;
+    if (g < a.total) decode_cell_mhd(a, g);
+}
+
+// gU = (dP/dU)^T gP for the MHD decode: u = (E - |B|^2/2)/rho - |v|^2/2, B and psi
+// copied, a = sqrt(gamma R u / Cv); divB does not enter the primitives.  The modes
+// of back_cell (the predictor-corrector adjoint's lam and b updates) over ten
+// conserved quantities.
+__device__ __forceinline__ void back_cell_mhd(const AdjArgs& a, long long g) {
     double U[10], gp[NPM];
     for (int q = 0; q < 10; ++q) U[q] = a.U[q * a.total + g];
     for (int m = 0; m < NPM; ++m) gp[m] = a.gP[m * a.total + g];
@@ -1355,7 +1358,29 @@ __global__ void adj_back_mhd_kernel(AdjArgs a) {
     r[ZB] = gp[8] - gu * dinv * U[ZB];
     r[PSI] = gp[9];
     r[DIVB] = 0.0;
-    for (int q = 0; q < 10; ++q) a.gU[q * a.total + g] = r[q];
+    if (a.mode == 0) {
+        for (int q = 0; q < 10; ++q) a.gU[q * a.total + g] = r[q];
+    } else if (a.mode == 1) {
+        for (int q = 0; q < 10; ++q) {
+            const double l = a.lam[q * a.total + g];
+            a.bbuf[q * a.total + g] = 0.5 * a.dt * l + a.dt * r[q];
+            a.lam[q * a.total + g] = l + r[q];
+        }
+    } else {
+        for (int q = 0; q < 10; ++q) a.lam[q * a.total + g] += r[q];
+    }
+}
+
+__global__ void adj_back_mhd_kernel(AdjArgs a) {
+    const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (g < a.total) back_cell_mhd(a, g);
+}
+
+__global__ void adj_back_decode_mhd_kernel(AdjArgs back, AdjArgs next) {
+    const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (g >= back.total) return;
+    back_cell_mhd(back, g);
+    decode_cell_mhd(next, g);
 }
 
 // gU = (dP/dU)^T gP for P = decode(U) (e4/fvcell.d:586-822 with ideal_gas.d:98-139)
@@ -1428,14 +1453,15 @@ void launch_faces(const AdjArgs& a, int flux, const unsigned* nb, cudaStream_t s
     else launch_faces_flux<FLUX_AUSMDV>(a, rare, nb, s);
 }
 
-// residual_only: gdfv_residual_vjp, which also takes MHD (the step and rollout adjoints
-// take the Euler path only)
+// residual_only: gdfv_residual_vjp, which takes MHD with GLM cleaning too (the step and
+// rollout adjoints take MHD without cleaning: with it each step's c_h and psi damping
+// would enter)
 bool vjp_supported(int ctx, const AdjView& v, bool residual_only = false) {
     if (!v.prepared) { adjoint_set_error(ctx, "call gdfv_prepare first"); return false; }
     if (v.mhd) {
-        if (!residual_only) {
-            adjoint_set_error(ctx, "the step and rollout adjoints support the Euler path (the MHD residual "
-                                   "has gdfv_residual_vjp)");
+        if (!residual_only && v.P.divergence_cleaning) {
+            adjoint_set_error(ctx, "the MHD step and rollout adjoints take divergence_cleaning = 0 (with GLM "
+                                   "cleaning only the residual has a VJP, gdfv_residual_vjp)");
             return false;
         }
         for (const BlockDesc& B : v.h_blocks)
@@ -1566,20 +1592,27 @@ extern "C" int gdfv_residual_vjp(int ctx, const double* U_dev, const double* W_d
 namespace {
 
 // A chain of products: the reverse decode of each product runs fused with the
-// decode of the next one (adj_back_decode_kernel); finish() ends the chain.
+// decode of the next one (adj_back_decode_kernel, or its MHD form); finish() ends
+// the chain.
 struct VjpChain {
     bool pending = false;
     AdjArgs back{};
     cudaError_t product(const AdjView& v, const AdjArgs& a, const std::vector<long long>& off) {
         const int nt = 256;
         const unsigned nb_cells = (unsigned)((v.total + nt - 1) / nt);
-        if (pending) adj_back_decode_kernel<<<nb_cells, nt, 0, v.stream>>>(back, a);
-        else adj_decode_kernel<<<nb_cells, nt, 0, v.stream>>>(a);
+        if (v.mhd) {
+            if (pending) adj_back_decode_mhd_kernel<<<nb_cells, nt, 0, v.stream>>>(back, a);
+            else adj_decode_mhd_kernel<<<nb_cells, nt, 0, v.stream>>>(a);
+        } else {
+            if (pending) adj_back_decode_kernel<<<nb_cells, nt, 0, v.stream>>>(back, a);
+            else adj_decode_kernel<<<nb_cells, nt, 0, v.stream>>>(a);
+        }
         cudaError_t e = cudaGetLastError();
         if (e == cudaSuccess) {
             unsigned nb[3];
             for (int d = 0; d < 3; ++d) nb[d] = (unsigned)((off[d * (v.nblocks + 1) + v.nblocks] + 127) / 128);
-            launch_faces(a, v.flux, nb, v.stream);
+            if (v.mhd) adj_faces_mhd_kernel<<<nb[0] + nb[1] + nb[2], 128, 0, v.stream>>>(a, nb[0], nb[1]);
+            else launch_faces(a, v.flux, nb, v.stream);
             e = cudaGetLastError();
         }
         back = a;
@@ -1590,7 +1623,9 @@ struct VjpChain {
         if (!pending) return cudaSuccess;
         pending = false;
         const int nt = 256;
-        adj_decode_back_kernel<<<(unsigned)((v.total + nt - 1) / nt), nt, 0, v.stream>>>(back);
+        const unsigned nb_cells = (unsigned)((v.total + nt - 1) / nt);
+        if (v.mhd) adj_back_mhd_kernel<<<nb_cells, nt, 0, v.stream>>>(back);
+        else adj_decode_back_kernel<<<nb_cells, nt, 0, v.stream>>>(back);
         return cudaGetLastError();
     }
 };

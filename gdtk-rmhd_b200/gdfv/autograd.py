@@ -19,7 +19,9 @@
       U1 = U0 + dt R(U0),  U2 = U0 + dt (R(U0)/2 + R(U1)/2)
       mu  = J(U1)^T (dt/2 lam)
       lam <- lam + mu + J(U0)^T (dt/2 lam + dt mu)
-  with dt frozen at its forward value (the CFL rule is not differentiated).
+  with dt frozen at its forward value (the CFL rule is not differentiated).  MHD
+  rollouts take this path without divergence cleaning (hlle; with GLM cleaning each
+  step's c_h and psi damping would enter, and only the residual has a VJP).
 Tensors are float64 on the simulation's device, shaped [nq, total cells].
 """
 import torch
@@ -90,7 +92,7 @@ def steps_dt(sim, U, dts, outs, preds):
 def step_adjoint(sim, U0, U1, dt, lam, gin):
     """lam <- (dU2/dU0)^T lam for the predictor-corrector step U0 -> U2 of frozen dt
     (U1 its predictor state), in place; inflow cotangents added into gin [n_inflow, 6]
-    on the device.  Enqueued without a host synchronisation."""
+    (MHD: [n_inflow, 10]) on the device.  Enqueued without a host synchronisation."""
     check(sim.ctx, sim.L.gdfv_step_adjoint(sim.ctx, _p(U0), _p(U1), float(dt), _p(lam), _p(gin)))
 
 
@@ -114,12 +116,13 @@ def residual(sim, U):
 
 def inflow_chain(sim, theta, gprim):
     """d/d(p, T, vel.x) of an inflow ghost state (FlowState:new{p=,T=}: rho = p/(R T),
-    u = Cv T, a = sqrt(gamma R T)) from its cotangent (rho, vx, vy, vz, u, a)."""
+    u = Cv T, a = sqrt(gamma R T)) from its cotangent (rho, vx, vy, vz, u, a; an MHD
+    state's B and psi cotangents follow and do not enter)."""
     p, T, _ = [float(x) for x in theta]
     R, g = sim.gas.R, sim.gas.gamma
     Cv = R / (g - 1.0)
     a = (g * R * T) ** 0.5
-    gr, gvx, _, _, gu, ga = [float(x) for x in gprim]
+    gr, gvx, _, _, gu, ga = [float(x) for x in gprim[:6]]
     dp = gr / (R * T)
     dT = gr * (-p / (R * T * T)) + gu * Cv + ga * g * R / (2.0 * a)
     return torch.tensor([dp, dT, gvx], dtype=torch.float64)
@@ -196,7 +199,9 @@ class Rollout(torch.autograd.Function):
     def backward(ctx, gUN):
         sim, dts, ckpts, K = ctx.sim, ctx.dts, ctx.ckpts, ctx.k
         lam = gUN.contiguous().clone()
-        gin = torch.zeros((max(1, getattr(sim, "n_inflow", 1)), 6), dtype=torch.float64, device=lam.device)
+        # the inflow ghost state's cotangents: rho, vel, u, a (MHD: and B, psi)
+        gin = torch.zeros((max(1, getattr(sim, "n_inflow", 1)), 10 if sim.nq == 10 else 6), dtype=torch.float64,
+                          device=lam.device)
         nseg = (len(dts) + K - 1) // K
         pc = ffi.new("double*[]", [_p(ckpts[s * K]) for s in range(nseg)])
         sets = ctx.work if len(ctx.work) == 4 * K else ctx.work + ctx.work

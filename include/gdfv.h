@@ -231,9 +231,10 @@ int gdfv_steps_dt(int ctx, const double* U_in_dev, double* const* U_out_dev, dou
  * and U1 (its predictor state): lam <- lam + mu + (dR/dU(U0))^T (dt/2 lam + dt mu)
  * with mu = (dR/dU(U1))^T (dt/2 lam), in place on the device array lam [nq][total].
  * The inflow ghost-state cotangents of both products are added into g_inflow_dev
- * (device, [n_inflow][6], caller-zeroed).  Enqueued on the context's stream with
- * no host synchronisation.  Same scope as gdfv_residual_vjp; no reference
- * counterpart. */
+ * (device, [n_inflow][6], MHD [n_inflow][10], caller-zeroed).  Enqueued on the
+ * context's stream with no host synchronisation.  Same scope as gdfv_residual_vjp,
+ * except that MHD takes divergence_cleaning = 0 only (GDFV_ERR_ARG otherwise: with
+ * cleaning the step's c_h and psi damping would enter); no reference counterpart. */
 int gdfv_step_adjoint(int ctx, const double* U0_dev, const double* U1_dev, double dt, double* lam_dev,
                       double* g_inflow_dev);
 
@@ -248,7 +249,7 @@ int gdfv_step_adjoint(int ctx, const double* U0_dev, const double* U1_dev, doubl
  * after both finish.  last_ready != 0: the first set already holds the last
  * segment's states and predictor states (kept by the forward pass, see
  * gdfv_last_predictor_state), which are then not recomputed.  Same scope as
- * gdfv_residual_vjp; no reference counterpart. */
+ * gdfv_step_adjoint; no reference counterpart. */
 int gdfv_rollout_adjoint(int ctx, const double* const* ckpt_dev, int n_ckpt, const double* dts, int nsteps,
                          int checkpoint_every, double* const* work_dev, int last_ready, double* lam_dev,
                          double* g_inflow_dev);

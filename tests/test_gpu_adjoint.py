@@ -236,6 +236,64 @@ def test_rollout_gradients_smooth_configuration():
                       ((1e-6, 1e-4), (1e-7, 2e-5)))
 
 
+@pytest.mark.parametrize("checkpoint_every", [5, None])
+def test_rollout_gradients_mhd_without_cleaning(checkpoint_every):
+    """MHD rollouts (hlle, no divergence cleaning): the step adjoint's chain through the
+    MHD decode, face and reverse-decode kernels, checkpointed (every 5 of 12 steps) and
+    resident.  Orszag-Tang 24x24x4 in the smooth configuration (limiter and clipping
+    off, so that central differences converge quadratically); J = <W, U_N> with fixed
+    random weights; the forward's dt sequence replayed for the differences."""
+    from gdfv.autograd import rollout, step_dt
+    case = cases.orszag_tang(n=(24, 24, 4), cleaning=False)
+    case.config.update(apply_limiter=False, extrema_clipping=False)
+    _, sim = cases.build_pair(case)
+    U0 = torch.from_numpy(sim.get_conserved(0)).cuda()
+    rng = np.random.default_rng(11)
+    W = torch.from_numpy(rng.standard_normal(tuple(U0.shape))).cuda()
+    theta = torch.tensor([1.0, 1.0, 0.0], dtype=torch.float64, requires_grad=True)   # no inflow faces
+    U0r = U0.clone().requires_grad_(True)
+    nsteps = 12
+    UN = rollout(sim, U0r, theta, nsteps, checkpoint_every)
+    (UN * W).sum().backward()
+    gU0 = U0r.grad.detach()
+    assert float(theta.grad.abs().sum()) == 0.0
+    _, sim_r = cases.build_pair(case)
+    dts = []
+    for _ in range(nsteps):
+        sim_r.run(max_step=1)
+        dts.append(sim_r.time()["dt"])
+
+    def J_of(U):
+        X = U
+        for dt in dts:
+            X = step_dt(sim_r, X, dt)
+        return float((X * W).sum())
+
+    assert abs(J_of(U0) - float((UN.detach() * W).sum())) <= 1e-12 * abs(J_of(U0))
+    scale = torch.from_numpy(np.abs(U0.cpu().numpy()).max(axis=1, keepdims=True)).cuda()
+    scale[9] = 1.0   # divB starts at 0
+    for trial in range(2):
+        v = torch.from_numpy(rng.standard_normal(tuple(U0.shape))).cuda() * scale
+        ad = float((gU0 * v).sum())
+        h = 1e-6
+        fd = (J_of(U0 + h * v) - J_of(U0 - h * v)) / (2 * h)
+        assert abs(fd - ad) <= 1e-5 * max(abs(fd), abs(ad)), (trial, fd, ad)
+
+
+def test_mhd_rollout_with_cleaning_is_refused():
+    """With GLM cleaning each step's c_h and psi damping would enter the step adjoint:
+    the rollout's backward reports it instead of returning a wrong gradient."""
+    from gdfv._lib import GdfvError
+    from gdfv.autograd import rollout
+    case = cases.orszag_tang(n=(16, 16, 4))
+    _, sim = cases.build_pair(case)
+    U0 = torch.from_numpy(sim.get_conserved(0)).cuda().requires_grad_(True)
+    theta = torch.tensor([1.0, 1.0, 0.0], dtype=torch.float64, requires_grad=True)
+    UN = rollout(sim, U0, theta, 3, 3)
+    with pytest.raises(GdfvError, match="divergence_cleaning"):
+        UN.sum().backward()
+
+
 def test_rollout_theta_drives_every_inflow_face():
     """The rollout's inflow state theta = (p, T, vel.x) is the state of every
     supersonic-inflow face in the forward: at a theta other than the configured one,
