@@ -735,6 +735,10 @@ struct AdjArgs {
     int mode;          // 0: gU = result; 1: mu -> bbuf, lam += mu; 2: lam += result
     NumParams P;
     double c_h;        // MHD: the GLM wave speed of the residual (the context's current one)
+    // MHD with cleaning in a step adjoint: {c_h, psi damping factor} of the step (device;
+    // null: c_h above, no damping); chd_slot is where the step adjoint forms them
+    const double* chd;
+    double* chd_slot;
 };
 
 __device__ __forceinline__ void decode_cell(const AdjArgs& a, long long g) {
@@ -1265,7 +1269,7 @@ __device__ void face_mhd(const AdjArgs& a, long long f) {
     double gpsiL = 0.0, gpsiR = 0.0;
     gR.Bx += 0.5 * gF[DIVB]; gL.Bx -= 0.5 * gF[DIVB];
     if (clean) {
-        const double ch = a.c_h;
+        const double ch = a.chd ? a.chd[0] : a.c_h;
         const double gt3 = P.glm_reference_indexing ? gF[XB] : gF[ZB];
         const double gpa = gF[XB] + gF[YB] + gt3;
         gR.Bx -= 0.5 * ch * gF[XB]; gL.Bx += 0.5 * ch * gF[XB];
@@ -1320,6 +1324,13 @@ __global__ void __launch_bounds__(128) adj_faces_mhd_kernel(AdjArgs a, unsigned 
 __device__ __forceinline__ void decode_cell_mhd(const AdjArgs& a, long long g) {
     double u[10];
     for (int q = 0; q < 10; ++q) u[q] = a.U[q * a.total + g];
+    if (a.mode == 1 && a.chd) {
+        // the corrector's stencils read the predictor state with psi damped, U1' = D U1
+        // (D: psi times the step's damping factor), and its cotangent is D lam
+        const double damp = a.chd[1];
+        u[PSI] *= damp;
+        a.lam[PSI * a.total + g] *= damp;
+    }
     Prim<double> s;
     double p, T;
     decode(a.P, u, s, p, T);
@@ -1361,6 +1372,7 @@ __device__ __forceinline__ void back_cell_mhd(const AdjArgs& a, long long g) {
     if (a.mode == 0) {
         for (int q = 0; q < 10; ++q) a.gU[q * a.total + g] = r[q];
     } else if (a.mode == 1) {
+        if (a.chd) r[PSI] *= a.chd[1];   // mu is the cotangent of U1' = D U1: D mu is U1's
         for (int q = 0; q < 10; ++q) {
             const double l = a.lam[q * a.total + g];
             a.bbuf[q * a.total + g] = 0.5 * a.dt * l + a.dt * r[q];
@@ -1453,17 +1465,10 @@ void launch_faces(const AdjArgs& a, int flux, const unsigned* nb, cudaStream_t s
     else launch_faces_flux<FLUX_AUSMDV>(a, rare, nb, s);
 }
 
-// residual_only: gdfv_residual_vjp, which takes MHD with GLM cleaning too (the step and
-// rollout adjoints take MHD without cleaning: with it each step's c_h and psi damping
-// would enter)
-bool vjp_supported(int ctx, const AdjView& v, bool residual_only = false) {
+// The forms the VJP, step and rollout adjoints take.
+bool vjp_supported(int ctx, const AdjView& v) {
     if (!v.prepared) { adjoint_set_error(ctx, "call gdfv_prepare first"); return false; }
     if (v.mhd) {
-        if (!residual_only && v.P.divergence_cleaning) {
-            adjoint_set_error(ctx, "the MHD step and rollout adjoints take divergence_cleaning = 0 (with GLM "
-                                   "cleaning only the residual has a VJP, gdfv_residual_vjp)");
-            return false;
-        }
         for (const BlockDesc& B : v.h_blocks)
             for (int f = 0; f < 6; ++f)
                 if (B.bc_type[f] == BC_FIXED_P || B.bc_type[f] == BC_FIXED_PT) {
@@ -1507,6 +1512,7 @@ cudaError_t vjp_setup(const AdjView& v, AdjArgs& a, std::vector<long long>& off)
     a.bbuf = base + 2 * np * total;
     a.face_off = reinterpret_cast<const long long*>(base + (2 * np + nq) * total);
     a.gInflow = base + (2 * np + nq) * total + 3 * (v.nblocks + 1);
+    a.chd_slot = a.gInflow + np * v.ninflow;   // two doubles of the tail
     a.c_h = v.c_h;
     a.total = total;
     a.nblocks = v.nblocks;
@@ -1570,7 +1576,7 @@ extern "C" int gdfv_residual_vjp(int ctx, const double* U_dev, const double* W_d
                                  double* g_inflow_host) {
     AdjView v;
     if (!adjoint_view(ctx, &v)) return GDFV_ERR_ARG;
-    if (!vjp_supported(ctx, v, true)) return v.prepared ? GDFV_ERR_ARG : GDFV_ERR_STATE;
+    if (!vjp_supported(ctx, v)) return v.prepared ? GDFV_ERR_ARG : GDFV_ERR_STATE;
     if (!U_dev || !W_dev || !G_dev) { adjoint_set_error(ctx, "null pointer"); return GDFV_ERR_ARG; }
     AdjArgs a;
     std::vector<long long> off;
@@ -1632,8 +1638,20 @@ struct VjpChain {
 
 // The adjoint of one predictor-corrector step, enqueued on v.stream:
 // mu = J(U1)^T (dt/2 lam); b = dt/2 lam + dt mu; lam += mu; then lam += J(U0)^T b.
-cudaError_t enqueue_step_adjoint(const AdjView& v, AdjArgs a, const std::vector<long long>& off, const double* U0,
-                                 const double* U1, double dt, double* lam, VjpChain& chain) {
+// MHD with cleaning: the step's c_h and psi damping factor are formed first from U0
+// (as gdfv_run forms them at the step's start); the corrector evaluated R at U1 with
+// psi damped, and damped psi again in U2:
+//   U2 = D (U0 + dt/2 R(U0) + dt/2 R(D U1)),  U1 = U0 + dt R(U0),
+// so lam' = D lam, mu = J(D U1)^T (dt/2 lam'), b = dt/2 lam' + dt D mu,
+// lam <- lam' + D mu + J(U0)^T b (the mode-1 decode and reverse decode apply D).
+cudaError_t enqueue_step_adjoint(int ctx, const AdjView& v, AdjArgs a, const std::vector<long long>& off,
+                                 const double* U0, const double* U1, double dt, double* lam, VjpChain& chain) {
+    a.chd = nullptr;
+    if (v.mhd && v.P.divergence_cleaning) {
+        cudaError_t e = enqueue_step_ch(ctx, v.stream, U0, dt, a.chd_slot);
+        if (e != cudaSuccess) return e;
+        a.chd = a.chd_slot;
+    }
     a.lam = lam;
     a.dt = dt;
     a.U = U1;
@@ -1660,12 +1678,16 @@ extern "C" int gdfv_step_adjoint(int ctx, const double* U0_dev, const double* U1
         adjoint_set_error(ctx, "gdfv_step_adjoint needs U0, U1, lam (and g_inflow with inflow faces) and dt > 0");
         return GDFV_ERR_ARG;
     }
+    if (v.mhd && v.P.divergence_cleaning) {   // the scan scratch of the step's c_h
+        const int st = steps_dt_prepare(ctx);
+        if (st) return st;
+    }
     AdjArgs a;
     std::vector<long long> off;
     cudaError_t e = vjp_setup(v, a, off);
     if (v.ninflow > 0) a.gInflow = g_inflow_dev;
     VjpChain chain;
-    if (e == cudaSuccess) e = enqueue_step_adjoint(v, a, off, U0_dev, U1_dev, dt, lam_dev, chain);
+    if (e == cudaSuccess) e = enqueue_step_adjoint(ctx, v, a, off, U0_dev, U1_dev, dt, lam_dev, chain);
     if (e == cudaSuccess) e = chain.finish(v);
     if (e != cudaSuccess) { adjoint_set_error(ctx, cudaGetErrorString(e)); return GDFV_ERR_CUDA; }
     return GDFV_OK;
@@ -1735,7 +1757,7 @@ extern "C" int gdfv_rollout_adjoint(int ctx, const double* const* ckpt_dev, int 
         double* const* preds = work_dev + 2 * K * p + K;
         for (int n = seg_len(s) - 1; n >= 0 && e == cudaSuccess; --n) {
             const double* U0 = n == 0 ? ckpt_dev[s] : outs[n - 1];
-            e = enqueue_step_adjoint(vh, a, off, U0, preds[n], dts[(size_t)s * K + n], lam_dev, chain);
+            e = enqueue_step_adjoint(ctx, vh, a, off, U0, preds[n], dts[(size_t)s * K + n], lam_dev, chain);
         }
         // each segment ends its chain, so that every reader of the set precedes adj_done
         if (e == cudaSuccess) e = chain.finish(vh);

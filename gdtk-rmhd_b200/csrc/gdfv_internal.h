@@ -51,6 +51,7 @@ int steps_dt_prepare(int ctx);
 cudaError_t enqueue_steps_dt(int ctx, cudaStream_t stream, const double* U_in, double* const* U_out,
                              double* const* U1_out, const double* dts, int n, bool fresh);
 int steps_dt_status(int ctx, cudaStream_t stream);
+cudaError_t enqueue_step_ch(int ctx, cudaStream_t stream, const double* U, double dt, double* out);
 cudaStream_t context_aux_stream(int ctx, int which);
 
 }  // namespace gdfv

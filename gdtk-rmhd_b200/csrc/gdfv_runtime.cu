@@ -276,6 +276,9 @@ struct Context {
     Control* step_ctl = nullptr;       // control record of gdfv_step_dt
     unsigned long long* step_maxsig = nullptr;
     double* step_lastsig = nullptr;
+    unsigned long long* ch_maxsig = nullptr;   // signal scan of the MHD step adjoint (its own stream)
+    double* ch_lastsig = nullptr;
+    int* ch_bad = nullptr;
 
     ~Context() {
         if (graph) cudaGraphExecDestroy(graph);
@@ -283,7 +286,8 @@ struct Context {
         for (void* p : {(void*)U[0], (void*)U[1], (void*)dU0, (void*)d_blocks, (void*)d_tiles, (void*)d_inflow,
                         (void*)d_ctl, (void*)d_maxsig, (void*)d_lastsig, (void*)d_bad, (void*)adj_scratch, (void*)jvp_scratch,
                         (void*)norm_scratch, (void*)prim[0], (void*)prim[1], (void*)prim1, (void*)d_geom, (void*)d_rot, (void*)d_rec,
-                        (void*)step_ctl, (void*)step_maxsig, (void*)step_lastsig})
+                        (void*)step_ctl, (void*)step_maxsig, (void*)step_lastsig, (void*)ch_maxsig,
+                        (void*)ch_lastsig, (void*)ch_bad})
             if (p) cudaFree(p);
         if (h_ctl) cudaFreeHost(h_ctl);
         for (cudaStream_t s : aux_stream)
@@ -431,6 +435,23 @@ cudaError_t enqueue_step(Context* c) {
     return cudaGetLastError();
 }
 
+// Scratch of the fixed-dt steps and the autotuner's trial steps (control record,
+// signal maxima), and of the MHD step adjoint's signal scans; allocated on first use.
+int step_scratch(Context* c) {
+    if (c->step_ctl) return 0;
+    const size_t nb = c->blocks.size();
+    if (cudaMalloc(&c->step_ctl, sizeof(Control)) != cudaSuccess ||
+        cudaMalloc(&c->step_maxsig, sizeof(unsigned long long) * nb) != cudaSuccess ||
+        cudaMalloc(&c->step_lastsig, sizeof(double) * nb) != cudaSuccess ||
+        cudaMalloc(&c->ch_maxsig, sizeof(unsigned long long) * nb) != cudaSuccess ||
+        cudaMalloc(&c->ch_lastsig, sizeof(double) * nb) != cudaSuccess ||
+        cudaMalloc(&c->ch_bad, sizeof(int)) != cudaSuccess) {
+        fail(c, GDFV_ERR_CUDA, "cudaMalloc of the step scratch failed");
+        return 1;
+    }
+    return 0;
+}
+
 // Per-block signal maxima of the current state (needed by the first dt check).
 int scan_signal(Context* c) {
     CK(cudaMemsetAsync(c->d_maxsig, 0, sizeof(unsigned long long) * c->blocks.size(), c->stream));
@@ -451,6 +472,20 @@ int scan_signal(Context* c) {
     if (bad) return fail(c, GDFV_ERR_ARG, "state contains cells that do not decode");
     c->signal_valid = true;
     return GDFV_OK;
+}
+
+// Per-block signal maxima of the state U into maxsig, enqueued on s (no host
+// synchronisation; cells that do not decode are counted in *bad and left out).
+cudaError_t enqueue_signal_scan(Context* c, cudaStream_t s, const double* U, unsigned long long* maxsig,
+                                double* lastsig, int* bad) {
+    cudaError_t e = cudaMemsetAsync(maxsig, 0, sizeof(unsigned long long) * c->blocks.size(), s);
+    for (size_t b = 0; b < c->blocks.size() && e == cudaSuccess; ++b) {
+        const long long n = (long long)c->blocks[b].n[0] * c->blocks[b].n[1] * c->blocks[b].n[2];
+        signal_scan_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(U, c->total, c->d_blocks, (int)b, c->P, maxsig,
+                                                                        lastsig, bad);
+        e = cudaGetLastError();
+    }
+    return e;
 }
 
 void fill_weights(double len, double* w) {
@@ -1119,6 +1154,42 @@ __global__ void step_dt_next_kernel(Control* c, double dt) {
     c->step = 0;
 }
 
+// c_h of a step of dt from the per-block signal maxima of its start state, with the
+// operations of step_begin_kernel (e4/simcore.d:1625-1648, e4/fluidblock.d:975-995);
+// the maxima are cleared for the next reduction.
+__device__ double ch_from_maxsig(const BlockDesc* blocks, unsigned long long* maxsig, int nblocks, double dt) {
+    double c_h = 0.0;
+    for (int b = 0; b < nblocks; ++b) {
+        const double smax = __longlong_as_double((long long)maxsig[b]);
+        const double cfl_max = smax * dt;
+        const double ch = cfl_max * blocks[b].L_min / dt;
+        c_h = b == 0 ? ch : fmin(ch, c_h);
+        maxsig[b] = 0ull;
+    }
+    return c_h;
+}
+
+// The next fixed-dt step of an MHD chain with divergence cleaning: dt and its c_h.
+__global__ void step_dt_ch_kernel(Control* c, const BlockDesc* blocks, unsigned long long* maxsig, int nblocks,
+                                  double dt) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    c->dt_global = dt;
+    c->step = 0;
+    c->c_h = ch_from_maxsig(blocks, maxsig, nblocks, dt);
+}
+
+// c_h of a step of dt and the psi damping factor the stages take from it
+// (e4/fvcell.d:1068-1074, the stage kernels' operations): out[0], out[1].
+__global__ void step_ch_damp_kernel(const BlockDesc* blocks, unsigned long long* maxsig, int nblocks, double dt,
+                                    double damping_length, double* out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const double c_h = ch_from_maxsig(blocks, maxsig, nblocks, dt);
+    const double c_h2 = c_h * c_h;
+    const double c_p2 = 0.18 * damping_length * c_h;
+    out[0] = c_h;
+    out[1] = exp(-(c_h2 / c_p2) * dt);
+}
+
 }  // namespace gdfv
 
 // ====================================================================== C ABI
@@ -1481,11 +1552,7 @@ namespace gdfv {
 int steps_dt_prepare(int ctx) {
     Context* c = get_ctx(ctx);
     if (!c) return GDFV_ERR_ARG;
-    if (!c->step_ctl) {
-        CK(cudaMalloc(&c->step_ctl, sizeof(Control)));
-        CK(cudaMalloc(&c->step_maxsig, sizeof(unsigned long long) * c->blocks.size()));
-        CK(cudaMalloc(&c->step_lastsig, sizeof(double) * c->blocks.size()));
-    }
+    if (step_scratch(c)) return GDFV_ERR_CUDA;
     if (read_ctl(c)) return GDFV_ERR_CUDA;
     return GDFV_OK;
 }
@@ -1508,6 +1575,7 @@ cudaError_t enqueue_steps_dt(int ctx, cudaStream_t stream, const double* U_in, d
     A.ctl = c->step_ctl;
     A.max_signal = c->step_maxsig;
     A.last_signal = c->step_lastsig;
+    const bool ch_rule = c->cfg.mhd && c->P.divergence_cleaning;
     for (int m = 0; m < n; ++m) {
         const double* src = m == 0 ? U_in : U_out[m - 1];
         A.Ubuf[0] = const_cast<double*>(src);
@@ -1516,9 +1584,20 @@ cudaError_t enqueue_steps_dt(int ctx, cudaStream_t stream, const double* U_in, d
         if (m == 0 && fresh)
             step_dt_begin_kernel<<<1, 256, 0, stream>>>(c->step_ctl, c->step_maxsig, (int)c->blocks.size(), dts[0],
                                                         c->h_ctl->c_h);
-        else
+        else if (!ch_rule)
             step_dt_next_kernel<<<1, 1, 0, stream>>>(c->step_ctl, dts[m]);
         cudaError_t e = cudaGetLastError();
+        if (ch_rule) {
+            // the step's c_h from the signal maxima of its start state, as gdfv_run forms
+            // it: a scan of the chain's input, then the maxima each corrector leaves
+            if (e == cudaSuccess && m == 0)
+                e = enqueue_signal_scan(c, stream, src, c->step_maxsig, c->step_lastsig, c->ch_bad);
+            if (e == cudaSuccess) {
+                step_dt_ch_kernel<<<1, 1, 0, stream>>>(c->step_ctl, c->d_blocks, c->step_maxsig, (int)c->blocks.size(),
+                                                       dts[m]);
+                e = cudaGetLastError();
+            }
+        }
         if (e == cudaSuccess) e = c->cfg.precision == 0 ? launch_stage_fp64(1, c->cfg.flux, c->cfg.mhd, A, stream)
                                                         : launch_stage_fp32(1, c->cfg.flux, c->cfg.mhd, A, stream);
         A.R_out = nullptr;
@@ -1528,6 +1607,19 @@ cudaError_t enqueue_steps_dt(int ctx, cudaStream_t stream, const double* U_in, d
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
+}
+
+// The c_h of a step of dt that starts at U and the psi damping factor of its stages
+// (out[0], out[1], device), as gdfv_run forms them, enqueued on `stream` with the
+// context's adjoint scan scratch (steps_dt_prepare must have run).
+cudaError_t enqueue_step_ch(int ctx, cudaStream_t stream, const double* U, double dt, double* out) {
+    Context* c = get_ctx(ctx);
+    if (!c || !c->ch_maxsig || !U || !out) return cudaErrorInvalidValue;
+    cudaError_t e = enqueue_signal_scan(c, stream, U, c->ch_maxsig, c->ch_lastsig, c->ch_bad);
+    if (e != cudaSuccess) return e;
+    step_ch_damp_kernel<<<1, 1, 0, stream>>>(c->d_blocks, c->ch_maxsig, (int)c->blocks.size(), dt,
+                                            c->cfg.divB_damping_length, out);
+    return cudaGetLastError();
 }
 
 // Waits for `stream` and reports the failure counters of the chains run since the
@@ -1584,11 +1676,7 @@ int upload_tiles(Context* c, const std::vector<TileDesc>& tiles, int n1, int n2,
 // The trial steps use a scratch control record with dt = 0 and write only the
 // idle state buffer and dU0, so the solution is not changed.
 int autotune(Context* c) {
-    if (!c->step_ctl) {
-        CK(cudaMalloc(&c->step_ctl, sizeof(Control)));
-        CK(cudaMalloc(&c->step_maxsig, sizeof(unsigned long long) * c->blocks.size()));
-        CK(cudaMalloc(&c->step_lastsig, sizeof(double) * c->blocks.size()));
-    }
+    if (step_scratch(c)) return GDFV_ERR_CUDA;
     if (read_ctl(c)) return GDFV_ERR_CUDA;
     const int parity = c->h_ctl->step & 1;
     const double c_h = c->h_ctl->c_h > 0.0 ? c->h_ctl->c_h : 1.0;
@@ -1905,11 +1993,7 @@ int gdfv_step_dt(int ctx, const double* U_in_dev, double* U_out_dev, double dt, 
     if (st) return st;
     if (!U_in_dev || !U_out_dev || U_in_dev == U_out_dev || !(dt > 0.0))
         return fail(c, GDFV_ERR_ARG, "gdfv_step_dt needs distinct input/output arrays and dt > 0");
-    if (!c->step_ctl) {
-        CK(cudaMalloc(&c->step_ctl, sizeof(Control)));
-        CK(cudaMalloc(&c->step_maxsig, sizeof(unsigned long long) * c->blocks.size()));
-        CK(cudaMalloc(&c->step_lastsig, sizeof(double) * c->blocks.size()));
-    }
+    if (step_scratch(c)) return GDFV_ERR_CUDA;
     if (read_ctl(c)) return GDFV_ERR_CUDA;
     StageArgs A = stage_args(c);
     A.Ubuf[0] = const_cast<double*>(U_in_dev);
@@ -1920,6 +2004,11 @@ int gdfv_step_dt(int ctx, const double* U_in_dev, double* U_out_dev, double dt, 
     step_dt_begin_kernel<<<1, 256, 0, c->stream>>>(c->step_ctl, c->step_maxsig, (int)c->blocks.size(), dt,
                                                    c->h_ctl->c_h);
     CK(cudaGetLastError());
+    if (c->cfg.mhd && c->P.divergence_cleaning) {   // c_h of U_in, as gdfv_run forms it
+        CK(enqueue_signal_scan(c, c->stream, U_in_dev, c->step_maxsig, c->step_lastsig, c->ch_bad));
+        step_dt_ch_kernel<<<1, 1, 0, c->stream>>>(c->step_ctl, c->d_blocks, c->step_maxsig, (int)c->blocks.size(), dt);
+        CK(cudaGetLastError());
+    }
     CK(launch_stage(c, 1, A));
     if (U1_out_dev) {
         long long n = (long long)c->nq * c->total;

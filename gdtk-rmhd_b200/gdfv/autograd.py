@@ -20,8 +20,8 @@
       mu  = J(U1)^T (dt/2 lam)
       lam <- lam + mu + J(U0)^T (dt/2 lam + dt mu)
   with dt frozen at its forward value (the CFL rule is not differentiated).  MHD
-  rollouts take this path without divergence cleaning (hlle; with GLM cleaning each
-  step's c_h and psi damping would enter, and only the residual has a VJP).
+  rollouts with GLM cleaning hold each step's c_h fixed likewise, and the step's psi
+  damping D enters as U1 -> D U1 in the corrector and U2 -> D U2.
 Tensors are float64 on the simulation's device, shaped [nq, total cells].
 """
 import torch

@@ -213,7 +213,8 @@ int gdfv_residual_vjp(int ctx, const double* U_dev, const double* W_dev, double*
 
 /* One predictor-corrector step of a given dt from U_in_dev to U_out_dev (device arrays
  * [nq][total], distinct), without the dt rule: the recomputation step of a
- * checkpointed adjoint, bit-identical to the step gdfv_run took with that dt.
+ * checkpointed adjoint, bit-identical to the step gdfv_run took with that dt (MHD with
+ * divergence cleaning: c_h from the signal of U_in_dev, as gdfv_run forms it).
  * U1_out_dev (may be NULL) receives the predictor state U1 = U0 + dt R(U0). */
 int gdfv_step_dt(int ctx, const double* U_in_dev, double* U_out_dev, double dt, double* U1_out_dev);
 
@@ -232,9 +233,11 @@ int gdfv_steps_dt(int ctx, const double* U_in_dev, double* const* U_out_dev, dou
  * with mu = (dR/dU(U1))^T (dt/2 lam), in place on the device array lam [nq][total].
  * The inflow ghost-state cotangents of both products are added into g_inflow_dev
  * (device, [n_inflow][6], MHD [n_inflow][10], caller-zeroed).  Enqueued on the
- * context's stream with no host synchronisation.  Same scope as gdfv_residual_vjp,
- * except that MHD takes divergence_cleaning = 0 only (GDFV_ERR_ARG otherwise: with
- * cleaning the step's c_h and psi damping would enter); no reference counterpart. */
+ * context's stream with no host synchronisation.  Same scope as gdfv_residual_vjp.
+ * MHD with divergence cleaning: the step's c_h is formed from U0 as gdfv_run forms it
+ * (the signal of the step's start state) and held fixed; the corrector's read of U1
+ * with psi damped, and the damping of U2's psi, are reversed.  No reference
+ * counterpart. */
 int gdfv_step_adjoint(int ctx, const double* U0_dev, const double* U1_dev, double dt, double* lam_dev,
                       double* g_inflow_dev);
 

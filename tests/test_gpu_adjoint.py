@@ -280,18 +280,93 @@ def test_rollout_gradients_mhd_without_cleaning(checkpoint_every):
         assert abs(fd - ad) <= 1e-5 * max(abs(fd), abs(ad)), (trial, fd, ad)
 
 
-def test_mhd_rollout_with_cleaning_is_refused():
-    """With GLM cleaning each step's c_h and psi damping would enter the step adjoint:
-    the rollout's backward reports it instead of returning a wrong gradient."""
-    from gdfv._lib import GdfvError
-    from gdfv.autograd import rollout
-    case = cases.orszag_tang(n=(16, 16, 4))
+def test_fixed_dt_steps_mhd_cleaning_replay_gdfv_run():
+    """With GLM cleaning each step's c_h follows the signal of its start state: the
+    fixed-dt steps (gdfv_step_dt, and the chains gdfv_steps_dt that recompute a rollout's
+    segments) form it as gdfv_run does -- a scan of the chain's input, then the maxima
+    each corrector leaves -- and replay gdfv_run's steps bit for bit."""
+    from gdfv.autograd import step_dt, steps_dt
+    case = cases.orszag_tang(n=(24, 24, 4))
     _, sim = cases.build_pair(case)
-    U0 = torch.from_numpy(sim.get_conserved(0)).cuda().requires_grad_(True)
-    theta = torch.tensor([1.0, 1.0, 0.0], dtype=torch.float64, requires_grad=True)
-    UN = rollout(sim, U0, theta, 3, 3)
-    with pytest.raises(GdfvError, match="divergence_cleaning"):
-        UN.sum().backward()
+    U0 = torch.from_numpy(sim.get_conserved(0)).cuda()
+    states, dts = [], []
+    for _ in range(5):
+        sim.run(max_step=1)
+        dts.append(sim.time()["dt"])
+        states.append(sim.get_conserved(0))
+    _, sim_r = cases.build_pair(case)
+    X = U0
+    for n, dt in enumerate(dts):
+        X = step_dt(sim_r, X, dt)
+        assert np.array_equal(X.cpu().numpy(), states[n]), n
+    outs = [torch.empty_like(U0) for _ in dts]
+    preds = [torch.empty_like(U0) for _ in dts]
+    steps_dt(sim_r, U0, dts, outs, preds)
+    for n in range(len(dts)):
+        assert np.array_equal(outs[n].cpu().numpy(), states[n]), n
+
+
+def test_step_adjoint_mhd_with_cleaning_against_oracle():
+    """The step adjoint with GLM cleaning is the transpose of the step's Jacobian at
+    frozen dt and c_h: U2 = D (U0 + dt/2 R(U0) + dt/2 R(D U1)), U1 = U0 + dt R(U0), D
+    damping psi by exp(-c_h dt / (0.18 L)) (e4/fvcell.d:1068-1074).  J_step v is
+    composed from the oracle's complex-step residual JVPs at U0 and D U1 with the GPU
+    step's c_h; <lam, J_step v> = <J_step^T lam, v> to 1e-10."""
+    from gdfv.autograd import step_adjoint
+    from gdfv._lib import ffi
+    case = cases.orszag_tang(n=(24, 24, 4))
+    orc, sim = cases.build_pair(case)
+    sim.run(max_step=3)   # psi away from zero
+    U0 = torch.from_numpy(sim.get_conserved(0)).cuda()
+    sim.run(max_step=1)
+    t = sim.time()
+    dt, c_h = t["dt"], t["c_h"]
+    U1 = torch.empty_like(U0)
+    assert sim.L.gdfv_last_predictor_state(sim.ctx, ffi.cast("double*", U0.data_ptr()),
+                                           ffi.cast("double*", U1.data_ptr())) == 0
+    torch.cuda.synchronize()
+    damp = np.exp(-(c_h * c_h / (0.18 * 1.0 * c_h)) * dt)
+    assert 0.0 < damp < 1.0
+    D = np.ones((10, 1))
+    D[8] = damp
+    rng = np.random.default_rng(21)
+    U0n, U1n = U0.cpu().numpy(), U1.cpu().numpy()
+    v = rng.standard_normal(U0n.shape) * np.maximum(np.abs(U0n).max(axis=1, keepdims=True), 1e-3)
+    lam = rng.standard_normal(U0n.shape)
+    orc.set("c_h", c_h)   # the residual JVPs take the step's c_h
+    lay = lambda X: _gpu_to_oracle_layout(case, X)
+    unlay = lambda x: x.reshape(U0n.shape)   # one block: the same [nq][cells] order
+    J0v = unlay(orc.jvp_complex(lay(U0n), lay(v)))
+    w1 = D * (v + dt * J0v)
+    J1w = unlay(orc.jvp_complex(lay(D * U1n), lay(w1)))
+    JSv = D * (v + 0.5 * dt * J0v + 0.5 * dt * J1w)
+    lhs = float(np.sum(lam * JSv))
+    lam_t = torch.from_numpy(lam.copy()).cuda()
+    gin = torch.zeros((1, 10), dtype=torch.float64, device="cuda")
+    step_adjoint(sim, U0, U1, dt, lam_t, gin)
+    torch.cuda.synchronize()
+    rhs = float(np.sum(lam_t.cpu().numpy() * v))
+    assert abs(lhs - rhs) <= 1e-10 * max(abs(lhs), abs(rhs)), (lhs, rhs)
+
+
+def test_mhd_rollout_with_cleaning_resident_matches_checkpointed():
+    """MHD rollout with GLM cleaning: the checkpointed backward recomputes each segment
+    with each step's c_h and damps psi as the forward did, so its gradients equal the
+    resident trajectory's to the rounding of the FP64 atomic accumulation."""
+    from gdfv.autograd import rollout
+    case = cases.orszag_tang(n=(24, 24, 4))
+    _, sim = cases.build_pair(case)
+    U0 = torch.from_numpy(sim.get_conserved(0)).cuda()
+    W = torch.from_numpy(np.random.default_rng(4).standard_normal(tuple(U0.shape))).cuda()
+    grads = []
+    for K in (9, 3):
+        theta = torch.tensor([1.0, 1.0, 0.0], dtype=torch.float64, requires_grad=True)
+        U0r = U0.clone().requires_grad_(True)
+        UN = rollout(sim, U0r, theta, 9, K)
+        (UN * W).sum().backward()
+        grads.append(U0r.grad.clone())
+    assert float(grads[0][8].abs().max()) > 0.0   # psi carries a cotangent
+    assert torch.allclose(grads[0], grads[1], rtol=1e-11, atol=1e-11 * float(grads[1].abs().max()))
 
 
 def test_rollout_theta_drives_every_inflow_face():
