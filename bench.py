@@ -254,6 +254,55 @@ def adjoint_over_forward(nsteps=50, shape=(128, 128, 64), autotune=True, forms=(
     return out
 
 
+def adjoint_mhd_leg(stream, nsteps=30, n=(256, 256, 4)):
+    """MHD rollout adjoint: Orszag-Tang 256x256x4 (FP64, hlle with GLM cleaning), J = <W, U_N>
+    with fixed random weights after 30 steps, the trajectory resident; the backward time
+    (each step's c_h and psi damping formed from its start state, then the two MHD VJP
+    products) over the autotuned forward gdfv_run of the same steps, both warm."""
+    import numpy as np
+    import torch
+    import cases
+    from gdfv.autograd import rollout
+    case = cases.orszag_tang(n=n)
+    sim = cases.build_gpu(case, autotune=True)
+    sim.set_stream(stream.cuda_stream)
+    U0 = torch.from_numpy(sim.get_conserved(0)).cuda()
+    sim.run(max_step=2)
+    W = torch.from_numpy(np.random.default_rng(3).standard_normal(tuple(U0.shape))).cuda()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    fwd = []
+    for _ in range(2):
+        sim.set_conserved(0, U0.cpu().numpy())
+        sim.set_time(0.0, 0, sim.config.dt_init)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        sim.run(max_step=nsteps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        fwd.append(e0.elapsed_time(e1))
+    fwd_ms = min(fwd)
+    adj = []
+    for rep in range(3):   # the first pass allocates the adjoint's scratch
+        theta = torch.tensor([1.0, 1.0, 0.0], dtype=torch.float64, requires_grad=True)
+        U0r = U0.clone().requires_grad_(True)
+        with torch.cuda.stream(stream):
+            UN = rollout(sim, U0r, theta, nsteps, nsteps)
+            J = (UN * W).sum()
+        torch.cuda.synchronize()
+        b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        b0.record()
+        J.backward()
+        b1.record()
+        torch.cuda.synchronize()
+        if rep:
+            adj.append(b0.elapsed_time(b1))
+    adj_ms = min(adj)
+    sim.close()
+    return dict(workload=f"Orszag-Tang {n[0]}x{n[1]}x{n[2]} FP64 hlle+GLM, {nsteps} steps, trajectory resident",
+                forward_ms=fwd_ms, adjoint_ms=adj_ms, adjoint_ms_max=max(adj), ratio=adj_ms / fwd_ms,
+                grad_U0_norm=float(U0r.grad.norm()))
+
+
 def _timed_run(sim, stream, steps):
     import torch
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -600,6 +649,7 @@ def main():
             sim[1].close()
         torch.cuda.empty_cache()
         legs = [("adjoint", adjoint_over_forward),
+                ("adjoint_mhd", lambda: adjoint_mhd_leg(stream)),
                 ("accuracy_other_flux", lambda: accuracy_leg(None, n, "hllc" if args.flux == "ausmdv" else "ausmdv",
                                                              acc_steps, stream)),
                 ("multiblock", lambda: multiblock_leg(stream)),

@@ -1,5 +1,7 @@
 // gdfv_adjoint.cu -- hand-written vector-Jacobian product of the residual,
-// g = (dR/dU)^T w, for the Euler path (2D or 3D) with the ausmdv or hllc flux (FP64).
+// g = (dR/dU)^T w, for the Euler path (2D or 3D) with the ausmdv or hllc flux and for
+// MHD with hlle and GLM cleaning (FP64), and the adjoints of the predictor-corrector
+// step and of a rollout built on it.
 //
 // The residual (e4/fvcell.d:824-856) is R_c = (1/V) sum_faces +-A F_f, each face
 // flux F_f a function of the four stencil states (e4/onedinterp.d:751-989 and
