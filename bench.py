@@ -462,14 +462,15 @@ def main():
                     help="steps after which the FP32 form is compared with FP64 (0: at the timed steps)")
     ap.add_argument("--no-extra", action="store_true", help="skip the multi-block, MHD and adjoint legs")
     ap.add_argument("--profile-case", nargs="?", const="stage", default=None,
-                    choices=["stage", "corrector", "narrow", "mhd", "adjoint", "norms"],
+                    choices=["stage", "corrector", "narrow", "mhd", "adjoint", "adjoint_mhd", "norms"],
                     help="small case for ncu captures, then exit: stage = the 128^3 inflow box "
                          "(FP32 then FP64 form, warmup steps); corrector = the inflow box at 256x128x128, "
                          "FP32 form, with the 256^3 run's tile k-chunk; narrow = the inflow box at "
                          "240x128x128, FP32 form in 16-wide tiles (the tuner's choice at 240^3); mhd = "
                          "Orszag-Tang 512x512x4 (both forms, warmup steps); adjoint = 128x128x64 FP64 "
-                         "rollout of 10 steps and its backward; norms = the 256^3 box, FP32 form, warmup "
-                         "steps then the residual norms twice")
+                         "rollout of 10 steps and its backward; adjoint_mhd = Orszag-Tang 256x256x4 FP64 "
+                         "rollout of 10 steps (resident) and its backward; norms = the 256^3 box, FP32 form, "
+                         "warmup steps then the residual norms twice")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -539,6 +540,10 @@ def main():
         return 0
     if args.profile_case == "adjoint":
         adjoint_over_forward(nsteps=10, forms=(("checkpointed", 10),))
+        torch.cuda.synchronize()
+        return 0
+    if args.profile_case == "adjoint_mhd":
+        adjoint_mhd_leg(torch.cuda.Stream(), nsteps=10)
         torch.cuda.synchronize()
         return 0
 

@@ -1203,7 +1203,7 @@ __global__ void __launch_bounds__(FACE_CTA, GDFV_ADJ_MINB) adj_faces_kernel(AdjA
 // primitives, scattered through the ghost rules.  The limiter's arithmetic is the Euler
 // path's; psi is reconstructed only with divergence cleaning (a copy of the cell's
 // otherwise); c_h is the residual's, frozen.
-template <int D>
+template <int D, bool RARE>
 __device__ void face_mhd(const AdjArgs& a, long long f) {
     const long long* off = a.face_off + D * (a.nblocks + 1);
     if (f >= off[a.nblocks]) return;
@@ -1215,7 +1215,7 @@ __device__ void face_mhd(const AdjArgs& a, long long f) {
     double xs[4], ys[4];
     double c[4][NPM];
     for (int m = 0; m < 4; ++m) {
-        src[m] = stencil_src<D, true>(a, B, i, j, k, m);
+        src[m] = stencil_src<D, RARE>(a, B, i, j, k, m);
         const int ci = i - (D == 0 ? 2 - m : 0), cj = j - (D == 1 ? 2 - m : 0);
         xs[m] = B.x0 + ((double)ci + 0.5) * B.len[0];
         ys[m] = B.y0 + ((double)cj + 0.5) * B.len[1];
@@ -1315,11 +1315,25 @@ __device__ void face_mhd(const AdjArgs& a, long long f) {
     for (int m = 0; m < 4; ++m) adj_scatter_mhd(a, src[m], xs[m], ys[m], gc[m]);
 }
 
-__global__ void __launch_bounds__(128) adj_faces_mhd_kernel(AdjArgs a, unsigned nb0, unsigned nb1) {
+// RARE: some exchange rotates its ghosts' vectors (the only rare rule MHD takes).
+// GDFV_ADJ_MHD_MINB: CTAs of 128 threads per SM the register budget is set for; 3 (168
+// registers, 408 B of spill loads) ran the Orszag-Tang 256x256x4 rollout adjoint 4%
+// faster than 2 (230 registers, no spills); 4 (128 registers) spills 1.9 KB.
+#ifndef GDFV_ADJ_MHD_MINB
+#define GDFV_ADJ_MHD_MINB 3
+#endif
+template <bool RARE>
+__global__ void __launch_bounds__(128, GDFV_ADJ_MHD_MINB) adj_faces_mhd_kernel(AdjArgs a, unsigned nb0, unsigned nb1) {
     const unsigned bid = blockIdx.x;
-    if (bid < nb0) face_mhd<0>(a, (long long)bid * 128 + threadIdx.x);
-    else if (bid < nb0 + nb1) face_mhd<1>(a, (long long)(bid - nb0) * 128 + threadIdx.x);
-    else face_mhd<2>(a, (long long)(bid - nb0 - nb1) * 128 + threadIdx.x);
+    if (bid < nb0) face_mhd<0, RARE>(a, (long long)bid * 128 + threadIdx.x);
+    else if (bid < nb0 + nb1) face_mhd<1, RARE>(a, (long long)(bid - nb0) * 128 + threadIdx.x);
+    else face_mhd<2, RARE>(a, (long long)(bid - nb0 - nb1) * 128 + threadIdx.x);
+}
+
+void launch_faces_mhd(const AdjArgs& a, const unsigned* nb, cudaStream_t s) {
+    const unsigned n = nb[0] + nb[1] + nb[2];
+    if (a.P.rotating) adj_faces_mhd_kernel<true><<<n, 128, 0, s>>>(a, nb[0], nb[1]);
+    else adj_faces_mhd_kernel<false><<<n, 128, 0, s>>>(a, nb[0], nb[1]);
 }
 
 // MHD decode (e4/fvcell.d:586-822): the ten primitives of each cell, gP cleared.
@@ -1547,7 +1561,7 @@ cudaError_t enqueue_vjp_mhd(const AdjView& v, const AdjArgs& a, const std::vecto
     if (e != cudaSuccess) return e;
     unsigned nb[3];
     for (int d = 0; d < 3; ++d) nb[d] = (unsigned)((off[d * (v.nblocks + 1) + v.nblocks] + 127) / 128);
-    adj_faces_mhd_kernel<<<nb[0] + nb[1] + nb[2], 128, 0, v.stream>>>(a, nb[0], nb[1]);
+    launch_faces_mhd(a, nb, v.stream);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     adj_back_mhd_kernel<<<nb_cells, nt, 0, v.stream>>>(a);
     return cudaGetLastError();
@@ -1619,7 +1633,7 @@ struct VjpChain {
         if (e == cudaSuccess) {
             unsigned nb[3];
             for (int d = 0; d < 3; ++d) nb[d] = (unsigned)((off[d * (v.nblocks + 1) + v.nblocks] + 127) / 128);
-            if (v.mhd) adj_faces_mhd_kernel<<<nb[0] + nb[1] + nb[2], 128, 0, v.stream>>>(a, nb[0], nb[1]);
+            if (v.mhd) launch_faces_mhd(a, nb, v.stream);
             else launch_faces(a, v.flux, nb, v.stream);
             e = cudaGetLastError();
         }
