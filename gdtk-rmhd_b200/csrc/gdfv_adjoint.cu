@@ -1204,7 +1204,7 @@ __global__ void __launch_bounds__(FACE_CTA, GDFV_ADJ_MINB) adj_faces_kernel(AdjA
 // path's; psi is reconstructed only with divergence cleaning (a copy of the cell's
 // otherwise); c_h is the residual's, frozen.
 template <int D, bool RARE>
-__device__ void face_mhd(const AdjArgs& a, long long f) {
+__device__ void face_mhd(const AdjArgs& a, long long f, double* smt) {
     const long long* off = a.face_off + D * (a.nblocks + 1);
     if (f >= off[a.nblocks]) return;
     int i = 0, j = 0, k = 0;
@@ -1213,7 +1213,9 @@ __device__ void face_mhd(const AdjArgs& a, long long f) {
     const NumParams& P = a.P;
     Src src[4];
     double xs[4], ys[4];
-    double c[4][NPM];
+    // the stencil's primitives and their cotangents in this thread's shared-memory slot
+    double (*c)[NPM] = reinterpret_cast<double (*)[NPM]>(smt);
+    double (*gc)[NPM] = reinterpret_cast<double (*)[NPM]>(smt + 4 * NPM);
     for (int m = 0; m < 4; ++m) {
         src[m] = stencil_src<D, RARE>(a, B, i, j, k, m);
         const int ci = i - (D == 0 ? 2 - m : 0), cj = j - (D == 1 ? 2 - m : 0);
@@ -1284,7 +1286,6 @@ __device__ void face_mhd(const AdjArgs& a, long long f) {
     }
     const double gF8[8] = {gF[MASS], gF[XMOM], gF[YMOM], gF[ZMOM], gF[TOTENERGY], gF[XB], gF[YB], gF[ZB]};
     hlle_mhd_vjp(P, L, R, gF8, gL, gR);
-    double gc[4][NPM];
     for (int m = 0; m < 4; ++m)
         for (int q = 0; q < NPM; ++q) gc[m][q] = 0.0;
     double gqL[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, gqR[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -1316,24 +1317,32 @@ __device__ void face_mhd(const AdjArgs& a, long long f) {
 }
 
 // RARE: some exchange rotates its ghosts' vectors (the only rare rule MHD takes).
-// GDFV_ADJ_MHD_MINB: CTAs of 128 threads per SM the register budget is set for; 3 (168
-// registers, 408 B of spill loads) ran the Orszag-Tang 256x256x4 rollout adjoint 4%
-// faster than 2 (230 registers, no spills); 4 (128 registers) spills 1.9 KB.
-#ifndef GDFV_ADJ_MHD_MINB
-#define GDFV_ADJ_MHD_MINB 3
-#endif
+// Each thread keeps its stencil's primitives and cotangents (80 doubles) in shared
+// memory at a stride of 81 doubles (conflict-free for 8-byte accesses): 83 KB per CTA
+// of 128 threads, 2 CTAs per SM.
+constexpr int MHD_SLOT = 8 * NPM + 1;
+constexpr size_t MHD_FACE_SMEM = sizeof(double) * MHD_SLOT * 128;
 template <bool RARE>
-__global__ void __launch_bounds__(128, GDFV_ADJ_MHD_MINB) adj_faces_mhd_kernel(AdjArgs a, unsigned nb0, unsigned nb1) {
+__global__ void __launch_bounds__(128, 2) adj_faces_mhd_kernel(AdjArgs a, unsigned nb0, unsigned nb1) {
+    extern __shared__ double smem_mhd[];
+    double* smt = smem_mhd + threadIdx.x * MHD_SLOT;
     const unsigned bid = blockIdx.x;
-    if (bid < nb0) face_mhd<0, RARE>(a, (long long)bid * 128 + threadIdx.x);
-    else if (bid < nb0 + nb1) face_mhd<1, RARE>(a, (long long)(bid - nb0) * 128 + threadIdx.x);
-    else face_mhd<2, RARE>(a, (long long)(bid - nb0 - nb1) * 128 + threadIdx.x);
+    if (bid < nb0) face_mhd<0, RARE>(a, (long long)bid * 128 + threadIdx.x, smt);
+    else if (bid < nb0 + nb1) face_mhd<1, RARE>(a, (long long)(bid - nb0) * 128 + threadIdx.x, smt);
+    else face_mhd<2, RARE>(a, (long long)(bid - nb0 - nb1) * 128 + threadIdx.x, smt);
 }
 
 void launch_faces_mhd(const AdjArgs& a, const unsigned* nb, cudaStream_t s) {
+    static bool attr_set[2] = {false, false};   // dynamic shared memory above 48 KB, once per instantiation
+    const int r = a.P.rotating ? 1 : 0;
+    if (!attr_set[r]) {
+        if (r) cudaFuncSetAttribute(adj_faces_mhd_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MHD_FACE_SMEM);
+        else cudaFuncSetAttribute(adj_faces_mhd_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MHD_FACE_SMEM);
+        attr_set[r] = true;
+    }
     const unsigned n = nb[0] + nb[1] + nb[2];
-    if (a.P.rotating) adj_faces_mhd_kernel<true><<<n, 128, 0, s>>>(a, nb[0], nb[1]);
-    else adj_faces_mhd_kernel<false><<<n, 128, 0, s>>>(a, nb[0], nb[1]);
+    if (r) adj_faces_mhd_kernel<true><<<n, 128, MHD_FACE_SMEM, s>>>(a, nb[0], nb[1]);
+    else adj_faces_mhd_kernel<false><<<n, 128, MHD_FACE_SMEM, s>>>(a, nb[0], nb[1]);
 }
 
 // MHD decode (e4/fvcell.d:586-822): the ten primitives of each cell, gP cleared.
