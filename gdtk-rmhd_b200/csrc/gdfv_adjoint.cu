@@ -249,16 +249,12 @@ __device__ void ausmdv_vjp(const NumParams& P, const FS& L, const FS& R, const d
     double duL = 0.5 * (L.u + fabs(L.u));
     bool subL = fabs(ML) <= 1.0;
     double QL = (L.u + am) * (L.u + am) * (0.25 * iam);
-    double pLplus, uLplus;
-    if (subL) { pLplus = L.p * (ML + 1.0) * (ML + 1.0) * (2.0 - ML) * 0.25; uLplus = alphaL * (QL - duL) + duL; }
-    else { pLplus = L.p * duL * rcp(L.u); uLplus = duL; }
+    // p_half enters F linearly: only the cotangents of pLplus and pRminus are needed
+    const double uLplus = subL ? alphaL * (QL - duL) + duL : duL;
     double duR = 0.5 * (R.u - fabs(R.u));
     bool subR = fabs(MR) <= 1.0;
     double QR = -(R.u - am) * (R.u - am) * (0.25 * iam);
-    double pRminus, uRminus;
-    if (subR) { pRminus = R.p * (MR - 1.0) * (MR - 1.0) * (2.0 + MR) * 0.25; uRminus = alphaR * (QR - duR) + duR; }
-    else { pRminus = R.p * duR * rcp(R.u); uRminus = duR; }
-    (void)pLplus; (void)pRminus;  // p_half enters F linearly: only its cotangent is needed
+    const double uRminus = subR ? alphaR * (QR - duR) + duR : duR;
     double ru_half = uLplus * L.r + uRminus * R.r;
     double dp0 = L.p - R.p;
     bool minL = L.p <= R.p;
