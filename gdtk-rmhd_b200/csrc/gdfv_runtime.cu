@@ -278,7 +278,8 @@ struct Context {
     double* step_lastsig = nullptr;
     unsigned long long* ch_maxsig = nullptr;   // signal scan of the MHD step adjoint (its own stream)
     double* ch_lastsig = nullptr;
-    int* ch_bad = nullptr;
+    int* ch_bad = nullptr;   // cells the c_h scans could not decode: counted, never read (the
+                             // stages' own decode checks report a failed step)
 
     ~Context() {
         if (graph) cudaGraphExecDestroy(graph);
