@@ -1199,6 +1199,9 @@ __global__ void __launch_bounds__(FACE_CTA, GDFV_ADJ_MINB) adj_faces_kernel(AdjA
 // primitives, scattered through the ghost rules.  The limiter's arithmetic is the Euler
 // path's; psi is reconstructed only with divergence cleaning (a copy of the cell's
 // otherwise); c_h is the residual's, frozen.
+// Slot of primitive v in a face thread's shared-memory copy of its stencil: the sound
+// speed (5) is never reconstructed, so the nine others are kept.
+__device__ __forceinline__ constexpr int SL(int v) { return v < 5 ? v : v - 1; }
 template <int D, bool RARE>
 __device__ void face_mhd(const AdjArgs& a, long long f, double* smt) {
     const long long* off = a.face_off + D * (a.nblocks + 1);
@@ -1210,14 +1213,17 @@ __device__ void face_mhd(const AdjArgs& a, long long f, double* smt) {
     Src src[4];
     double xs[4], ys[4];
     // the stencil's primitives and their cotangents in this thread's shared-memory slot
-    double (*c)[NPM] = reinterpret_cast<double (*)[NPM]>(smt);
-    double (*gc)[NPM] = reinterpret_cast<double (*)[NPM]>(smt + 4 * NPM);
+    double (*c)[9] = reinterpret_cast<double (*)[9]>(smt);
+    double (*gc)[9] = reinterpret_cast<double (*)[9]>(smt + 4 * 9);
     for (int m = 0; m < 4; ++m) {
         src[m] = stencil_src<D, RARE>(a, B, i, j, k, m);
         const int ci = i - (D == 0 ? 2 - m : 0), cj = j - (D == 1 ? 2 - m : 0);
         xs[m] = B.x0 + ((double)ci + 0.5) * B.len[0];
         ys[m] = B.y0 + ((double)cj + 0.5) * B.len[1];
-        adj_load_mhd(a, src[m], xs[m], ys[m], c[m]);
+        double t[NPM];
+        adj_load_mhd(a, src[m], xs[m], ys[m], t);
+#pragma unroll
+        for (int v = 0; v < NPM; ++v) if (v != 5) c[m][SL(v)] = t[v];
     }
     const double AV = B.area[D] * B.vol_inv * a.w_scale;
     const int nD = B.n[D];
@@ -1243,17 +1249,17 @@ __device__ void face_mhd(const AdjArgs& a, long long f, double* smt) {
     const bool clean = P.divergence_cleaning;
     double qL[9], qR[9];
     for (int sc = 0; sc < 9; ++sc) {
-        if (sc == 8 && !clean) { qL[8] = c[1][9]; qR[8] = c[2][9]; continue; }
+        if (sc == 8 && !clean) { qL[8] = c[1][SL(9)]; qR[8] = c[2][SL(9)]; continue; }
         L2R2Rec rec;
-        l2r2_fwd<true>(w, P, c[0][pv[sc]], c[1][pv[sc]], c[2][pv[sc]], c[3][pv[sc]], qL[sc], qR[sc], rec);
+        l2r2_fwd<true>(w, P, c[0][SL(pv[sc])], c[1][SL(pv[sc])], c[2][SL(pv[sc])], c[3][SL(pv[sc])], qL[sc], qR[sc], rec);
     }
     const double Rg = P.gas.R, Cvinv = P.gas.Cvinv;
     const bool badL = qL[4] <= 0.0 || qL[3] <= 0.0, badR = qR[4] <= 0.0 || qR[3] <= 0.0;
     auto state = [&](bool bad, const double* q, const double* cell, FSm& S, double& psi) {
         if (bad) {   // e4/onedinterp.d:44-74: the cell-centre state
-            S = FSm{cell[0], cell[0] * Rg * (cell[4] * Cvinv), cell[pv[0]], cell[pv[1]], cell[pv[2]],
-                    cell[pv[5]], cell[pv[6]], cell[pv[7]], cell[4]};
-            psi = cell[9];
+            S = FSm{cell[SL(0)], cell[SL(0)] * Rg * (cell[SL(4)] * Cvinv), cell[SL(pv[0])], cell[SL(pv[1])], cell[SL(pv[2])],
+                    cell[SL(pv[5])], cell[SL(pv[6])], cell[SL(pv[7])], cell[SL(4)]};
+            psi = cell[SL(9)];
         } else {
             S = FSm{q[3], q[3] * Rg * (q[4] * Cvinv), q[0], q[1], q[2], q[5], q[6], q[7], q[4]};
             psi = q[8];
@@ -1283,15 +1289,15 @@ __device__ void face_mhd(const AdjArgs& a, long long f, double* smt) {
     const double gF8[8] = {gF[MASS], gF[XMOM], gF[YMOM], gF[ZMOM], gF[TOTENERGY], gF[XB], gF[YB], gF[ZB]};
     hlle_mhd_vjp(P, L, R, gF8, gL, gR);
     for (int m = 0; m < 4; ++m)
-        for (int q = 0; q < NPM; ++q) gc[m][q] = 0.0;
+        for (int q = 0; q < 9; ++q) gc[m][q] = 0.0;
     double gqL[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, gqR[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     auto back = [&](bool bad, const FSm& S, const FSm& gS, double gpsi, double* gq, double* gcell) {
         // p = rho R (u Cvinv)
         const double gr_ = gS.r + gS.p * Rg * (S.e * Cvinv), ge_ = gS.e + gS.p * S.r * Rg * Cvinv;
         if (bad) {
-            gcell[0] += gr_; gcell[4] += ge_;
-            gcell[pv[0]] += gS.u; gcell[pv[1]] += gS.v; gcell[pv[2]] += gS.w;
-            gcell[pv[5]] += gS.Bx; gcell[pv[6]] += gS.By; gcell[pv[7]] += gS.Bz; gcell[9] += gpsi;
+            gcell[SL(0)] += gr_; gcell[SL(4)] += ge_;
+            gcell[SL(pv[0])] += gS.u; gcell[SL(pv[1])] += gS.v; gcell[SL(pv[2])] += gS.w;
+            gcell[SL(pv[5])] += gS.Bx; gcell[SL(pv[6])] += gS.By; gcell[SL(pv[7])] += gS.Bz; gcell[SL(9)] += gpsi;
         } else {
             gq[3] += gr_; gq[4] += ge_;
             gq[0] += gS.u; gq[1] += gS.v; gq[2] += gS.w;
@@ -1302,24 +1308,30 @@ __device__ void face_mhd(const AdjArgs& a, long long f, double* smt) {
     back(badR, R, gR, gpsiR, gqR, gc[2]);
     for (int sc = 0; sc < 9; ++sc) {
         const int v = pv[sc];
-        if (sc == 8 && !clean) { gc[1][9] += gqL[8]; gc[2][9] += gqR[8]; continue; }
+        if (sc == 8 && !clean) { gc[1][SL(9)] += gqL[8]; gc[2][SL(9)] += gqR[8]; continue; }
         L2R2Rec rec;
         double ql, qr;
-        l2r2_fwd<true>(w, P, c[0][v], c[1][v], c[2][v], c[3][v], ql, qr, rec);
-        l2r2_rev<true>(w, P, c[0][v], c[1][v], c[2][v], c[3][v], rec, gqL[sc], gqR[sc], gc[0][v], gc[1][v], gc[2][v],
-                       gc[3][v]);
+        l2r2_fwd<true>(w, P, c[0][SL(v)], c[1][SL(v)], c[2][SL(v)], c[3][SL(v)], ql, qr, rec);
+        l2r2_rev<true>(w, P, c[0][SL(v)], c[1][SL(v)], c[2][SL(v)], c[3][SL(v)], rec, gqL[sc], gqR[sc], gc[0][SL(v)], gc[1][SL(v)], gc[2][SL(v)],
+                       gc[3][SL(v)]);
     }
-    for (int m = 0; m < 4; ++m) adj_scatter_mhd(a, src[m], xs[m], ys[m], gc[m]);
+    for (int m = 0; m < 4; ++m) {
+        double t[NPM];
+#pragma unroll
+        for (int v = 0; v < NPM; ++v) t[v] = v == 5 ? 0.0 : gc[m][SL(v)];
+        adj_scatter_mhd(a, src[m], xs[m], ys[m], t);
+    }
 }
 
 // RARE: some exchange rotates its ghosts' vectors (the only rare rule MHD takes).
-// Each thread keeps its stencil's primitives and cotangents (80 doubles) in shared
-// memory at a stride of 81 doubles (conflict-free for 8-byte accesses): 83 KB per CTA
-// of 128 threads, 2 CTAs per SM.
-constexpr int MHD_SLOT = 8 * NPM + 1;
+// Each thread keeps its stencil's primitives and cotangents (nine of each per cell, 72
+// doubles) in shared memory at a stride of 73 doubles (conflict-free for 8-byte
+// accesses): 74.75 KB per CTA of 128 threads, 3 CTAs per SM at 168 registers, with the
+// carveout that gives shared memory the most room.
+constexpr int MHD_SLOT = 8 * 9 + 1;
 constexpr size_t MHD_FACE_SMEM = sizeof(double) * MHD_SLOT * 128;
 template <bool RARE>
-__global__ void __launch_bounds__(128, 2) adj_faces_mhd_kernel(AdjArgs a, unsigned nb0, unsigned nb1) {
+__global__ void __launch_bounds__(128, 3) adj_faces_mhd_kernel(AdjArgs a, unsigned nb0, unsigned nb1) {
     extern __shared__ double smem_mhd[];
     double* smt = smem_mhd + threadIdx.x * MHD_SLOT;
     const unsigned bid = blockIdx.x;
@@ -1330,10 +1342,13 @@ __global__ void __launch_bounds__(128, 2) adj_faces_mhd_kernel(AdjArgs a, unsign
 
 void launch_faces_mhd(const AdjArgs& a, const unsigned* nb, cudaStream_t s) {
     static bool attr_set[2] = {false, false};   // dynamic shared memory above 48 KB, once per instantiation
+    // (the attributes are the function's, for the process's device)
     const int r = a.P.rotating ? 1 : 0;
     if (!attr_set[r]) {
         if (r) cudaFuncSetAttribute(adj_faces_mhd_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MHD_FACE_SMEM);
         else cudaFuncSetAttribute(adj_faces_mhd_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MHD_FACE_SMEM);
+        if (r) cudaFuncSetAttribute(adj_faces_mhd_kernel<true>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        else cudaFuncSetAttribute(adj_faces_mhd_kernel<false>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         attr_set[r] = true;
     }
     const unsigned n = nb[0] + nb[1] + nb[2];
